@@ -1,0 +1,82 @@
+"""ctypes view of oracle/_ref/libref_host.so: the reference's own host C++
+(mesh.cpp, rwg.cpp, rhs.cpp, orient.cpp, graglia.h) built by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY.  ``available()`` is False when the library has not
+been built (for instance on a machine without the reference sources)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "libref_host.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(_LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(_LIB_PATH)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def make_mesh(kind: str, param: float, ref: int):
+    """kind 'ico' -> icosphere(radius=param, ref); 'hex' -> hex_prism(AR=param, ref).
+    Returns (verts, tris, rwg-dict) in the reference's own RWG order."""
+    L = lib()
+    nv, nt, nr = C.c_int(), C.c_int(), C.c_int()
+    L.ref_make_mesh(0 if kind == "ico" else 1, C.c_double(param), ref,
+                    C.byref(nv), C.byref(nt), C.byref(nr))
+    return _fetch(nv.value, nt.value, nr.value)
+
+
+def _fetch(nv, nt, nr):
+    L = lib()
+    verts = np.zeros((nv, 3))
+    tris = np.zeros((nt, 3), dtype=np.int32)
+    L.ref_get_mesh(_p(verts), _p(tris))
+    tp = np.zeros(nr, dtype=np.int32)
+    tm = np.zeros(nr, dtype=np.int32)
+    fp = np.zeros((nr, 3))
+    fm = np.zeros((nr, 3))
+    ln, ap, am = np.zeros(nr), np.zeros(nr), np.zeros(nr)
+    L.ref_get_rwg(_p(tp), _p(tm), _p(fp), _p(fm), _p(ln), _p(ap), _p(am))
+    rwg = {"N": nr, "tri_p": tp.astype(np.int64), "tri_m": tm.astype(np.int64),
+           "free_p": fp, "free_m": fm, "length": ln, "area_p": ap, "area_m": am}
+    return verts, tris.astype(np.int64), rwg
+
+
+def rhs(k_ext: complex, eta_ext: float, E0, k_hat, quad_order: int, N: int):
+    """compute_rhs_planewave on the mesh made by the last make_mesh call."""
+    b = np.zeros(2 * N, dtype=np.complex128)
+    E0 = np.ascontiguousarray(E0, dtype=np.float64)
+    kh = np.ascontiguousarray(k_hat, dtype=np.float64)
+    lib().ref_rhs(C.c_double(complex(k_ext).real), C.c_double(complex(k_ext).imag),
+                  C.c_double(eta_ext), _p(E0), _p(kh), quad_order, _p(b))
+    return b
+
+
+def orientations(na, nb, ng, beta_sym=1, gamma_sym=1, gamma_mirror=False, sort=False):
+    n = lib().ref_orientations(na, nb, ng, beta_sym, gamma_sym, int(gamma_mirror), int(sort))
+    RT = np.zeros((n, 3, 3))
+    w = np.zeros(n)
+    lib().ref_get_orientations(_p(RT), _p(w))
+    return RT, w
+
+
+def graglia(r, v0, v1, v2, quad_order=7):
+    """(P, V) = potential_integral_triangle and vector_potential_integral_triangle."""
+    args = [np.ascontiguousarray(x, dtype=np.float64) for x in (r, v0, v1, v2)]
+    P = np.zeros(1)
+    V = np.zeros(3)
+    lib().ref_graglia(*[_p(a) for a in args], quad_order, _p(P), _p(V))
+    return float(P[0]), V

@@ -1,0 +1,90 @@
+// C entry points over the reference's own host-side C++ (mesh.cpp, rwg.cpp,
+// rhs.cpp, orient.cpp, graglia.h), compiled from the reference sources in
+// place by oracle/Makefile into oracle/_ref/libref_host.so.
+//
+// TEST INFRASTRUCTURE ONLY: the tests load this library to pin the oracle
+// and the product's host code against the reference's own implementation.
+#include "mesh.h"
+#include "rwg.h"
+#include "rhs.h"
+#include "orient.h"
+#include "graglia.h"
+#include <cstring>
+#include <vector>
+
+static Mesh g_mesh;
+static RWG g_rwg;
+static std::vector<Orientation> g_or;
+
+extern "C" {
+
+// kind 0 = icosphere(radius=param, ref), 1 = hex_prism(aspect=param, ref)
+int ref_make_mesh(int kind, double param, int ref, int* nv, int* nt, int* nrwg) {
+    g_mesh = (kind == 0) ? icosphere(param, ref) : hex_prism(param, ref);
+    g_rwg = build_rwg(g_mesh);
+    *nv = g_mesh.nv();
+    *nt = g_mesh.nt();
+    *nrwg = g_rwg.N;
+    return 0;
+}
+
+int ref_subdivide_flat(void) {
+    g_mesh = subdivide_flat(g_mesh);
+    g_rwg = build_rwg(g_mesh);
+    return g_rwg.N;
+}
+
+void ref_get_mesh(double* verts, int* tris) {
+    for (int i = 0; i < g_mesh.nv(); i++) {
+        verts[3 * i] = g_mesh.verts[i].x;
+        verts[3 * i + 1] = g_mesh.verts[i].y;
+        verts[3 * i + 2] = g_mesh.verts[i].z;
+    }
+    std::memcpy(tris, g_mesh.tris.data(), g_mesh.tris.size() * sizeof(int));
+}
+
+void ref_get_rwg(int* tri_p, int* tri_m, double* free_p, double* free_m,
+                 double* length, double* area_p, double* area_m) {
+    for (int n = 0; n < g_rwg.N; n++) {
+        tri_p[n] = g_rwg.tri_p[n];
+        tri_m[n] = g_rwg.tri_m[n];
+        free_p[3 * n] = g_rwg.free_p[n].x; free_p[3 * n + 1] = g_rwg.free_p[n].y; free_p[3 * n + 2] = g_rwg.free_p[n].z;
+        free_m[3 * n] = g_rwg.free_m[n].x; free_m[3 * n + 1] = g_rwg.free_m[n].y; free_m[3 * n + 2] = g_rwg.free_m[n].z;
+        length[n] = g_rwg.length[n];
+        area_p[n] = g_rwg.area_p[n];
+        area_m[n] = g_rwg.area_m[n];
+    }
+}
+
+// b (2N complex as interleaved doubles)
+void ref_rhs(double k_re, double k_im, double eta_ext, const double* E0,
+             const double* khat, int quad_order, double* b) {
+    compute_rhs_planewave(g_rwg, g_mesh, std::complex<double>(k_re, k_im), eta_ext,
+                          Vec3(E0[0], E0[1], E0[2]), Vec3(khat[0], khat[1], khat[2]),
+                          quad_order, reinterpret_cast<std::complex<double>*>(b));
+}
+
+int ref_orientations(int na, int nb, int ng, int bsym, int gsym, int mirror, int sort) {
+    g_or = generate_orientations(na, nb, ng, bsym, gsym, mirror != 0);
+    if (sort) sort_orientations_nearest(g_or);
+    return (int)g_or.size();
+}
+
+void ref_get_orientations(double* RT, double* w) {
+    for (size_t o = 0; o < g_or.size(); o++) {
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) RT[9 * o + 3 * i + j] = g_or[o].RT.m[i][j];
+        w[o] = g_or[o].weight;
+    }
+}
+
+void ref_graglia(const double* r, const double* v0, const double* v1, const double* v2,
+                 int quad_order, double* P, double* V) {
+    Vec3 R(r[0], r[1], r[2]), a(v0[0], v0[1], v0[2]), b(v1[0], v1[1], v1[2]), c(v2[0], v2[1], v2[2]);
+    TriQuad q = tri_quadrature(quad_order);
+    *P = potential_integral_triangle(R, a, b, c);
+    Vec3 vv = vector_potential_integral_triangle(R, a, b, c, q);
+    V[0] = vv.x; V[1] = vv.y; V[2] = vv.z;
+}
+
+}  // extern "C"
