@@ -1,0 +1,448 @@
+"""Python host layer over libbemdense (the C ABI in include/bem_dense.h).
+
+Function names and argument meanings mirror the reference's CPU interface for
+the dense path (python/bem_core.py: icosphere, build_rwg, tri_quadrature,
+assemble_pmchwt, compute_rhs_planewave, compute_mueller_matrix,
+orientation_average_mueller_batched, amplitude_to_mueller) and its C++ one
+(solver.h: lu_factorize_cuda / lu_solve_cuda / lu_solve_full).  Every numeric
+step runs in the CUDA library; device buffers are torch tensors, used only as
+memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from ._lib import (ASM_GSMOOTH_EXACT, PREC_FP32_REFINE, PREC_FP64, BemError, Problem, Result,
+                   SolveStats, check, lib)
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _dptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ------------------------------------------------------------------ context
+class Context:
+    """A libbemdense context on one GPU; kernels run on torch's current stream
+    of that device at construction time unless ``stream`` is given."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+        self.device = device
+        h = C.c_void_p()
+        check(lib().bem_ctx_create(device, C.byref(h)))
+        self.h = h
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        self.stream = stream
+        check(lib().bem_ctx_set_stream(self.h, C.c_void_p(stream.cuda_stream)), self.h)
+
+    def check(self, status):
+        check(status, self.h)
+
+    def synchronize(self):
+        self.check(lib().bem_ctx_synchronize(self.h))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().bem_ctx_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            lib().bem_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- geometry
+def _mesh_call(fn, *args):
+    nv, nt = C.c_int(), C.c_int()
+    check(fn(*args, C.byref(nv), C.byref(nt), None, None))
+    v = np.zeros((nv.value, 3))
+    t = np.zeros((nt.value, 3), dtype=np.int32)
+    check(fn(*args, C.byref(nv), C.byref(nt), _ptr(v), _ptr(t)))
+    return v, t
+
+
+def icosphere(radius=1.0, refinements=2):
+    """(verts, tris) -- mesh.cpp:11-68 / bem_core.py:24-61."""
+    return _mesh_call(lib().bem_mesh_icosphere, C.c_double(radius), int(refinements))
+
+
+def hex_prism(aspect_ratio=1.0, refinements=2):
+    """(verts, tris) -- mesh.cpp:102-154."""
+    return _mesh_call(lib().bem_mesh_hex_prism, C.c_double(aspect_ratio), int(refinements))
+
+
+def subdivide_flat(verts, tris):
+    v, t = _f64(verts), _i32(tris)
+    nv, nt = C.c_int(), C.c_int()
+    L = lib()
+    check(L.bem_mesh_subdivide_flat(_ptr(v), len(v), _ptr(t), len(t), C.byref(nv), C.byref(nt),
+                                    None, None))
+    vo = np.zeros((nv.value, 3))
+    to = np.zeros((nt.value, 3), dtype=np.int32)
+    check(L.bem_mesh_subdivide_flat(_ptr(v), len(v), _ptr(t), len(t), C.byref(nv), C.byref(nt),
+                                    _ptr(vo), _ptr(to)))
+    return vo, to
+
+
+def load_obj(path):
+    """(verts, tris, n_degenerate_removed, n_nonmanifold_edges) -- mesh.cpp:156-250."""
+    nv, nt, nd, nm = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    L = lib()
+    p = str(path).encode()
+    check(L.bem_mesh_load_obj(p, C.byref(nv), C.byref(nt), None, None, C.byref(nd), C.byref(nm)))
+    v = np.zeros((nv.value, 3))
+    t = np.zeros((nt.value, 3), dtype=np.int32)
+    check(L.bem_mesh_load_obj(p, C.byref(nv), C.byref(nt), _ptr(v), _ptr(t), C.byref(nd),
+                              C.byref(nm)))
+    return v, t, nd.value, nm.value
+
+
+def normalize_mesh(verts, tris):
+    v, t = _f64(verts).copy(), _i32(tris)
+    a = C.c_double()
+    check(lib().bem_mesh_normalize(_ptr(v), len(v), _ptr(t), len(t), C.byref(a)))
+    return v, a.value
+
+
+def mesh_volume(verts, tris):
+    v, t = _f64(verts), _i32(tris)
+    return lib().bem_mesh_volume(_ptr(v), len(v), _ptr(t), len(t))
+
+
+def mesh_dmax(verts):
+    v = _f64(verts)
+    return lib().bem_mesh_dmax(_ptr(v), len(v))
+
+
+def build_rwg(verts, tris):
+    """RWG dict like bem_core.build_rwg, in the C++ edge order (rwg.cpp:5-43)."""
+    v, t = _f64(verts), _i32(tris)
+    N = C.c_int()
+    L = lib()
+    check(L.bem_rwg_build(_ptr(v), len(v), _ptr(t), len(t), C.byref(N), *([None] * 7)))
+    n = N.value
+    tp, tm = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    fp, fm = np.zeros((n, 3)), np.zeros((n, 3))
+    ln, ap, am = np.zeros(n), np.zeros(n), np.zeros(n)
+    check(L.bem_rwg_build(_ptr(v), len(v), _ptr(t), len(t), C.byref(N), _ptr(tp), _ptr(tm),
+                          _ptr(fp), _ptr(fm), _ptr(ln), _ptr(ap), _ptr(am)))
+    return {"N": n, "tri_p": tp.astype(np.int64), "tri_m": tm.astype(np.int64),
+            "free_p": fp, "free_m": fm, "length": ln, "area_p": ap, "area_m": am}
+
+
+def tri_quadrature(order=7):
+    n = C.c_int()
+    L = lib()
+    check(L.bem_tri_quadrature(int(order), C.byref(n), None, None))
+    p = np.zeros((n.value, 2))
+    w = np.zeros(n.value)
+    check(L.bem_tri_quadrature(int(order), C.byref(n), _ptr(p), _ptr(w)))
+    return p, w
+
+
+def generate_orientations(n_alpha, n_beta, n_gamma, beta_sym=1, gamma_sym=1,
+                          gamma_mirror=False, sort_nearest=False):
+    """(RT (n,3,3), weights (n,)) -- orient.cpp:73-163."""
+    n = C.c_int()
+    L = lib()
+    args = (int(n_alpha), int(n_beta), int(n_gamma), int(beta_sym), int(gamma_sym),
+            int(bool(gamma_mirror)), int(bool(sort_nearest)))
+    check(L.bem_orientations(*args, C.byref(n), None, None))
+    RT = np.zeros((n.value, 3, 3))
+    w = np.zeros(n.value)
+    check(L.bem_orientations(*args, C.byref(n), _ptr(RT), _ptr(w)))
+    return RT, w
+
+
+def gauss_legendre(n):
+    x, w = np.zeros(n), np.zeros(n)
+    check(lib().bem_gauss_legendre(int(n), _ptr(x), _ptr(w)))
+    return x, w
+
+
+def physics(ka, m):
+    """k_ext = ka, k_int = k_ext m, eta_ext = 1, eta_int = 1/|m| (main.cpp:192-196)."""
+    m = complex(m)
+    return complex(ka, 0.0), complex(ka, 0.0) * m, 1.0, 1.0 / abs(m)
+
+
+class Geometry:
+    """Device-resident mesh + RWG + quadrature data (bem_geom)."""
+
+    def __init__(self, ctx: Context, verts, tris, quad_order=7):
+        self.ctx = ctx
+        self.verts = _f64(verts)
+        self.tris = _i32(tris)
+        h = C.c_void_p()
+        N = C.c_int()
+        ctx.check(lib().bem_geom_create(ctx.h, _ptr(self.verts), len(self.verts),
+                                        _ptr(self.tris), len(self.tris), int(quad_order),
+                                        C.byref(h), C.byref(N)))
+        self.h = h
+        self.N = N.value
+        self.n = 2 * self.N
+        self.quad_order = quad_order
+
+    def close(self):
+        if self.h:
+            lib().bem_geom_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _empty(shape, dtype, device):
+    import torch
+    return torch.empty(shape, dtype=dtype, device=f"cuda:{device}")
+
+
+def assemble_pmchwt_dev(geom: Geometry, k_ext, k_int, eta_ext, eta_int, Z=None,
+                        exact_gsmooth=False):
+    """Device Z (torch complex128, row-major 2N x 2N) -- pmchwt.cu:6-56."""
+    import torch
+    n = geom.n
+    if Z is None:
+        Z = _empty((n, n), torch.complex128, geom.ctx.device)
+    assert Z.dtype == torch.complex128 and Z.is_contiguous() and Z.shape[0] == n
+    k_ext, k_int = complex(k_ext), complex(k_int)
+    geom.ctx.check(lib().bem_assemble_pmchwt_dev(
+        geom.ctx.h, geom.h, k_ext.real, k_ext.imag, k_int.real, k_int.imag, float(eta_ext),
+        float(eta_int), ASM_GSMOOTH_EXACT if exact_gsmooth else 0, _dptr(Z), Z.stride(0)))
+    return Z
+
+
+def assemble_L_K_dev(geom: Geometry, k, exact_gsmooth=False):
+    """Device (L, K) for one wavenumber -- assemble_L_K_cuda, assembly.h:11-13."""
+    import torch
+    N = geom.N
+    Lm = _empty((N, N), torch.complex128, geom.ctx.device)
+    Km = _empty((N, N), torch.complex128, geom.ctx.device)
+    k = complex(k)
+    geom.ctx.check(lib().bem_assemble_LK_dev(geom.ctx.h, geom.h, k.real, k.imag,
+                                             ASM_GSMOOTH_EXACT if exact_gsmooth else 0,
+                                             _dptr(Lm), _dptr(Km), N))
+    return Lm, Km
+
+
+# ---------------------------------------------------------------------- LU
+def _as_cols(B, n, device):
+    """Column-major n x nrhs device buffer as a torch (nrhs, n) tensor."""
+    import torch
+    if isinstance(B, np.ndarray):
+        B = torch.from_numpy(np.ascontiguousarray(np.asarray(B, dtype=np.complex128).reshape(n, -1).T))
+    B = B.to(device=f"cuda:{device}", dtype=torch.complex128)
+    if B.dim() == 1:
+        B = B.reshape(1, n)
+    return B.contiguous()
+
+
+class LU:
+    """Device-resident factorisation of a row-major complex128 Z (torch tensor).
+
+    precision PREC_FP64: Z is overwritten by its factors (P Z = L U).
+    precision PREC_FP32_REFINE: Z is kept (the FP64 refinement residual uses it;
+    keep the tensor alive) and complex64 factors are made alongside."""
+
+    def __init__(self, ctx: Context, Z, precision=PREC_FP64):
+        import torch
+        assert Z.dtype == torch.complex128 and Z.dim() == 2 and Z.stride(1) == 1
+        self.ctx = ctx
+        self.Z = Z
+        self.n = Z.shape[0]
+        self.precision = precision
+        h = C.c_void_p()
+        info = C.c_int()
+        ctx.check(lib().bem_lu_factor_dev(ctx.h, _dptr(Z), self.n, Z.stride(0), int(precision),
+                                          C.byref(h), C.byref(info)))
+        self.h = h
+        self.info = info.value
+
+    def solve(self, B, X=None, tol=0.0, max_iter=0, raise_noconv=True):
+        """X = Z^-1 B.  B: torch (nrhs, n) complex128 on the device (column c of
+        the column-major n x nrhs right-hand side is row c), or a numpy (n, nrhs)
+        array.  Returns (X as torch (nrhs, n), stats dict)."""
+        B = _as_cols(B, self.n, self.ctx.device)
+        if X is None:
+            X = torch_empty_like(B)
+        st = SolveStats()
+        s = lib().bem_lu_solve_dev(self.ctx.h, self.h, _dptr(B), self.n, _dptr(X), self.n,
+                                   B.shape[0], float(tol), int(max_iter), C.byref(st))
+        if s != 0 and not (s == 5 and not raise_noconv):
+            self.ctx.check(s)
+        return X, st.as_dict()
+
+    def close(self):
+        if self.h:
+            lib().bem_lu_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def torch_empty_like(t):
+    import torch
+    return torch.empty_like(t)
+
+
+def lu_factorize_cuda(ctx: Context, Z):
+    """Host mirror of solver.h:11 -- returns (factors, ipiv (1-based), info);
+    the factors are those of the row-major Z (P Z = L U)."""
+    Zc = np.ascontiguousarray(Z, dtype=np.complex128).copy()
+    n = Zc.shape[0]
+    ipiv = np.zeros(n, dtype=np.int32)
+    info = C.c_int()
+    ctx.check(lib().bem_lu_factorize(ctx.h, _ptr(Zc), n, _ptr(ipiv), C.byref(info)))
+    return Zc, ipiv, info.value
+
+
+def lu_solve_cuda(ctx: Context, Z_lu, ipiv, B):
+    """Host mirror of solver.h:16-17: B (n,) or (n, nrhs) -> X."""
+    n = Z_lu.shape[0]
+    Bf = np.asfortranarray(np.asarray(B, dtype=np.complex128).reshape(n, -1)).copy(order="F")
+    Zl = np.ascontiguousarray(Z_lu, dtype=np.complex128)
+    ip = _i32(ipiv)
+    ctx.check(lib().bem_lu_solve(ctx.h, _ptr(Zl), _ptr(ip), n,
+                                 C.c_void_p(Bf.ctypes.data), Bf.shape[1]))
+    return Bf.reshape(np.shape(B)) if np.ndim(B) == 1 else Bf
+
+
+def lu_solve_full(ctx: Context, Z, B, precision=PREC_FP64):
+    """Host mirror of solver.h:21-22: returns (X, stats)."""
+    Zc = np.ascontiguousarray(Z, dtype=np.complex128).copy()
+    n = Zc.shape[0]
+    Bf = np.asfortranarray(np.asarray(B, dtype=np.complex128).reshape(n, -1)).copy(order="F")
+    st = SolveStats()
+    ctx.check(lib().bem_lu_solve_full(ctx.h, _ptr(Zc), n, C.c_void_p(Bf.ctypes.data), Bf.shape[1],
+                                      int(precision), C.byref(st)))
+    return (Bf.reshape(np.shape(B)) if np.ndim(B) == 1 else Bf), st.as_dict()
+
+
+# --------------------------------------------------------------- excitation
+def rhs_planewave_dev(geom: Geometry, k_ext, eta_ext, RT, B=None):
+    """Right-hand sides for orientations RT (n,3,3): torch (2n_orient, 2N) whose
+    row 2o is par (E0 = RT x), 2o+1 perp (E0 = RT y), k_hat = RT z
+    (rhs.cpp:6-64, main.cpp:739-751)."""
+    import torch
+    RT = _f64(RT).reshape(-1, 9)
+    no = RT.shape[0]
+    if B is None:
+        B = _empty((2 * no, geom.n), torch.complex128, geom.ctx.device)
+    k = complex(k_ext)
+    geom.ctx.check(lib().bem_rhs_planewave_dev(geom.ctx.h, geom.h, k.real, k.imag, float(eta_ext),
+                                               _ptr(RT), no, _dptr(B), B.stride(0)))
+    return B
+
+
+def compute_rhs_planewave(geom: Geometry, k_ext, eta_ext, E0=(1.0, 0.0, 0.0),
+                          k_hat=(0.0, 0.0, 1.0)):
+    """b = [<f,E_inc>; <f,H_inc>] (host, complex128[2N]) -- rhs.h:11-15."""
+    b = np.zeros(geom.n, dtype=np.complex128)
+    k = complex(k_ext)
+    E0, k_hat = _f64(E0), _f64(k_hat)  # keep the contiguous copies alive
+    geom.ctx.check(lib().bem_rhs_planewave(geom.ctx.h, geom.h, k.real, k.imag, float(eta_ext),
+                                           _ptr(E0), _ptr(k_hat),
+                                           C.c_void_p(b.ctypes.data)))
+    return b
+
+
+# ------------------------------------------------------- far field, Mueller
+def compute_farfield_batch(geom: Geometry, coeffs_J, coeffs_M, r_hats, k_ext, eta_ext):
+    """compute_farfield_batch_cuda (farfield.h:35-48): coeffs (n_calls, N) complex,
+    r_hats (n_orient, ndir, 3); returns Fv (n_calls, ndir, 3) complex."""
+    cJ = np.ascontiguousarray(coeffs_J, dtype=np.complex128)
+    cM = np.ascontiguousarray(coeffs_M, dtype=np.complex128)
+    rh = _f64(r_hats)
+    n_calls = cJ.shape[0]
+    no, nd = rh.shape[0], rh.shape[1]
+    Fv = np.zeros((n_calls, nd, 3), dtype=np.complex128)
+    k = complex(k_ext)
+    geom.ctx.check(lib().bem_farfield_batch(geom.ctx.h, geom.h, C.c_void_p(cJ.ctypes.data),
+                                            C.c_void_p(cM.ctypes.data), _ptr(rh), k.real, k.imag,
+                                            float(eta_ext), n_calls, no, nd,
+                                            C.c_void_p(Fv.ctypes.data)))
+    return Fv
+
+
+def mueller_from_solutions_dev(geom: Geometry, X, RT, w, k_ext, eta_ext, ntheta=181,
+                               gamma_mirror=False, M_orient=None):
+    """Orientation-weighted Mueller sum (4,4,ntheta) from device solutions X
+    (torch (2 n_orient, 2N), rows (par, perp) per orientation)."""
+    RT = _f64(RT).reshape(-1, 9)
+    w = _f64(w)
+    M = np.zeros((4, 4, ntheta))
+    k = complex(k_ext)
+    geom.ctx.check(lib().bem_farfield_mueller_dev(
+        geom.ctx.h, geom.h, _dptr(X), X.stride(0), _ptr(RT), _ptr(w), RT.shape[0], k.real, k.imag,
+        float(eta_ext), int(ntheta), int(bool(gamma_mirror)), _ptr(M),
+        _dptr(M_orient) if M_orient is not None else None))
+    return M
+
+
+def amplitude_to_mueller(S1, S2, S3, S4):
+    """Bohren & Huffman 3.16 (farfield.cu:464-508) -> (4, 4, ntheta)."""
+    S = [np.ascontiguousarray(s, dtype=np.complex128) for s in (S1, S2, S3, S4)]
+    nt = len(S[0])
+    M = np.zeros((4, 4, nt))
+    check(lib().bem_amplitude_to_mueller(*[C.c_void_p(s.ctypes.data) for s in S], nt, _ptr(M)))
+    return M
+
+
+# ------------------------------------------------------------ whole pipeline
+def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=False,
+              orient=(8, 8, 1), orient_sym=(1, 1), gamma_mirror=False, orient_range=None,
+              ntheta=181, precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False):
+    """The --solver dense pipeline (main.cpp:660-854) through bem_dense_run.
+    Returns (mueller (4,4,ntheta), info dict)."""
+    v, t = _f64(verts), _i32(tris)
+    m = complex(m)
+    i0, i1 = orient_range if orient_range is not None else (-1, -1)
+    p = Problem(verts=v.ctypes.data, nv=len(v), tris=t.ctypes.data, nt=len(t), ka=float(ka),
+                m_re=m.real, m_im=m.imag, quad_order=int(quad_order), single=int(bool(single)),
+                n_alpha=int(orient[0]), n_beta=int(orient[1]), n_gamma=int(orient[2]),
+                beta_sym=int(orient_sym[0]), gamma_sym=int(orient_sym[1]),
+                gamma_mirror=int(bool(gamma_mirror)), orient_i0=int(i0), orient_i1=int(i1),
+                ntheta=int(ntheta), precision=int(precision), refine_tol=float(refine_tol),
+                max_refine=int(max_refine), asm_flags=ASM_GSMOOTH_EXACT if exact_gsmooth else 0)
+    M = np.zeros((4, 4, ntheta))
+    r = Result(mueller=M.ctypes.data)
+    ctx.check(lib().bem_dense_run(ctx.h, C.byref(p), C.byref(r)))
+    info = {"N": r.N, "n_orient": r.n_orient, "t_assembly_s": r.t_assembly_s,
+            "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s, "t_total_s": r.t_total_s,
+            "stats": r.stats.as_dict()}
+    return M, info

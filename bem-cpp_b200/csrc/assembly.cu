@@ -1,0 +1,670 @@
+// PMCHWT assembly on the device (FP64).
+//
+// Restates assemble_LK_kernel (assembly.cu:14-135), precompute_half
+// (assembly.cu:150-201), apply_singular_corrections (assembly.cu:208-321),
+// the symmetrisation (assembly.cu:494-502) and the block fill of
+// assemble_pmchwt (pmchwt.cu:36-51) as one device pipeline:
+//
+//   1. graglia_kernel     -- per (triangle, point): Graglia P and the
+//                            finite-difference vector potential V (FP64).
+//   2. assemble_kernel    -- per 16x16 tile of RWG pairs (m <= n tiles only):
+//                            all four half pairs, both media, quadrature part of
+//                            L and K, written straight into the four Z blocks and
+//                            mirrored (L and K are symmetric).
+//   3. singular_fixup     -- per RWG pair sharing a triangle: the symmetrised
+//                            same-triangle correction (S[m,n] + S[n,m])/2.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "bem_internal.h"
+
+namespace bem {
+
+#define INV4PI_D 0.079577471545947667884
+
+// ------------------------------------------------------------ geometry upload
+bool host_mesh_from(const double* verts, int nv, const int* tris, int nt, HostMesh* m);
+
+int geom_upload(bem_ctx* ctx, bem_geom* g) {
+    const HostMesh& m = g->mesh;
+    const HostRWG& r = g->rwg;
+    const Quad& q = g->quad;
+    const int N = r.N, Nq = q.n, nt = m.nt();
+    const size_t P = (size_t)2 * N * Nq;
+    // host staging
+    std::vector<double> px(P), py(P), pz(P), fx(P), fy(P), fz(P), cx(P), cy(P), cz(P), jw(P);
+    std::vector<double> div(2 * N), coef(2 * N), frx(2 * N), fry(2 * N), frz(2 * N);
+    std::vector<int> tri(2 * N);
+    for (int h = 0; h < 2; h++) {
+        int sign = h == 0 ? 1 : -1;
+        for (int n = 0; n < N; n++) {
+            int t = h == 0 ? r.tri_p[n] : r.tri_m[n];
+            V3 fr = h == 0 ? r.free_p[n] : r.free_m[n];
+            double area = h == 0 ? r.area_p[n] : r.area_m[n];
+            double c = sign * r.length[n] / (2.0 * area);
+            int hn = h * N + n;
+            div[hn] = sign * r.length[n] / area;
+            coef[hn] = c;
+            frx[hn] = fr.x, fry[hn] = fr.y, frz[hn] = fr.z;
+            tri[hn] = t;
+            V3 v0 = m.verts[m.tris[3 * t]], v1 = m.verts[m.tris[3 * t + 1]],
+               v2 = m.verts[m.tris[3 * t + 2]];
+            for (int k = 0; k < Nq; k++) {
+                double l1 = q.l1[k], l2 = q.l2[k], l0 = 1.0 - l1 - l2;
+                // r = v0 l0 + v1 l1 + v2 l2, evaluated left to right as the reference
+                double rx = (v0.x * l0 + v1.x * l1) + v2.x * l2;
+                double ry = (v0.y * l0 + v1.y * l1) + v2.y * l2;
+                double rz = (v0.z * l0 + v1.z * l1) + v2.z * l2;
+                double ffx = (rx - fr.x) * c, ffy = (ry - fr.y) * c, ffz = (rz - fr.z) * c;
+                size_t i = (size_t)hn * Nq + k;
+                px[i] = rx, py[i] = ry, pz[i] = rz;
+                fx[i] = ffx, fy[i] = ffy, fz[i] = ffz;
+                cx[i] = ffy * rz - ffz * ry;
+                cy[i] = ffz * rx - ffx * rz;
+                cz[i] = ffx * ry - ffy * rx;
+                jw[i] = area * q.w[k];
+            }
+        }
+    }
+    // singular pairs: halves per triangle, ordered (test, source) items per
+    // unordered RWG pair
+    std::vector<std::vector<int>> on_tri(nt);
+    for (int h = 0; h < 2; h++)
+        for (int n = 0; n < N; n++) on_tri[h == 0 ? r.tri_p[n] : r.tri_m[n]].push_back(h * N + n);
+    std::map<std::pair<int, int>, std::vector<int>> slot;  // (m<=n) -> items (t, a, b)
+    for (int t = 0; t < nt; t++)
+        for (int a : on_tri[t])
+            for (int b : on_tri[t]) {
+                int mm = a % N, nn = b % N;
+                auto& v = slot[{std::min(mm, nn), std::max(mm, nn)}];
+                v.push_back(t);
+                v.push_back(a);
+                v.push_back(b);
+            }
+    std::vector<int> pair_mn, item_ptr{0}, item;
+    for (auto& kv : slot) {
+        pair_mn.push_back(kv.first.first);
+        pair_mn.push_back(kv.first.second);
+        item.insert(item.end(), kv.second.begin(), kv.second.end());
+        item_ptr.push_back((int)item.size() / 3);
+    }
+    std::vector<double> tv(9 * (size_t)nt);
+    for (int t = 0; t < nt; t++)
+        for (int j = 0; j < 3; j++) {
+            V3 v = m.verts[m.tris[3 * t + j]];
+            tv[9 * t + 3 * j] = v.x, tv[9 * t + 3 * j + 1] = v.y, tv[9 * t + 3 * j + 2] = v.z;
+        }
+    g->sing.npairs = (int)pair_mn.size() / 2;
+    g->sing.nitems = (int)item.size() / 3;
+
+    // one device allocation, 256-byte aligned sub-arrays
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    size_t o_pt[10];
+    for (int i = 0; i < 10; i++) o_pt[i] = take(P * 8);
+    size_t o_div = take(2 * N * 8), o_coef = take(2 * N * 8), o_fr = take(3 * 2 * N * 8);
+    size_t o_tri = take(2 * N * 4);
+    size_t o_pmn = take(pair_mn.size() * 4), o_iptr = take(item_ptr.size() * 4),
+           o_item = take(item.size() * 4);
+    size_t o_P = take((size_t)nt * Nq * 8), o_V = take((size_t)nt * Nq * 3 * 8),
+           o_tv = take(tv.size() * 8);
+    BEM_TRY_CUDA(ctx, cudaMalloc(&g->dmem, off));
+    char* base = (char*)g->dmem;
+    double** pts[10] = {&g->half.px, &g->half.py, &g->half.pz, &g->half.fx, &g->half.fy,
+                        &g->half.fz, &g->half.cx, &g->half.cy, &g->half.cz, &g->half.jw};
+    std::vector<double>* src[10] = {&px, &py, &pz, &fx, &fy, &fz, &cx, &cy, &cz, &jw};
+    for (int i = 0; i < 10; i++) {
+        *pts[i] = (double*)(base + o_pt[i]);
+        BEM_TRY_CUDA(ctx, cudaMemcpy(*pts[i], src[i]->data(), P * 8, cudaMemcpyHostToDevice));
+    }
+    g->half.div = (double*)(base + o_div);
+    g->half.tri = (int*)(base + o_tri);
+    double* d_coef = (double*)(base + o_coef);
+    double* d_fr = (double*)(base + o_fr);
+    BEM_TRY_CUDA(ctx, cudaMemcpy(g->half.div, div.data(), 2 * N * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(d_coef, coef.data(), 2 * N * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(d_fr, frx.data(), 2 * N * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(d_fr + 2 * N, fry.data(), 2 * N * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(d_fr + 4 * N, frz.data(), 2 * N * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(g->half.tri, tri.data(), 2 * N * 4, cudaMemcpyHostToDevice));
+    g->sing.pair_mn = (int*)(base + o_pmn);
+    g->sing.item_ptr = (int*)(base + o_iptr);
+    g->sing.item = (int*)(base + o_item);
+    g->sing.P = (double*)(base + o_P);
+    g->sing.V = (double*)(base + o_V);
+    g->sing.tv = (double*)(base + o_tv);
+    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.pair_mn, pair_mn.data(), pair_mn.size() * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.item_ptr, item_ptr.data(), item_ptr.size() * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.item, item.data(), item.size() * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.tv, tv.data(), tv.size() * 8, cudaMemcpyHostToDevice));
+    // half coefficient and free vertex live right after div (see fixup kernel)
+    (void)d_coef;
+    (void)d_fr;
+    g->sing_coef = d_coef;
+    g->sing_free = d_fr;
+    return BEM_OK;
+}
+
+// ------------------------------------------------------------ Graglia (FP64)
+struct TriQ {
+    int n;
+    double l1[25], l2[25], w[25];
+};
+
+// int_T 1/|r - r'| dS' (Graglia 1993) -- graglia.h:11-66, same guards.
+__device__ double potential_integral(double rx, double ry, double rz, const double* v) {
+    const double ax = v[0], ay = v[1], az = v[2], bx = v[3], by = v[4], bz = v[5],
+                 cx = v[6], cy = v[7], cz = v[8];
+    double e1x = bx - ax, e1y = by - ay, e1z = bz - az;
+    double e2x = cx - ax, e2y = cy - ay, e2z = cz - az;
+    double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    double nn = sqrt(nx * nx + ny * ny + nz * nz);
+    if (nn < 1e-15) return 0.0;
+    nx /= nn, ny /= nn, nz /= nn;
+    double res = 0.0;
+    for (int i = 0; i < 3; i++) {
+        const double* vi = v + 3 * i;
+        const double* vj = v + 3 * ((i + 1) % 3);
+        double ex = vj[0] - vi[0], ey = vj[1] - vi[1], ez = vj[2] - vi[2];
+        double le = sqrt(ex * ex + ey * ey + ez * ez);
+        if (le < 1e-15) continue;
+        double tx = ex / le, ty = ey / le, tz = ez / le;
+        double mx = ny * tz - nz * ty, my = nz * tx - nx * tz, mz = nx * ty - ny * tx;
+        double dix = rx - vi[0], diy = ry - vi[1], diz = rz - vi[2];
+        double d = dix * mx + diy * my + diz * mz;
+        double h = dix * nx + diy * ny + diz * nz;
+        double djx = vj[0] - rx, djy = vj[1] - ry, djz = vj[2] - rz;
+        double dkx = vi[0] - rx, dky = vi[1] - ry, dkz = vi[2] - rz;
+        double sp = djx * tx + djy * ty + djz * tz;
+        double sm = dkx * tx + dky * ty + dkz * tz;
+        double Rp = sqrt(djx * djx + djy * djy + djz * djz);
+        double Rm = sqrt(dkx * dkx + dky * dky + dkz * dkz);
+        if (Rp + sp > 1e-15 && Rm + sm > 1e-15) {
+            double arg = (Rp + sp) / (Rm + sm);
+            if (arg > 0) res += d * log(arg);
+        }
+        double ah = fabs(h);
+        if (ah > 1e-15) {
+            double R0 = d * d + h * h;
+            double t1 = atan2(d * sp, R0 + ah * Rp);
+            double t2 = atan2(d * sm, R0 + ah * Rm);
+            res -= ah * (t1 - t2);
+        }
+    }
+    return res;
+}
+
+// int_T |r - r'| dS' by the triangle rule -- graglia.h:69-85.  Evaluated with
+// explicitly rounded operations (no FMA contraction) in the reference's
+// order: the central difference below divides by 2e-6, so W must round the
+// way the reference rounds it.
+__device__ double integral_R(double rx, double ry, double rz, const double* v, const TriQ& q) {
+    double e1x = __dsub_rn(v[3], v[0]), e1y = __dsub_rn(v[4], v[1]), e1z = __dsub_rn(v[5], v[2]);
+    double e2x = __dsub_rn(v[6], v[0]), e2y = __dsub_rn(v[7], v[1]), e2z = __dsub_rn(v[8], v[2]);
+    double nx = __dsub_rn(__dmul_rn(e1y, e2z), __dmul_rn(e1z, e2y));
+    double ny = __dsub_rn(__dmul_rn(e1z, e2x), __dmul_rn(e1x, e2z));
+    double nz = __dsub_rn(__dmul_rn(e1x, e2y), __dmul_rn(e1y, e2x));
+    double area = __dmul_rn(0.5, __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)),
+                                                      __dmul_rn(nz, nz))));
+    double acc = 0.0;
+    for (int k = 0; k < q.n; k++) {
+        double l0 = __dsub_rn(__dsub_rn(1.0, q.l1[k]), q.l2[k]);
+        double px = __dadd_rn(__dadd_rn(__dmul_rn(l0, v[0]), __dmul_rn(q.l1[k], v[3])), __dmul_rn(q.l2[k], v[6]));
+        double py = __dadd_rn(__dadd_rn(__dmul_rn(l0, v[1]), __dmul_rn(q.l1[k], v[4])), __dmul_rn(q.l2[k], v[7]));
+        double pz = __dadd_rn(__dadd_rn(__dmul_rn(l0, v[2]), __dmul_rn(q.l1[k], v[5])), __dmul_rn(q.l2[k], v[8]));
+        double dx = __dsub_rn(px, rx), dy = __dsub_rn(py, ry), dz = __dsub_rn(pz, rz);
+        double R = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+        acc = __dadd_rn(acc, __dmul_rn(q.w[k], R));
+    }
+    return __dmul_rn(area, acc);
+}
+
+// One thread per (triangle, point): P and V = r P - grad W (central
+// differences, eps = 1e-6) -- graglia.h:90-112.
+__global__ void graglia_kernel(const double* __restrict__ tv, int nt, TriQ q,
+                               double* __restrict__ P, double* __restrict__ V) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt * q.n) return;
+    int t = i / q.n, k = i % q.n;
+    double v[9];
+    for (int j = 0; j < 9; j++) v[j] = tv[9 * t + j];
+    double l1 = q.l1[k], l2 = q.l2[k];
+    double l0 = __dsub_rn(__dsub_rn(1.0, l1), l2);
+    double r[3];
+    for (int d = 0; d < 3; d++)
+        r[d] = __dadd_rn(__dadd_rn(__dmul_rn(v[d], l0), __dmul_rn(v[3 + d], l1)), __dmul_rn(v[6 + d], l2));
+    double p = potential_integral(r[0], r[1], r[2], v);
+    const double eps = 1e-6;
+    double g[3];
+    for (int d = 0; d < 3; d++) {
+        double rp[3] = {r[0], r[1], r[2]}, rm[3] = {r[0], r[1], r[2]};
+        rp[d] = __dadd_rn(rp[d], eps);
+        rm[d] = __dsub_rn(rm[d], eps);
+        double wp = integral_R(rp[0], rp[1], rp[2], v, q);
+        double wm = integral_R(rm[0], rm[1], rm[2], v, q);
+        g[d] = __ddiv_rn(__dsub_rn(wp, wm), 2.0 * eps);
+    }
+    P[i] = p;
+    for (int d = 0; d < 3; d++) V[3 * i + d] = __dsub_rn(__dmul_rn(r[d], p), g[d]);
+}
+
+// ------------------------------------------------------------ complex helpers
+struct cplx {
+    double re, im;
+};
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+struct Medium {
+    double kr, ki;  // k = kr + i ki
+};
+
+// ------------------------------------------------------------ main assembly
+constexpr int TILE = 16;
+constexpr int MAXQ = 13;
+
+struct AsmArgs {
+    DevHalf h;
+    int N, Nq;
+    int ntile;       // tiles per side
+    Medium med[2];   // ext, int (only med[0] when nmed == 1)
+    double eta_e, eta_i;
+    unsigned flags;
+    // outputs
+    double2* Z;      // row-major 2N x 2N (nmed == 2)
+    int64_t ldz;
+    double2* L;      // row-major N x N (nmed == 1)
+    double2* K;
+    int64_t ld;
+};
+
+// G_smooth = (exp(ikR) - 1)/(4 pi R) without cancellation (limit ik/(4 pi)).
+__device__ __forceinline__ cplx g_smooth_exact(Medium k, double R) {
+    if (R == 0.0) return {-k.ki * INV4PI_D, k.kr * INV4PI_D};
+    double s, c, sh, ch;
+    sincos(k.kr * R, &s, &c);
+    sincos(0.5 * k.kr * R, &sh, &ch);
+    double re = expm1(-k.ki * R) * c - 2.0 * sh * sh;
+    double im = exp(-k.ki * R) * s;
+    double f = INV4PI_D / R;
+    return {re * f, im * f};
+}
+
+template <int NMED>
+__global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
+    // upper-triangular tile index -> (tile row bi, tile col bj), bi <= bj
+    int64_t lin = blockIdx.x;
+    int T = a.ntile;
+    // row bi starts at offset bi*T - bi*(bi-1)/2
+    int bi = (int)floor((2.0 * T + 1.0 - sqrt((2.0 * T + 1.0) * (2.0 * T + 1.0) - 8.0 * (double)lin)) * 0.5);
+    if (bi < 0) bi = 0;
+    while (bi > 0 && (int64_t)bi * T - (int64_t)bi * (bi - 1) / 2 > lin) bi--;
+    while ((int64_t)(bi + 1) * T - (int64_t)(bi + 1) * bi / 2 <= lin) bi++;
+    int bj = bi + (int)(lin - ((int64_t)bi * T - (int64_t)bi * (bi - 1) / 2));
+
+    const int N = a.N, Nq = a.Nq;
+    const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
+    const int m0 = bi * TILE, n0 = bj * TILE;
+
+    // source data of the tile's columns: [half][q][col]
+    __shared__ double s_px[2][MAXQ][TILE], s_py[2][MAXQ][TILE], s_pz[2][MAXQ][TILE];
+    __shared__ double s_fx[2][MAXQ][TILE], s_fy[2][MAXQ][TILE], s_fz[2][MAXQ][TILE];
+    __shared__ double s_cx[2][MAXQ][TILE], s_cy[2][MAXQ][TILE], s_cz[2][MAXQ][TILE];
+    __shared__ double s_jw[2][MAXQ][TILE];
+    __shared__ double s_div[2][TILE];
+    __shared__ int s_tri[2][TILE];
+    for (int i = threadIdx.x; i < 2 * Nq * TILE; i += blockDim.x) {
+        int col = i % TILE, q = (i / TILE) % Nq, h = i / (TILE * Nq);
+        int n = min(n0 + col, N - 1);
+        size_t p = ((size_t)(h * N + n)) * Nq + q;
+        s_px[h][q][col] = a.h.px[p];
+        s_py[h][q][col] = a.h.py[p];
+        s_pz[h][q][col] = a.h.pz[p];
+        s_fx[h][q][col] = a.h.fx[p];
+        s_fy[h][q][col] = a.h.fy[p];
+        s_fz[h][q][col] = a.h.fz[p];
+        s_cx[h][q][col] = a.h.cx[p];
+        s_cy[h][q][col] = a.h.cy[p];
+        s_cz[h][q][col] = a.h.cz[p];
+        s_jw[h][q][col] = a.h.jw[p];
+    }
+    if (threadIdx.x < 2 * TILE) {
+        int h = threadIdx.x / TILE, col = threadIdx.x % TILE;
+        int n = min(n0 + col, N - 1);
+        s_div[h][col] = a.h.div[h * N + n];
+        s_tri[h][col] = a.h.tri[h * N + n];
+    }
+    __syncthreads();
+
+    const int m = min(m0 + ty, N - 1);
+    const bool exact = (a.flags & BEM_ASM_GSMOOTH_EXACT) != 0;
+    cplx Lv[NMED], Ls[NMED], Kk[NMED];
+    for (int e = 0; e < NMED; e++) Lv[e] = Ls[e] = Kk[e] = {0.0, 0.0};
+
+    for (int th = 0; th < 2; th++) {
+        const int thn = th * N + m;
+        const int ttri = a.h.tri[thn];
+        const double tdiv = a.h.div[thn];
+        for (int sh = 0; sh < 2; sh++) {
+            const bool sing = (ttri == s_tri[sh][tx]);
+            const double dd = tdiv * s_div[sh][tx];
+            cplx Lsb[NMED];
+            for (int e = 0; e < NMED; e++) Lsb[e] = {0.0, 0.0};
+            for (int q = 0; q < Nq; q++) {
+                size_t tp = (size_t)thn * Nq + q;
+                const double tpx = a.h.px[tp], tpy = a.h.py[tp], tpz = a.h.pz[tp];
+                const double tfx = a.h.fx[tp], tfy = a.h.fy[tp], tfz = a.h.fz[tp];
+                const double tcx = a.h.cx[tp], tcy = a.h.cy[tp], tcz = a.h.cz[tp];
+                const double tjw = a.h.jw[tp];
+                for (int qs = 0; qs < Nq; qs++) {
+                    double dx = tpx - s_px[sh][qs][tx];
+                    double dy = tpy - s_py[sh][qs][tx];
+                    double dz = tpz - s_pz[sh][qs][tx];
+                    double R = sqrt(dx * dx + dy * dy + dz * dz);
+                    double Rs = fmax(R, 1e-15);
+                    double invR = 1.0 / Rs;
+                    double i4R = INV4PI_D * invR;
+                    double jwp = tjw * s_jw[sh][qs][tx];
+                    double fdot = tfx * s_fx[sh][qs][tx] + tfy * s_fy[sh][qs][tx] + tfz * s_fz[sh][qs][tx];
+                    // f_t . ((r_t - r_s) x f_s) = (f_t x r_t).f_s + f_t.(f_s x r_s)
+                    double trip = (tcx * s_fx[sh][qs][tx] + tcy * s_fy[sh][qs][tx] + tcz * s_fz[sh][qs][tx]) +
+                                  (tfx * s_cx[sh][qs][tx] + tfy * s_cy[sh][qs][tx] + tfz * s_cz[sh][qs][tx]);
+                    bool kval = !sing && R > 1e-12;
+#pragma unroll
+                    for (int e = 0; e < NMED; e++) {
+                        const Medium k = a.med[e];
+                        double s, c;
+                        sincos(k.kr * Rs, &s, &c);
+                        double ea = (k.ki != 0.0) ? exp(-k.ki * Rs) : 1.0;
+                        cplx G = {ea * c * i4R, ea * s * i4R};
+                        cplx Gu = G;
+                        if (sing) {
+                            if (exact) Gu = g_smooth_exact(k, R);
+                            else Gu.re -= i4R;
+                        }
+                        cplx Gj = {Gu.re * jwp, Gu.im * jwp};
+                        Lv[e].re += fdot * Gj.re;
+                        Lv[e].im += fdot * Gj.im;
+                        Lsb[e].re += Gj.re;
+                        Lsb[e].im += Gj.im;
+                        if (kval) {
+                            // grad G coefficient (ik - 1/R)/R
+                            cplx gc = cmul(G, cplx{(-k.ki - invR) * invR, k.kr * invR});
+                            double w = jwp * trip;
+                            Kk[e].re += gc.re * w;
+                            Kk[e].im += gc.im * w;
+                        }
+                    }
+                }
+            }
+            for (int e = 0; e < NMED; e++) {
+                Ls[e].re += dd * Lsb[e].re;
+                Ls[e].im += dd * Lsb[e].im;
+            }
+        }
+    }
+    const int n = n0 + tx;
+    const int mm = m0 + ty;
+    if (mm >= N || n >= N) return;
+    // L = ik Lvec - (i/k) sum(div div Lscl)
+    cplx Lf[NMED];
+    for (int e = 0; e < NMED; e++) {
+        Medium k = a.med[e];
+        cplx ik = {-k.ki, k.kr};
+        double k2 = k.kr * k.kr + k.ki * k.ki;
+        cplx iok = {k.ki / k2, k.kr / k2};  // i/k
+        cplx t1 = cmul(ik, Lv[e]), t2 = cmul(iok, Ls[e]);
+        Lf[e] = {t1.re - t2.re, t1.im - t2.im};
+    }
+    const bool mirror = (bi != bj);
+    if (NMED == 2) {
+        cplx TL = {a.eta_e * Lf[0].re + a.eta_i * Lf[1].re, a.eta_e * Lf[0].im + a.eta_i * Lf[1].im};
+        cplx BR = {Lf[0].re / a.eta_e + Lf[1].re / a.eta_i, Lf[0].im / a.eta_e + Lf[1].im / a.eta_i};
+        cplx Ks = {Kk[0].re + Kk[1].re, Kk[0].im + Kk[1].im};
+        double2* Z = a.Z;
+        int64_t ld = a.ldz;
+        Z[(int64_t)mm * ld + n] = make_double2(TL.re, TL.im);
+        Z[(int64_t)mm * ld + N + n] = make_double2(-Ks.re, -Ks.im);
+        Z[(int64_t)(N + mm) * ld + n] = make_double2(Ks.re, Ks.im);
+        Z[(int64_t)(N + mm) * ld + N + n] = make_double2(BR.re, BR.im);
+        if (mirror) {
+            Z[(int64_t)n * ld + mm] = make_double2(TL.re, TL.im);
+            Z[(int64_t)n * ld + N + mm] = make_double2(-Ks.re, -Ks.im);
+            Z[(int64_t)(N + n) * ld + mm] = make_double2(Ks.re, Ks.im);
+            Z[(int64_t)(N + n) * ld + N + mm] = make_double2(BR.re, BR.im);
+        }
+    } else {
+        a.L[(int64_t)mm * a.ld + n] = make_double2(Lf[0].re, Lf[0].im);
+        a.K[(int64_t)mm * a.ld + n] = make_double2(Kk[0].re, Kk[0].im);
+        if (mirror) {
+            a.L[(int64_t)n * a.ld + mm] = make_double2(Lf[0].re, Lf[0].im);
+            a.K[(int64_t)n * a.ld + mm] = make_double2(Kk[0].re, Kk[0].im);
+        }
+    }
+}
+
+// ------------------------------------------------------------ singular fixup
+struct FixArgs {
+    DevHalf h;
+    DevSingular s;
+    const double* coef;  // (2N) sign*l/(2A)
+    const double* fr;    // (3*2N) free vertex: x block, y block, z block
+    int N, Nq, nmed;
+    Medium med[2];
+    double eta_e, eta_i;
+    double2* Z;
+    int64_t ldz;
+    double2* L;
+    int64_t ld;
+};
+
+// One thread per unordered RWG pair {m, n} sharing a triangle.  For every
+// (triangle t, test half a, source half b) item:
+//   A = div_a div_b sum_q P_q jw_a,q / (4 pi)
+//   B = sum_q f_a,q . coef_b (V_q - r_free,b P_q) jw_a,q / (4 pi)
+// and S = -(i/k) A + i k B (assembly.cu:290-317).  The symmetrised
+// correction (S[m,n] + S[n,m])/2 is added to both L entries.
+__global__ void singular_fixup_kernel(FixArgs a) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.s.npairs) return;
+    const int N = a.N, Nq = a.Nq;
+    int m = a.s.pair_mn[2 * p], n = a.s.pair_mn[2 * p + 1];
+    double SA = 0.0, SB = 0.0;
+    for (int it = a.s.item_ptr[p]; it < a.s.item_ptr[p + 1]; it++) {
+        int t = a.s.item[3 * it], ha = a.s.item[3 * it + 1], hb = a.s.item[3 * it + 2];
+        double sbase = 0.0, vec = 0.0;
+        double cb = a.coef[hb];
+        double frx = a.fr[hb], fry = a.fr[2 * N + hb], frz = a.fr[4 * N + hb];
+        for (int q = 0; q < Nq; q++) {
+            size_t ip = (size_t)ha * Nq + q;
+            size_t tq = (size_t)t * Nq + q;
+            double P = a.s.P[tq];
+            double jw = a.h.jw[ip];
+            sbase += P * jw;
+            double gx = cb * (a.s.V[3 * tq] - frx * P);
+            double gy = cb * (a.s.V[3 * tq + 1] - fry * P);
+            double gz = cb * (a.s.V[3 * tq + 2] - frz * P);
+            vec += (a.h.fx[ip] * gx + a.h.fy[ip] * gy + a.h.fz[ip] * gz) * jw;
+        }
+        SA += a.h.div[ha] * a.h.div[hb] * (sbase * INV4PI_D);
+        SB += vec * INV4PI_D;
+    }
+    if (m != n) {
+        SA *= 0.5;
+        SB *= 0.5;
+    }
+    cplx dL[2];
+    for (int e = 0; e < a.nmed; e++) {
+        Medium k = a.med[e];
+        double k2 = k.kr * k.kr + k.ki * k.ki;
+        cplx iok = {k.ki / k2, k.kr / k2};
+        cplx ik = {-k.ki, k.kr};
+        dL[e] = {-iok.re * SA + ik.re * SB, -iok.im * SA + ik.im * SB};
+    }
+    if (a.nmed == 2) {
+        cplx TL = {a.eta_e * dL[0].re + a.eta_i * dL[1].re, a.eta_e * dL[0].im + a.eta_i * dL[1].im};
+        cplx BR = {dL[0].re / a.eta_e + dL[1].re / a.eta_i, dL[0].im / a.eta_e + dL[1].im / a.eta_i};
+        double2* z;
+        z = &a.Z[(int64_t)m * a.ldz + n];
+        z->x += TL.re, z->y += TL.im;
+        z = &a.Z[(int64_t)(N + m) * a.ldz + N + n];
+        z->x += BR.re, z->y += BR.im;
+        if (m != n) {
+            z = &a.Z[(int64_t)n * a.ldz + m];
+            z->x += TL.re, z->y += TL.im;
+            z = &a.Z[(int64_t)(N + n) * a.ldz + N + m];
+            z->x += BR.re, z->y += BR.im;
+        }
+    } else {
+        double2* z = &a.L[(int64_t)m * a.ld + n];
+        z->x += dL[0].re, z->y += dL[0].im;
+        if (m != n) {
+            z = &a.L[(int64_t)n * a.ld + m];
+            z->x += dL[0].re, z->y += dL[0].im;
+        }
+    }
+}
+
+// mode 2: PMCHWT into Z; mode 1: L and K of medium 0 into L, K.
+int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
+                 double ki_im, double eta_e, double eta_i, unsigned flags, int mode, void* Z,
+                 int64_t ldz, void* L, void* K) {
+    const int N = g->N;
+    if (N < 1) return fail(ctx, BEM_ERR_INVALID, "empty basis");
+    if (mode == 2 && (!Z || ldz < 2 * N)) return fail(ctx, BEM_ERR_INVALID, "bad Z / ldz");
+    if (mode == 1 && (!L || !K || ldz < N)) return fail(ctx, BEM_ERR_INVALID, "bad L/K / ld");
+    if (!(ke_re != 0.0 || ke_im != 0.0) || (mode == 2 && !(ki_re != 0.0 || ki_im != 0.0)))
+        return fail(ctx, BEM_ERR_INVALID, "zero wavenumber");
+    if (mode == 2 && (!(eta_e > 0) || !(eta_i > 0))) return fail(ctx, BEM_ERR_INVALID, "eta <= 0");
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    // 1. Graglia P, V per (triangle, point)
+    TriQ tq;
+    tq.n = g->quad.n;
+    for (int i = 0; i < 25; i++) tq.l1[i] = g->quad.l1[i], tq.l2[i] = g->quad.l2[i], tq.w[i] = g->quad.w[i];
+    int nthr = g->nt * g->Nq;
+    graglia_kernel<<<(nthr + 127) / 128, 128, 0, st>>>(g->sing.tv, g->nt, tq, g->sing.P, g->sing.V);
+    BEM_LAUNCHED(ctx);
+    // 2. quadrature part, upper tiles
+    AsmArgs a;
+    a.h = g->half;
+    a.N = N;
+    a.Nq = g->Nq;
+    a.ntile = (N + TILE - 1) / TILE;
+    a.med[0] = {ke_re, ke_im};
+    a.med[1] = {ki_re, ki_im};
+    a.eta_e = eta_e;
+    a.eta_i = eta_i;
+    a.flags = flags;
+    a.Z = (double2*)Z;
+    a.ldz = ldz;
+    a.L = (double2*)L;
+    a.K = (double2*)K;
+    a.ld = ldz;
+    int64_t ntiles = (int64_t)a.ntile * (a.ntile + 1) / 2;
+    if (ntiles > 0x7fffffffLL) return fail(ctx, BEM_ERR_INVALID, "too many tiles");
+    if (mode == 2)
+        assemble_kernel<2><<<(unsigned)ntiles, 256, 0, st>>>(a);
+    else
+        assemble_kernel<1><<<(unsigned)ntiles, 256, 0, st>>>(a);
+    BEM_LAUNCHED(ctx);
+    // 3. singular correction
+    if (g->sing.npairs > 0) {
+        FixArgs f;
+        f.h = g->half;
+        f.s = g->sing;
+        f.coef = g->sing_coef;
+        f.fr = g->sing_free;
+        f.N = N;
+        f.Nq = g->Nq;
+        f.nmed = mode;
+        f.med[0] = {ke_re, ke_im};
+        f.med[1] = {ki_re, ki_im};
+        f.eta_e = eta_e;
+        f.eta_i = eta_i;
+        f.Z = (double2*)Z;
+        f.ldz = ldz;
+        f.L = (double2*)L;
+        f.ld = ldz;
+        singular_fixup_kernel<<<(g->sing.npairs + 127) / 128, 128, 0, st>>>(f);
+        BEM_LAUNCHED(ctx);
+    }
+    return BEM_OK;
+}
+
+}  // namespace bem
+
+using namespace bem;
+
+extern "C" {
+
+int bem_geom_create(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
+                    int quad_order, bem_geom** out, int* N) {
+    if (!ctx || !out) return BEM_ERR_INVALID;
+    *out = nullptr;
+    bem_geom* g = new bem_geom();
+    g->ctx = ctx;
+    g->device = ctx->device;
+    if (!host_mesh_from(verts, nv, tris, nt, &g->mesh)) {
+        delete g;
+        return fail(ctx, BEM_ERR_INVALID, "bad mesh arrays");
+    }
+    if (!quadrature(quad_order, &g->quad)) {
+        delete g;
+        return fail(ctx, BEM_ERR_INVALID, "quadrature order %d unsupported (4, 7, 13)", quad_order);
+    }
+    g->quad_order = quad_order;
+    g->rwg = build_rwg(g->mesh);
+    g->N = g->rwg.N;
+    g->Nq = g->quad.n;
+    g->nv = nv;
+    g->nt = nt;
+    if (g->N < 1) {
+        delete g;
+        return fail(ctx, BEM_ERR_INVALID, "mesh has no interior edges");
+    }
+    int s = cudaSetDevice(ctx->device) == cudaSuccess ? geom_upload(ctx, g) : BEM_ERR_CUDA;
+    if (s != BEM_OK) {
+        if (g->dmem) cudaFree(g->dmem);
+        delete g;
+        return s;
+    }
+    *out = g;
+    if (N) *N = g->N;
+    return BEM_OK;
+}
+
+int bem_geom_free(bem_geom* g) {
+    if (!g) return BEM_OK;
+    if (g->dmem) {
+        cudaSetDevice(g->device);
+        cudaFree(g->dmem);  // implicitly waits for work using it
+    }
+    delete g;
+    return BEM_OK;
+}
+
+int bem_geom_size(const bem_geom* g) { return g ? g->N : 0; }
+
+int bem_assemble_pmchwt_dev(bem_ctx* ctx, const bem_geom* g, double kext_re, double kext_im,
+                            double kint_re, double kint_im, double eta_ext, double eta_int,
+                            unsigned flags, void* Z_dev, int64_t ldz) {
+    if (!ctx || !g) return BEM_ERR_INVALID;
+    return assemble_dev(ctx, g, kext_re, kext_im, kint_re, kint_im, eta_ext, eta_int, flags, 2,
+                        Z_dev, ldz, nullptr, nullptr);
+}
+
+int bem_assemble_LK_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
+                        unsigned flags, void* L_dev, void* K_dev, int64_t ld) {
+    if (!ctx || !g) return BEM_ERR_INVALID;
+    return assemble_dev(ctx, g, k_re, k_im, 0, 0, 1, 1, flags, 1, nullptr, ld, L_dev, K_dev);
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// Internal declarations shared by the libbemdense translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "bem_dense.h"
+
+namespace bem {
+
+// ---------------------------------------------------------------- errors
+struct Error {
+    int status;
+    std::string msg;
+};
+
+// Records a failure on the context and returns its status.
+int fail(bem_ctx* ctx, int status, const char* fmt, ...);
+
+#define BEM_TRY_CUDA(ctx, call)                                                         \
+    do {                                                                                \
+        cudaError_t e__ = (call);                                                       \
+        if (e__ != cudaSuccess) {                                                       \
+            return ::bem::fail((ctx), e__ == cudaErrorMemoryAllocation ? BEM_ERR_OOM    \
+                                                                       : BEM_ERR_CUDA,  \
+                               "%s:%d %s: %s", __FILE__, __LINE__, #call,              \
+                               cudaGetErrorString(e__));                                \
+        }                                                                               \
+    } while (0)
+
+#define BEM_TRY(call)              \
+    do {                           \
+        int s__ = (call);          \
+        if (s__ != BEM_OK) return s__; \
+    } while (0)
+
+// Launch check: records the launch and reports launch-configuration errors.
+#define BEM_LAUNCHED(ctx)                                                              \
+    do {                                                                               \
+        (ctx)->launches++;                                                             \
+        cudaError_t e__ = cudaGetLastError();                                          \
+        if (e__ != cudaSuccess)                                                        \
+            return ::bem::fail((ctx), BEM_ERR_CUDA, "%s:%d launch: %s", __FILE__,     \
+                               __LINE__, cudaGetErrorString(e__));                     \
+    } while (0)
+
+// ------------------------------------------------------------ host geometry
+struct V3 {
+    double x, y, z;
+};
+
+struct HostMesh {
+    std::vector<V3> verts;
+    std::vector<int> tris;  // 3 per triangle
+    int nv() const { return (int)verts.size(); }
+    int nt() const { return (int)tris.size() / 3; }
+};
+
+struct HostRWG {
+    int N = 0;
+    std::vector<int> tri_p, tri_m;
+    std::vector<int> vfree_p, vfree_m;  // vertex index of the free vertices
+    std::vector<V3> free_p, free_m;
+    std::vector<double> length, area_p, area_m;
+};
+
+struct Quad {
+    int n = 0;
+    double l1[25], l2[25], w[25];
+};
+
+HostMesh make_icosphere(double radius, int refinements);
+HostMesh make_hex_prism(double aspect_ratio, int refinements);
+HostMesh subdivide_flat(const HostMesh& m);
+HostRWG build_rwg(const HostMesh& m);
+bool quadrature(int order, Quad* q);  // false: unsupported order
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
+void orientations(int na, int nb, int ng, int bsym, int gsym, bool mirror, bool sort,
+                  std::vector<double>& RT, std::vector<double>& w);
+double tri_area(const HostMesh& m, int t);
+
+// ---------------------------------------------------------- device geometry
+// Quadrature data of every (RWG, half): index h*N + n, point q at
+// ((h*N + n)*Nq + q).  Structure of arrays, all FP64.
+struct DevHalf {
+    double *px, *py, *pz;   // quadrature points
+    double *fx, *fy, *fz;   // basis values sign*(l/2A)(r - r_free)
+    double *cx, *cy, *cz;   // f x r (for the K triple product)
+    double* jw;             // A * w_q
+    double* div;            // (2N) sign*l/A
+    int* tri;               // (2N) triangle of the half
+};
+
+// Same-triangle (singular) bookkeeping.  Every unordered pair {m, n} of RWG
+// functions that share a triangle gets one slot; item_* lists the
+// (triangle, test half, source half) combinations feeding it, CSR by slot.
+struct DevSingular {
+    int npairs = 0, nitems = 0;
+    int* pair_mn;       // (2*npairs) m <= n
+    int* item_ptr;      // (npairs+1)
+    int* item;          // (nitems*3): triangle, test half index h*N+m, source half h*N+n
+    double* P;          // (nt*Nq) Graglia potential at the triangle's points
+    double* V;          // (nt*Nq*3) vector potential at the triangle's points
+    double* tv;         // (nt*9) triangle vertices
+};
+
+}  // namespace bem
+
+struct bem_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int sm_count = 148;
+    int64_t launches = 0;
+    std::string last_error;
+    // bounded-wait status word for device-side barriers (0 = ok)
+    int* d_status = nullptr;
+    // reusable device workspace
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    int ensure_ws(size_t bytes);
+};
+
+struct bem_geom {
+    bem_ctx* ctx = nullptr;  // creating context (not used after bem_geom_free starts)
+    int device = 0;
+    int N = 0, Nq = 0, nv = 0, nt = 0, quad_order = 7;
+    bem::HostMesh mesh;
+    bem::HostRWG rwg;
+    bem::Quad quad;
+    bem::DevHalf half{};
+    bem::DevSingular sing{};
+    double* sing_coef = nullptr;  // (2N) sign*l/(2A) per half
+    double* sing_free = nullptr;  // (3*2N) free vertex per half, x | y | z blocks
+    void* dmem = nullptr;  // one allocation backing every device array
+};
+
+namespace bem {
+// assembly.cu
+int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
+                 double ki_im, double eta_e, double eta_i, unsigned flags, int mode,
+                 void* Z, int64_t ldz, void* L, void* K);
+int geom_upload(bem_ctx* ctx, bem_geom* g);
+// rhs / farfield
+int rhs_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im, double eta,
+            const double* RT_host, const double* E0_host, const double* khat_host, int n_orient,
+            void* B, int64_t ldb);
+int farfield_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, int n_calls_x,
+                 const double* coeffJ_host, const double* coeffM_host, const double* rhat_host,
+                 int n_orient, int ndir, double k_re, double k_im, double eta, double* Fv_host);
+int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, const double* RT,
+                const double* w, int n_orient, double k_re, double k_im, double eta,
+                int ntheta, int gamma_mirror, double* M_avg, double* M_orient_dev);
+}  // namespace bem

@@ -1,0 +1,558 @@
+// Complex LU with partial pivoting and multi-RHS solves, FP64 and FP32.
+//
+// Replaces cusolverDnZgetrf / cusolverDnZgetrs (solver.cu:7-142) with a
+// blocked right-looking factorisation of the row-major matrix (P Z = L U,
+// unit L, LAPACK-style 0-based row pivots kept on the device):
+//
+//   for each block column of width NB:
+//     for each sub-panel of width W inside it:
+//       panel_kernel  -- cooperative kernel, whole sub-panel held in shared
+//                        memory across all SMs, one grid barrier per column
+//                        (pivot search, swap, scale, rank-1 update)
+//       laswp + small TRSM + thin GEMM for the rest of the block column
+//     laswp of the block's pivots on the other columns
+//     U12 = L11^-1 A12  (blocked TRSM)
+//     A22 -= L21 U12    (the trailing update: CUDA-core GEMM for FP64,
+//                        3xTF32 tcgen05 GEMM for FP32)
+//
+// The pivot rule is the one of LAPACK izamax: largest |re| + |im|, first
+// index on ties.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bem_internal.h"
+#include "cgemm_simt.cuh"
+#include "lu_internal.h"
+
+namespace bem {
+
+// ------------------------------------------------------------------- GEMM
+template <typename R>
+int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int64_t lda,
+          const typename C2T<R>::type* B, int64_t ldb, bool b_kmajor,
+          typename C2T<R>::type* C, int64_t ldc, bool c_colmajor,
+          typename C2T<R>::type alpha, typename C2T<R>::type beta) {
+    if (M <= 0 || N <= 0) return BEM_OK;
+    if (K <= 0) {
+        // C = beta*C only; our callers never need it with beta != 1
+        return BEM_OK;
+    }
+    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "gemm M too large");
+    if (b_kmajor) {
+        if (c_colmajor)
+            cgemm_simt_kernel<R, true, true><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
+        else
+            cgemm_simt_kernel<R, true, false><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
+    } else {
+        if (c_colmajor)
+            cgemm_simt_kernel<R, false, true><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
+        else
+            cgemm_simt_kernel<R, false, false><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
+    }
+    BEM_LAUNCHED(ctx);
+    return BEM_OK;
+}
+
+template <typename C2> static C2 mk(double re, double im) {
+    C2 c;
+    c.x = re;
+    c.y = im;
+    return c;
+}
+
+// ------------------------------------------------------------- grid barrier
+// Monotonic arrival counter, reset to 0 before the launch.  Thread 0 of each
+// CTA arrives and waits for `target` arrivals, giving up after ~2 s of clock
+// cycles (status word := BEM_ERR_TIMEOUT); the kernel then returns.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, int* status,
+                                             int* s_flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(bar, 1u);
+        long long t0 = clock64();
+        int ok = 1;
+        while (true) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= target) break;
+            if (*(volatile int*)status != 0 || clock64() - t0 > 4000000000LL) {
+                atomicCAS(status, 0, (int)BEM_ERR_TIMEOUT);
+                ok = 0;
+                break;
+            }
+            __nanosleep(20);
+        }
+        __threadfence();
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0;
+}
+
+template <typename R> __device__ __forceinline__ R cabs1(typename C2T<R>::type v) {
+    return fabs(v.x) + fabs(v.y);
+}
+
+// ------------------------------------------------------------ panel kernel
+// Factors the sub-panel rows [r0, n), columns [r0, r0+w) of the row-major
+// matrix A.  CTA b owns panel rows [b*Rp, min((b+1)*Rp, nrows)) (relative
+// to r0) in shared memory; Rp >= w so the w pivot rows live in CTA 0.
+template <typename R>
+__global__ void __launch_bounds__(256)
+panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nrows, int w, int Rp,
+             int* __restrict__ ipiv, int* __restrict__ info, PanelWS ws) {
+    using C2 = typename C2T<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C2* tile = (C2*)smem_raw;                   // Rp * w
+    C2* s_piv = tile + (size_t)Rp * w;          // w
+    __shared__ R s_val[8];
+    __shared__ int s_row[8];
+    __shared__ int s_owner[8];
+    __shared__ int s_flag;
+    __shared__ R s_best;
+    __shared__ int s_brow, s_bown;
+
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int lo = b * Rp;
+    const int nloc = max(0, min(Rp, nrows - lo));
+    R* cval = (R*)ws.cval;
+    C2* cdata = (C2*)ws.cdata;
+    C2* disp = (C2*)ws.disp;
+
+    for (int e = tid; e < nloc * w; e += blockDim.x) {
+        int i = e / w, c = e % w;
+        tile[e] = A[(int64_t)(r0 + lo + i) * lda + r0 + c];
+    }
+    __syncthreads();
+
+    for (int jj = 0; jj < w; jj++) {
+        const int par = jj & 1;
+        // 1. local pivot candidate among rows >= jj
+        R bv = (R)-1;
+        int br = 0x7fffffff;
+        for (int i = tid; i < nloc; i += blockDim.x) {
+            int gr = lo + i;
+            if (gr < jj) continue;
+            R v = cabs1<R>(tile[i * w + jj]);
+            if (v > bv || (v == bv && gr < br)) bv = v, br = gr;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            R ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int orw = __shfl_down_sync(0xffffffffu, br, o);
+            if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw;
+        }
+        if (lane == 0) s_val[warp] = bv, s_row[warp] = br;
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+                if (s_val[k] > bv || (s_val[k] == bv && s_row[k] < br)) bv = s_val[k], br = s_row[k];
+            s_best = bv;
+            s_brow = br;
+            __stcg(&cval[par * G + b], bv);
+            __stcg(&ws.crow[par * G + b], br);
+        }
+        __syncthreads();
+        br = s_brow;
+        if (br != 0x7fffffff)
+            for (int c = tid; c < w; c += blockDim.x) __stcg(&cdata[((size_t)par * G + b) * w + c], tile[(br - lo) * w + c]);
+        if (b == 0)
+            for (int c = tid; c < w; c += blockDim.x) __stcg(&disp[par * w + c], tile[jj * w + c]);
+        // 2. all candidates published
+        if (!grid_barrier(ws.bar, (unsigned)(jj + 1) * G, ws.status, &s_flag)) return;
+        // 3. global argmax (|re|+|im| max, smallest row on ties)
+        bv = (R)-1;
+        br = 0x7fffffff;
+        int bo = -1;
+        for (int k = tid; k < G; k += blockDim.x) {
+            R v = __ldcg(&cval[par * G + k]);
+            int r = __ldcg(&ws.crow[par * G + k]);
+            if (r == 0x7fffffff) continue;
+            if (v > bv || (v == bv && r < br)) bv = v, br = r, bo = k;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            R ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int orw = __shfl_down_sync(0xffffffffu, br, o);
+            int oo = __shfl_down_sync(0xffffffffu, bo, o);
+            if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bo = oo;
+        }
+        if (lane == 0) s_val[warp] = bv, s_row[warp] = br, s_owner[warp] = bo;
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+                if (s_val[k] > bv || (s_val[k] == bv && s_row[k] < br)) bv = s_val[k], br = s_row[k], bo = s_owner[k];
+            bool zero = !(bv > (R)0);
+            if (zero) {
+                br = jj;  // no interchange; LAPACK records info and skips the scaling
+                bo = -1;
+                atomicCAS(info, 0, r0 + jj + 1);
+            }
+            s_brow = br;
+            s_bown = bo;
+            s_best = bv;
+            if (b == 0) ipiv[r0 + jj] = r0 + br;
+        }
+        __syncthreads();
+        const int piv = s_brow, own = s_bown;
+        const bool zero = !(s_best > (R)0);
+        for (int c = tid; c < w; c += blockDim.x)
+            s_piv[c] = own >= 0 ? __ldcg(&cdata[((size_t)par * G + own) * w + c]) : __ldcg(&disp[par * w + c]);
+        __syncthreads();
+        // 4. interchange rows jj and piv
+        if (piv != jj) {
+            if (b == 0)
+                for (int c = tid; c < w; c += blockDim.x) tile[jj * w + c] = s_piv[c];
+            if (piv >= lo && piv < lo + nloc)
+                for (int c = tid; c < w; c += blockDim.x) tile[(piv - lo) * w + c] = __ldcg(&disp[par * w + c]);
+        }
+        __syncthreads();
+        // 5. scale column jj below the diagonal, rank-1 update of the rest
+        if (!zero) {
+            C2 p = s_piv[jj];
+            R den = p.x * p.x + p.y * p.y;
+            C2 inv;
+            inv.x = p.x / den;
+            inv.y = -p.y / den;
+            for (int i = tid; i < nloc; i += blockDim.x) {
+                int gr = lo + i;
+                if (gr <= jj) continue;
+                C2 a = tile[i * w + jj];
+                C2 l;
+                l.x = a.x * inv.x - a.y * inv.y;
+                l.y = a.x * inv.y + a.y * inv.x;
+                tile[i * w + jj] = l;
+            }
+            __syncthreads();
+            const int wr = w - jj - 1;
+            if (wr > 0)
+                for (int e = tid; e < nloc * wr; e += blockDim.x) {
+                    int i = e / wr, c = jj + 1 + e % wr;
+                    int gr = lo + i;
+                    if (gr <= jj) continue;
+                    C2 l = tile[i * w + jj], u = s_piv[c], x = tile[i * w + c];
+                    x.x -= l.x * u.x - l.y * u.y;
+                    x.y -= l.x * u.y + l.y * u.x;
+                    tile[i * w + c] = x;
+                }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nloc * w; e += blockDim.x) {
+        int i = e / w, c = e % w;
+        A[(int64_t)(r0 + lo + i) * lda + r0 + c] = tile[e];
+    }
+}
+
+// ------------------------------------------------------------------ laswp
+// Row interchanges k = k0..k1-1 (rows k <-> ipiv[k]) on the columns of up to
+// two ranges [c0a, c1a) and [c0b, c1b); one thread per column.
+template <typename R>
+__global__ void laswp_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, const int* __restrict__ ipiv,
+                             int k0, int k1, int c0a, int c1a, int c0b, int c1b) {
+    using C2 = typename C2T<R>::type;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int na = c1a - c0a;
+    int c;
+    if (t < na) c = c0a + t;
+    else if (t < na + (c1b - c0b)) c = c0b + (t - na);
+    else return;
+    for (int k = k0; k < k1; k++) {
+        int p = ipiv[k];
+        if (p == k) continue;
+        C2 x = A[(int64_t)k * lda + c];
+        A[(int64_t)k * lda + c] = A[(int64_t)p * lda + c];
+        A[(int64_t)p * lda + c] = x;
+    }
+}
+
+// Row gather for the solve: X[k] = B[perm[k]] for every column (column-major).
+template <typename R>
+__global__ void permute_rows_kernel(const typename C2T<R>::type* __restrict__ B, int64_t ldb,
+                                    typename C2T<R>::type* __restrict__ X, int64_t ldx, const int* __restrict__ perm,
+                                    int n, int nrhs) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * nrhs) return;
+    int r = (int)(i % n), c = (int)(i / n);
+    X[(int64_t)c * ldx + r] = B[(int64_t)c * ldb + perm[r]];
+}
+
+// ------------------------------------------------------------ small TRSM
+// Solves T x = b for one TB x TB diagonal block T = A[r0.., r0..] of the
+// row-major factor (UPPER: non-unit upper, backward; else unit lower,
+// forward), for every column in [c0, c1) of the right-hand side held either
+// row-major in the same matrix (B_ROWMAJOR: element (i, c) at
+// B[(r0+i)*ldb + c]) or column-major (B[c*ldb + r0 + i]).  kb <= TB rows.
+template <typename R, int TB, bool UPPER, bool B_ROWMAJOR>
+__global__ void __launch_bounds__(128)
+trsm_small_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int r0, int kb,
+                  typename C2T<R>::type* __restrict__ B, int64_t ldb, int c0, int c1) {
+    using C2 = typename C2T<R>::type;
+    __shared__ C2 sT[TB][TB + 1];
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+        int i = e / kb, j = e % kb;
+        sT[i][j] = T[(int64_t)(r0 + i) * ldt + r0 + j];
+    }
+    __syncthreads();
+    int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= c1) return;
+    C2 x[TB];
+#pragma unroll
+    for (int i = 0; i < TB; i++)
+        if (i < kb) x[i] = B_ROWMAJOR ? B[(int64_t)(r0 + i) * ldb + c] : B[(int64_t)c * ldb + r0 + i];
+    if (!UPPER) {
+#pragma unroll
+        for (int i = 1; i < TB; i++) {
+            if (i >= kb) break;
+            C2 s = x[i];
+#pragma unroll
+            for (int k = 0; k < TB; k++) {
+                if (k >= i) break;
+                C2 l = sT[i][k];
+                s.x -= l.x * x[k].x - l.y * x[k].y;
+                s.y -= l.x * x[k].y + l.y * x[k].x;
+            }
+            x[i] = s;
+        }
+    } else {
+#pragma unroll
+        for (int ii = TB - 1; ii >= 0; ii--) {
+            if (ii >= kb) continue;
+            C2 s = x[ii];
+#pragma unroll
+            for (int k = 0; k < TB; k++) {
+                if (k <= ii || k >= kb) continue;
+                C2 u = sT[ii][k];
+                s.x -= u.x * x[k].x - u.y * x[k].y;
+                s.y -= u.x * x[k].y + u.y * x[k].x;
+            }
+            C2 d = sT[ii][ii];
+            R den = d.x * d.x + d.y * d.y;
+            C2 q;
+            q.x = (s.x * d.x + s.y * d.y) / den;
+            q.y = (s.y * d.x - s.x * d.y) / den;
+            x[ii] = q;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < TB; i++)
+        if (i < kb) {
+            if (B_ROWMAJOR) B[(int64_t)(r0 + i) * ldb + c] = x[i];
+            else B[(int64_t)c * ldb + r0 + i] = x[i];
+        }
+}
+
+template <typename R> struct TBsel { static constexpr int v = 16; };
+
+// Unit-lower TRSM on rows [r0, r0+kb) of the row-major matrix itself, for
+// columns [c0, c1): the U12 step of the factorisation.
+template <typename R>
+int trsm_rows_lower_unit(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int r0, int kb,
+                         int c0, int c1) {
+    using C2 = typename C2T<R>::type;
+    constexpr int TB = TBsel<R>::v;
+    int nc = c1 - c0;
+    if (nc <= 0 || kb <= 0) return BEM_OK;
+    for (int b = 0; b < kb; b += TB) {
+        int tb = std::min(TB, kb - b);
+        trsm_small_kernel<R, TB, false, true><<<(nc + 127) / 128, 128, 0, ctx->stream>>>(
+            A, lda, r0 + b, tb, A, lda, c0, c1);
+        BEM_LAUNCHED(ctx);
+        int rest = kb - b - tb;
+        if (rest > 0)
+            BEM_TRY(cgemm<R>(ctx, rest, nc, tb, A + (int64_t)(r0 + b + tb) * lda + r0 + b, lda,
+                             A + (int64_t)(r0 + b) * lda + c0, lda, false,
+                             A + (int64_t)(r0 + b + tb) * lda + c0, lda, false, mk<C2>(-1, 0),
+                             mk<C2>(1, 0)));
+    }
+    return BEM_OK;
+}
+
+// ------------------------------------------------------------------ getrf
+template <typename R>
+int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipiv, int* d_info,
+          const TrailingUpdate<R>* tc) {
+    using C2 = typename C2T<R>::type;
+    const int NB = 256;
+    const int W = sizeof(R) == 8 ? 16 : 32;
+    // panel workspace
+    int occ = 0;
+    const int Gmax_sm = ctx->sm_count;
+    // rows per CTA for the first (largest) panel decides the shared memory
+    // Rows per CTA: ceil(nrows / G) with G = min(SMs, nrows / w); it is at
+    // most ceil(n / SMs) while G is capped by the SM count and below 2w
+    // once G is nrows / w, so this bounds every panel launch.
+    int G0 = std::min(Gmax_sm, std::max(1, n / W));
+    int Rp0 = std::max((n + G0 - 1) / G0, 2 * W);
+    size_t smem0 = ((size_t)Rp0 * W + W) * sizeof(C2);
+    if (smem0 > 220 * 1024)
+        return fail(ctx, BEM_ERR_INVALID, "n=%d too large for the panel kernel (%zu B smem)", n, smem0);
+    BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem0));
+    BEM_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<R>, 256, smem0));
+    if (occ < 1) return fail(ctx, BEM_ERR_INVALID, "panel kernel does not fit on an SM");
+    const int Gcap = occ * ctx->sm_count;
+    // workspace: cval[2G] (R), crow[2G], cdata[2G*W], disp[2W], bar, status
+    size_t ws_bytes = 0;
+    auto take = [&](size_t b) { size_t o = ws_bytes; ws_bytes += (b + 255) & ~(size_t)255; return o; };
+    size_t o_cval = take(2 * (size_t)Gcap * sizeof(R)), o_crow = take(2 * (size_t)Gcap * 4),
+           o_cdata = take(2 * (size_t)Gcap * W * sizeof(C2)), o_disp = take(2 * W * sizeof(C2)),
+           o_bar = take(256);
+    BEM_TRY(ctx->ensure_ws(ws_bytes));
+    char* ws = (char*)ctx->ws;
+    PanelWS pw;
+    pw.cval = ws + o_cval;
+    pw.crow = (int*)(ws + o_crow);
+    pw.cdata = ws + o_cdata;
+    pw.disp = ws + o_disp;
+    pw.bar = (unsigned*)(ws + o_bar);
+    pw.status = ctx->d_status;
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = std::min(NB, n - j0);
+        for (int i0 = j0; i0 < j0 + jb; i0 += W) {
+            const int iw = std::min(W, j0 + jb - i0);
+            const int nrows = n - i0;
+            int G = std::min(Gcap, std::max(1, nrows / iw));
+            G = std::min(G, Gmax_sm);
+            int Rp = (nrows + G - 1) / G;
+            G = (nrows + Rp - 1) / Rp;
+            size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
+            if (smem > smem0) return fail(ctx, BEM_ERR_INVALID, "panel smem bound violated");
+            BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
+            void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
+                            &d_ipiv, &d_info, &pw};
+            BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G), dim3(256),
+                                                          args, smem, ctx->stream));
+            BEM_LAUNCHED(ctx);
+            // interchanges on the rest of this block column
+            int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
+            int ncol = (ca1 - ca0) + (cb1 - cb0);
+            if (ncol > 0) {
+                laswp_kernel<R><<<(ncol + 255) / 256, 256, 0, ctx->stream>>>(A, lda, d_ipiv, i0, i0 + iw,
+                                                                          ca0, ca1, cb0, cb1);
+                BEM_LAUNCHED(ctx);
+            }
+            if (cb1 > cb0) {
+                BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, i0, iw, cb0, cb1));
+                BEM_TRY(cgemm<R>(ctx, n - i0 - iw, cb1 - cb0, iw, A + (int64_t)(i0 + iw) * lda + i0, lda,
+                                 A + (int64_t)i0 * lda + cb0, lda, false,
+                                 A + (int64_t)(i0 + iw) * lda + cb0, lda, false, mk<C2>(-1, 0),
+                                 mk<C2>(1, 0)));
+            }
+        }
+        // interchanges on the columns outside the block column
+        int ncol = j0 + (n - j0 - jb);
+        if (ncol > 0) {
+            laswp_kernel<R><<<(ncol + 255) / 256, 256, 0, ctx->stream>>>(A, lda, d_ipiv, j0, j0 + jb, 0,
+                                                                      j0, j0 + jb, n);
+            BEM_LAUNCHED(ctx);
+        }
+        const int c0 = j0 + jb;
+        if (c0 < n) {
+            BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0, jb, c0, n));
+            const int Mt = n - c0;
+            if (tc && tc->fn)
+                BEM_TRY(tc->fn(ctx, tc->state, Mt, Mt, jb, A + (int64_t)c0 * lda + j0, lda,
+                               A + (int64_t)j0 * lda + c0, lda, A + (int64_t)c0 * lda + c0, lda));
+            else
+                BEM_TRY(cgemm<R>(ctx, Mt, Mt, jb, A + (int64_t)c0 * lda + j0, lda, A + (int64_t)j0 * lda + c0,
+                                 lda, false, A + (int64_t)c0 * lda + c0, lda, false, mk<C2>(-1, 0),
+                                 mk<C2>(1, 0)));
+        }
+    }
+    return BEM_OK;
+}
+
+// ------------------------------------------------------------------ getrs
+// X = (P^T L U)^-1 B, column-major n x nrhs; X may alias B only if perm is
+// applied through the workspace (the caller passes distinct buffers).
+template <typename R>
+int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, const int* d_perm,
+          const typename C2T<R>::type* B, int64_t ldb, typename C2T<R>::type* X, int64_t ldx,
+          int nrhs, const TrailingUpdate<R>* tc) {
+    using C2 = typename C2T<R>::type;
+    constexpr int TB = TBsel<R>::v;
+    const int NB = 256;
+    if (nrhs <= 0) return BEM_OK;
+    int64_t tot = (int64_t)n * nrhs;
+    permute_rows_kernel<R><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, X, ldx, d_perm,
+                                                                                  n, nrhs);
+    BEM_LAUNCHED(ctx);
+    // forward: L Y = P B
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        int jb = std::min(NB, n - j0);
+        for (int b = 0; b < jb; b += TB) {
+            int tb = std::min(TB, jb - b);
+            trsm_small_kernel<R, TB, false, false><<<(nrhs + 127) / 128, 128, 0, ctx->stream>>>(
+                LU, lda, j0 + b, tb, X, ldx, 0, nrhs);
+            BEM_LAUNCHED(ctx);
+            int rest = jb - b - tb;
+            if (rest > 0)
+                BEM_TRY(cgemm<R>(ctx, rest, nrhs, tb, LU + (int64_t)(j0 + b + tb) * lda + j0 + b, lda,
+                                 X + j0 + b, ldx, true, X + j0 + b + tb, ldx, true, mk<C2>(-1, 0),
+                                 mk<C2>(1, 0)));
+        }
+        int below = n - j0 - jb;
+        if (below > 0) {
+            if (tc && tc->fn_solve)
+                BEM_TRY(tc->fn_solve(ctx, tc->state, below, nrhs, jb, LU + (int64_t)(j0 + jb) * lda + j0, lda,
+                                     X + j0, ldx, X + j0 + jb, ldx));
+            else
+                BEM_TRY(cgemm<R>(ctx, below, nrhs, jb, LU + (int64_t)(j0 + jb) * lda + j0, lda, X + j0, ldx,
+                                 true, X + j0 + jb, ldx, true, mk<C2>(-1, 0), mk<C2>(1, 0)));
+        }
+    }
+    // backward: U X = Y
+    int nblk = (n + NB - 1) / NB;
+    for (int bi = nblk - 1; bi >= 0; bi--) {
+        int j0 = bi * NB, jb = std::min(NB, n - j0);
+        int nsub = (jb + TB - 1) / TB;
+        for (int s = nsub - 1; s >= 0; s--) {
+            int b = s * TB, tb = std::min(TB, jb - b);
+            trsm_small_kernel<R, TB, true, false><<<(nrhs + 127) / 128, 128, 0, ctx->stream>>>(
+                LU, lda, j0 + b, tb, X, ldx, 0, nrhs);
+            BEM_LAUNCHED(ctx);
+            if (b > 0)
+                BEM_TRY(cgemm<R>(ctx, b, nrhs, tb, LU + (int64_t)j0 * lda + j0 + b, lda, X + j0 + b, ldx, true,
+                                 X + j0, ldx, true, mk<C2>(-1, 0), mk<C2>(1, 0)));
+        }
+        if (j0 > 0) {
+            if (tc && tc->fn_solve)
+                BEM_TRY(tc->fn_solve(ctx, tc->state, j0, nrhs, jb, LU + j0, lda, X + j0, ldx, X, ldx));
+            else
+                BEM_TRY(cgemm<R>(ctx, j0, nrhs, jb, LU + j0, lda, X + j0, ldx, true, X, ldx, true,
+                                 mk<C2>(-1, 0), mk<C2>(1, 0)));
+        }
+    }
+    return BEM_OK;
+}
+
+template int getrf<double>(bem_ctx*, double2*, int64_t, int, int*, int*, const TrailingUpdate<double>*);
+template int getrf<float>(bem_ctx*, float2*, int64_t, int, int*, int*, const TrailingUpdate<float>*);
+template int getrs<double>(bem_ctx*, const double2*, int64_t, int, const int*, const double2*, int64_t,
+                           double2*, int64_t, int, const TrailingUpdate<double>*);
+template int getrs<float>(bem_ctx*, const float2*, int64_t, int, const int*, const float2*, int64_t,
+                          float2*, int64_t, int, const TrailingUpdate<float>*);
+template int cgemm<double>(bem_ctx*, int, int, int, const double2*, int64_t, const double2*, int64_t, bool,
+                           double2*, int64_t, bool, double2, double2);
+template int cgemm<float>(bem_ctx*, int, int, int, const float2*, int64_t, const float2*, int64_t, bool,
+                          float2*, int64_t, bool, float2, float2);
+
+// Row pivots (LAPACK interchange sequence, 0-based) -> gather permutation.
+void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm) {
+    int n = (int)ipiv.size();
+    perm.resize(n);
+    for (int i = 0; i < n; i++) perm[i] = i;
+    for (int k = 0; k < n; k++) std::swap(perm[k], perm[ipiv[k]]);
+}
+
+}  // namespace bem

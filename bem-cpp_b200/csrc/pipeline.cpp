@@ -1,0 +1,157 @@
+// Host-buffer assembly mirrors and the whole dense pipeline (the dense branch
+// of main.cpp:660-854) over the device kernels.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "bem_internal.h"
+
+using namespace bem;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+double secs(std::chrono::steady_clock::time_point a) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+// assemble_L_K_cuda (assembly.h:11-13): L, K host row-major N x N complex128.
+int bem_assemble_L_K(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt, double k_re,
+                     double k_im, int quad_order, double* L, double* K) {
+    if (!ctx || !L || !K) return BEM_ERR_INVALID;
+    bem_geom* g = nullptr;
+    int N = 0;
+    BEM_TRY(bem_geom_create(ctx, verts, nv, tris, nt, quad_order, &g, &N));
+    size_t bytes = (size_t)N * N * 16;
+    DevBuf dL, dK;
+    int s = BEM_OK;
+    if (cudaMalloc(&dL.p, bytes) != cudaSuccess || cudaMalloc(&dK.p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
+    }
+    if (s == BEM_OK) s = assemble_dev(ctx, g, k_re, k_im, 0, 0, 1, 1, 0, 1, nullptr, N, dL.p, dK.p);
+    if (s == BEM_OK && (cudaMemcpy(L, dL.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                        cudaMemcpy(K, dK.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess))
+        s = fail(ctx, BEM_ERR_CUDA, "download L/K");
+    bem_geom_free(g);
+    return s;
+}
+
+// assemble_pmchwt (pmchwt.h:12-18): Z host row-major 2N x 2N; L_ext, K_ext optional.
+int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
+                        double kext_re, double kext_im, double kint_re, double kint_im, double eta_ext,
+                        double eta_int, int quad_order, double* Z, double* L_ext, double* K_ext) {
+    if (!ctx || !Z) return BEM_ERR_INVALID;
+    bem_geom* g = nullptr;
+    int N = 0;
+    BEM_TRY(bem_geom_create(ctx, verts, nv, tris, nt, quad_order, &g, &N));
+    size_t zb = (size_t)4 * N * N * 16;
+    DevBuf dZ;
+    int s = BEM_OK;
+    if (cudaMalloc(&dZ.p, zb) != cudaSuccess) {
+        cudaGetLastError();
+        s = fail(ctx, BEM_ERR_OOM, "Z device buffer (%zu bytes)", zb);
+    }
+    if (s == BEM_OK)
+        s = assemble_dev(ctx, g, kext_re, kext_im, kint_re, kint_im, eta_ext, eta_int, 0, 2, dZ.p, 2 * N,
+                         nullptr, nullptr);
+    if (s == BEM_OK && cudaMemcpy(Z, dZ.p, zb, cudaMemcpyDeviceToHost) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "download Z");
+    if (s == BEM_OK && (L_ext || K_ext)) {
+        size_t b = (size_t)N * N * 16;
+        DevBuf dL, dK;
+        if (cudaMalloc(&dL.p, b) != cudaSuccess || cudaMalloc(&dK.p, b) != cudaSuccess) {
+            cudaGetLastError();
+            s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
+        }
+        if (s == BEM_OK) s = assemble_dev(ctx, g, kext_re, kext_im, 0, 0, 1, 1, 0, 1, nullptr, N, dL.p, dK.p);
+        if (s == BEM_OK && L_ext && cudaMemcpy(L_ext, dL.p, b, cudaMemcpyDeviceToHost) != cudaSuccess)
+            s = fail(ctx, BEM_ERR_CUDA, "download L_ext");
+        if (s == BEM_OK && K_ext && cudaMemcpy(K_ext, dK.p, b, cudaMemcpyDeviceToHost) != cudaSuccess)
+            s = fail(ctx, BEM_ERR_CUDA, "download K_ext");
+    }
+    bem_geom_free(g);
+    return s;
+}
+
+// main.cpp:660-854 on the device.
+int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
+    if (!ctx || !p || !r || !r->mueller) return BEM_ERR_INVALID;
+    if (!(p->ka > 0) || p->ntheta < 2) return fail(ctx, BEM_ERR_INVALID, "ka must be > 0, ntheta >= 2");
+    auto t_all = std::chrono::steady_clock::now();
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::complex<double> m(p->m_re, p->m_im), kext(p->ka, 0.0), kint = kext * m;
+    double eta_e = 1.0, eta_i = 1.0 / std::abs(m);
+    bem_geom* g = nullptr;
+    int N = 0;
+    BEM_TRY(bem_geom_create(ctx, p->verts, p->nv, p->tris, p->nt, p->quad_order, &g, &N));
+    const int n = 2 * N;
+    // orientations
+    std::vector<double> RT, w;
+    if (p->single) {
+        RT = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        w = {1.0};
+    } else {
+        orientations(p->n_alpha, p->n_beta, p->n_gamma, p->beta_sym < 1 ? 1 : p->beta_sym,
+                     p->gamma_sym < 1 ? 1 : p->gamma_sym, p->gamma_mirror != 0, true, RT, w);
+        int tot = (int)w.size(), i0 = 0, i1 = tot;
+        if (p->orient_i0 >= 0 && p->orient_i1 > p->orient_i0) {
+            i0 = std::min(p->orient_i0, tot);
+            i1 = std::min(p->orient_i1, tot);
+        }
+        RT = std::vector<double>(RT.begin() + 9 * i0, RT.begin() + 9 * i1);
+        w = std::vector<double>(w.begin() + i0, w.begin() + i1);
+    }
+    const int no = (int)w.size();
+    const int nrhs = 2 * no;
+    DevBuf dZ, dB, dX;
+    int s = BEM_OK;
+    if (cudaMalloc(&dZ.p, (size_t)n * n * 16) != cudaSuccess || cudaMalloc(&dB.p, (size_t)n * nrhs * 16) != cudaSuccess ||
+        cudaMalloc(&dX.p, (size_t)n * nrhs * 16) != cudaSuccess) {
+        cudaGetLastError();
+        bem_geom_free(g);
+        return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs);
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    s = assemble_dev(ctx, g, kext.real(), kext.imag(), kint.real(), kint.imag(), eta_e, eta_i, p->asm_flags, 2,
+                     dZ.p, n, nullptr, nullptr);
+    if (s == BEM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "assembly: %s", cudaGetErrorString(cudaGetLastError()));
+    r->t_assembly_s = secs(t0);
+    auto t1 = std::chrono::steady_clock::now();
+    if (s == BEM_OK) s = rhs_dev(ctx, g, kext.real(), kext.imag(), eta_e, RT.data(), nullptr, nullptr, no, dB.p, n);
+    bem_lu* lu = nullptr;
+    int info = 0;
+    if (s == BEM_OK) s = bem_lu_factor_dev(ctx, dZ.p, n, n, p->precision, &lu, &info);
+    if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+    if (s == BEM_OK)
+        s = bem_lu_solve_dev(ctx, lu, dB.p, n, dX.p, n, nrhs, p->refine_tol, p->max_refine, &r->stats);
+    if (lu) bem_lu_free(lu);
+    r->t_solve_s = secs(t1);
+    auto t2 = std::chrono::steady_clock::now();
+    if (s == BEM_OK)
+        s = mueller_dev(ctx, g, dX.p, n, RT.data(), w.data(), no, kext.real(), kext.imag(), eta_e, p->ntheta,
+                        p->gamma_mirror, r->mueller, nullptr);
+    r->t_farfield_s = secs(t2);
+    r->t_total_s = secs(t_all);
+    r->N = N;
+    r->n_orient = no;
+    bem_geom_free(g);
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,428 @@
+// Factorisation objects, FP64 solves and FP32 + FP64-refinement solves,
+// and the host-buffer mirrors of solver.h (lu_factorize_cuda, lu_solve_cuda,
+// lu_solve_full; solver.cu:7-142).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bem_internal.h"
+#include "lu_internal.h"
+
+struct bem_lu {
+    bem_ctx* ctx = nullptr;
+    int device = 0;
+    int n = 0;
+    int precision = BEM_PREC_FP64;
+    double2* Z = nullptr;   // FP64: the factors (in the caller's buffer); FP32: the original Z
+    int64_t ldz = 0;
+    float2* A32 = nullptr;  // FP32 factors (owned)
+    int* d_ipiv = nullptr;  // owned
+    int* d_perm = nullptr;  // owned
+    std::vector<int> ipiv;  // 0-based interchange rows
+    double znorm = 0.0;     // ||Z||_F
+    double t_factor_ms = 0.0;
+};
+
+namespace bem {
+
+__global__ void z_to_c_kernel(const double2* __restrict__ Z, int64_t ldz, float2* __restrict__ A,
+                              int64_t lda, int n, double* __restrict__ fro_part) {
+    // one CTA row-block: converts and accumulates |z|^2 into fro_part[blockIdx.x]
+    __shared__ double s[256];
+    double acc = 0.0;
+    int64_t tot = (int64_t)n * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int r = (int)(i / n), c = (int)(i % n);
+        double2 z = Z[(int64_t)r * ldz + c];
+        acc += z.x * z.x + z.y * z.y;
+        if (A) A[(int64_t)r * lda + c] = make_float2((float)z.x, (float)z.y);
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) fro_part[blockIdx.x] = s[0];
+}
+
+// per column (column-major n x nrhs): out[c] = max_i |x_ic| (modulus)
+template <typename C2>
+__global__ void colmax_kernel(const C2* __restrict__ X, int64_t ldx, int n, double* __restrict__ out) {
+    __shared__ double s[256];
+    const C2* col = X + (int64_t)blockIdx.x * ldx;
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double a = hypot((double)col[i].x, (double)col[i].y);
+        m = fmax(m, a);
+    }
+    s[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) s[threadIdx.x] = fmax(s[threadIdx.x], s[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
+// R32[:, c] = R64[:, c] / scale[c]
+__global__ void scale_down_kernel(const double2* __restrict__ R, int64_t ldr, float2* __restrict__ S,
+                                  int64_t lds, const double* __restrict__ scale, int n, int nrhs) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * nrhs) return;
+    int r = (int)(i % n), c = (int)(i / n);
+    double sc = scale[c];
+    double inv = sc > 0 ? 1.0 / sc : 0.0;
+    double2 v = R[(int64_t)c * ldr + r];
+    S[(int64_t)c * lds + r] = make_float2((float)(v.x * inv), (float)(v.y * inv));
+}
+
+// X[:, c] (+)= scale[c] * D[:, c]
+__global__ void scale_up_kernel(const float2* __restrict__ D, int64_t ldd, double2* __restrict__ X,
+                                int64_t ldx, const double* __restrict__ scale, int n, int nrhs, int add) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * nrhs) return;
+    int r = (int)(i % n), c = (int)(i / n);
+    double sc = scale[c];
+    float2 d = D[(int64_t)c * ldd + r];
+    double2* x = &X[(int64_t)c * ldx + r];
+    if (add) {
+        x->x += sc * (double)d.x;
+        x->y += sc * (double)d.y;
+    } else {
+        *x = make_double2(sc * (double)d.x, sc * (double)d.y);
+    }
+}
+
+__global__ void copy_cols_kernel(const double2* __restrict__ B, int64_t ldb, double2* __restrict__ X,
+                                 int64_t ldx, int n, int nrhs) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * nrhs) return;
+    int r = (int)(i % n), c = (int)(i / n);
+    X[(int64_t)c * ldx + r] = B[(int64_t)c * ldb + r];
+}
+
+static unsigned nblk(int64_t tot) { return (unsigned)((tot + 255) / 256); }
+
+static int finish_factor(bem_ctx* ctx, bem_lu* lu, int* d_info, int* info) {
+    int h[2] = {0, 0};
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(&h[0], d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(&h[1], ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h[1] != 0) return fail(ctx, h[1], "device-side wait in the panel factorisation gave up");
+    lu->ipiv.resize(lu->n);
+    BEM_TRY_CUDA(ctx, cudaMemcpy(lu->ipiv.data(), lu->d_ipiv, lu->n * sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int> perm;
+    pivots_to_perm(lu->ipiv, perm);
+    BEM_TRY_CUDA(ctx, cudaMemcpy(lu->d_perm, perm.data(), lu->n * sizeof(int), cudaMemcpyHostToDevice));
+    if (info) *info = h[0];
+    return BEM_OK;
+}
+
+static void lu_release(bem_lu* lu) {
+    if (!lu) return;
+    cudaSetDevice(lu->device);
+    if (lu->A32) cudaFree(lu->A32);
+    if (lu->d_ipiv) cudaFree(lu->d_ipiv);
+    if (lu->d_perm) cudaFree(lu->d_perm);
+    delete lu;
+}
+
+int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu** out, int* info) {
+    if (!ctx || !Z || !out || n < 1 || ldz < n) return fail(ctx, BEM_ERR_INVALID, "bad lu_factor args");
+    if (precision != BEM_PREC_FP64 && precision != BEM_PREC_FP32_REFINE)
+        return fail(ctx, BEM_ERR_INVALID, "unknown precision %d", precision);
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    *out = nullptr;
+    bem_lu* lu = new bem_lu();
+    lu->ctx = ctx;
+    lu->device = ctx->device;
+    lu->n = n;
+    lu->precision = precision;
+    lu->Z = (double2*)Z;
+    lu->ldz = ldz;
+    auto t0 = std::chrono::steady_clock::now();
+    int s = BEM_OK;
+    int* d_info = nullptr;
+    double* fro = nullptr;
+    do {
+        if (cudaMalloc(&lu->d_ipiv, n * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&lu->d_perm, n * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&d_info, sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&fro, 1024 * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            s = fail(ctx, BEM_ERR_OOM, "lu workspace");
+            break;
+        }
+        if (precision == BEM_PREC_FP32_REFINE) {
+            if (cudaMalloc(&lu->A32, (size_t)n * n * sizeof(float2)) != cudaSuccess) {
+                cudaGetLastError();
+                s = fail(ctx, BEM_ERR_OOM, "FP32 factor storage (%zu bytes)", (size_t)n * n * sizeof(float2));
+                break;
+            }
+        }
+        z_to_c_kernel<<<1024, 256, 0, ctx->stream>>>(lu->Z, ldz, lu->A32, n, n, fro);
+        ctx->launches++;
+        std::vector<double> hf(1024);
+        if (cudaMemcpyAsync(hf.data(), fro, 1024 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            s = fail(ctx, BEM_ERR_CUDA, "norm of Z: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        double acc = 0;
+        for (double v : hf) acc += v;
+        lu->znorm = std::sqrt(acc);
+        if (precision == BEM_PREC_FP64) {
+            s = getrf<double>(ctx, lu->Z, ldz, n, lu->d_ipiv, d_info, nullptr);
+        } else {
+            TrailingUpdate<float> tc = tc_update_fp32(ctx);
+            s = getrf<float>(ctx, lu->A32, n, n, lu->d_ipiv, d_info, &tc);
+        }
+        if (s != BEM_OK) break;
+        s = finish_factor(ctx, lu, d_info, info);
+    } while (0);
+    if (d_info) cudaFree(d_info);
+    if (fro) cudaFree(fro);
+    if (s != BEM_OK) {
+        lu_release(lu);
+        return s;
+    }
+    lu->t_factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    *out = lu;
+    return BEM_OK;
+}
+
+int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, int64_t ldx, int nrhs,
+             double tol, int max_iter, bem_solve_stats* st) {
+    if (!ctx || !lu || !Bv || !Xv || nrhs < 0 || ldb < lu->n || ldx < lu->n)
+        return fail(ctx, BEM_ERR_INVALID, "bad lu_solve args");
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int n = lu->n;
+    const double2* B = (const double2*)Bv;
+    double2* X = (double2*)Xv;
+    bem_solve_stats stats;
+    std::memset(&stats, 0, sizeof stats);
+    stats.t_factor_ms = lu->t_factor_ms;
+    auto t0 = std::chrono::steady_clock::now();
+    if (nrhs == 0) {
+        if (st) *st = stats;
+        return BEM_OK;
+    }
+    if (tol <= 0) tol = 1e-12;
+    if (max_iter <= 0) max_iter = 10;
+    const size_t nn = (size_t)n * nrhs;
+    if (lu->precision == BEM_PREC_FP64) {
+        // distinct input/output buffers for the row permutation
+        const double2* src = B;
+        double2* tmp = nullptr;
+        if ((const void*)B == (const void*)X) {
+            BEM_TRY(ctx->ensure_ws(nn * sizeof(double2)));
+            tmp = (double2*)ctx->ws;
+            copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, tmp, n, n, nrhs);
+            BEM_LAUNCHED(ctx);
+            src = tmp;
+            ldb = n;
+        }
+        BEM_TRY(getrs<double>(ctx, lu->Z, lu->ldz, n, lu->d_perm, src, ldb, X, ldx, nrhs, nullptr));
+        BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        stats.converged = 1;
+        stats.t_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (st) *st = stats;
+        return BEM_OK;
+    }
+    // FP32 factors + FP64 iterative refinement.
+    // workspace: Bc (copy of B when X aliases B), R64, S32, D32, scale, xmax
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
+    bool alias = (const void*)B == (const void*)X;
+    size_t o_B = alias ? take(nn * sizeof(double2)) : 0;
+    size_t o_R = take(nn * sizeof(double2)), o_S = take(nn * sizeof(float2)), o_D = take(nn * sizeof(float2)),
+           o_sc = take(nrhs * sizeof(double)), o_xm = take(nrhs * sizeof(double)),
+           o_dm = take(nrhs * sizeof(double));
+    BEM_TRY(ctx->ensure_ws(off));
+    char* ws = (char*)ctx->ws;
+    if (alias) {
+        double2* Bc = (double2*)(ws + o_B);
+        copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, Bc, n, n, nrhs);
+        BEM_LAUNCHED(ctx);
+        B = Bc;
+        ldb = n;
+    }
+    double2* R = (double2*)(ws + o_R);
+    float2* S = (float2*)(ws + o_S);
+    float2* D = (float2*)(ws + o_D);
+    double* scale = (double*)(ws + o_sc);
+    double* xmax = (double*)(ws + o_xm);
+    double* dmax = (double*)(ws + o_dm);
+    TrailingUpdate<float> tc = tc_update_fp32(ctx);
+    std::vector<double> h_dm(nrhs), h_xm(nrhs), h_sc(nrhs);
+    // x0 = (LU32)^-1 B
+    colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(B, ldb, n, scale);
+    BEM_LAUNCHED(ctx);
+    scale_down_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, S, n, scale, n, nrhs);
+    BEM_LAUNCHED(ctx);
+    BEM_TRY(getrs<float>(ctx, lu->A32, n, n, lu->d_perm, S, n, D, n, nrhs, &tc));
+    scale_up_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(D, n, X, ldx, scale, n, nrhs, 0);
+    BEM_LAUNCHED(ctx);
+    BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    stats.t_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    auto t1 = std::chrono::steady_clock::now();
+    double2 m1 = make_double2(-1, 0), p1 = make_double2(1, 0);
+    for (int it = 1; it <= max_iter; it++) {
+        // R = B - Z X  (FP64)
+        copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, R, n, n, nrhs);
+        BEM_LAUNCHED(ctx);
+        BEM_TRY(cgemm<double>(ctx, n, nrhs, n, lu->Z, lu->ldz, X, ldx, true, R, n, true, m1, p1));
+        colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(R, n, n, scale);
+        BEM_LAUNCHED(ctx);
+        colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(X, ldx, n, xmax);
+        BEM_LAUNCHED(ctx);
+        scale_down_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(R, n, S, n, scale, n, nrhs);
+        BEM_LAUNCHED(ctx);
+        BEM_TRY(getrs<float>(ctx, lu->A32, n, n, lu->d_perm, S, n, D, n, nrhs, &tc));
+        colmax_kernel<float2><<<nrhs, 256, 0, ctx->stream>>>(D, n, n, dmax);
+        BEM_LAUNCHED(ctx);
+        scale_up_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(D, n, X, ldx, scale, n, nrhs, 1);
+        BEM_LAUNCHED(ctx);
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(h_dm.data(), dmax, nrhs * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(h_xm.data(), xmax, nrhs * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(h_sc.data(), scale, nrhs * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        double upd = 0, res = 0;
+        for (int c = 0; c < nrhs; c++) {
+            double xm = h_xm[c] > 0 ? h_xm[c] : 1.0;
+            upd = std::max(upd, h_sc[c] * h_dm[c] / xm);
+            res = std::max(res, h_sc[c] / xm);
+        }
+        stats.iterations = it;
+        stats.max_rel_update = upd;
+        // max-norm residual relative to ||Z||_F ||x||_max (a bound-style measure)
+        stats.max_rel_residual = res / (lu->znorm > 0 ? lu->znorm : 1.0);
+        if (upd <= tol) {
+            stats.converged = 1;
+            break;
+        }
+    }
+    stats.t_refine_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    if (st) *st = stats;
+    if (!stats.converged)
+        return fail(ctx, BEM_ERR_NOCONV, "refinement stopped after %d sweeps at relative update %.3e",
+                    stats.iterations, stats.max_rel_update);
+    return BEM_OK;
+}
+
+}  // namespace bem
+
+using namespace bem;
+
+extern "C" {
+
+int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precision, bem_lu** out,
+                      int* info) {
+    return lu_factor(ctx, Z_dev, n, ldz, precision, out, info);
+}
+
+int bem_lu_solve_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb, void* X_dev, int64_t ldx,
+                     int nrhs, double tol, int max_iter, bem_solve_stats* stats) {
+    return lu_solve(ctx, lu, B_dev, ldb, X_dev, ldx, nrhs, tol, max_iter, stats);
+}
+
+int bem_lu_free(bem_lu* lu) {
+    lu_release(lu);
+    return BEM_OK;
+}
+
+// lu_factorize_cuda (solver.cu:7-48): Z host row-major n x n is overwritten
+// by the packed factors of P Z = L U; ipiv host, 1-based interchange rows.
+int bem_lu_factorize(bem_ctx* ctx, double* Z, int n, int* ipiv, int* info) {
+    if (!ctx || !Z || !ipiv || n < 1) return BEM_ERR_INVALID;
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    size_t bytes = (size_t)n * n * sizeof(double2);
+    void* d = nullptr;
+    BEM_TRY_CUDA(ctx, cudaMalloc(&d, bytes));
+    bem_lu* lu = nullptr;
+    int s = BEM_OK, inf = 0;
+    if (cudaMemcpy(d, Z, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "copy Z to device");
+    if (s == BEM_OK) s = lu_factor(ctx, d, n, n, BEM_PREC_FP64, &lu, &inf);
+    if (s == BEM_OK && cudaMemcpy(Z, d, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "copy factors to host");
+    if (s == BEM_OK)
+        for (int i = 0; i < n; i++) ipiv[i] = lu->ipiv[i] + 1;
+    if (lu) lu_release(lu);
+    cudaFree(d);
+    if (info) *info = inf;
+    return s;
+}
+
+// lu_solve_cuda (solver.cu:51-84): consumes the pair made by bem_lu_factorize.
+int bem_lu_solve(bem_ctx* ctx, const double* Z_lu, const int* ipiv, int n, double* B, int nrhs) {
+    if (!ctx || !Z_lu || !ipiv || !B || n < 1 || nrhs < 0) return BEM_ERR_INVALID;
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    size_t zb = (size_t)n * n * sizeof(double2), bb = (size_t)n * nrhs * sizeof(double2);
+    void *dz = nullptr, *db = nullptr, *dx = nullptr;
+    int* dp = nullptr;
+    int s = BEM_OK;
+    std::vector<int> piv(n), perm;
+    for (int i = 0; i < n; i++) {
+        piv[i] = ipiv[i] - 1;
+        if (piv[i] < 0 || piv[i] >= n) return fail(ctx, BEM_ERR_INVALID, "ipiv[%d] out of range", i);
+    }
+    pivots_to_perm(piv, perm);
+    if (cudaMalloc(&dz, zb) != cudaSuccess || cudaMalloc(&db, bb + 16) != cudaSuccess ||
+        cudaMalloc(&dx, bb + 16) != cudaSuccess || cudaMalloc(&dp, n * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        s = fail(ctx, BEM_ERR_OOM, "lu_solve buffers");
+    }
+    if (s == BEM_OK && (cudaMemcpy(dz, Z_lu, zb, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(db, B, bb, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(dp, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess))
+        s = fail(ctx, BEM_ERR_CUDA, "upload");
+    if (s == BEM_OK)
+        s = getrs<double>(ctx, (const double2*)dz, n, n, dp, (const double2*)db, n, (double2*)dx, n, nrhs, nullptr);
+    if (s == BEM_OK && cudaMemcpy(B, dx, bb, cudaMemcpyDeviceToHost) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "download");
+    cudaFree(dz);
+    cudaFree(db);
+    cudaFree(dx);
+    cudaFree(dp);
+    return s;
+}
+
+// lu_solve_full (solver.cu:87-142): factor + solve; B (column-major n x nrhs)
+// is overwritten with X.  FP64: Z is overwritten with the factors as in the
+// reference; FP32_REFINE: Z is left unchanged.
+int bem_lu_solve_full(bem_ctx* ctx, double* Z, int n, double* B, int nrhs, int precision,
+                      bem_solve_stats* stats) {
+    if (!ctx || !Z || !B || n < 1 || nrhs < 0) return BEM_ERR_INVALID;
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    size_t zb = (size_t)n * n * sizeof(double2), bb = (size_t)n * nrhs * sizeof(double2);
+    void *dz = nullptr, *db = nullptr;
+    int s = BEM_OK, info = 0;
+    bem_lu* lu = nullptr;
+    if (cudaMalloc(&dz, zb) != cudaSuccess || cudaMalloc(&db, bb + 16) != cudaSuccess) {
+        cudaGetLastError();
+        s = fail(ctx, BEM_ERR_OOM, "lu_solve_full buffers");
+    }
+    if (s == BEM_OK && (cudaMemcpy(dz, Z, zb, cudaMemcpyHostToDevice) != cudaSuccess ||
+                        cudaMemcpy(db, B, bb, cudaMemcpyHostToDevice) != cudaSuccess))
+        s = fail(ctx, BEM_ERR_CUDA, "upload");
+    if (s == BEM_OK) s = lu_factor(ctx, dz, n, n, precision, &lu, &info);
+    if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+    if (s == BEM_OK) s = lu_solve(ctx, lu, db, n, db, n, nrhs, 0.0, 0, stats);
+    if (s == BEM_OK && cudaMemcpy(B, db, bb, cudaMemcpyDeviceToHost) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "download X");
+    if (s == BEM_OK && precision == BEM_PREC_FP64 && cudaMemcpy(Z, dz, zb, cudaMemcpyDeviceToHost) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "download factors");
+    if (lu) lu_release(lu);
+    cudaFree(dz);
+    cudaFree(db);
+    return s;
+}
+
+}  // extern "C"

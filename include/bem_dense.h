@@ -1,0 +1,244 @@
+/*
+ * bem_dense.h -- C ABI of libbemdense.so, a B200-native (sm_100a) implementation
+ * of the dense PMCHWT path of BEM-CPP: RWG Galerkin assembly of the 2N x 2N
+ * system, complex LU with a multi-RHS solve (FP64, or FP32 factors with FP64
+ * iterative refinement), and the far-field / Mueller reduction.
+ *
+ * Plain C types only.  Complex numbers are interleaved (re, im) doubles, the
+ * layout of std::complex<double> / cuDoubleComplex.  Matrices named Z are
+ * row-major n x n (the reference's Z[i*n + j]); right-hand sides and solutions
+ * are column-major n x nrhs (column c at B[c*n]), as in the reference.
+ *
+ * Every entry point returns a bem_status.  Nothing calls exit(); the message of
+ * the last failure on a context is available from bem_last_error().
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * file:line of KirillSalnikov/BEM-CPP.
+ */
+#ifndef BEM_DENSE_H
+#define BEM_DENSE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bem_status {
+    BEM_OK = 0,
+    BEM_ERR_INVALID = 1,    /* bad argument (size, pointer, order, option) */
+    BEM_ERR_CUDA = 2,       /* CUDA runtime / launch failure */
+    BEM_ERR_OOM = 3,        /* device allocation failed */
+    BEM_ERR_SINGULAR = 4,   /* zero pivot; the LU info is returned separately */
+    BEM_ERR_NOCONV = 5,     /* iterative refinement did not reach the tolerance */
+    BEM_ERR_TIMEOUT = 6,    /* a bounded device-side wait gave up */
+    BEM_ERR_NODEVICE = 7    /* no usable sm_100 device */
+} bem_status;
+
+typedef enum bem_precision {
+    BEM_PREC_FP64 = 0,         /* complex128 LU and solves */
+    BEM_PREC_FP32_REFINE = 1   /* complex64 LU (3xTF32 tensor-core updates) + FP64 refinement */
+} bem_precision;
+
+/* Assembly flags */
+#define BEM_ASM_GSMOOTH_EXACT 1u  /* cancellation-free G_smooth limit ik/(4 pi) at R = 0
+                                     (default: the reference's exp(ikR)/(4piR) - 1/(4piR)
+                                     with R clamped to 1e-15, assembly.cu:63-77) */
+
+typedef struct bem_ctx bem_ctx;        /* device, stream, workspace */
+typedef struct bem_geom bem_geom;      /* device-resident mesh + RWG quadrature data */
+typedef struct bem_lu bem_lu;          /* device-resident factorisation */
+
+/* ---------------------------------------------------------------- context */
+
+/* Opens a context on `device` (an sm_100 GPU).  One context per host thread. */
+int bem_ctx_create(int device, bem_ctx** out);
+int bem_ctx_destroy(bem_ctx* ctx);
+/* Kernels of this context run on `stream` (a cudaStream_t).  A new context
+ * uses a private non-blocking stream; NULL selects the legacy default stream. */
+int bem_ctx_set_stream(bem_ctx* ctx, void* stream);
+int bem_ctx_synchronize(bem_ctx* ctx);
+const char* bem_last_error(const bem_ctx* ctx);
+/* Number of kernel launches issued by this context so far. */
+int64_t bem_ctx_launch_count(const bem_ctx* ctx);
+const char* bem_version(void);
+
+/* ----------------------------------------------------- geometry (host) */
+/* Meshes are returned through caller buffers.  Pass NULL buffers to query
+ * the sizes first. */
+
+/* icosphere(radius, refinements) -- mesh.cpp:11-68 */
+int bem_mesh_icosphere(double radius, int refinements, int* nv, int* nt,
+                       double* verts, int* tris);
+/* hex_prism(aspect_ratio, refinements) -- mesh.cpp:102-154 */
+int bem_mesh_hex_prism(double aspect_ratio, int refinements, int* nv, int* nt,
+                       double* verts, int* tris);
+/* subdivide_flat(mesh) -- mesh.cpp:70-100 (out buffers sized by a NULL query) */
+int bem_mesh_subdivide_flat(const double* verts, int nv, const int* tris, int nt,
+                            int* nv_out, int* nt_out, double* verts_out, int* tris_out);
+/* load_obj(filename) -- mesh.cpp:156-250; removes degenerate triangles and
+ * counts non-manifold edges into *n_nonmanifold (may be NULL). */
+int bem_mesh_load_obj(const char* filename, int* nv, int* nt, double* verts, int* tris,
+                      int* n_degenerate, int* n_nonmanifold);
+/* normalize_mesh / mesh_volume / mesh_dmax -- mesh.cpp:252-294 */
+int bem_mesh_normalize(double* verts, int nv, const int* tris, int nt, double* a_eq);
+double bem_mesh_volume(const double* verts, int nv, const int* tris, int nt);
+double bem_mesh_dmax(const double* verts, int nv);
+
+/* build_rwg(mesh) -- rwg.cpp:5-43: interior edges in (min,max) vertex order.
+ * Arrays of length N; free_p / free_m are 3N doubles.  NULL arrays = size query. */
+int bem_rwg_build(const double* verts, int nv, const int* tris, int nt, int* N,
+                  int* tri_p, int* tri_m, double* free_p, double* free_m,
+                  double* length, double* area_p, double* area_m);
+
+/* tri_quadrature(order) -- quadrature.h:14-70.  pts: 2*npts (l1, l2), wts: npts. */
+int bem_tri_quadrature(int order, int* npts, double* pts, double* wts);
+
+/* generate_orientations (+ optional sort_orientations_nearest) -- orient.cpp:73-163.
+ * RT: 9 doubles per orientation (row-major R^T), w: weights. NULL = size query. */
+int bem_orientations(int n_alpha, int n_beta, int n_gamma, int beta_sym, int gamma_sym,
+                     int gamma_mirror, int sort_nearest, int* count, double* RT, double* w);
+/* gauss_legendre(n) -- orient.cpp:39-70 */
+int bem_gauss_legendre(int n, double* nodes, double* weights);
+
+/* ----------------------------------------------------- device geometry */
+
+/* Uploads a mesh and builds its RWG basis and quadrature data on the device
+ * (precompute_half, assembly.cu:150-201; FFCache::init, farfield.cu:9-52).
+ * *N receives the number of RWG functions (system size 2N). */
+int bem_geom_create(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
+                    int quad_order, bem_geom** out, int* N);
+int bem_geom_free(bem_geom* g);
+int bem_geom_size(const bem_geom* g);
+
+/* --------------------------------------------------------------- assembly */
+
+/* Device-resident PMCHWT matrix (pmchwt.cu:6-56 with assemble_L_K_cuda,
+ * assembly.cu:328-505, for both media in one pass):
+ *   Z = [[eta_e L_e + eta_i L_i, -(K_e + K_i)], [K_e + K_i, L_e/eta_e + L_i/eta_i]]
+ * Z_dev: row-major 2N x 2N complex128 with leading dimension ldz (elements). */
+int bem_assemble_pmchwt_dev(bem_ctx* ctx, const bem_geom* g,
+                            double kext_re, double kext_im, double kint_re, double kint_im,
+                            double eta_ext, double eta_int, unsigned flags,
+                            void* Z_dev, int64_t ldz);
+/* Device-resident L and K for one wavenumber (assemble_L_K_cuda, assembly.h:11-13):
+ * row-major N x N complex128, leading dimension ld. */
+int bem_assemble_LK_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
+                        unsigned flags, void* L_dev, void* K_dev, int64_t ld);
+/* Host-buffer mirrors: assemble_L_K_cuda (assembly.h:11-13) and assemble_pmchwt
+ * (pmchwt.h:12-18).  L_ext / K_ext of the latter may be NULL. */
+int bem_assemble_L_K(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
+                     double k_re, double k_im, int quad_order, double* L, double* K);
+int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
+                        double kext_re, double kext_im, double kint_re, double kint_im,
+                        double eta_ext, double eta_int, int quad_order,
+                        double* Z, double* L_ext, double* K_ext);
+
+/* ------------------------------------------------------------ excitation */
+
+/* Plane-wave right-hand sides for a batch of orientations (rhs.cpp:6-64,
+ * main.cpp:739-751): column 2o = par (E0 = RT x), 2o+1 = perp (E0 = RT y),
+ * k_hat = RT z.  RT: host, 9 doubles per orientation.  B_dev: column-major
+ * 2N x (2 n_orient) complex128, leading dimension ldb. */
+int bem_rhs_planewave_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
+                          double eta_ext, const double* RT, int n_orient,
+                          void* B_dev, int64_t ldb);
+/* One plane wave, host output (compute_rhs_planewave, rhs.h:11-15). */
+int bem_rhs_planewave(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
+                      double eta_ext, const double* E0, const double* k_hat, double* b);
+
+/* -------------------------------------------------------------------- LU */
+
+typedef struct bem_solve_stats {
+    int iterations;          /* refinement sweeps run (0 for FP64) */
+    int converged;           /* 1 when every column met the tolerance */
+    double max_rel_update;   /* max over columns of ||dX||/||X|| in the last sweep */
+    double max_rel_residual; /* max over columns of ||B - Z X|| / (||Z||_F ||X||) */
+    double t_factor_ms, t_solve_ms, t_refine_ms;
+} bem_solve_stats;
+
+/* Factorises the row-major n x n complex128 matrix Z_dev (leading dimension
+ * ldz) with partial pivoting.  FP64: Z_dev is overwritten by the factors.
+ * FP32_REFINE: Z_dev is kept (the refinement residual needs it; it must stay
+ * valid until bem_lu_free) and complex64 factors are made in new memory.
+ * *info: 0, or k > 0 when U(k,k) is exactly zero (1-based, LAPACK convention). */
+int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precision,
+                      bem_lu** out, int* info);
+/* X = Z^-1 B for nrhs columns (column-major, leading dimensions ldb / ldx; X may
+ * alias B).  FP32_REFINE refines in FP64 until every column's relative update
+ * is below `tol` (default 1e-12 when tol <= 0) or max_iter sweeps were run. */
+int bem_lu_solve_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb,
+                     void* X_dev, int64_t ldx, int nrhs, double tol, int max_iter,
+                     bem_solve_stats* stats);
+int bem_lu_free(bem_lu* lu);
+
+/* Host-buffer mirrors of solver.h:11-22.  The reference factors its row-major
+ * Z as a column-major Z^T (solver.cu:25-31) and solves with op = T; these keep
+ * that contract: bem_lu_factorize overwrites Z with the packed LU factors of
+ * the row-major Z (P Z = L U, unit L) and returns 1-based row pivots, and
+ * bem_lu_solve consumes exactly that pair. */
+int bem_lu_factorize(bem_ctx* ctx, double* Z, int n, int* ipiv, int* info);
+int bem_lu_solve(bem_ctx* ctx, const double* Z_lu, const int* ipiv, int n, double* B, int nrhs);
+int bem_lu_solve_full(bem_ctx* ctx, double* Z, int n, double* B, int nrhs, int precision,
+                      bem_solve_stats* stats);
+
+/* ------------------------------------------------------ far field, Mueller */
+
+/* Far-field vectors Fv for coefficient columns (farfield_batch_kernel,
+ * farfield.cu:100-262): coeffs_J / coeffs_M host (n_calls x N complex128),
+ * r_hats host (n_orient x ndir x 3), call c uses r_hat block c/2.
+ * Fv host (n_calls x ndir x 3 complex128). */
+int bem_farfield_batch(bem_ctx* ctx, const bem_geom* g, const double* coeffs_J,
+                       const double* coeffs_M, const double* r_hats, double k_re, double k_im,
+                       double eta_ext, int n_calls, int n_orient, int ndir, double* Fv);
+
+/* Orientation-averaged Mueller matrix from device solutions (main.cpp:757-846
+ * with amplitude_to_mueller, farfield.cu:464-508): X_dev column-major
+ * 2N x (2 n_orient), columns (par, perp) per orientation.  Writes
+ * M_avg[16 * ntheta] (host, M[(i*4+j)*ntheta + t]) = sum_o w_o M_o / |k|^2.
+ * gamma_mirror zeroes the odd blocks of each M_o (main.cpp:837-842).
+ * M_orient_dev (may be NULL): device buffer of n_orient*16*ntheta doubles that
+ * receives the per-orientation w_o M_o/|k|^2 terms. */
+int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev, int64_t ldx,
+                             const double* RT, const double* w, int n_orient,
+                             double k_re, double k_im, double eta_ext, int ntheta,
+                             int gamma_mirror, double* M_avg, double* M_orient_dev);
+
+/* amplitude_to_mueller (farfield.cu:464-508); S*, complex128[ntheta]. */
+int bem_amplitude_to_mueller(const double* S1, const double* S2, const double* S3,
+                             const double* S4, int ntheta, double* M);
+
+/* ---------------------------------------------------------- whole pipeline */
+
+typedef struct bem_problem {
+    /* mesh (host) */
+    const double* verts; int nv; const int* tris; int nt;
+    double ka;             /* k_ext = ka (unit equivalent radius) */
+    double m_re, m_im;     /* relative refractive index; k_int = k_ext m, eta_int = 1/|m| */
+    int quad_order;        /* 4, 7 or 13 */
+    int single;            /* 1: k_hat = z, E = x / y (main.cpp:671-718) */
+    int n_alpha, n_beta, n_gamma;
+    int beta_sym, gamma_sym, gamma_mirror;
+    int orient_i0, orient_i1;  /* orientation range [i0, i1), -1 = all */
+    int ntheta;
+    int precision;         /* bem_precision */
+    double refine_tol;     /* <= 0: 1e-12 */
+    int max_refine;        /* <= 0: 10 */
+    unsigned asm_flags;
+} bem_problem;
+
+typedef struct bem_result {
+    double* mueller;       /* caller buffer, 16 * ntheta doubles */
+    double t_assembly_s, t_solve_s, t_farfield_s, t_total_s;
+    int N, n_orient;
+    bem_solve_stats stats;
+} bem_result;
+
+/* The dense branch of main.cpp (:660-854) end to end on the device: assemble,
+ * factor, solve every orientation x polarisation at once, far field, Mueller. */
+int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEM_DENSE_H */

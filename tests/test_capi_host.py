@@ -1,0 +1,140 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry point
+of include/bem_dense.h, and its host-side geometry matches the reference's own
+C++ (oracle/_ref) and the oracle."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO, rel
+from oracle import bem_oracle as bo
+from oracle import ref_host
+
+
+def test_library_exports_every_declared_entry_point():
+    import bem_b200 as bb
+    from bem_b200 import _lib
+    hdr = open(os.path.join(REPO, "include", "bem_dense.h")).read()
+    declared = set(re.findall(r"^\s*(?:int|double|const char\*|int64_t)\s+(bem_\w+)\(", hdr, re.M))
+    assert declared, "no declarations parsed"
+    assert declared == set(_lib.SIGNATURES), declared ^ set(_lib.SIGNATURES)
+    L = bb.lib()
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_no_gpu_context_fails_cleanly():
+    import torch
+    import bem_b200 as bb
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    s = bb.lib().bem_ctx_create(0, C.byref(h))
+    assert s == 7  # BEM_ERR_NODEVICE, no exit()
+
+
+@pytest.mark.parametrize("ref", [0, 1, 2, 3])
+def test_icosphere_and_rwg_match_reference_cpp(ref):
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("oracle/_ref not built")
+    v, t = bb.icosphere(1.0, ref)
+    vr, tr, rr = ref_host.make_mesh("ico", 1.0, ref)
+    assert np.array_equal(t, tr) and np.abs(v - vr).max() == 0.0
+    r = bb.build_rwg(v, t)
+    for k in ("tri_p", "tri_m"):
+        assert np.array_equal(r[k], rr[k])
+    for k in ("free_p", "free_m", "length", "area_p", "area_m"):
+        assert np.abs(r[k] - rr[k]).max() == 0.0, k
+
+
+@pytest.mark.parametrize("ar,ref", [(1.4286, 2), (0.7, 1), (2.0, 3)])
+def test_hex_prism_matches_reference_cpp(ar, ref):
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("oracle/_ref not built")
+    v, t = bb.hex_prism(ar, ref)
+    vr, tr, rr = ref_host.make_mesh("hex", ar, ref)
+    assert np.array_equal(t, tr) and np.abs(v - vr).max() == 0.0
+    assert bb.build_rwg(v, t)["N"] == rr["N"]
+
+
+def test_hex_sizes_are_the_reference_mesher_sizes():
+    # hex_prism starts at 24 triangles: ref 2 -> 2N = 1152, ref 3 -> 2N = 4608
+    import bem_b200 as bb
+    assert 2 * bb.build_rwg(*bb.hex_prism(1.4286, 2))["N"] == 1152
+    assert 2 * bb.build_rwg(*bb.hex_prism(1.4286, 3))["N"] == 4608
+    assert 2 * bb.build_rwg(*bb.icosphere(1.0, 5))["N"] == 61440
+
+
+def test_subdivide_volume_dmax_normalize():
+    import bem_b200 as bb
+    v, t = bb.hex_prism(1.0, 0)
+    v2, t2 = bb.subdivide_flat(v, t)
+    vo, to = bo.subdivide_flat(v, t.astype(np.int64))
+    assert np.array_equal(t2, to) and np.abs(v2 - vo).max() == 0.0
+    assert abs(bb.mesh_volume(v, t) - 4 * np.pi / 3) < 1e-12
+    vs, a = bb.normalize_mesh(3.0 * v, t)
+    assert abs(a - 3.0) < 1e-12 and abs(bb.mesh_volume(vs, t) - 4 * np.pi / 3) < 1e-12
+    ext = v.max(0) - v.min(0)
+    assert abs(bb.mesh_dmax(v) - np.linalg.norm(ext)) < 1e-15
+
+
+def test_load_obj_removes_degenerates(tmp_path):
+    import bem_b200 as bb
+    v, t = bb.icosphere(1.0, 1)
+    p = tmp_path / "m.obj"
+    with open(p, "w") as f:
+        for x in v:
+            f.write(f"v {x[0]:.17g} {x[1]:.17g} {x[2]:.17g}\n")
+        for tri in t:
+            f.write(f"f {tri[0]+1}/1/1 {tri[1]+1}/2/2 {tri[2]+1}/3/3\n")
+        f.write("f 1 1 2\n")  # repeated vertex -> removed
+    v2, t2, nd, nm = bb.load_obj(p)
+    assert nd == 1 and nm == 0 and np.array_equal(t2, t)
+    assert np.abs(v2 - v).max() < 1e-15
+
+
+@pytest.mark.parametrize("order", [4, 7, 13])
+def test_quadrature(order):
+    import bem_b200 as bb
+    p, w = bb.tri_quadrature(order)
+    po, wo = bo.tri_quadrature(order)
+    assert np.array_equal(p, po) and np.array_equal(w, wo)
+    assert abs(w.sum() - 1.0) < 1e-12
+
+
+def test_quadrature_rejects_unknown_order():
+    import bem_b200 as bb
+    with pytest.raises(bb.BemError):
+        bb.tri_quadrature(5)
+
+
+@pytest.mark.parametrize("args", [(8, 8, 1, 1, 1, False), (45, 31, 1, 1, 1, False),
+                                  (4, 3, 2, 2, 6, True), (5, 4, 3, 1, 1, True)])
+def test_orientations_match_reference_cpp(args):
+    import bem_b200 as bb
+    RT, w = bb.generate_orientations(*args)
+    assert abs(w.sum() - 1.0) < 1e-12 or args[3] != 1 or args[5]
+    if ref_host.available():
+        RTr, wr = ref_host.orientations(*args)
+        assert np.abs(RT - RTr).max() == 0.0 and np.abs(w - wr).max() == 0.0
+        RTs, ws = bb.generate_orientations(*args, sort_nearest=True)
+        RTrs, wrs = ref_host.orientations(*args, sort=True)
+        assert np.abs(RTs - RTrs).max() == 0.0 and np.abs(ws - wrs).max() == 0.0
+
+
+def test_gauss_legendre():
+    import bem_b200 as bb
+    x, w = bb.gauss_legendre(31)
+    xo, wo = bo.gauss_legendre(31)
+    assert np.abs(x - xo).max() == 0.0 and np.abs(w - wo).max() == 0.0
+
+
+def test_amplitude_to_mueller_host():
+    import bem_b200 as bb
+    rng = np.random.default_rng(3)
+    S = [rng.standard_normal(17) + 1j * rng.standard_normal(17) for _ in range(4)]
+    assert rel(bb.amplitude_to_mueller(*S), bo.amplitude_to_mueller(*S)) < 1e-15
