@@ -34,11 +34,14 @@ class BemError(RuntimeError):
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int),
                 ("max_rel_update", C.c_double), ("max_rel_residual", C.c_double),
+                ("est_rel_error", C.c_double),
                 ("t_factor_ms", C.c_double), ("t_solve_ms", C.c_double),
-                ("t_refine_ms", C.c_double)]
+                ("t_refine_ms", C.c_double), ("update_hist", C.c_double * 12)]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["update_hist"] = [self.update_hist[i] for i in range(min(12, self.iterations))]
+        return d
 
 
 class Problem(C.Structure):
@@ -74,6 +77,11 @@ SIGNATURES = {
     "bem_last_error": (C.c_char_p, [_P]),
     "bem_ctx_launch_count": (_L, [_P]),
     "bem_version": (C.c_char_p, []),
+    "bem_ctx_profile": (_I, [_P, _I]),
+    "bem_ctx_set_tensor_cores": (_I, [_P, _I]),
+    "bem_cgemm_tf32x3": (_I, [_P, _I, _I, _I, _P, _L, _P, _L, _I, _P, _L, _I]),
+    "bem_ctx_profile_read": (_I, [_P, _I, C.POINTER(_L), C.POINTER(_D), C.POINTER(_D),
+                                  C.POINTER(_D)]),
     "bem_mesh_icosphere": (_I, [_D, _I, _IP, _IP, _P, _P]),
     "bem_mesh_hex_prism": (_I, [_D, _I, _IP, _IP, _P, _P]),
     "bem_mesh_subdivide_flat": (_I, [_P, _I, _P, _I, _IP, _IP, _P, _P]),
@@ -86,6 +94,8 @@ SIGNATURES = {
     "bem_orientations": (_I, [_I, _I, _I, _I, _I, _I, _I, _IP, _P, _P]),
     "bem_gauss_legendre": (_I, [_I, _P, _P]),
     "bem_geom_create": (_I, [_P, _P, _I, _P, _I, _I, C.POINTER(_P), _IP]),
+    "bem_geom_create_rwg": (_I, [_P, _P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I,
+                                 C.POINTER(_P)]),
     "bem_geom_free": (_I, [_P]),
     "bem_geom_size": (_I, [_P]),
     "bem_assemble_pmchwt_dev": (_I, [_P, _P, _D, _D, _D, _D, _D, _D, C.c_uint, _P, _L]),

@@ -61,6 +61,21 @@ class Context:
     def launches(self) -> int:
         return int(lib().bem_ctx_launch_count(self.h))
 
+    PROF_CLASSES = ("lu_update", "solve_update", "residual", "panel", "assembly", "farfield")
+
+    def profile(self, enable=True):
+        self.check(lib().bem_ctx_profile(self.h, int(bool(enable))))
+
+    def profile_read(self):
+        """{class: (launches, device ms, algorithmic flops, algorithmic bytes)}."""
+        out = {}
+        for i, name in enumerate(self.PROF_CLASSES):
+            n, ms, fl, by = C.c_int64(), C.c_double(), C.c_double(), C.c_double()
+            self.check(lib().bem_ctx_profile_read(self.h, i, C.byref(n), C.byref(ms),
+                                                  C.byref(fl), C.byref(by)))
+            out[name] = (n.value, ms.value, fl.value, by.value)
+        return out
+
     def close(self):
         if self.h:
             lib().bem_ctx_destroy(self.h)
@@ -446,3 +461,22 @@ def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=Fals
             "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s, "t_total_s": r.t_total_s,
             "stats": r.stats.as_dict()}
     return M, info
+
+
+def cgemm_tf32x3(ctx: Context, A, B, C, b_rowmajor=True, c_colmajor=False):
+    """C -= A B on the tensor cores (3xTF32), torch complex64 device tensors.
+    A: (M, K) row-major; B: (K, N) row-major if b_rowmajor else given as its
+    transpose (N, K) row-major; C: (M, N) row-major, or (N, M) if c_colmajor."""
+    M, K = A.shape
+    if b_rowmajor:
+        N = B.shape[1]
+    else:
+        N = B.shape[0]
+    ctx.check(lib().bem_cgemm_tf32x3(ctx.h, M, N, K, _dptr(A), A.stride(0), _dptr(B), B.stride(0),
+                                     int(bool(b_rowmajor)), _dptr(C), C.stride(0),
+                                     int(bool(c_colmajor))))
+    return C
+
+
+def set_tensor_cores(ctx: Context, enable: bool):
+    ctx.check(lib().bem_ctx_set_tensor_cores(ctx.h, int(bool(enable))))

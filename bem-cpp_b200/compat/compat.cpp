@@ -1,0 +1,512 @@
+// libbem_compat: the reference's C++ call surface for the dense path
+// (mesh.h, rwg.h, assembly.h, pmchwt.h, solver.h, rhs.h, orient.h,
+// farfield.h, output.h of BEM-CPP) implemented over the C ABI of
+// libbemdense.  A reference build links this library instead of compiling
+// assembly.cu, pmchwt.cu, solver.cu, farfield.cu, mesh.cpp, rwg.cpp, rhs.cpp,
+// orient.cpp and output.cpp; main.cpp compiles unchanged against
+// include/bem/*.h.
+//
+// Error behaviour follows the reference: a CUDA failure prints a message and
+// exits with status 1 (types.h:12-35); a zero pivot is returned as info > 0.
+// All calls share one context on device $BEM_DEVICE (default 0).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "bem/assembly.h"
+#include "bem/farfield.h"
+#include "bem/mesh.h"
+#include "bem/orient.h"
+#include "bem/output.h"
+#include "bem/pmchwt.h"
+#include "bem/rhs.h"
+#include "bem/rwg.h"
+#include "bem/solver.h"
+#include "bem_dense.h"
+
+namespace {
+
+bem_ctx* g_ctx = nullptr;
+std::mutex g_mu;
+
+bem_ctx* ctx() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx) {
+        const char* d = std::getenv("BEM_DEVICE");
+        int dev = d ? std::atoi(d) : 0;
+        int s = bem_ctx_create(dev, &g_ctx);
+        if (s != BEM_OK) {
+            std::fprintf(stderr, "libbem_compat: no usable sm_100 device %d (status %d)\n", dev, s);
+            std::exit(1);
+        }
+    }
+    return g_ctx;
+}
+
+void check(int s, const char* what) {
+    if (s != BEM_OK) {
+        std::fprintf(stderr, "%s failed (status %d): %s\n", what, s, bem_last_error(g_ctx));
+        std::exit(1);
+    }
+}
+
+void flatten(const Mesh& m, std::vector<double>& v) {
+    v.resize(3 * m.verts.size());
+    for (size_t i = 0; i < m.verts.size(); i++) {
+        v[3 * i] = m.verts[i].x;
+        v[3 * i + 1] = m.verts[i].y;
+        v[3 * i + 2] = m.verts[i].z;
+    }
+}
+
+Mesh unflatten(const std::vector<double>& v, const std::vector<int>& t) {
+    Mesh m;
+    m.verts.resize(v.size() / 3);
+    for (size_t i = 0; i < m.verts.size(); i++) m.verts[i] = Vec3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    m.tris = t;
+    return m;
+}
+
+// Device geometry for (rwg, mesh) with the caller's RWG order.
+bem_geom* make_geom(const RWG& rwg, const Mesh& mesh, int quad_order) {
+    std::vector<double> v, fp(3 * rwg.N), fm(3 * rwg.N);
+    flatten(mesh, v);
+    for (int n = 0; n < rwg.N; n++) {
+        fp[3 * n] = rwg.free_p[n].x, fp[3 * n + 1] = rwg.free_p[n].y, fp[3 * n + 2] = rwg.free_p[n].z;
+        fm[3 * n] = rwg.free_m[n].x, fm[3 * n + 1] = rwg.free_m[n].y, fm[3 * n + 2] = rwg.free_m[n].z;
+    }
+    int order = (quad_order == 4 || quad_order == 13) ? quad_order : 7;
+    bem_geom* g = nullptr;
+    check(bem_geom_create_rwg(ctx(), v.data(), mesh.nv(), mesh.tris.data(), mesh.nt(), rwg.N, rwg.tri_p.data(),
+                              rwg.tri_m.data(), fp.data(), fm.data(), rwg.length.data(), rwg.area_p.data(),
+                              rwg.area_m.data(), order, &g),
+          "geometry upload");
+    return g;
+}
+
+Mesh mesh_call(int (*fn)(double, int, int*, int*, double*, int*), double p, int r) {
+    int nv = 0, nt = 0;
+    if (fn(p, r, &nv, &nt, nullptr, nullptr) != BEM_OK) {
+        std::fprintf(stderr, "mesh generation failed\n");
+        std::exit(1);
+    }
+    std::vector<double> v(3 * (size_t)nv);
+    std::vector<int> t(3 * (size_t)nt);
+    fn(p, r, &nv, &nt, v.data(), t.data());
+    return unflatten(v, t);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ mesh.h
+Mesh icosphere(double radius, int refinements) { return mesh_call(bem_mesh_icosphere, radius, refinements); }
+
+Mesh hex_prism(double aspect_ratio, int refinements) {
+    Mesh m = mesh_call(bem_mesh_hex_prism, aspect_ratio, refinements);
+    double a = std::pow(8.0 * M_PI / (27.0 * aspect_ratio), 1.0 / 3.0);
+    std::printf("  Hex prism: AR=%.2f, a=%.4f, H=%.4f, %d tris\n", aspect_ratio, a, aspect_ratio * a * std::sqrt(3.0),
+                m.nt());
+    return m;
+}
+
+Mesh subdivide_flat(const Mesh& m) {
+    std::vector<double> v;
+    flatten(m, v);
+    int nv = 0, nt = 0;
+    bem_mesh_subdivide_flat(v.data(), m.nv(), m.tris.data(), m.nt(), &nv, &nt, nullptr, nullptr);
+    std::vector<double> vo(3 * (size_t)nv);
+    std::vector<int> to(3 * (size_t)nt);
+    bem_mesh_subdivide_flat(v.data(), m.nv(), m.tris.data(), m.nt(), &nv, &nt, vo.data(), to.data());
+    return unflatten(vo, to);
+}
+
+Mesh load_obj(const char* filename) {
+    int nv = 0, nt = 0, nd = 0, nm = 0;
+    if (bem_mesh_load_obj(filename, &nv, &nt, nullptr, nullptr, &nd, &nm) != BEM_OK) {
+        std::fprintf(stderr, "Error: cannot open OBJ file: %s\n", filename);
+        std::exit(1);
+    }
+    std::vector<double> v(3 * (size_t)nv);
+    std::vector<int> t(3 * (size_t)nt);
+    bem_mesh_load_obj(filename, &nv, &nt, v.data(), t.data(), &nd, &nm);
+    std::printf("  Loaded OBJ: %d vertices, %d triangles from %s\n", nv, nt + nd, filename);
+    if (nd > 0) std::fprintf(stderr, "Warning: removed %d degenerate triangles from OBJ\n", nd);
+    if (nm > 0) std::fprintf(stderr, "Warning: %d non-manifold edges (shared by >2 triangles) in OBJ\n", nm);
+    return unflatten(v, t);
+}
+
+double mesh_volume(const Mesh& m) {
+    std::vector<double> v;
+    flatten(m, v);
+    return bem_mesh_volume(v.data(), m.nv(), m.tris.data(), m.nt());
+}
+
+double normalize_mesh(Mesh& m) {
+    std::vector<double> v;
+    flatten(m, v);
+    double a = 0;
+    bem_mesh_normalize(v.data(), m.nv(), m.tris.data(), m.nt(), &a);
+    for (int i = 0; i < m.nv(); i++) m.verts[i] = Vec3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    return a;
+}
+
+double mesh_dmax(const Mesh& m) {
+    std::vector<double> v;
+    flatten(m, v);
+    return bem_mesh_dmax(v.data(), m.nv());
+}
+
+// ------------------------------------------------------------------- rwg.h
+RWG build_rwg(const Mesh& mesh) {
+    std::vector<double> v;
+    flatten(mesh, v);
+    int N = 0;
+    bem_rwg_build(v.data(), mesh.nv(), mesh.tris.data(), mesh.nt(), &N, nullptr, nullptr, nullptr, nullptr, nullptr,
+                  nullptr, nullptr);
+    RWG r;
+    r.N = N;
+    r.tri_p.resize(N);
+    r.tri_m.resize(N);
+    r.length.resize(N);
+    r.area_p.resize(N);
+    r.area_m.resize(N);
+    std::vector<double> fp(3 * (size_t)N), fm(3 * (size_t)N);
+    bem_rwg_build(v.data(), mesh.nv(), mesh.tris.data(), mesh.nt(), &N, r.tri_p.data(), r.tri_m.data(), fp.data(),
+                  fm.data(), r.length.data(), r.area_p.data(), r.area_m.data());
+    r.free_p.resize(N);
+    r.free_m.resize(N);
+    for (int n = 0; n < N; n++) {
+        r.free_p[n] = Vec3(fp[3 * n], fp[3 * n + 1], fp[3 * n + 2]);
+        r.free_m[n] = Vec3(fm[3 * n], fm[3 * n + 1], fm[3 * n + 2]);
+    }
+    return r;
+}
+
+// -------------------------------------------------------------- assembly.h
+void assemble_L_K_cuda(const RWG& rwg, const Mesh& mesh, std::complex<double> k, int quad_order,
+                       std::complex<double>* L, std::complex<double>* K) {
+    bem_geom* g = make_geom(rwg, mesh, quad_order);
+    const int N = rwg.N;
+    size_t bytes = (size_t)N * N * sizeof(std::complex<double>);
+    void *dL = nullptr, *dK = nullptr;
+    if (cudaMalloc(&dL, bytes) != cudaSuccess || cudaMalloc(&dK, bytes) != cudaSuccess) {
+        std::fprintf(stderr, "CUDA error: cannot allocate L/K (%zu bytes each)\n", bytes);
+        std::exit(1);
+    }
+    check(bem_assemble_LK_dev(ctx(), g, k.real(), k.imag(), 0, dL, dK, N), "assemble_L_K_cuda");
+    check(bem_ctx_synchronize(ctx()), "assemble_L_K_cuda");
+    cudaMemcpy(L, dL, bytes, cudaMemcpyDeviceToHost);
+    cudaMemcpy(K, dK, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dL);
+    cudaFree(dK);
+    bem_geom_free(g);
+}
+
+// ---------------------------------------------------------------- pmchwt.h
+void assemble_pmchwt(const RWG& rwg, const Mesh& mesh, std::complex<double> k_ext, std::complex<double> k_int,
+                     double eta_ext, double eta_int, int quad_order, std::complex<double>* Z,
+                     std::complex<double>* L_ext, std::complex<double>* K_ext) {
+    const int N = rwg.N, n = 2 * N;
+    std::printf("  Assembling %dx%d PMCHWT matrix (%d RWG functions)...\n", n, n, N);
+    Timer t;
+    bem_geom* g = make_geom(rwg, mesh, quad_order);
+    size_t bytes = (size_t)n * n * sizeof(std::complex<double>);
+    void* dZ = nullptr;
+    if (cudaMalloc(&dZ, bytes) != cudaSuccess) {
+        std::fprintf(stderr, "CUDA error: cannot allocate Z (%zu bytes)\n", bytes);
+        std::exit(1);
+    }
+    check(bem_assemble_pmchwt_dev(ctx(), g, k_ext.real(), k_ext.imag(), k_int.real(), k_int.imag(), eta_ext, eta_int,
+                                  0, dZ, n),
+          "assemble_pmchwt");
+    check(bem_ctx_synchronize(ctx()), "assemble_pmchwt");
+    cudaMemcpy(Z, dZ, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dZ);
+    if (L_ext || K_ext) {
+        size_t b = (size_t)N * N * sizeof(std::complex<double>);
+        void *dL = nullptr, *dK = nullptr;
+        if (cudaMalloc(&dL, b) != cudaSuccess || cudaMalloc(&dK, b) != cudaSuccess) {
+            std::fprintf(stderr, "CUDA error: cannot allocate L/K\n");
+            std::exit(1);
+        }
+        check(bem_assemble_LK_dev(ctx(), g, k_ext.real(), k_ext.imag(), 0, dL, dK, N), "assemble_pmchwt L/K");
+        check(bem_ctx_synchronize(ctx()), "assemble_pmchwt L/K");
+        if (L_ext) cudaMemcpy(L_ext, dL, b, cudaMemcpyDeviceToHost);
+        if (K_ext) cudaMemcpy(K_ext, dK, b, cudaMemcpyDeviceToHost);
+        cudaFree(dL);
+        cudaFree(dK);
+    }
+    bem_geom_free(g);
+    std::printf("  Total PMCHWT assembly: %.1fs\n", t.elapsed_s());
+}
+
+// ---------------------------------------------------------------- solver.h
+int lu_factorize_cuda(std::complex<double>* Z, int n, int* ipiv) {
+    Timer t;
+    int info = 0;
+    check(bem_lu_factorize(ctx(), reinterpret_cast<double*>(Z), n, ipiv, &info), "lu_factorize_cuda");
+    if (info != 0) std::fprintf(stderr, "  LU factorization failed: info=%d\n", info);
+    std::printf("  LU factorization (%dx%d): %.1fs\n", n, n, t.elapsed_s());
+    return info;
+}
+
+int lu_solve_cuda(const std::complex<double>* Z, const int* ipiv, int n, std::complex<double>* B, int nrhs) {
+    Timer t;
+    check(bem_lu_solve(ctx(), reinterpret_cast<const double*>(Z), ipiv, n, reinterpret_cast<double*>(B), nrhs),
+          "lu_solve_cuda");
+    std::printf("  LU solve (%dx%d, %d RHS): %.2fs\n", n, n, nrhs, t.elapsed_s());
+    return 0;
+}
+
+int lu_solve_full(std::complex<double>* Z, int n, std::complex<double>* B, int nrhs) {
+    Timer t;
+    int prec = BEM_PREC_FP64;
+    const char* p = std::getenv("BEM_PRECISION");
+    if (p && std::strcmp(p, "fp32-refine") == 0) prec = BEM_PREC_FP32_REFINE;
+    bem_solve_stats st;
+    int s = bem_lu_solve_full(ctx(), reinterpret_cast<double*>(Z), n, reinterpret_cast<double*>(B), nrhs, prec, &st);
+    if (s == BEM_ERR_SINGULAR) {
+        std::fprintf(stderr, "  LU factorization failed: %s\n", bem_last_error(g_ctx));
+        return 1;
+    }
+    check(s, "lu_solve_full");
+    std::printf("  LU solve full (%dx%d, %d RHS): %.2fs\n", n, n, nrhs, t.elapsed_s());
+    return 0;
+}
+
+// ------------------------------------------------------------------- rhs.h
+void compute_rhs_planewave(const RWG& rwg, const Mesh& mesh, std::complex<double> k_ext, double eta_ext,
+                           const Vec3& E0, const Vec3& k_hat, int quad_order, std::complex<double>* b) {
+    bem_geom* g = make_geom(rwg, mesh, quad_order);
+    double e[3] = {E0.x, E0.y, E0.z}, kh[3] = {k_hat.x, k_hat.y, k_hat.z};
+    check(bem_rhs_planewave(ctx(), g, k_ext.real(), k_ext.imag(), eta_ext, e, kh, reinterpret_cast<double*>(b)),
+          "compute_rhs_planewave");
+    bem_geom_free(g);
+}
+
+// ---------------------------------------------------------------- orient.h
+Mat3 euler_rotation(double alpha, double beta, double gamma) {
+    // R = Rz(alpha) Ry(beta) Rz(gamma) (orient.cpp:4-36)
+    double ca = std::cos(alpha), sa = std::sin(alpha), cb = std::cos(beta), sb = std::sin(beta);
+    double cg = std::cos(gamma), sg = std::sin(gamma);
+    double A[3][3] = {{ca, -sa, 0}, {sa, ca, 0}, {0, 0, 1}}, Bm[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}},
+           Cm[3][3] = {{cg, -sg, 0}, {sg, cg, 0}, {0, 0, 1}};
+    Mat3 R;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            R.m[i][j] = 0;
+            for (int k = 0; k < 3; k++) {
+                double t = 0;
+                for (int l = 0; l < 3; l++) t += Bm[k][l] * Cm[l][j];
+                R.m[i][j] += A[i][k] * t;
+            }
+        }
+    return R;
+}
+
+void gauss_legendre(int n, std::vector<double>& nodes, std::vector<double>& weights) {
+    nodes.assign(n, 0.0);
+    weights.assign(n, 0.0);
+    bem_gauss_legendre(n, nodes.data(), weights.data());
+}
+
+std::vector<Orientation> generate_orientations(int n_alpha, int n_beta, int n_gamma, int beta_sym, int gamma_sym,
+                                               bool gamma_mirror) {
+    int cnt = 0;
+    std::vector<Orientation> out;
+    if (bem_orientations(n_alpha, n_beta, n_gamma, beta_sym, gamma_sym, gamma_mirror, 0, &cnt, nullptr, nullptr) !=
+        BEM_OK)
+        return out;
+    std::vector<double> RT(9 * (size_t)cnt), w(cnt);
+    bem_orientations(n_alpha, n_beta, n_gamma, beta_sym, gamma_sym, gamma_mirror, 0, &cnt, RT.data(), w.data());
+    out.resize(cnt);
+    for (int o = 0; o < cnt; o++) {
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) out[o].RT.m[i][j] = RT[9 * o + 3 * i + j];
+        out[o].weight = w[o];
+    }
+    return out;
+}
+
+void sort_orientations_nearest(std::vector<Orientation>& orients) {
+    // greedy nearest neighbour in Frobenius distance from orientation 0
+    // (orient.cpp:127-163)
+    int n = (int)orients.size();
+    if (n <= 2) return;
+    std::vector<char> used(n, 0);
+    std::vector<Orientation> s;
+    s.push_back(orients[0]);
+    used[0] = 1;
+    for (int step = 1; step < n; step++) {
+        const Mat3& P = s.back().RT;
+        int best = -1;
+        double bd = 1e30;
+        for (int j = 0; j < n; j++) {
+            if (used[j]) continue;
+            double d = 0;
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) {
+                    double df = P.m[r][c] - orients[j].RT.m[r][c];
+                    d += df * df;
+                }
+            if (d < bd) bd = d, best = j;
+        }
+        s.push_back(orients[best]);
+        used[best] = 1;
+    }
+    orients = s;
+}
+
+// -------------------------------------------------------------- farfield.h
+void FFCache::init(const RWG& rwg, const Mesh& mesh, int order) {
+    TriQuad q = tri_quadrature(order);
+    N = rwg.N;
+    Nq = q.npts;
+    quad_order = (order == 4 || order == 13) ? order : 7;
+    flatten(mesh, mesh_verts);
+    mesh_tris = mesh.tris;
+    int total = 2 * N * Nq;
+    qpts.assign(3 * (size_t)total, 0.0);
+    fvals.assign(3 * (size_t)total, 0.0);
+    jw.assign(total, 0.0);
+    for (int h = 0; h < 2; h++) {
+        int sign = h == 0 ? 1 : -1;
+        for (int n = 0; n < N; n++) {
+            int ti = h == 0 ? rwg.tri_p[n] : rwg.tri_m[n];
+            Vec3 fr = h == 0 ? rwg.free_p[n] : rwg.free_m[n];
+            double area = h == 0 ? rwg.area_p[n] : rwg.area_m[n];
+            double c = sign * rwg.length[n] / (2.0 * area);
+            Vec3 v0, v1, v2;
+            mesh.tri_verts(ti, v0, v1, v2);
+            for (int k = 0; k < Nq; k++) {
+                double l1 = q.pts[k][0], l2 = q.pts[k][1], l0 = 1.0 - l1 - l2;
+                Vec3 r = v0 * l0 + v1 * l1 + v2 * l2;
+                Vec3 f = (r - fr) * c;
+                size_t i = (size_t)(h * N + n) * Nq + k;
+                qpts[3 * i] = r.x, qpts[3 * i + 1] = r.y, qpts[3 * i + 2] = r.z;
+                fvals[3 * i] = f.x, fvals[3 * i + 1] = f.y, fvals[3 * i + 2] = f.z;
+                jw[i] = area * q.wts[k];
+            }
+        }
+    }
+}
+
+// The device copy is the library's own geometry (same RWG order: the cache
+// was made from build_rwg of this mesh).
+void FFCacheGPU::upload(const FFCache& cache) {
+    N = cache.N;
+    Nq = cache.Nq;
+    int nv = (int)cache.mesh_verts.size() / 3, nt = (int)cache.mesh_tris.size() / 3, Ng = 0;
+    bem_geom* g = nullptr;
+    check(bem_geom_create(ctx(), cache.mesh_verts.data(), nv, cache.mesh_tris.data(), nt, cache.quad_order, &g, &Ng),
+          "FFCacheGPU::upload");
+    if (Ng != N) {
+        std::fprintf(stderr, "FFCacheGPU::upload: RWG count %d differs from the cache (%d)\n", Ng, N);
+        std::exit(1);
+    }
+    geom = g;
+    initialized = true;
+    std::printf("  FFCacheGPU: uploaded %d quad points (%.1f MB)\n", 2 * N * Nq,
+                (2.0 * N * Nq * 7.0 * sizeof(double)) / (1024.0 * 1024.0));
+}
+
+void FFCacheGPU::free() {
+    if (initialized && geom) bem_geom_free((bem_geom*)geom);
+    geom = nullptr;
+    initialized = false;
+}
+
+FFCacheGPU::~FFCacheGPU() { free(); }
+
+void compute_farfield_batch_cuda(const FFCacheGPU& gpu_cache, const std::complex<double>* coeffs_J,
+                                 const std::complex<double>* coeffs_M, const double* r_hats,
+                                 std::complex<double> k_ext, double eta_ext, int n_calls, int n_orient, int ndir,
+                                 std::complex<double>* Fv_out) {
+    Timer t;
+    check(bem_farfield_batch(ctx(), (const bem_geom*)gpu_cache.geom, reinterpret_cast<const double*>(coeffs_J),
+                             reinterpret_cast<const double*>(coeffs_M), r_hats, k_ext.real(), k_ext.imag(), eta_ext,
+                             n_calls, n_orient, ndir, reinterpret_cast<double*>(Fv_out)),
+          "compute_farfield_batch_cuda");
+    std::printf("  GPU far-field (%d calls x %d dirs): %.2fs\n", n_calls, ndir, t.elapsed_s());
+}
+
+void compute_far_field_vec_batch_cpu(const FFCache& cache, const std::complex<double>* coeffs_J,
+                                     const std::complex<double>* coeffs_M, std::complex<double> k_ext,
+                                     double eta_ext, const Vec3* r_hats, int ndir, std::complex<double>* Fv_out) {
+    // same result on the device: one call, the perp slot carries zero coefficients
+    FFCacheGPU gc;
+    gc.upload(cache);
+    std::vector<std::complex<double>> J(2 * (size_t)cache.N), M(2 * (size_t)cache.N);
+    std::memcpy(J.data(), coeffs_J, cache.N * sizeof(std::complex<double>));
+    std::memcpy(M.data(), coeffs_M, cache.N * sizeof(std::complex<double>));
+    std::vector<double> rh(3 * (size_t)ndir);
+    for (int d = 0; d < ndir; d++) rh[3 * d] = r_hats[d].x, rh[3 * d + 1] = r_hats[d].y, rh[3 * d + 2] = r_hats[d].z;
+    std::vector<std::complex<double>> Fv(2 * (size_t)ndir * 3);
+    check(bem_farfield_batch(ctx(), (const bem_geom*)gc.geom, reinterpret_cast<const double*>(J.data()),
+                             reinterpret_cast<const double*>(M.data()), rh.data(), k_ext.real(), k_ext.imag(), eta_ext,
+                             2, 1, ndir, reinterpret_cast<double*>(Fv.data())),
+          "compute_far_field_vec_batch_cpu");
+    std::memcpy(Fv_out, Fv.data(), (size_t)ndir * 3 * sizeof(std::complex<double>));
+}
+
+void compute_far_field(const FFCache& cache, const std::complex<double>* coeffs_J,
+                       const std::complex<double>* coeffs_M, std::complex<double> k_ext, double eta_ext,
+                       const double* theta_arr, int ntheta, std::complex<double>* F_theta,
+                       std::complex<double>* F_phi) {
+    // phi = 0 scattering plane (farfield.cu:435-460)
+    std::vector<Vec3> rh(ntheta);
+    for (int i = 0; i < ntheta; i++) rh[i] = Vec3(std::sin(theta_arr[i]), 0.0, std::cos(theta_arr[i]));
+    std::vector<std::complex<double>> Fv(3 * (size_t)ntheta);
+    compute_far_field_vec_batch_cpu(cache, coeffs_J, coeffs_M, k_ext, eta_ext, rh.data(), ntheta, Fv.data());
+    for (int i = 0; i < ntheta; i++) {
+        double ct = std::cos(theta_arr[i]), st = std::sin(theta_arr[i]);
+        F_theta[i] = Fv[3 * i] * ct + Fv[3 * i + 2] * (-st);
+        F_phi[i] = Fv[3 * i + 1];
+    }
+}
+
+void amplitude_to_mueller(const std::complex<double>* S1, const std::complex<double>* S2,
+                          const std::complex<double>* S3, const std::complex<double>* S4, int ntheta, double* M) {
+    bem_amplitude_to_mueller(reinterpret_cast<const double*>(S1), reinterpret_cast<const double*>(S2),
+                             reinterpret_cast<const double*>(S3), reinterpret_cast<const double*>(S4), ntheta, M);
+}
+
+// ---------------------------------------------------------------- output.h
+// JSON layout of output.cpp:5-64 (theta in degrees "%.4f", Mueller "%.8e").
+void write_json(const char* filename, const double* M, const double* theta, int ntheta, double ka, double n_re,
+                double n_im, int refinements, int n_alpha, int n_beta, int n_gamma, double time_assembly,
+                double time_solve, double time_farfield, double time_total) {
+    FILE* f = std::fopen(filename, "w");
+    if (!f) {
+        std::fprintf(stderr, "Cannot open %s for writing\n", filename);
+        return;
+    }
+    std::fprintf(f, "{\n  \"ka\": %.6f,\n  \"ri\": [%.6f, %.6f],\n  \"refinements\": %d,\n", ka, n_re, n_im,
+                 refinements);
+    std::fprintf(f, "  \"orient\": [%d, %d, %d],\n  \"ntheta\": %d,\n", n_alpha, n_beta, n_gamma, ntheta);
+    std::fprintf(f,
+                 "  \"timing\": {\n    \"assembly_s\": %.2f,\n    \"solve_s\": %.2f,\n    \"farfield_s\": %.2f,\n"
+                 "    \"total_s\": %.2f\n  },\n",
+                 time_assembly, time_solve, time_farfield, time_total);
+    std::fprintf(f, "  \"theta\": [");
+    for (int t = 0; t < ntheta; t++) std::fprintf(f, t + 1 < ntheta ? "%.4f, " : "%.4f", theta[t] * 180.0 / M_PI);
+    std::fprintf(f, "],\n  \"mueller\": [\n");
+    for (int i = 0; i < 4; i++) {
+        std::fprintf(f, "    [\n");
+        for (int j = 0; j < 4; j++) {
+            std::fprintf(f, "      [");
+            for (int t = 0; t < ntheta; t++)
+                std::fprintf(f, t + 1 < ntheta ? "%.8e, " : "%.8e", M[(i * 4 + j) * ntheta + t]);
+            std::fprintf(f, j < 3 ? "],\n" : "]\n");
+        }
+        std::fprintf(f, i < 3 ? "    ],\n" : "    ]\n");
+    }
+    std::fprintf(f, "  ]\n}\n");
+    std::fclose(f);
+    std::printf("Results written to %s\n", filename);
+}

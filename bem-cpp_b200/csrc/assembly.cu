@@ -570,11 +570,17 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
     a.ld = ldz;
     int64_t ntiles = (int64_t)a.ntile * (a.ntile + 1) / 2;
     if (ntiles > 0x7fffffffLL) return fail(ctx, BEM_ERR_INVALID, "too many tiles");
+    cudaEvent_t ev = ctx->prof_begin(PROF_ASSEMBLY);
     if (mode == 2)
         assemble_kernel<2><<<(unsigned)ntiles, 256, 0, st>>>(a);
     else
         assemble_kernel<1><<<(unsigned)ntiles, 256, 0, st>>>(a);
     BEM_LAUNCHED(ctx);
+    // algorithmic unit: one quadrature-pair evaluation per medium, every
+    // ordered RWG pair (no symmetry credit): 64 flop + sincos + exp each
+    if (ev)
+        ctx->prof_end(PROF_ASSEMBLY, ev, 64.0 * mode * 4.0 * N * (double)N * g->Nq * g->Nq,
+                      (mode == 2 ? 64.0 : 32.0) * (double)N * N);
     // 3. singular correction
     if (g->sing.npairs > 0) {
         FixArgs f;
@@ -638,6 +644,52 @@ int bem_geom_create(bem_ctx* ctx, const double* verts, int nv, const int* tris, 
     }
     *out = g;
     if (N) *N = g->N;
+    return BEM_OK;
+}
+
+int bem_geom_create_rwg(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt, int N,
+                        const int* tri_p, const int* tri_m, const double* free_p, const double* free_m,
+                        const double* length, const double* area_p, const double* area_m, int quad_order,
+                        bem_geom** out) {
+    if (!ctx || !out || N < 1 || !tri_p || !tri_m || !free_p || !free_m || !length || !area_p || !area_m)
+        return BEM_ERR_INVALID;
+    *out = nullptr;
+    bem_geom* g = new bem_geom();
+    g->ctx = ctx;
+    g->device = ctx->device;
+    if (!host_mesh_from(verts, nv, tris, nt, &g->mesh) || !quadrature(quad_order, &g->quad)) {
+        delete g;
+        return fail(ctx, BEM_ERR_INVALID, "bad mesh arrays or quadrature order");
+    }
+    HostRWG& r = g->rwg;
+    r.N = N;
+    for (int n = 0; n < N; n++) {
+        if (tri_p[n] < 0 || tri_p[n] >= nt || tri_m[n] < 0 || tri_m[n] >= nt) {
+            delete g;
+            return fail(ctx, BEM_ERR_INVALID, "RWG %d refers to a missing triangle", n);
+        }
+        r.tri_p.push_back(tri_p[n]);
+        r.tri_m.push_back(tri_m[n]);
+        r.vfree_p.push_back(-1);
+        r.vfree_m.push_back(-1);
+        r.free_p.push_back({free_p[3 * n], free_p[3 * n + 1], free_p[3 * n + 2]});
+        r.free_m.push_back({free_m[3 * n], free_m[3 * n + 1], free_m[3 * n + 2]});
+        r.length.push_back(length[n]);
+        r.area_p.push_back(area_p[n]);
+        r.area_m.push_back(area_m[n]);
+    }
+    g->quad_order = quad_order;
+    g->N = N;
+    g->Nq = g->quad.n;
+    g->nv = nv;
+    g->nt = nt;
+    int s = cudaSetDevice(ctx->device) == cudaSuccess ? geom_upload(ctx, g) : BEM_ERR_CUDA;
+    if (s != BEM_OK) {
+        if (g->dmem) cudaFree(g->dmem);
+        delete g;
+        return s;
+    }
+    *out = g;
     return BEM_OK;
 }
 

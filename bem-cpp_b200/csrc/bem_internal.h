@@ -109,8 +109,38 @@ struct DevSingular {
 
 }  // namespace bem
 
+// Per-kernel-class timing (CUDA events around the launches of one class on
+// the context's stream), enabled by bem_ctx_profile.
+enum ProfClass {
+    PROF_LU_UPDATE = 0,    // trailing update GEMM of the factorisation
+    PROF_SOLVE_UPDATE = 1, // block updates of the triangular solves
+    PROF_RESIDUAL = 2,     // FP64 refinement residual B - Z X
+    PROF_PANEL = 3,        // panel factorisation kernels
+    PROF_ASSEMBLY = 4,     // PMCHWT assembly kernel
+    PROF_FARFIELD = 5,     // far-field / Mueller kernel
+    PROF_NCLASS = 6
+};
+
+struct ProfPending {
+    int cls;
+    cudaEvent_t a, b;
+    double flops, bytes;
+};
+
 struct bem_ctx {
     int device = 0;
+    bool use_tc = true;  // FP32 updates on the tensor cores (else CUDA cores)
+    float* tc_buf = nullptr;  // packed hi/lo operands of the tensor-core GEMM
+    size_t tc_bytes = 0;
+    bool tc_attr = false;
+    bool prof = false;
+    std::vector<ProfPending> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    int64_t prof_launches[PROF_NCLASS] = {0};
+    double prof_ms[PROF_NCLASS] = {0}, prof_flops[PROF_NCLASS] = {0}, prof_bytes[PROF_NCLASS] = {0};
+    cudaEvent_t prof_begin(int cls);
+    void prof_end(int cls, cudaEvent_t a, double flops, double bytes);
+    int prof_collect();
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     int sm_count = 148;

@@ -5,10 +5,10 @@
 // (B[k*ldb + j]).  C is row-major (C[i*ldc + j]) or column-major
 // (C[j*ldc + i]).  Complex values are interleaved (double2 / float2).
 //
-// Tiling: 64 x 64 complex outputs per 256-thread CTA, 4 x 4 per thread,
-// K in steps of BK staged through shared memory (double buffered, register
-// prefetch of the next step).  A and B are stored k-outer in shared memory so
-// each thread reads its 4 rows / 4 columns as consecutive complex values.
+// Tiling: 64 x 64 complex outputs per 256-thread CTA, 4 x 4 per thread
+// (rows ty + 16 i, columns tx + 16 j, so a warp's shared-memory reads of a
+// k-slice touch consecutive 16-byte words), K in steps of BK staged through
+// shared memory (double buffered, register prefetch of the next step).
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -97,9 +97,9 @@ cgemm_simt_kernel(int M, int N, int K, const typename C2T<R>::type* __restrict__
         for (int kk = 0; kk < BK; kk++) {
             C2 a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) a[i] = As[buf][kk][ty * 4 + i];
+            for (int i = 0; i < 4; i++) a[i] = As[buf][kk][ty + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bs[buf][kk][tx * 4 + j];
+            for (int j = 0; j < 4; j++) b[j] = Bs[buf][kk][tx + 16 * j];
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -112,11 +112,11 @@ cgemm_simt_kernel(int M, int N, int K, const typename C2T<R>::type* __restrict__
     const bool has_beta = (beta.x != 0 || beta.y != 0);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        int gi = m0 + ty * 4 + i;
+        int gi = m0 + ty + 16 * i;
         if (gi >= M) continue;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            int gj = n0 + tx * 4 + j;
+            int gj = n0 + tx + 16 * j;
             if (gj >= N) continue;
             int64_t idx = C_COLMAJOR ? (int64_t)gj * ldc + gi : (int64_t)gi * ldc + gj;
             C2 v;

@@ -20,6 +20,54 @@ int fail(bem_ctx* ctx, int status, const char* fmt, ...) {
 
 }  // namespace bem
 
+cudaEvent_t bem_ctx::prof_begin(int cls) {
+    (void)cls;
+    if (!prof) return nullptr;
+    cudaEvent_t e;
+    if (!prof_pool.empty()) {
+        e = prof_pool.back();
+        prof_pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaEventRecord(e, stream);
+    return e;
+}
+
+void bem_ctx::prof_end(int cls, cudaEvent_t a, double flops, double bytes) {
+    if (!prof || !a) return;
+    cudaEvent_t b;
+    if (!prof_pool.empty()) {
+        b = prof_pool.back();
+        prof_pool.pop_back();
+    } else if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaGetLastError();
+        prof_pool.push_back(a);
+        return;
+    }
+    cudaEventRecord(b, stream);
+    prof_pending.push_back({cls, a, b, flops, bytes});
+    if (prof_pending.size() > 4096) prof_collect();
+}
+
+int bem_ctx::prof_collect() {
+    if (prof_pending.empty()) return BEM_OK;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return BEM_ERR_CUDA;
+    for (auto& p : prof_pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        prof_launches[p.cls]++;
+        prof_ms[p.cls] += ms;
+        prof_flops[p.cls] += p.flops;
+        prof_bytes[p.cls] += p.bytes;
+        prof_pool.push_back(p.a);
+        prof_pool.push_back(p.b);
+    }
+    prof_pending.clear();
+    return BEM_OK;
+}
+
 int bem_ctx::ensure_ws(size_t bytes) {
     if (bytes <= ws_bytes) return BEM_OK;
     if (ws) cudaFree(ws);
@@ -73,7 +121,10 @@ int bem_ctx_destroy(bem_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->ws) cudaFree(ctx->ws);
+    if (ctx->tc_buf) cudaFree(ctx->tc_buf);
     if (ctx->d_status) cudaFree(ctx->d_status);
+    for (auto& p : ctx->prof_pending) cudaEventDestroy(p.a), cudaEventDestroy(p.b);
+    for (auto e : ctx->prof_pool) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return BEM_OK;
@@ -95,5 +146,33 @@ int bem_ctx_synchronize(bem_ctx* ctx) {
 const char* bem_last_error(const bem_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
 int64_t bem_ctx_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int bem_ctx_set_tensor_cores(bem_ctx* ctx, int enable) {
+    if (!ctx) return BEM_ERR_INVALID;
+    ctx->use_tc = enable != 0;
+    return BEM_OK;
+}
+
+int bem_ctx_profile(bem_ctx* ctx, int enable) {
+    if (!ctx) return BEM_ERR_INVALID;
+    int s = ctx->prof_collect();
+    if (enable) {
+        for (int i = 0; i < PROF_NCLASS; i++)
+            ctx->prof_launches[i] = 0, ctx->prof_ms[i] = ctx->prof_flops[i] = ctx->prof_bytes[i] = 0;
+    }
+    ctx->prof = enable != 0;
+    return s;
+}
+
+int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
+                         double* bytes) {
+    if (!ctx || cls < 0 || cls >= PROF_NCLASS) return BEM_ERR_INVALID;
+    int s = ctx->prof_collect();
+    if (launches) *launches = ctx->prof_launches[cls];
+    if (ms) *ms = ctx->prof_ms[cls];
+    if (flops) *flops = ctx->prof_flops[cls];
+    if (bytes) *bytes = ctx->prof_bytes[cls];
+    return s;
+}
 
 }  // extern "C"

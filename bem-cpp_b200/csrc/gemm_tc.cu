@@ -1,7 +1,436 @@
-// 3xTF32 complex GEMM on the fifth-generation tensor cores (tcgen05).
-// (placeholder: hooks disabled until the tensor-core kernel lands)
+// 3xTF32 complex GEMM on the fifth-generation tensor cores (tcgen05 + TMA +
+// TMEM), used for the big updates of the FP32 factorisation and solves:
+//
+//   C -= A * B      A: M x K complex (K contiguous), B: K x N complex,
+//                   C: M x N complex64, row-major (LU) or column-major (solves)
+//
+// The complex product is written as one real GEMM over interleaved columns:
+//   C'[i, 2j+{0,1}] -= sum_k' A'[i, k'] B'[2j+{0,1}, k']
+// with A'[i, 2k] = Re a_ik, A'[i, 2k+1] = Im a_ik (the raw float layout of a
+// complex row) and B' rows (Re b, -Im b) / (Im b, Re b) interleaved over k.
+// Every operand is split x = hi + lo with hi, lo rounded to TF32 and the
+// product taken as hi*hi + hi*lo + lo*hi, accumulated in FP32 in TMEM.
+//
+// Pack kernels write the hi / lo operands K-major; the GEMM kernel streams
+// 128 x 32 (A) and 256 x 32 (B) float tiles with TMA (128-byte swizzle, no
+// multicast) through a 2-stage mbarrier pipeline; one thread issues
+// tcgen05.mma (M=128, N=256, K=8) into a 128 x 256 FP32 TMEM accumulator; four
+// warps read it back with tcgen05.ld and apply C -= acc.  Every wait is
+// bounded (~1 s of clock cycles): on expiry the kernel records
+// BEM_ERR_TIMEOUT in the status word, frees its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+
+#include "bem_internal.h"
 #include "lu_internal.h"
 
 namespace bem {
-TrailingUpdate<float> tc_update_fp32(bem_ctx*) { return TrailingUpdate<float>(); }
+
+namespace tc {
+
+constexpr int BM = 128;       // rows per tile
+constexpr int BN = 256;       // real columns per tile (128 complex)
+constexpr int BK = 32;        // floats of K per stage (one 128-byte swizzle row)
+constexpr int STAGES = 2;
+constexpr int A_BYTES = BM * BK * 4;   // 16 KB
+constexpr int B_BYTES = BN * BK * 4;   // 32 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // hi + lo of each: 96 KB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr uint32_t TMEM_COLS = 256;
+constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase; false (and the status word set) on expiry
+// or when another thread of the CTA already gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* status, volatile int* abort_flag) {
+    long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > WAIT_CYCLES) {
+            atomicCAS(status, 0, (int)BEM_ERR_TIMEOUT);
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// K-major operand tile with 128-byte swizzle: rows of 128 B, 8-row groups
+// 1024 B apart (SBO), LBO unused (1), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (16 B units), unused for SW128 K-major
+    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                 // descriptor version (Blackwell)
+    d |= (uint64_t)2 << 61;                 // layout: SWIZZLE_128B
+    return d;
+}
+
+// kind::tf32, FP32 accumulate, A and B K-major, M = 128, N = 256.
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// C (complex64) -= A' B'^T over one 128 x 256 tile.  c_colmajor: C[j*ldc + i].
+__global__ void __launch_bounds__(128, 1)
+gemm_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+            const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
+            float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);  // full[S], empty[S], accum
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 1);
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nk = (K2 + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(smem_u32(&bars[s]), 1);
+            mbar_init(smem_u32(&bars[STAGES + s]), 1);
+        }
+        mbar_init(smem_u32(&bars[2 * STAGES]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (threadIdx.x == 0) {
+        // TMA producer
+        for (int kt = 0; kt < nk; kt++) {
+            const int s = kt % STAGES;
+            if (kt >= STAGES && !mbar_wait(smem_u32(&bars[STAGES + s]), ((kt / STAGES) - 1) & 1, status, &abort_flag))
+                break;
+            unsigned char* st = smem + s * STAGE_BYTES;
+            const uint32_t full = smem_u32(&bars[s]);
+            mbar_expect_tx(full, STAGE_BYTES);
+            tma_load_2d(smem_u32(st), &tA_hi, kt * BK, m0, full);
+            tma_load_2d(smem_u32(st + A_BYTES), &tA_lo, kt * BK, m0, full);
+            tma_load_2d(smem_u32(st + 2 * A_BYTES), &tB_hi, kt * BK, n0, full);
+            tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tB_lo, kt * BK, n0, full);
+        }
+    } else if (threadIdx.x == 32) {
+        // MMA issuer
+        bool ok = true;
+        for (int kt = 0; kt < nk && ok; kt++) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(smem_u32(&bars[s]), (kt / STAGES) & 1, status, &abort_flag)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            unsigned char* st = smem + s * STAGE_BYTES;
+            const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + A_BYTES);
+            const uint32_t b_hi = smem_u32(st + 2 * A_BYTES), b_lo = smem_u32(st + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+            for (int ks = 0; ks < BK / 8; ks++) {
+                // advance 8 floats (32 B) along K inside the swizzle row
+                const uint32_t off = ks * 32;
+                const uint64_t dah = smem_desc(a_hi + off), dal = smem_desc(a_lo + off);
+                const uint64_t dbh = smem_desc(b_hi + off), dbl = smem_desc(b_lo + off);
+                mma_tf32(tmem, dah, dbh, (kt > 0 || ks > 0) ? 1u : 0u);
+                mma_tf32(tmem, dah, dbl, 1u);
+                mma_tf32(tmem, dal, dbh, 1u);
+            }
+            mma_commit(smem_u32(&bars[STAGES + s]));  // stage s free once these MMAs read it
+        }
+        mma_commit(smem_u32(&bars[2 * STAGES]));      // accumulator ready
+    }
+    __syncwarp();
+
+    // epilogue: 4 warps x 32 TMEM lanes = 128 rows
+    bool ok = mbar_wait(smem_u32(&bars[2 * STAGES]), 0, status, &abort_flag);
+    ok = __all_sync(0xffffffffu, ok);
+    if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int ch = 0; ch < BN / 32; ch++) {
+            float v[32];
+            tmem_ld32(lane_base + ch * 32, v);
+            if (row < M) {
+                const int c0 = (n0 >> 1) + ch * 16;
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    const int col = c0 + j;
+                    if (col < Nc) {
+                        float2* p = c_colmajor ? &C[(int64_t)col * ldc + row] : &C[(int64_t)row * ldc + col];
+                        float2 c = *p;
+                        c.x -= v[2 * j];
+                        c.y -= v[2 * j + 1];
+                        *p = c;
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// ---------------------------------------------------------------- packing
+// A (complex, K contiguous): hi/lo[i*ld + 2k + {0,1}] = split(Re/Im a_ik), zero padded
+__global__ void pack_a_kernel(const float2* __restrict__ A, int64_t lda, int M, int K, float* __restrict__ hi,
+                              float* __restrict__ lo, int ld) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t tot = (int64_t)M * (ld / 2);
+    if (t >= tot) return;
+    int i = (int)(t / (ld / 2)), k = (int)(t % (ld / 2));
+    float2 a = k < K ? A[(int64_t)i * lda + k] : make_float2(0.f, 0.f);
+    float h0 = to_tf32(a.x), h1 = to_tf32(a.y);
+    float l0 = to_tf32(a.x - h0), l1 = to_tf32(a.y - h1);
+    reinterpret_cast<float2*>(hi + (int64_t)i * ld)[k] = make_float2(h0, h1);
+    reinterpret_cast<float2*>(lo + (int64_t)i * ld)[k] = make_float2(l0, l1);
+}
+
+// B given column-major (B[j*ldb + k], K contiguous): rows 2j, 2j+1 of B'.
+__global__ void pack_b_col_kernel(const float2* __restrict__ B, int64_t ldb, int N, int K, float* __restrict__ hi,
+                                  float* __restrict__ lo, int ld) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t tot = (int64_t)N * (ld / 2);
+    if (t >= tot) return;
+    int j = (int)(t / (ld / 2)), k = (int)(t % (ld / 2));
+    float2 b = k < K ? B[(int64_t)j * ldb + k] : make_float2(0.f, 0.f);
+    float hr = to_tf32(b.x), hi_ = to_tf32(b.y);
+    float lr = to_tf32(b.x - hr), li = to_tf32(b.y - hi_);
+    float2* r0h = reinterpret_cast<float2*>(hi + (int64_t)(2 * j) * ld);
+    float2* r1h = reinterpret_cast<float2*>(hi + (int64_t)(2 * j + 1) * ld);
+    float2* r0l = reinterpret_cast<float2*>(lo + (int64_t)(2 * j) * ld);
+    float2* r1l = reinterpret_cast<float2*>(lo + (int64_t)(2 * j + 1) * ld);
+    r0h[k] = make_float2(hr, -hi_);
+    r1h[k] = make_float2(hi_, hr);
+    r0l[k] = make_float2(lr, -li);
+    r1l[k] = make_float2(li, lr);
+}
+
+// B given row-major (B[k*ldb + j], N contiguous): transposed through shared memory.
+__global__ void pack_b_row_kernel(const float2* __restrict__ B, int64_t ldb, int N, int K, float* __restrict__ hi,
+                                  float* __restrict__ lo, int ld) {
+    __shared__ float2 tile[32][33];
+    const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 256 threads: 8 rows per pass
+    for (int r = ty; r < 32; r += 8) {
+        int k = k0 + r, j = j0 + tx;
+        tile[r][tx] = (k < K && j < N) ? B[(int64_t)k * ldb + j] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        int j = j0 + r, k = k0 + tx;
+        if (j >= N || k >= ld / 2) continue;
+        float2 b = tile[tx][r];
+        float hr = to_tf32(b.x), hi_ = to_tf32(b.y);
+        float lr = to_tf32(b.x - hr), li = to_tf32(b.y - hi_);
+        reinterpret_cast<float2*>(hi + (int64_t)(2 * j) * ld)[k] = make_float2(hr, -hi_);
+        reinterpret_cast<float2*>(hi + (int64_t)(2 * j + 1) * ld)[k] = make_float2(hi_, hr);
+        reinterpret_cast<float2*>(lo + (int64_t)(2 * j) * ld)[k] = make_float2(lr, -li);
+        reinterpret_cast<float2*>(lo + (int64_t)(2 * j + 1) * ld)[k] = make_float2(li, lr);
+    }
+}
+
+}  // namespace tc
+
+// ---------------------------------------------------------------- host side
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static int tc_encode_init(bem_ctx* ctx) {
+    if (g_encode) return BEM_OK;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    BEM_TRY_CUDA(ctx, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn)
+        return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    return BEM_OK;
+}
+
+static int make_map(bem_ctx* ctx, CUtensorMap* map, float* base, int rows, int ld, int box_rows) {
+    cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return BEM_OK;
+}
+
+// C -= A * B on the tensor cores.  b_rowmajor: B[k*ldb + j] (U12 block),
+// else B[j*ldb + k].  c_colmajor: C[j*ldc + i], else C[i*ldc + j].
+static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, const float2* B, int64_t ldb,
+                   bool b_rowmajor, float2* C, int64_t ldc, bool c_colmajor, int prof_cls) {
+    if (M <= 0 || N <= 0 || K <= 0) return BEM_OK;
+    BEM_TRY(tc_encode_init(ctx));
+    // K-major operand rows padded to a multiple of 32 floats (128 B)
+    const int ld = ((2 * K + tc::BK - 1) / tc::BK) * tc::BK;
+    size_t a_elems = (size_t)M * ld, b_elems = (size_t)2 * N * ld;
+    size_t need = 2 * (a_elems + b_elems) * sizeof(float) + 1024;
+    if (need > ctx->tc_bytes) {
+        if (ctx->tc_buf) {
+            BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            cudaFree(ctx->tc_buf);
+        }
+        ctx->tc_buf = nullptr;
+        ctx->tc_bytes = 0;
+        BEM_TRY_CUDA(ctx, cudaMalloc(&ctx->tc_buf, need));
+        ctx->tc_bytes = need;
+    }
+    float* a_hi = ctx->tc_buf;
+    float* a_lo = a_hi + a_elems;
+    float* b_hi = a_lo + a_elems;
+    float* b_lo = b_hi + b_elems;
+    cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
+    {
+        int64_t tot = (int64_t)M * (ld / 2);
+        tc::pack_a_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, M, K, a_hi, a_lo, ld);
+        BEM_LAUNCHED(ctx);
+    }
+    if (b_rowmajor) {
+        dim3 g((N + 31) / 32, (ld / 2 + 31) / 32);
+        tc::pack_b_row_kernel<<<g, 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld);
+    } else {
+        int64_t tot = (int64_t)N * (ld / 2);
+        tc::pack_b_col_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld);
+    }
+    BEM_LAUNCHED(ctx);
+    CUtensorMap mah, mal, mbh, mbl;
+    BEM_TRY(make_map(ctx, &mah, a_hi, M, ld, tc::BM));
+    BEM_TRY(make_map(ctx, &mal, a_lo, M, ld, tc::BM));
+    BEM_TRY(make_map(ctx, &mbh, b_hi, 2 * N, ld, tc::BN));
+    BEM_TRY(make_map(ctx, &mbl, b_lo, 2 * N, ld, tc::BN));
+    if (!ctx->tc_attr) {
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               tc::SMEM_BYTES));
+        ctx->tc_attr = true;
+    }
+    dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
+    if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");
+    tc::gemm_kernel<<<grid, 128, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc, c_colmajor ? 1 : 0, M,
+                                                                 N, ld, ctx->d_status);
+    BEM_LAUNCHED(ctx);
+    if (ev)
+        ctx->prof_end(prof_cls, ev, 8.0 * M * (double)N * K,
+                      8.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
+    return BEM_OK;
+}
+
+static int tc_lu_update(bem_ctx* ctx, void*, int M, int N, int K, const float2* A, int64_t lda, const float2* B,
+                        int64_t ldb, float2* C, int64_t ldc) {
+    return tc_gemm(ctx, M, N, K, A, lda, B, ldb, true, C, ldc, false, PROF_LU_UPDATE);
+}
+
+static int tc_solve_update(bem_ctx* ctx, void*, int M, int N, int K, const float2* A, int64_t lda, const float2* B,
+                           int64_t ldb, float2* C, int64_t ldc) {
+    return tc_gemm(ctx, M, N, K, A, lda, B, ldb, false, C, ldc, true, PROF_SOLVE_UPDATE);
+}
+
+TrailingUpdate<float> tc_update_fp32(bem_ctx* ctx) {
+    TrailingUpdate<float> t;
+    if (ctx && ctx->use_tc) {
+        t.fn = tc_lu_update;
+        t.fn_solve = tc_solve_update;
+    }
+    return t;
+}
+
 }  // namespace bem
+
+extern "C" int bem_cgemm_tf32x3(bem_ctx* ctx, int M, int N, int K, const void* A, int64_t lda, const void* B,
+                                int64_t ldb, int b_rowmajor, void* C, int64_t ldc, int c_colmajor) {
+    if (!ctx || !A || !B || !C) return BEM_ERR_INVALID;
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    BEM_TRY(bem::tc_gemm(ctx, M, N, K, (const float2*)A, lda, (const float2*)B, ldb, b_rowmajor != 0, (float2*)C,
+                         ldc, c_colmajor != 0, -1));
+    int st = 0;
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return st == 0 ? BEM_OK : bem::fail(ctx, st, "tensor-core GEMM: a bounded wait expired");
+}

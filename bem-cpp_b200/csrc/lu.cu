@@ -36,7 +36,7 @@ template <typename R>
 int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int64_t lda,
           const typename C2T<R>::type* B, int64_t ldb, bool b_kmajor,
           typename C2T<R>::type* C, int64_t ldc, bool c_colmajor,
-          typename C2T<R>::type alpha, typename C2T<R>::type beta) {
+          typename C2T<R>::type alpha, typename C2T<R>::type beta, int prof_cls) {
     if (M <= 0 || N <= 0) return BEM_OK;
     if (K <= 0) {
         // C = beta*C only; our callers never need it with beta != 1
@@ -44,6 +44,7 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
     }
     dim3 grid((N + 63) / 64, (M + 63) / 64);
     if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "gemm M too large");
+    cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
     if (b_kmajor) {
         if (c_colmajor)
             cgemm_simt_kernel<R, true, true><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
@@ -56,6 +57,9 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
             cgemm_simt_kernel<R, false, false><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
     }
     BEM_LAUNCHED(ctx);
+    if (ev)
+        ctx->prof_end(prof_cls, ev, 8.0 * M * N * K,
+                      (double)sizeof(typename C2T<R>::type) * ((double)M * K + (double)K * N + 2.0 * M * N));
     return BEM_OK;
 }
 
@@ -430,9 +434,11 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
             BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
             void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
                             &d_ipiv, &d_info, &pw};
+            cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
             BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G), dim3(256),
                                                           args, smem, ctx->stream));
             BEM_LAUNCHED(ctx);
+            if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2, (double)nrows * iw * 2 * sizeof(C2));
             // interchanges on the rest of this block column
             int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
             int ncol = (ca1 - ca0) + (cb1 - cb0);
@@ -466,7 +472,7 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
             else
                 BEM_TRY(cgemm<R>(ctx, Mt, Mt, jb, A + (int64_t)c0 * lda + j0, lda, A + (int64_t)j0 * lda + c0,
                                  lda, false, A + (int64_t)c0 * lda + c0, lda, false, mk<C2>(-1, 0),
-                                 mk<C2>(1, 0)));
+                                 mk<C2>(1, 0), PROF_LU_UPDATE));
         }
     }
     return BEM_OK;
@@ -508,7 +514,7 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
                                      X + j0, ldx, X + j0 + jb, ldx));
             else
                 BEM_TRY(cgemm<R>(ctx, below, nrhs, jb, LU + (int64_t)(j0 + jb) * lda + j0, lda, X + j0, ldx,
-                                 true, X + j0 + jb, ldx, true, mk<C2>(-1, 0), mk<C2>(1, 0)));
+                                 true, X + j0 + jb, ldx, true, mk<C2>(-1, 0), mk<C2>(1, 0), PROF_SOLVE_UPDATE));
         }
     }
     // backward: U X = Y
@@ -530,7 +536,7 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
                 BEM_TRY(tc->fn_solve(ctx, tc->state, j0, nrhs, jb, LU + j0, lda, X + j0, ldx, X, ldx));
             else
                 BEM_TRY(cgemm<R>(ctx, j0, nrhs, jb, LU + j0, lda, X + j0, ldx, true, X, ldx, true,
-                                 mk<C2>(-1, 0), mk<C2>(1, 0)));
+                                 mk<C2>(-1, 0), mk<C2>(1, 0), PROF_SOLVE_UPDATE));
         }
     }
     return BEM_OK;
@@ -543,9 +549,9 @@ template int getrs<double>(bem_ctx*, const double2*, int64_t, int, const int*, c
 template int getrs<float>(bem_ctx*, const float2*, int64_t, int, const int*, const float2*, int64_t,
                           float2*, int64_t, int, const TrailingUpdate<float>*);
 template int cgemm<double>(bem_ctx*, int, int, int, const double2*, int64_t, const double2*, int64_t, bool,
-                           double2*, int64_t, bool, double2, double2);
+                           double2*, int64_t, bool, double2, double2, int);
 template int cgemm<float>(bem_ctx*, int, int, int, const float2*, int64_t, const float2*, int64_t, bool,
-                          float2*, int64_t, bool, float2, float2);
+                          float2*, int64_t, bool, float2, float2, int);
 
 // Row pivots (LAPACK interchange sequence, 0-based) -> gather permutation.
 void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm) {

@@ -35,7 +35,7 @@ template <typename R>
 int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int64_t lda,
           const typename C2T<R>::type* B, int64_t ldb, bool b_kmajor,
           typename C2T<R>::type* C, int64_t ldc, bool c_colmajor,
-          typename C2T<R>::type alpha, typename C2T<R>::type beta);
+          typename C2T<R>::type alpha, typename C2T<R>::type beta, int prof_cls = -1);
 
 template <typename R>
 int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipiv, int* d_info,

@@ -335,8 +335,13 @@ static int launch_ff(bem_ctx* ctx, FFArgs& a) {
     BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(farfield_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
     dim3 grid(nchunk, a.n_orient);
+    cudaEvent_t ev = ctx->prof_begin(PROF_FARFIELD);
     farfield_kernel<<<grid, threads, smem, ctx->stream>>>(a, dpb);
     BEM_LAUNCHED(ctx);
+    // algorithmic unit: one (orientation, direction, point) term, ~110 flop
+    if (ev)
+        ctx->prof_end(PROF_FARFIELD, ev, 110.0 * a.n_orient * (double)a.ndir * 2.0 * a.N * a.Nq,
+                      (double)a.n_orient * a.ndir * 16 * 8);
     return BEM_OK;
 }
 

@@ -213,7 +213,7 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         if (st) *st = stats;
         return BEM_OK;
     }
-    if (tol <= 0) tol = 1e-12;
+    if (tol <= 0) tol = 1e-11;
     if (max_iter <= 0) max_iter = 10;
     const size_t nn = (size_t)n * nrhs;
     if (lu->precision == BEM_PREC_FP64) {
@@ -273,11 +273,12 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
     stats.t_solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     auto t1 = std::chrono::steady_clock::now();
     double2 m1 = make_double2(-1, 0), p1 = make_double2(1, 0);
+    double prev_upd = -1.0;
     for (int it = 1; it <= max_iter; it++) {
         // R = B - Z X  (FP64)
         copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, R, n, n, nrhs);
         BEM_LAUNCHED(ctx);
-        BEM_TRY(cgemm<double>(ctx, n, nrhs, n, lu->Z, lu->ldz, X, ldx, true, R, n, true, m1, p1));
+        BEM_TRY(cgemm<double>(ctx, n, nrhs, n, lu->Z, lu->ldz, X, ldx, true, R, n, true, m1, p1, PROF_RESIDUAL));
         colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(R, n, n, scale);
         BEM_LAUNCHED(ctx);
         colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(X, ldx, n, xmax);
@@ -301,9 +302,17 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         }
         stats.iterations = it;
         stats.max_rel_update = upd;
+        if (it <= 12) stats.update_hist[it - 1] = upd;
         // max-norm residual relative to ||Z||_F ||x||_max (a bound-style measure)
         stats.max_rel_residual = res / (lu->znorm > 0 ? lu->znorm : 1.0);
-        if (upd <= tol) {
+        // Error of the new iterate: the sweep contracts the error by rho, so
+        // err(x_k) <~ rho / (1 - rho) * |d_k|, with rho estimated from two
+        // successive updates (first sweep: assume rho = 0.5, i.e. |d_1|).
+        double rho = prev_upd > 0 ? std::min(upd / prev_upd, 0.99) : 0.5;
+        double est = upd * rho / (1.0 - rho);
+        stats.est_rel_error = est;
+        prev_upd = upd;
+        if (est <= tol || upd <= 1e-15) {
             stats.converged = 1;
             break;
         }

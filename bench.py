@@ -1,0 +1,346 @@
+#!/usr/bin/env python3
+"""Benchmark of the dense PMCHWT solve (the metric of this repository).
+
+Workload: icosphere refinement 5 (20480 triangles, 30720 RWG, 61440
+unknowns), ka = 15, m = 1.3116 + 1e-4 i, 7-point quadrature, 45 x 31 x 1
+orientations x 2 polarisations = 2790 right-hand sides.
+
+A step is one solve: FP32 factorisation of the FP64-assembled Z (3xTF32
+tensor-core updates), the 2790-column triangular solves, and FP64
+iterative refinement until every column's relative update is below 1e-12.
+value = seconds per solve (device time, CUDA events, max over ranks).  The
+plain FP64 LU + solve of the same Z is timed once beside it and is the
+oracle of the 1e-9 error check.  e2e = the whole pipeline through the C ABI
+call bem_dense_run (host mesh in, host Mueller matrix out).
+
+--impl reference: the reference's CPU path for the solve (LAPACK zgetrf /
+zgetrs through SciPy, bem_core.py:1637, 1713) on a bounded sample, scaled to
+the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "bem-cpp_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "s/solve at 2N=61440: FP32+refine vs FP64 LU on one B200 at 1e-9 rel err"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bem", choices=["bem", "reference"])
+    ap.add_argument("--ref", type=int, default=5, help="icosphere refinement (5: 2N=61440)")
+    ap.add_argument("--ka", type=float, default=15.0)
+    ap.add_argument("--m", type=complex, default=complex(1.3116, 1e-4))
+    ap.add_argument("--orient", type=int, nargs=3, default=[45, 31, 1])
+    ap.add_argument("--tol", type=float, default=1e-12)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a, n):
+    return {"workload": f"icosphere ref {a.ref} (2N={n}), ka={a.ka:g}, m={a.m.real:g}+{a.m.imag:g}i, "
+                        f"quad 7, {a.orient[0]}x{a.orient[1]}x{a.orient[2]} orientations x 2 pol",
+            "unknowns": n, "rhs": 2 * a.orient[0] * a.orient[1] * a.orient[2],
+            "l2_policy": "inputs larger than L2 (Z is 16 n^2 bytes)"}
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_sample(n_full, nrhs_full, n_s=8192, reps=1, seed=0):
+    """Oracle LAPACK solve (zgetrf + zgetrs, complex128) of an n_s x n_s
+    seeded matrix with nrhs_s = nrhs_full * n_s / n_full right-hand sides;
+    scaled by (n/n_s)^3 for the factorisation and (n/n_s)^2 (nrhs/nrhs_s) for
+    the solves.  Returns (s/solve scaled, cores, description)."""
+    import numpy as np
+    from oracle import bem_oracle  # noqa: F401  (the oracle's LU is scipy's LAPACK)
+    from scipy.linalg import lu_factor, lu_solve
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n_s, n_s)) + 1j * rng.standard_normal((n_s, n_s))
+    nr = max(1, round(nrhs_full * n_s / n_full))
+    B = rng.standard_normal((n_s, nr)) + 1j * rng.standard_normal((n_s, nr))
+    tf, ts = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        f = lu_factor(A)
+        t1 = time.perf_counter()
+        lu_solve(f, B)
+        t2 = time.perf_counter()
+        tf.append(t1 - t0)
+        ts.append(t2 - t1)
+    tfm, tsm = statistics.median(tf), statistics.median(ts)
+    scaled = tfm * (n_full / n_s) ** 3 + tsm * (n_full / n_s) ** 2 * (nrhs_full / nr)
+    cores = os.cpu_count() or 1
+    desc = (f"scipy LAPACK zgetrf+zgetrs on n={n_s}, nrhs={nr} (median of {reps}: factor "
+            f"{tfm:.2f} s, solve {tsm:.2f} s), scaled by n^3 / n^2 nrhs to n={n_full}, "
+            f"nrhs={nrhs_full}")
+    return scaled, cores, desc, tfm + tsm
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                pw = float(r[3])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        load = [s for s in sm if mx and s > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np  # noqa: F401
+    nrhs = 2 * a.orient[0] * a.orient[1] * a.orient[2]
+    n = 2 * _n_rwg_ico(a.ref)
+    vals = []
+    for i in range(a.warmup + a.steps):
+        v, cores, desc, wall = cpu_sample(n, nrhs, n_s=6144, reps=1, seed=i)
+        if i >= a.warmup:
+            vals.append(v)
+    val = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "s/solve",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": val * 1e3,
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "complex128", "data": "synthetic (seeded matrix of the workload's kind)",
+            "config": workload(a, n),
+            "cpu_baseline": {"value": val, "unit": "s/solve", "cores": cores, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": val, "unit": "s/solve", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _n_rwg_ico(ref):
+    # closed icosphere: E = 30 * 4^ref interior edges
+    return 30 * 4 ** ref
+
+
+# ---------------------------------------------------------------- our arm
+def run_bem(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import bem_b200 as bb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    ctx = bb.Context(local)
+    stream = torch.cuda.current_stream(local)
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if world > 1:
+            dist.barrier()
+
+    verts, tris = bb.icosphere(1.0, a.ref)
+    kx, ki, ee, ei = bb.physics(a.ka, a.m)
+    g = bb.Geometry(ctx, verts, tris, 7)
+    n = g.n
+    RT, w = bb.generate_orientations(*a.orient, sort_nearest=True)
+    no_all = len(w)
+    # strong scaling over right-hand sides: every rank factors its own copy,
+    # rank r solves its contiguous slice of the orientations
+    o0, o1 = rank * no_all // world, (rank + 1) * no_all // world
+    RTr, wr = RT[o0:o1], w[o0:o1]
+    nrhs = 2 * len(wr)
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.profile(True)
+    ev0.record(stream)
+    Z = bb.assemble_pmchwt_dev(g, kx, ki, ee, ei)
+    ev1.record(stream)
+    torch.cuda.synchronize(local)
+    t_asm = ev0.elapsed_time(ev1) / 1e3
+    prof_asm = ctx.profile_read()["assembly"]
+    ctx.profile(False)
+    B = bb.rhs_planewave_dev(g, kx, ee, RTr)
+
+    # FP64 comparator (also the oracle of the error check)
+    t64, X64, st64 = None, None, None
+    if not a.no_fp64:
+        Zc = Z.clone()
+        barrier()
+        ev0.record(stream)
+        lu64 = bb.LU(ctx, Zc, bb.PREC_FP64)
+        X64, st64 = lu64.solve(B)
+        ev1.record(stream)
+        torch.cuda.synchronize(local)
+        t64 = ev0.elapsed_time(ev1) / 1e3
+        lu64.close()
+        del Zc
+        torch.cuda.empty_cache()
+
+    X = torch.empty_like(B)
+    times, stats = [], []
+    launches0 = None
+    clocks = None
+    for i in range(a.warmup + a.steps):
+        timed = i >= a.warmup
+        if timed and i == a.warmup:
+            sampler = ClockSampler(local)
+            ctx.profile(True)
+            launches0 = ctx.launches
+        barrier()
+        ev0.record(stream)
+        lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+        Xs, st = lu.solve(B, X=X, tol=a.tol, max_iter=12, raise_noconv=False)
+        ev1.record(stream)
+        barrier()
+        lu.close()
+        if timed:
+            times.append(ev0.elapsed_time(ev1) / 1e3)
+            stats.append(st)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    t_step = max(times)
+    tt = torch.tensor([t_step, t64 or 0.0, t_asm], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    t_step, t64m, t_asm = tt.tolist()
+
+    err = None
+    if X64 is not None:
+        d = (X - X64).abs().pow(2).sum(dim=1).sqrt() / X64.abs().pow(2).sum(dim=1).sqrt()
+        err = float(d.max().item())
+        if world > 1:
+            e = torch.tensor([err], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(e, op=dist.ReduceOp.MAX)
+            err = float(e.item())
+
+    # dominant kernel of the timed steps -> roofline
+    pk, basis = peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (nl, ms, fl, by) = dom
+    ms_launch = ms / max(nl, 1)
+    achieved = fl / max(nl, 1) / (ms_launch / 1e3) / 1e12
+    if name in ("lu_update", "solve_update"):
+        peak = pk["bf16_tflops"] / 2.0 / 3.0
+        pbasis = f"3xTF32: {basis} bf16 {pk['bf16_tflops']} TF/s / 2 (tf32) / 3 (split terms)"
+    else:
+        peak = 40.0
+        pbasis = "FP64 CUDA-core nominal 40 TF/s (no measured FP64 peak on this pool)"
+    roof = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": None, "launches": nl, "ms_per_launch": ms_launch,
+            "peak_basis": pbasis,
+            "share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()}}
+
+    # free the step buffers before the end-to-end pipeline
+    del Z, B, X, X64
+    torch.cuda.empty_cache()
+    e2e = None
+    if not a.no_e2e:
+        t0 = time.perf_counter()
+        M, info = bb.dense_run(ctx, verts, tris, a.ka, a.m, orient=tuple(a.orient), ntheta=181,
+                               precision=bb.PREC_FP32_REFINE, refine_tol=a.tol, max_refine=12)
+        t_e2e = time.perf_counter() - t0
+        h2d = verts.nbytes + tris.astype(np.int32).nbytes + 9 * 8 * no_all + 8 * no_all
+        e2e = {"value": t_e2e, "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(M.nbytes),
+               "scope": "bem_dense_run: host mesh -> assembly, FP32 LU + refinement, far field -> host Mueller",
+               "t_assembly_s": info["t_assembly_s"], "t_solve_s": info["t_solve_s"],
+               "t_farfield_s": info["t_farfield_s"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        v, cores, desc, wall = cpu_sample(n, 2 * no_all, n_s=8192, reps=2)
+        cpu = {"value": v, "unit": "s/solve", "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        its = [s["iterations"] for s in stats]
+        line = {"metric": METRIC, "value": t_step, "unit": "s/solve", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_step * 1e3,
+                "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+                "dtype": "complex64 factors (3xTF32) + complex128 refinement",
+                "data": "synthetic (generated icosphere mesh and plane waves)",
+                "config": {**workload(a, n), "parallelism": f"rhs-split x{world}" if world > 1 else "single"},
+                "fp64_s_per_solve": t64m or None,
+                "speedup_vs_fp64": (t64m / t_step) if t64m else None,
+                "max_rel_err_vs_fp64": err, "refine_iterations": its,
+                "converged": all(s["converged"] for s in stats),
+                "assembly_s": t_asm,
+                "assembly_roofline": {"unit_evals_per_s": prof_asm[2] / 64.0 / max(prof_asm[1], 1e-9) * 1e3},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_bem(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -61,6 +61,19 @@ int bem_ctx_synchronize(bem_ctx* ctx);
 const char* bem_last_error(const bem_ctx* ctx);
 /* Number of kernel launches issued by this context so far. */
 int64_t bem_ctx_launch_count(const bem_ctx* ctx);
+
+/* Per-kernel-class device timing: CUDA events on the context's stream around
+ * every launch of a class.  bem_ctx_profile(ctx, 1) clears the counters and
+ * starts recording, 0 stops.  Classes: 0 LU trailing update, 1 triangular
+ * solve block updates, 2 FP64 refinement residual, 3 panel factorisation,
+ * 4 assembly, 5 far field / Mueller.  flops / bytes are the algorithmic
+ * counts of the recorded launches (complex GEMM: 8 M N K flop). */
+int bem_ctx_profile(bem_ctx* ctx, int enable);
+/* FP32 factorisation / solve updates on the tensor cores (3xTF32 tcgen05,
+ * default 1) or on the CUDA cores (0). */
+int bem_ctx_set_tensor_cores(bem_ctx* ctx, int enable);
+int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
+                         double* bytes);
 const char* bem_version(void);
 
 /* ----------------------------------------------------- geometry (host) */
@@ -108,6 +121,12 @@ int bem_gauss_legendre(int n, double* nodes, double* weights);
  * *N receives the number of RWG functions (system size 2N). */
 int bem_geom_create(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
                     int quad_order, bem_geom** out, int* N);
+/* Same with an explicit RWG basis (arrays of length N; free_p / free_m 3N
+ * doubles), for callers that built theirs with build_rwg (rwg.h:18). */
+int bem_geom_create_rwg(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt, int N,
+                        const int* tri_p, const int* tri_m, const double* free_p, const double* free_m,
+                        const double* length, const double* area_p, const double* area_m,
+                        int quad_order, bem_geom** out);
 int bem_geom_free(bem_geom* g);
 int bem_geom_size(const bem_geom* g);
 
@@ -151,10 +170,12 @@ int bem_rhs_planewave(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
 
 typedef struct bem_solve_stats {
     int iterations;          /* refinement sweeps run (0 for FP64) */
-    int converged;           /* 1 when every column met the tolerance */
-    double max_rel_update;   /* max over columns of ||dX||/||X|| in the last sweep */
-    double max_rel_residual; /* max over columns of ||B - Z X|| / (||Z||_F ||X||) */
+    int converged;           /* 1 when the error estimate met the tolerance */
+    double max_rel_update;   /* max over columns of max|dX| / max|X| in the last sweep */
+    double max_rel_residual; /* max over columns of max|B - Z X| / (||Z||_F max|X|) */
+    double est_rel_error;    /* estimated max-column relative error of the returned X */
     double t_factor_ms, t_solve_ms, t_refine_ms;
+    double update_hist[12];  /* max relative update of sweeps 1..12 */
 } bem_solve_stats;
 
 /* Factorises the row-major n x n complex128 matrix Z_dev (leading dimension
@@ -165,8 +186,11 @@ typedef struct bem_solve_stats {
 int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precision,
                       bem_lu** out, int* info);
 /* X = Z^-1 B for nrhs columns (column-major, leading dimensions ldb / ldx; X may
- * alias B).  FP32_REFINE refines in FP64 until every column's relative update
- * is below `tol` (default 1e-12 when tol <= 0) or max_iter sweeps were run. */
+ * alias B).  FP32_REFINE refines in FP64 (residual B - Z X with the FP64 Z,
+ * correction through the FP32 factors) until the estimated relative error of
+ * every column, rho/(1-rho) times its last relative update with rho the
+ * observed contraction, is below `tol` (default 1e-11 when tol <= 0), or
+ * max_iter sweeps (default 10) were run (BEM_ERR_NOCONV). */
 int bem_lu_solve_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb,
                      void* X_dev, int64_t ldx, int nrhs, double tol, int max_iter,
                      bem_solve_stats* stats);
@@ -207,6 +231,14 @@ int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev,
 /* amplitude_to_mueller (farfield.cu:464-508); S*, complex128[ntheta]. */
 int bem_amplitude_to_mueller(const double* S1, const double* S2, const double* S3,
                              const double* S4, int ntheta, double* M);
+
+/* The tensor-core update used by the FP32 factorisation, exposed for direct
+ * use and testing: C -= A B with complex64 device buffers.  A: M x K with K
+ * contiguous (A[i*lda + k]); B: K x N, b_rowmajor ? B[k*ldb + j] :
+ * B[j*ldb + k]; C: M x N, c_colmajor ? C[j*ldc + i] : C[i*ldc + j].
+ * Products are 3xTF32 (hi*hi + hi*lo + lo*hi), FP32 accumulation. */
+int bem_cgemm_tf32x3(bem_ctx* ctx, int M, int N, int K, const void* A, int64_t lda, const void* B,
+                     int64_t ldb, int b_rowmajor, void* C, int64_t ldc, int c_colmajor);
 
 /* ---------------------------------------------------------- whole pipeline */
 
