@@ -112,6 +112,7 @@ SIGNATURES = {
     "bem_lu_solve_full": (_I, [_P, _P, _I, _P, _I, _I, C.POINTER(SolveStats)]),
     "bem_farfield_batch": (_I, [_P, _P, _P, _P, _P, _D, _D, _D, _I, _I, _I, _P]),
     "bem_farfield_mueller_dev": (_I, [_P, _P, _P, _L, _P, _P, _I, _D, _D, _D, _I, _I, _P, _P]),
+    "bem_farfield_mueller_noalloc": (_I, [_P, _P, _P, _L, _P, _P, _I, _D, _D, _D, _I, _I, _P]),
     "bem_amplitude_to_mueller": (_I, [_P, _P, _P, _P, _I, _P]),
     "bem_dense_run": (_I, [_P, C.POINTER(Problem), C.POINTER(Result)]),
 }

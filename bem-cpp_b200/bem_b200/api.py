@@ -480,3 +480,17 @@ def cgemm_tf32x3(ctx: Context, A, B, C, b_rowmajor=True, c_colmajor=False):
 
 def set_tensor_cores(ctx: Context, enable: bool):
     ctx.check(lib().bem_ctx_set_tensor_cores(ctx.h, int(bool(enable))))
+
+
+def mueller_noalloc_dev(geom: Geometry, X, RT, w, k_ext, eta_ext, M_out, ntheta=181,
+                        gamma_mirror=False):
+    """bem_farfield_mueller_noalloc: same sum as mueller_from_solutions_dev into
+    the caller's device buffer M_out (torch float64, 16*ntheta), with no device
+    allocation by the library (scratch is a static device array)."""
+    RT = _f64(RT).reshape(-1, 9)
+    w = _f64(w)
+    k = complex(k_ext)
+    geom.ctx.check(lib().bem_farfield_mueller_noalloc(
+        geom.ctx.h, geom.h, _dptr(X), X.stride(0), _ptr(RT), _ptr(w), RT.shape[0], k.real, k.imag,
+        float(eta_ext), int(ntheta), int(bool(gamma_mirror)), _dptr(M_out)))
+    return M_out

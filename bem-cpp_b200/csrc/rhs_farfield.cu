@@ -11,6 +11,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bem_internal.h"
@@ -145,6 +146,11 @@ struct FFArgs {
     int gamma_mirror;
 };
 
+// theta_d = pi d / (ndir - 1) (main.cpp:331-333) unless an array is given
+__device__ __forceinline__ double theta_of(const FFArgs& a, int d) {
+    return a.theta ? a.theta[d] : (a.ndir > 1 ? M_PI * d / (a.ndir - 1) : 0.0);
+}
+
 constexpr int FF_LANES = 4;
 constexpr int FF_CHUNK = 256;  // points staged per step
 
@@ -171,7 +177,7 @@ __global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
             r[0] = rr[0], r[1] = rr[1], r[2] = rr[2];
         } else {
             double st, ct;
-            sincos(a.theta[d], &st, &ct);
+            sincos(theta_of(a, d), &st, &ct);
             const double* R = a.RT + 9 * o;
             for (int i = 0; i < 3; i++) r[i] = R[3 * i] * st + R[3 * i + 2] * ct;
         }
@@ -262,7 +268,7 @@ __global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
     if (a.Mo) {
         // e_par = R^T e_theta_lab, e_perp = R^T y (main.cpp:785-799, 817-831)
         double st, ct;
-        sincos(a.theta[d], &st, &ct);
+        sincos(theta_of(a, d), &st, &ct);
         const double* R = a.RT + 9 * o;
         double epa[3], epe[3];
         for (int i = 0; i < 3; i++) {
@@ -427,11 +433,88 @@ int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, con
     return BEM_OK;
 }
 
+// ---------------------------------------------------- allocation-free variant
+// Scratch of bem_farfield_mueller_noalloc: a file-scope device array, so the
+// entry point needs no cudaMalloc.  Host code must not use the symbol as an
+// address: its device address is looked up per device with
+// cudaGetSymbolAddress on the first call there.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BEM_NOALLOC_SCRATCH_BYTES];
+static void* g_noalloc_dev_ptr[64];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(bem_ctx* ctx, void** out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, BEM_ERR_INVALID, "device ordinal %d", ctx->device);
+    if (!g_noalloc_dev_ptr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // device is current (cudaSetDevice)
+        if (e != cudaSuccess || !p)
+            return fail(ctx, BEM_ERR_CUDA, "cudaGetSymbolAddress of the scratch array: %s", cudaGetErrorString(e));
+        g_noalloc_dev_ptr[ctx->device] = p;
+    }
+    *out = g_noalloc_dev_ptr[ctx->device];
+    return BEM_OK;
+}
+
+int mueller_noalloc(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, const double* RT,
+                    const double* w, int n_orient, double k_re, double k_im, double eta, int ntheta,
+                    int gamma_mirror, double* M_out_dev) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t rtb = al((size_t)n_orient * 9 * 8), wb = al((size_t)n_orient * 8),
+           mob = al((size_t)n_orient * 16 * ntheta * 8);
+    if (rtb + wb + mob > (size_t)BEM_NOALLOC_SCRATCH_BYTES)
+        return fail(ctx, BEM_ERR_INVALID,
+                    "%d orientations x %d angles need %zu bytes of scratch, above the %d-byte maximum of "
+                    "bem_farfield_mueller_noalloc; pass fewer orientations per call and add the results",
+                    n_orient, ntheta, rtb + wb + mob, (int)BEM_NOALLOC_SCRATCH_BYTES);
+    void* base = nullptr;
+    BEM_TRY(noalloc_scratch(ctx, &base));
+    char* sc = (char*)base;
+    double* d_RT = (double*)sc;
+    double* d_w = (double*)(sc + rtb);
+    double* d_Mo = (double*)(sc + rtb + wb);
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(d_RT, RT, (size_t)n_orient * 9 * 8, cudaMemcpyHostToDevice, ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(d_w, w, (size_t)n_orient * 8, cudaMemcpyHostToDevice, ctx->stream));
+    FFArgs a{};
+    a.h = g->half;
+    a.N = g->N;
+    a.Nq = g->Nq;
+    a.n_orient = n_orient;
+    a.ndir = ntheta;
+    a.n_calls = 2 * n_orient;
+    a.kr = k_re;
+    a.ki = k_im;
+    a.eta = eta;
+    a.cJ = (const double2*)X;
+    a.cM = (const double2*)X + g->N;
+    a.cs = ldx;
+    a.RT = d_RT;
+    a.theta = nullptr;  // computed in the kernel
+    a.w = d_w;
+    a.Mo = d_Mo;  // every (o, i, d) entry is written: nothing to clear
+    a.gamma_mirror = gamma_mirror;
+    BEM_TRY(launch_ff(ctx, a));
+    int nel = 16 * ntheta;
+    mueller_sum_kernel<<<(nel + 255) / 256, 256, 0, ctx->stream>>>(d_Mo, n_orient, nel, M_out_dev);
+    BEM_LAUNCHED(ctx);
+    return BEM_OK;
+}
+
 }  // namespace bem
 
 using namespace bem;
 
 extern "C" {
+
+int bem_farfield_mueller_noalloc(bem_ctx* ctx, const bem_geom* g, const void* X_dev, int64_t ldx,
+                                 const double* RT, const double* w, int n_orient, double k_re, double k_im,
+                                 double eta_ext, int ntheta, int gamma_mirror, double* M_avg_dev) {
+    if (!ctx || !g || !X_dev || !RT || !w || !M_avg_dev || n_orient < 1 || ntheta < 2 || ldx < 2 * g->N)
+        return ctx ? fail(ctx, BEM_ERR_INVALID, "bad bem_farfield_mueller_noalloc arguments") : BEM_ERR_INVALID;
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    return mueller_noalloc(ctx, g, X_dev, ldx, RT, w, n_orient, k_re, k_im, eta_ext, ntheta, gamma_mirror,
+                           M_avg_dev);
+}
 
 int bem_rhs_planewave_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im, double eta_ext,
                           const double* RT, int n_orient, void* B_dev, int64_t ldb) {

@@ -228,6 +228,26 @@ int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev,
                              double k_re, double k_im, double eta_ext, int ntheta,
                              int gamma_mirror, double* M_avg, double* M_orient_dev);
 
+/* Allocation-free variant of bem_farfield_mueller_dev, with no counterpart in
+ * the reference.  For callers that cannot allocate device memory: code
+ * running inside CUDA stream capture, where cudaMalloc is not allowed, and
+ * hosts whose device memory belongs to their own allocator (a serving stack
+ * with a fixed pool).  Its only scratch (staged orientations, per-orientation
+ * Mueller terms) is a file-scope device array of BEM_NOALLOC_SCRATCH_BYTES,
+ * held by every GPU that loads the library until exit; the call itself
+ * allocates nothing.  Calls whose n_orient * (16 ntheta + 10) doubles do not
+ * fit are rejected with BEM_ERR_INVALID: split the orientations and add the
+ * partial results (the average is a weighted sum).  RT, w: host arrays as in
+ * bem_farfield_mueller_dev.  M_avg_dev: caller's device buffer of 16*ntheta
+ * doubles, written on the context's stream.  The first call on a device looks
+ * up the scratch address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the one array: calls that overlap on
+ * the GPU (different streams or contexts on one device) race on it. */
+#define BEM_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
+int bem_farfield_mueller_noalloc(bem_ctx* ctx, const bem_geom* g, const void* X_dev, int64_t ldx,
+                                 const double* RT, const double* w, int n_orient, double k_re, double k_im,
+                                 double eta_ext, int ntheta, int gamma_mirror, double* M_avg_dev);
+
 /* amplitude_to_mueller (farfield.cu:464-508); S*, complex128[ntheta]. */
 int bem_amplitude_to_mueller(const double* S1, const double* S2, const double* S3,
                              const double* S4, int ntheta, double* M);
