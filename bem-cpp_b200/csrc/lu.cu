@@ -28,6 +28,7 @@
 #include "bem_internal.h"
 #include "cgemm_simt.cuh"
 #include "lu_internal.h"
+#include "zgemm_dmma.cuh"
 
 namespace bem {
 
@@ -45,7 +46,29 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
     dim3 grid((N + 63) / 64, (M + 63) / 64);
     if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "gemm M too large");
     cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
-    if (b_kmajor) {
+    if (sizeof(R) == 8) {
+        // FP64: the m8n8k4 f64 tensor path (zgemm_dmma.cuh)
+        static bool attr[4] = {false, false, false, false};
+        const double2* Ad = reinterpret_cast<const double2*>(A);
+        const double2* Bd = reinterpret_cast<const double2*>(B);
+        double2* Cd = reinterpret_cast<double2*>(C);
+        double2 al = make_double2(alpha.x, alpha.y), be = make_double2(beta.x, beta.y);
+        auto go = [&](auto kern, int slot) -> int {
+            if (!attr[slot]) {
+                BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       dmma::SMEM_BYTES));
+                attr[slot] = true;
+            }
+            kern<<<grid, 128, dmma::SMEM_BYTES, ctx->stream>>>(M, N, K, Ad, lda, Bd, ldb, Cd, ldc, al, be);
+            return BEM_OK;
+        };
+        int s;
+        if (b_kmajor)
+            s = c_colmajor ? go(dmma::zgemm_kernel<true, true>, 0) : go(dmma::zgemm_kernel<true, false>, 1);
+        else
+            s = c_colmajor ? go(dmma::zgemm_kernel<false, true>, 2) : go(dmma::zgemm_kernel<false, false>, 3);
+        BEM_TRY(s);
+    } else if (b_kmajor) {
         if (c_colmajor)
             cgemm_simt_kernel<R, true, true><<<grid, 256, 0, ctx->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
         else
