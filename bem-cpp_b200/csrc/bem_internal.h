@@ -133,6 +133,7 @@ struct bem_ctx {
     float* tc_buf = nullptr;  // packed hi/lo operands of the tensor-core GEMM
     size_t tc_bytes = 0;
     bool tc_attr = false;
+    bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)
     bool prof = false;
     std::vector<ProfPending> prof_pending;
     std::vector<cudaEvent_t> prof_pool;

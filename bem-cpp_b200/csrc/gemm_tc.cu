@@ -255,6 +255,211 @@ gemm_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ C
     }
 }
 
+// Persistent, warp-specialised version: one CTA per SM walks a grouped
+// raster of 128 x 256 tiles.  Warp 0 issues TMA, warp 1 issues tcgen05.mma
+// into one of two 256-column TMEM accumulators, warps 2-5 drain the other
+// accumulator into C, so the read-modify-write of tile i overlaps the MMAs of
+// tile i+1.  Barriers: full/empty per smem stage, tfull/tempty per
+// accumulator (tempty counts the four epilogue warps).
+constexpr int GROUP_M = 8;
+constexpr uint32_t TMEM_COLS2 = 512;
+
+struct TileMap {
+    int num_m, num_n;
+    __device__ __forceinline__ void tile(int t, int& mt, int& nt) const {
+        const int per_group = GROUP_M * num_n;
+        const int g = t / per_group, first_m = g * GROUP_M;
+        const int gsize = min(GROUP_M, num_m - first_m);
+        const int r = t % per_group;
+        mt = first_m + r % gsize;
+        nt = r / gsize;
+    }
+};
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(192, 1)
+gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+                       const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
+                       float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+    uint64_t* full = bars;                  // [STAGES]
+    uint64_t* empty = bars + STAGES;        // [STAGES]
+    uint64_t* tfull = bars + 2 * STAGES;    // [2]
+    uint64_t* tempty = bars + 2 * STAGES + 2;
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 4);
+    __shared__ volatile int abort_flag;
+    __shared__ int issued_total, consumed_total;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nk = (K2 + BK - 1) / BK;
+    TileMap tm;
+    tm.num_m = (M + BM - 1) / BM;
+    tm.num_n = (2 * Nc + BN - 1) / BN;
+    const int ntiles = tm.num_m * tm.num_n;
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        issued_total = consumed_total = 0;
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), 4);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS2));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;
+            for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+                int mt, ntl;
+                tm.tile(t, mt, ntl);
+                for (int kt = 0; kt < nk; kt++, it++) {
+                    const int s = it % STAGES;
+                    if (!mbar_wait(smem_u32(&empty[s]), ((it / STAGES) & 1) ^ 1, status, &abort_flag)) break;
+                    unsigned char* st = smem + s * STAGE_BYTES;
+                    const uint32_t fb = smem_u32(&full[s]);
+                    mbar_expect_tx(fb, STAGE_BYTES);
+                    tma_load_2d(smem_u32(st), &tA_hi, kt * BK, mt * BM, fb);
+                    tma_load_2d(smem_u32(st + A_BYTES), &tA_lo, kt * BK, mt * BM, fb);
+                    tma_load_2d(smem_u32(st + 2 * A_BYTES), &tB_hi, kt * BK, ntl * BN, fb);
+                    tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tB_lo, kt * BK, ntl * BN, fb);
+                    issued_total = it + 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int it = 0, lt = 0;
+            for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, lt++) {
+                const int b = lt & 1;
+                if (!mbar_wait(smem_u32(&tempty[b]), ((lt >> 1) & 1) ^ 1, status, &abort_flag)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * 256);
+                bool ok = true;
+                for (int kt = 0; kt < nk; kt++, it++) {
+                    const int s = it % STAGES;
+                    if (!mbar_wait(smem_u32(&full[s]), (it / STAGES) & 1, status, &abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    unsigned char* st = smem + s * STAGE_BYTES;
+                    const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + A_BYTES);
+                    const uint32_t b_hi = smem_u32(st + 2 * A_BYTES), b_lo = smem_u32(st + 2 * A_BYTES + B_BYTES);
+#pragma unroll
+                    for (int ks = 0; ks < BK / 8; ks++) {
+                        const uint32_t off = ks * 32;
+                        const uint64_t dah = smem_desc(a_hi + off), dal = smem_desc(a_lo + off);
+                        const uint64_t dbh = smem_desc(b_hi + off), dbl = smem_desc(b_lo + off);
+                        mma_tf32(acc, dah, dbh, (kt > 0 || ks > 0) ? 1u : 0u);
+                        mma_tf32(acc, dah, dbl, 1u);
+                        mma_tf32(acc, dal, dbh, 1u);
+                    }
+                    mma_commit(smem_u32(&empty[s]));
+                    consumed_total = it + 1;
+                }
+                mma_commit(smem_u32(&tfull[b]));
+                if (!ok) break;
+            }
+        }
+    } else {
+        // epilogue warps 2..5: TMEM lane quarter = warp % 4
+        const int q = warp & 3;
+        int lt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+            const int b = lt & 1;
+            bool ok = mbar_wait(smem_u32(&tfull[b]), (lt >> 1) & 1, status, &abort_flag);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int mt, ntl;
+            tm.tile(t, mt, ntl);
+            const int row = mt * BM + q * 32 + lane;
+            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
+#pragma unroll 1
+            for (int ch = 0; ch < BN / 32; ch++) {
+                float v[32];
+                tmem_ld32(base + ch * 32, v);
+                const int c0 = ntl * (BN / 2) + ch * 16;
+                if (row < M && c0 < Nc) {
+                    if (!c_colmajor) {
+                        float2* p = &C[(int64_t)row * ldc + c0];
+                        const bool vec = ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (c0 + 16 <= Nc);
+                        if (vec) {
+                            float4* p4 = reinterpret_cast<float4*>(p);
+#pragma unroll
+                            for (int j = 0; j < 8; j++) {
+                                float4 c = p4[j];
+                                c.x -= v[4 * j];
+                                c.y -= v[4 * j + 1];
+                                c.z -= v[4 * j + 2];
+                                c.w -= v[4 * j + 3];
+                                p4[j] = c;
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; j++)
+                                if (c0 + j < Nc) {
+                                    float2 c = p[j];
+                                    c.x -= v[2 * j];
+                                    c.y -= v[2 * j + 1];
+                                    p[j] = c;
+                                }
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 16; j++)
+                            if (c0 + j < Nc) {
+                                float2* p = &C[(int64_t)(c0 + j) * ldc + row];
+                                float2 c = *p;
+                                c.x -= v[2 * j];
+                                c.y -= v[2 * j + 1];
+                                *p = c;
+                            }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&tempty[b]));
+        }
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // teardown: on an aborted run, let the copies already issued land
+    if (threadIdx.x == 0 && abort_flag) {
+        for (int it = consumed_total; it < issued_total; it++) {
+            long long t0 = clock64();
+            while (!mbar_try(smem_u32(&full[it % STAGES]), (it / STAGES) & 1) && clock64() - t0 < WAIT_CYCLES) {
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS2));
+    }
+}
+
 // ---------------------------------------------------------------- packing
 // A (complex, K contiguous): hi/lo[i*ld + 2k + {0,1}] = split(Re/Im a_ik), zero padded
 __global__ void pack_a_kernel(const float2* __restrict__ A, int64_t lda, int M, int K, float* __restrict__ hi,
@@ -388,12 +593,22 @@ static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t l
     if (!ctx->tc_attr) {
         BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                tc::SMEM_BYTES));
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_persistent_kernel,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
         ctx->tc_attr = true;
     }
-    dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
-    if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");
-    tc::gemm_kernel<<<grid, 128, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc, c_colmajor ? 1 : 0, M,
-                                                                 N, ld, ctx->d_status);
+    if (ctx->tc_persistent) {
+        const int ntiles = ((M + tc::BM - 1) / tc::BM) * ((2 * N + tc::BN - 1) / tc::BN);
+        const int grid = std::min(ntiles, ctx->sm_count);
+        tc::gemm_persistent_kernel<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc,
+                                                                                c_colmajor ? 1 : 0, M, N, ld,
+                                                                                ctx->d_status);
+    } else {
+        dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
+        if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");
+        tc::gemm_kernel<<<grid, 128, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc, c_colmajor ? 1 : 0,
+                                                                     M, N, ld, ctx->d_status);
+    }
     BEM_LAUNCHED(ctx);
     if (ev)
         ctx->prof_end(prof_cls, ev, 8.0 * M * (double)N * K,

@@ -7,7 +7,9 @@ orientations x 2 polarisations = 2790 right-hand sides.
 
 A step is one solve: FP32 factorisation of the FP64-assembled Z (3xTF32
 tensor-core updates), the 2790-column triangular solves, and FP64
-iterative refinement until every column's relative update is below 1e-12.
+iterative refinement until every column's estimated relative error is below
+2e-10 (the metric asks for 1e-9; the measured error against the FP64 LU
+solution is reported as max_rel_err_vs_fp64).
 value = seconds per solve (device time, CUDA events, max over ranks).  The
 plain FP64 LU + solve of the same Z is timed once beside it and is the
 oracle of the 1e-9 error check.  e2e = the whole pipeline through the C ABI
@@ -34,6 +36,7 @@ for _p in (REPO, os.path.join(REPO, "bem-cpp_b200")):
         sys.path.insert(0, _p)
 
 METRIC = "s/solve at 2N=61440: FP32+refine vs FP64 LU on one B200 at 1e-9 rel err"
+FP64_PEAK_TFS = 37.0
 
 
 def parse():
@@ -46,7 +49,8 @@ def parse():
     ap.add_argument("--ka", type=float, default=15.0)
     ap.add_argument("--m", type=complex, default=complex(1.3116, 1e-4))
     ap.add_argument("--orient", type=int, nargs=3, default=[45, 31, 1])
-    ap.add_argument("--tol", type=float, default=1e-12)
+    ap.add_argument("--tol", type=float, default=2e-10,
+                    help="refinement target: estimated max-column relative error")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -282,10 +286,12 @@ def run_bem(a):
     achieved = fl / max(nl, 1) / (ms_launch / 1e3) / 1e12
     if name in ("lu_update", "solve_update"):
         peak = pk["bf16_tflops"] / 2.0 / 3.0
-        pbasis = f"3xTF32: {basis} bf16 {pk['bf16_tflops']} TF/s / 2 (tf32) / 3 (split terms)"
+        pbasis = (f"complex flops at 3xTF32: {basis} bf16 {pk['bf16_tflops']} TF/s / 2 (tf32 rate) "
+                  f"/ 3 (split terms)")
     else:
-        peak = 40.0
-        pbasis = "FP64 CUDA-core nominal 40 TF/s (no measured FP64 peak on this pool)"
+        peak = FP64_PEAK_TFS
+        pbasis = ("FP64: 37.0 TF/s measured on this pool (cuBLAS ZGEMM 8192^3; DFMA and m8n8k4 DMMA "
+                  "throughput probes 36-37 TF/s); MEASURED_PEAKS.json has no FP64 figure")
     roof = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": None, "launches": nl, "ms_per_launch": ms_launch,
             "peak_basis": pbasis,
@@ -323,6 +329,10 @@ def run_bem(a):
                 "fp64_s_per_solve": t64m or None,
                 "speedup_vs_fp64": (t64m / t_step) if t64m else None,
                 "max_rel_err_vs_fp64": err, "refine_iterations": its,
+                "refine_update_hist": stats[-1].get("update_hist"),
+                "est_rel_err": stats[-1].get("est_rel_error"),
+                "t_factor_s": stats[-1]["t_factor_ms"] / 1e3, "t_first_solve_s": stats[-1]["t_solve_ms"] / 1e3,
+                "t_refine_s": stats[-1]["t_refine_ms"] / 1e3,
                 "converged": all(s["converged"] for s in stats),
                 "assembly_s": t_asm,
                 "assembly_roofline": {"unit_evals_per_s": prof_asm[2] / 64.0 / max(prof_asm[1], 1e-9) * 1e3},
