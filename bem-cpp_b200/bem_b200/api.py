@@ -322,6 +322,7 @@ class LU:
         if self.h:
             lib().bem_lu_free(self.h)
             self.h = None
+        self.Z = None  # drop the reference to the (possibly 60 GB) matrix
 
     def __del__(self):
         try:

@@ -1,0 +1,63 @@
+"""Multi-GPU plumbing for the dense path: replicas, not a distributed LU.
+
+Every rank assembles and factors its own copy of Z (the factorisation of one
+2N x 2N matrix does not shard without a block-cyclic distributed LU); the
+orientation x polarisation right-hand sides are split into contiguous slices,
+each rank solves its slice and forms its part of the weighted Mueller sum,
+and one all-reduce (sum) of the 16 x ntheta partial Mueller matrices gives
+the orientation average -- the device-side counterpart of the reference's
+--orient-range split with a JSON sum (cluster_bem.py:76-127).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def orientation_slice(n_orient: int, rank: int, world: int):
+    """Contiguous [o0, o1) of orientations for `rank` (sizes differ by <= 1)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank / world size")
+    return rank * n_orient // world, (rank + 1) * n_orient // world
+
+
+def allreduce_sum(x, device=None):
+    """Sum a numpy array (e.g. a partial Mueller matrix) over all ranks of the
+    default process group; returns a numpy array."""
+    import torch
+    import torch.distributed as dist
+    t = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64))
+    if device is not None:
+        t = t.to(device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
+def allreduce_max(x: float, device=None) -> float:
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def orientation_average_distributed(ctx, geom, Z, RT, w, k_ext, eta_ext, ntheta=181,
+                                    precision=None, tol=0.0, rank=0, world=1, device=None):
+    """Orientation-averaged Mueller matrix with the orientations split across
+    ranks.  Z is this rank's full copy of the system matrix (device tensor).
+    Returns (M (4,4,ntheta) summed over ranks, this rank's solve stats)."""
+    from . import api
+    from ._lib import PREC_FP32_REFINE
+    if precision is None:
+        precision = PREC_FP32_REFINE
+    o0, o1 = orientation_slice(len(w), rank, world)
+    part = np.zeros((4, 4, ntheta))
+    stats = None
+    if o1 > o0:
+        B = api.rhs_planewave_dev(geom, k_ext, eta_ext, RT[o0:o1])
+        lu = api.LU(ctx, Z, precision)
+        X, stats = lu.solve(B, tol=tol)
+        lu.close()
+        part = api.mueller_from_solutions_dev(geom, X, RT[o0:o1], w[o0:o1], k_ext, eta_ext, ntheta)
+    return allreduce_sum(part, device).reshape(4, 4, ntheta), stats

@@ -236,7 +236,7 @@ def run_bem(a):
         torch.cuda.synchronize(local)
         t64 = ev0.elapsed_time(ev1) / 1e3
         lu64.close()
-        del Zc
+        del lu64, Zc
         torch.cuda.empty_cache()
 
     X = torch.empty_like(B)
@@ -256,6 +256,7 @@ def run_bem(a):
         ev1.record(stream)
         barrier()
         lu.close()
+        del lu
         if timed:
             times.append(ev0.elapsed_time(ev1) / 1e3)
             stats.append(st)
@@ -298,20 +299,23 @@ def run_bem(a):
             "share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()}}
 
     # free the step buffers before the end-to-end pipeline
-    del Z, B, X, X64
+    del Z, B, X, X64, Xs
     torch.cuda.empty_cache()
     e2e = None
     if not a.no_e2e:
-        t0 = time.perf_counter()
-        M, info = bb.dense_run(ctx, verts, tris, a.ka, a.m, orient=tuple(a.orient), ntheta=181,
-                               precision=bb.PREC_FP32_REFINE, refine_tol=a.tol, max_refine=12)
-        t_e2e = time.perf_counter() - t0
-        h2d = verts.nbytes + tris.astype(np.int32).nbytes + 9 * 8 * no_all + 8 * no_all
-        e2e = {"value": t_e2e, "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(M.nbytes),
-               "scope": "bem_dense_run: host mesh -> assembly, FP32 LU + refinement, far field -> host Mueller",
-               "t_assembly_s": info["t_assembly_s"], "t_solve_s": info["t_solve_s"],
-               "t_farfield_s": info["t_farfield_s"]}
+        try:
+            t0 = time.perf_counter()
+            M, info = bb.dense_run(ctx, verts, tris, a.ka, a.m, orient=tuple(a.orient), ntheta=181,
+                                   precision=bb.PREC_FP32_REFINE, refine_tol=a.tol, max_refine=12)
+            t_e2e = time.perf_counter() - t0
+            h2d = verts.nbytes + tris.astype(np.int32).nbytes + 9 * 8 * no_all + 8 * no_all
+            e2e = {"value": t_e2e, "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(M.nbytes),
+                   "scope": "bem_dense_run: host mesh -> assembly, FP32 LU + refinement, far field -> host Mueller",
+                   "t_assembly_s": info["t_assembly_s"], "t_solve_s": info["t_solve_s"],
+                   "t_farfield_s": info["t_farfield_s"], "refine": info["stats"]["iterations"]}
+        except bb.BemError as ex:
+            e2e = {"value": None, "unit": "s/solve", "error": str(ex)}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:

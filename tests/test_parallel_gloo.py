@@ -1,0 +1,67 @@
+"""Host logic of the multi-GPU path on CPU: world_size 2 gloo ranks split the
+orientations and all-reduce their partial Mueller sums (no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import sys
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                        "bem-cpp_b200"))
+        from bem_b200.parallel import allreduce_max, allreduce_sum, orientation_slice
+        n_orient, nt = 37, 19
+        rng = np.random.default_rng(0)
+        terms = rng.standard_normal((n_orient, 16, nt))  # per-orientation w_o M_o terms
+        o0, o1 = orientation_slice(n_orient, rank, world)
+        part = terms[o0:o1].sum(axis=0)
+        total = allreduce_sum(part)
+        tmax = allreduce_max(float(rank + 1))
+        q.put((rank, o0, o1, total, tmax))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_orientation_split_and_mueller_allreduce():
+    import torch.multiprocessing as mp
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    (r0, a0, a1, t0, m0), (r1, b0, b1, t1, m1) = res
+    assert (a0, a1, b0, b1) == (0, 18, 18, 37)
+    rng = np.random.default_rng(0)
+    full = rng.standard_normal((37, 16, 19)).sum(axis=0)
+    assert np.allclose(t0, full, rtol=1e-13, atol=1e-13) and np.allclose(t1, full, rtol=1e-13, atol=1e-13)
+    assert m0 == m1 == 2.0
+
+
+def test_orientation_slice_covers_all():
+    import sys
+    from bem_b200.parallel import orientation_slice
+    for n in (1, 7, 1395):
+        for world in (1, 2, 3, 8):
+            seen = []
+            for r in range(world):
+                o0, o1 = orientation_slice(n, r, world)
+                seen += list(range(o0, o1))
+            assert seen == list(range(n))
+    with pytest.raises(ValueError):
+        orientation_slice(5, 2, 2)
