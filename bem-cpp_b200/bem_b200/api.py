@@ -318,6 +318,18 @@ class LU:
             self.ctx.check(s)
         return X, st.as_dict()
 
+    def residual(self, B, X, method=1):
+        """R = B - Z X in FP64 (method 0: FP64 GEMM, 1: int8 Ozaki digits).
+        B, X: torch (nrhs, n) complex128 on the device.  Returns R like B."""
+        import torch
+        assert B.shape == X.shape and B.dtype == X.dtype == torch.complex128
+        B = B.contiguous()
+        X = X.contiguous()
+        R = torch.empty_like(B)
+        self.ctx.check(lib().bem_lu_residual_dev(self.ctx.h, self.h, _dptr(B), self.n, _dptr(X), self.n,
+                                                 _dptr(R), self.n, B.shape[0], int(method)))
+        return R
+
     def close(self):
         if self.h:
             lib().bem_lu_free(self.h)
@@ -481,6 +493,11 @@ def cgemm_tf32x3(ctx: Context, A, B, C, b_rowmajor=True, c_colmajor=False):
 
 def set_tensor_cores(ctx: Context, enable: bool):
     ctx.check(lib().bem_ctx_set_tensor_cores(ctx.h, int(bool(enable))))
+
+
+def set_residual_digits(ctx: Context, digits: int):
+    """Digits of the int8 refinement residual (0: FP64 GEMM residual)."""
+    ctx.check(lib().bem_ctx_set_residual_digits(ctx.h, int(digits)))
 
 
 def mueller_noalloc_dev(geom: Geometry, X, RT, w, k_ext, eta_ext, M_out, ntheta=181,

@@ -134,6 +134,10 @@ struct bem_ctx {
     size_t tc_bytes = 0;
     bool tc_attr = false;
     bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)
+    int oz_digits = 7;           // int8 digits of the Ozaki residual (0: FP64 DMMA residual)
+    void* oz_buf = nullptr;      // digit planes of X for the residual
+    size_t oz_bytes = 0;
+    bool oz_attr = false;
     bool prof = false;
     std::vector<ProfPending> prof_pending;
     std::vector<cudaEvent_t> prof_pool;

@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "bem_internal.h"
+#include "ozaki.h"
 
 namespace bem {
 
@@ -122,6 +123,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->tc_buf) cudaFree(ctx->tc_buf);
+    if (ctx->oz_buf) cudaFree(ctx->oz_buf);
     if (ctx->d_status) cudaFree(ctx->d_status);
     for (auto& p : ctx->prof_pending) cudaEventDestroy(p.a), cudaEventDestroy(p.b);
     for (auto e : ctx->prof_pool) cudaEventDestroy(e);
@@ -146,6 +148,14 @@ int bem_ctx_synchronize(bem_ctx* ctx) {
 const char* bem_last_error(const bem_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
 int64_t bem_ctx_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int bem_ctx_set_residual_digits(bem_ctx* ctx, int digits) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (digits != 0 && (digits < 2 || digits > bem::oz::S_MAX))
+        return bem::fail(ctx, BEM_ERR_INVALID, "residual digits must be 0 or 2..%d", bem::oz::S_MAX);
+    ctx->oz_digits = digits;
+    return BEM_OK;
+}
 
 int bem_ctx_set_tensor_cores(bem_ctx* ctx, int enable) {
     if (!ctx) return BEM_ERR_INVALID;

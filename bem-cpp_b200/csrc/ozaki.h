@@ -1,0 +1,29 @@
+// Int8 tensor-core (Ozaki scheme) FP64 residual: shared declarations.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bem_internal.h"
+
+namespace bem {
+namespace oz {
+constexpr int S_MAX = 8;  // largest digit count supported
+}
+
+// Digit planes of the fixed matrix Z' (made once per factorisation).
+struct OzakiZ {
+    int n = 0, S = 0;
+    int64_t ldk = 0;    // bytes per digit row (2n rounded up to 128)
+    int64_t plane = 0;  // bytes per digit plane (n * ldk)
+    int8_t* A = nullptr;
+    int* e = nullptr;   // per-row power-of-two exponents
+};
+
+size_t ozaki_z_bytes(int n, int S);
+int ozaki_prepare_z(bem_ctx* ctx, OzakiZ* oz, const double2* Z, int64_t ldz, int n, int S);
+void ozaki_free(OzakiZ* oz);
+// R -= Z X with FP64 accuracy (R holds B on entry).
+int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz, const double2* X, int64_t ldx, double2* R, int64_t ldr,
+                   int nrhs);
+}  // namespace bem

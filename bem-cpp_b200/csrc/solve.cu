@@ -11,6 +11,7 @@
 
 #include "bem_internal.h"
 #include "lu_internal.h"
+#include "ozaki.h"
 
 struct bem_lu {
     bem_ctx* ctx = nullptr;
@@ -25,6 +26,7 @@ struct bem_lu {
     std::vector<int> ipiv;  // 0-based interchange rows
     double znorm = 0.0;     // ||Z||_F
     double t_factor_ms = 0.0;
+    bem::OzakiZ oz;         // int8 digit planes of Z for the refinement residual (oz.A null: FP64 GEMM)
 };
 
 namespace bem {
@@ -130,6 +132,7 @@ static void lu_release(bem_lu* lu) {
     if (lu->A32) cudaFree(lu->A32);
     if (lu->d_ipiv) cudaFree(lu->d_ipiv);
     if (lu->d_perm) cudaFree(lu->d_perm);
+    bem::ozaki_free(&lu->oz);
     delete lu;
 }
 
@@ -180,6 +183,10 @@ int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu**
         if (precision == BEM_PREC_FP64) {
             s = getrf<double>(ctx, lu->Z, ldz, n, lu->d_ipiv, d_info, nullptr);
         } else {
+            // digit planes of Z for the int8 residual; without room for them the
+            // refinement keeps the FP64 tensor-core GEMM
+            if (ctx->oz_digits > 0 && ozaki_prepare_z(ctx, &lu->oz, lu->Z, ldz, n, ctx->oz_digits) != BEM_OK)
+                ozaki_free(&lu->oz);
             TrailingUpdate<float> tc = tc_update_fp32(ctx);
             s = getrf<float>(ctx, lu->A32, n, n, lu->d_ipiv, d_info, &tc);
         }
@@ -261,6 +268,8 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
     double* dmax = (double*)(ws + o_dm);
     TrailingUpdate<float> tc = tc_update_fp32(ctx);
     std::vector<double> h_dm(nrhs), h_xm(nrhs), h_sc(nrhs);
+    int h_st = 0;
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
     // x0 = (LU32)^-1 B
     colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(B, ldb, n, scale);
     BEM_LAUNCHED(ctx);
@@ -278,7 +287,10 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         // R = B - Z X  (FP64)
         copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, R, n, n, nrhs);
         BEM_LAUNCHED(ctx);
-        BEM_TRY(cgemm<double>(ctx, n, nrhs, n, lu->Z, lu->ldz, X, ldx, true, R, n, true, m1, p1, PROF_RESIDUAL));
+        int rs = lu->oz.A ? ozaki_residual(ctx, &lu->oz, X, ldx, R, n, nrhs) : BEM_ERR_OOM;
+        if (rs == BEM_ERR_OOM)
+            rs = cgemm<double>(ctx, n, nrhs, n, lu->Z, lu->ldz, X, ldx, true, R, n, true, m1, p1, PROF_RESIDUAL);
+        BEM_TRY(rs);
         colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(R, n, n, scale);
         BEM_LAUNCHED(ctx);
         colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(X, ldx, n, xmax);
@@ -293,7 +305,9 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         BEM_TRY_CUDA(ctx, cudaMemcpyAsync(h_dm.data(), dmax, nrhs * 8, cudaMemcpyDeviceToHost, ctx->stream));
         BEM_TRY_CUDA(ctx, cudaMemcpyAsync(h_xm.data(), xmax, nrhs * 8, cudaMemcpyDeviceToHost, ctx->stream));
         BEM_TRY_CUDA(ctx, cudaMemcpyAsync(h_sc.data(), scale, nrhs * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(&h_st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (h_st != 0) return fail(ctx, h_st, "device-side wait in a tensor-core kernel of the solve gave up");
         double upd = 0, res = 0;
         for (int c = 0; c < nrhs; c++) {
             double xm = h_xm[c] > 0 ? h_xm[c] : 1.0;
@@ -339,6 +353,35 @@ int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precisi
 int bem_lu_solve_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb, void* X_dev, int64_t ldx,
                      int nrhs, double tol, int max_iter, bem_solve_stats* stats) {
     return lu_solve(ctx, lu, B_dev, ldb, X_dev, ldx, nrhs, tol, max_iter, stats);
+}
+
+int bem_lu_residual_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb, const void* X_dev, int64_t ldx,
+                        void* R_dev, int64_t ldr, int nrhs, int method) {
+    if (!ctx || !lu || !B_dev || !X_dev || !R_dev || nrhs < 0 || ldb < lu->n || ldx < lu->n || ldr < lu->n)
+        return fail(ctx, BEM_ERR_INVALID, "bad lu_residual args");
+    if (lu->precision != BEM_PREC_FP32_REFINE)
+        return fail(ctx, BEM_ERR_INVALID, "residual needs an FP32_REFINE factorisation (Z kept)");
+    if (method == 1 && !lu->oz.A) return fail(ctx, BEM_ERR_INVALID, "factorisation has no int8 digit planes");
+    if (method != 0 && method != 1) return fail(ctx, BEM_ERR_INVALID, "unknown residual method %d", method);
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (nrhs == 0) return BEM_OK;
+    const int n = lu->n;
+    const double2* X = (const double2*)X_dev;
+    double2* R = (double2*)R_dev;
+    copy_cols_kernel<<<nblk((int64_t)n * nrhs), 256, 0, ctx->stream>>>((const double2*)B_dev, ldb, R, ldr, n, nrhs);
+    BEM_LAUNCHED(ctx);
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    if (method == 1) {
+        BEM_TRY(ozaki_residual(ctx, &lu->oz, X, ldx, R, ldr, nrhs));
+    } else {
+        BEM_TRY(cgemm<double>(ctx, n, nrhs, n, lu->Z, lu->ldz, X, ldx, true, R, ldr, true, make_double2(-1, 0),
+                              make_double2(1, 0), PROF_RESIDUAL));
+    }
+    int h_st = 0;
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(&h_st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h_st != 0) return fail(ctx, h_st, "device-side wait in the residual kernel gave up");
+    return BEM_OK;
 }
 
 int bem_lu_free(bem_lu* lu) {

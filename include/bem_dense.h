@@ -72,6 +72,12 @@ int bem_ctx_profile(bem_ctx* ctx, int enable);
 /* FP32 factorisation / solve updates on the tensor cores (3xTF32 tcgen05,
  * default 1) or on the CUDA cores (0). */
 int bem_ctx_set_tensor_cores(bem_ctx* ctx, int enable);
+/* FP64 refinement residual of BEM_PREC_FP32_REFINE factorisations made after
+ * this call: digits = 0 computes B - Z X with the FP64 (DMMA) complex GEMM;
+ * digits = 2..8 with the int8 tensor-core Ozaki scheme using that many 7-bit
+ * digits per entry (default 7, 49 bits; needs 2 digits x n^2 x digits bytes
+ * more device memory, and falls back to the FP64 GEMM when that is short). */
+int bem_ctx_set_residual_digits(bem_ctx* ctx, int digits);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
 const char* bem_version(void);
@@ -194,6 +200,13 @@ int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precisi
 int bem_lu_solve_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb,
                      void* X_dev, int64_t ldx, int nrhs, double tol, int max_iter,
                      bem_solve_stats* stats);
+/* R = B - Z X for a BEM_PREC_FP32_REFINE factorisation's Z (all column-major
+ * complex128, R distinct from B and X).  method 0: FP64 GEMM; method 1: the
+ * int8 Ozaki residual (BEM_ERR_INVALID when the factorisation has no digit
+ * planes).  This is the refinement's residual step on its own. */
+int bem_lu_residual_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb,
+                        const void* X_dev, int64_t ldx, void* R_dev, int64_t ldr, int nrhs,
+                        int method);
 int bem_lu_free(bem_lu* lu);
 
 /* Host-buffer mirrors of solver.h:11-22.  The reference factors its row-major
