@@ -404,15 +404,18 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                         float2* p = &C[(int64_t)row * ldc + c0];
                         const bool vec = ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (c0 + 16 <= Nc);
                         if (vec) {
+                            // all loads first: the chunk's eight 16-byte reads are in flight together
                             float4* p4 = reinterpret_cast<float4*>(p);
+                            float4 c[8];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) c[j] = p4[j];
 #pragma unroll
                             for (int j = 0; j < 8; j++) {
-                                float4 c = p4[j];
-                                c.x -= v[4 * j];
-                                c.y -= v[4 * j + 1];
-                                c.z -= v[4 * j + 2];
-                                c.w -= v[4 * j + 3];
-                                p4[j] = c;
+                                c[j].x -= v[4 * j];
+                                c[j].y -= v[4 * j + 1];
+                                c[j].z -= v[4 * j + 2];
+                                c[j].w -= v[4 * j + 3];
+                                p4[j] = c[j];
                             }
                         } else {
 #pragma unroll
@@ -425,14 +428,19 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                                 }
                         }
                     } else {
+                        // column-major C: each j is one coalesced 256-byte row segment of the warp;
+                        // issue the 16 reads before any write
+                        const int nj = min(16, Nc - c0);
+                        float2 c[16];
 #pragma unroll
                         for (int j = 0; j < 16; j++)
-                            if (c0 + j < Nc) {
-                                float2* p = &C[(int64_t)(c0 + j) * ldc + row];
-                                float2 c = *p;
-                                c.x -= v[2 * j];
-                                c.y -= v[2 * j + 1];
-                                *p = c;
+                            if (j < nj) c[j] = C[(int64_t)(c0 + j) * ldc + row];
+#pragma unroll
+                        for (int j = 0; j < 16; j++)
+                            if (j < nj) {
+                                c[j].x -= v[2 * j];
+                                c[j].y -= v[2 * j + 1];
+                                C[(int64_t)(c0 + j) * ldc + row] = c[j];
                             }
                     }
                 }

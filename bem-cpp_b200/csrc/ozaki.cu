@@ -279,18 +279,20 @@ residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
                 tmem_ld32(base + ch * 32, v);
                 const int j0 = ntl * (BN / 2) + ch * 16;
                 if (row < n) {
+                    // reads of the 16 column segments in flight together, then the writes
+                    const int nj = min(16, nrhs - j0);
+                    double2 r[16];
 #pragma unroll
-                    for (int jj = 0; jj < 16; jj++) {
-                        const int j = j0 + jj;
-                        if (j < nrhs) {
-                            const double sc = pow2i(er + f_col[j] - 7 * d);
-                            double2* p = &R[(int64_t)j * ldr + row];
-                            double2 r = *p;
-                            r.x -= sc * (double)v[2 * jj];
-                            r.y -= sc * (double)v[2 * jj + 1];
-                            *p = r;
+                    for (int jj = 0; jj < 16; jj++)
+                        if (jj < nj) r[jj] = R[(int64_t)(j0 + jj) * ldr + row];
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)
+                        if (jj < nj) {
+                            const double sc = pow2i(er + f_col[j0 + jj] - 7 * d);
+                            r[jj].x -= sc * (double)v[2 * jj];
+                            r[jj].y -= sc * (double)v[2 * jj + 1];
+                            R[(int64_t)(j0 + jj) * ldr + row] = r[jj];
                         }
-                    }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -524,8 +526,13 @@ int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ld
                                                                     ctx->d_status);
     BEM_LAUNCHED(ctx);
     if (ev) {
-        double flops = 8.0 * n * (double)n * nrhs;  // the complex product it replaces
-        ctx->prof_end(PROF_RESIDUAL, ev, flops, 16.0 * ((double)n * n + 2.0 * n * nrhs));
+        // int8 digit-pair products (2 M N K each, M = n, N = 2 nrhs, K = 2 n);
+        // bytes: the digit planes of Z and X once, R read and written once
+        int pairs = 0;
+        for (int i = 0; i < G.ng; i++) pairs += G.g[i].np;
+        double ops = (double)pairs * 2.0 * n * (2.0 * nrhs) * (2.0 * n);
+        double bytes = (double)S * n * 2.0 * n + (double)S * 2.0 * nrhs * 2.0 * n + 32.0 * n * (double)nrhs;
+        ctx->prof_end(PROF_RESIDUAL, ev, ops, bytes);
     }
     return BEM_OK;
 }

@@ -37,6 +37,7 @@ for _p in (REPO, os.path.join(REPO, "bem-cpp_b200")):
 
 METRIC = "s/solve at 2N=61440: FP32+refine vs FP64 LU on one B200 at 1e-9 rel err"
 FP64_PEAK_TFS = 37.0
+INT8_PEAK_TOPS = 3079.0
 
 
 def parse():
@@ -51,6 +52,8 @@ def parse():
     ap.add_argument("--orient", type=int, nargs=3, default=[45, 31, 1])
     ap.add_argument("--tol", type=float, default=2e-10,
                     help="refinement target: estimated max-column relative error")
+    ap.add_argument("--residual-digits", type=int, default=7,
+                    help="int8 digits of the refinement residual (0: FP64 DMMA GEMM)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -239,6 +242,7 @@ def run_bem(a):
         del lu64, Zc
         torch.cuda.empty_cache()
 
+    bb.set_residual_digits(ctx, a.residual_digits)
     X = torch.empty_like(B)
     times, stats = [], []
     launches0 = None
@@ -289,6 +293,10 @@ def run_bem(a):
         peak = pk["bf16_tflops"] / 2.0 / 3.0
         pbasis = (f"complex flops at 3xTF32: {basis} bf16 {pk['bf16_tflops']} TF/s / 2 (tf32 rate) "
                   f"/ 3 (split terms)")
+    elif name == "residual" and a.residual_digits > 0:
+        peak = INT8_PEAK_TOPS
+        pbasis = ("int8 tensor ops (digit-pair GEMMs): torch._int_mm (cuBLASLt) int8 8192^3 "
+                  "measured on this pool")
     else:
         peak = FP64_PEAK_TFS
         pbasis = ("FP64: 37.0 TF/s measured on this pool (cuBLAS ZGEMM 8192^3; DFMA and m8n8k4 DMMA "
@@ -327,7 +335,9 @@ def run_bem(a):
         line = {"metric": METRIC, "value": t_step, "unit": "s/solve", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_step * 1e3,
                 "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
-                "dtype": "complex64 factors (3xTF32) + complex128 refinement",
+                "dtype": "complex64 factors (3xTF32) + complex128 refinement" +
+                         (f" (int8 Ozaki residual, {a.residual_digits} digits)" if a.residual_digits else
+                          " (FP64 DMMA residual)"),
                 "data": "synthetic (generated icosphere mesh and plane waves)",
                 "config": {**workload(a, n), "parallelism": f"rhs-split x{world}" if world > 1 else "single"},
                 "fp64_s_per_solve": t64m or None,
