@@ -383,9 +383,33 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     } else {
         // epilogue warps 2..5: TMEM lane quarter = warp % 4
         const int q = warp & 3;
+        // C of the tile after the current one is prefetched into L2 while the
+        // tensor cores work on it, so the read-modify-write below hits L2
+        auto prefetch_c = [&](int t) {
+            if (t >= ntiles) return;
+            int mt, ntl;
+            tm.tile(t, mt, ntl);
+            const int i = q * 32 + lane;  // 128 threads: one row (row-major C) or one column (column-major C)
+            const int c0 = ntl * (BN / 2);
+            if (!c_colmajor) {
+                const int row = mt * BM + i;
+                if (row >= M || c0 >= Nc) return;
+                const char* p = reinterpret_cast<const char*>(&C[(int64_t)row * ldc + c0]);
+                const int bytes = min(BN / 2, Nc - c0) * (int)sizeof(float2);
+                for (int o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + o));
+            } else {
+                const int col = c0 + i, r0 = mt * BM;
+                if (col >= Nc || r0 >= M) return;
+                const char* p = reinterpret_cast<const char*>(&C[(int64_t)col * ldc + r0]);
+                const int bytes = min(BM, M - r0) * (int)sizeof(float2);
+                for (int o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + o));
+            }
+        };
+        prefetch_c(blockIdx.x);
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
             const int b = lt & 1;
+            prefetch_c(t + gridDim.x);
             bool ok = mbar_wait(smem_u32(&tfull[b]), (lt >> 1) & 1, status, &abort_flag);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;

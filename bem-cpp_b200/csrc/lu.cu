@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -377,28 +378,170 @@ trsm_small_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
 
 template <typename R> struct TBsel { static constexpr int v = 16; };
 
+// ------------------------------------------------------------ block TRSM
+// Solves T X = X for a whole diagonal block T = A[r0.., r0..] (kb <= 256 rows;
+// UPPER: non-unit upper, backward substitution; else unit lower, forward) in
+// one launch, for the columns [c0, c1) of a right-hand side held row-major in
+// the factor itself (B_ROWMAJOR, the U12 step) or column-major (the solves).
+// One CTA owns RB columns with their kb rows in shared memory (column-major,
+// pitch 257) and walks the 16-row diagonal sub-blocks in order: the RB
+// threads of the first warps solve the sub-block in registers, then every
+// thread updates the one row it owns with the sub-block's 16 solved rows
+// (T's row segment in registers, the solved values broadcast from shared
+// memory).  This replaces a TRSM + GEMM launch pair per 16 rows.
+constexpr int TRSM_KB = 256, TRSM_TS = 16, TRSM_PITCH = TRSM_KB + 1;
+
+template <typename R, bool UPPER, bool B_ROWMAJOR, int RB>
+__global__ void __launch_bounds__(TRSM_KB)
+trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int r0, int kb,
+                  typename C2T<R>::type* __restrict__ B, int64_t ldb, int c0, int c1) {
+    using C2 = typename C2T<R>::type;
+    constexpr int TS = TRSM_TS, XP = TRSM_PITCH;
+    extern __shared__ __align__(16) unsigned char trsm_smem[];
+    C2* xs = reinterpret_cast<C2*>(trsm_smem);  // xs[c * XP + r]
+    __shared__ C2 sT[TS][TS + 1];
+    C2 zero;
+    zero.x = 0;
+    zero.y = 0;
+    const int cb = c0 + blockIdx.x * RB;
+    const int nc = min(RB, c1 - cb);
+    for (int e = threadIdx.x; e < kb * RB; e += blockDim.x) {
+        int r, c;
+        if (B_ROWMAJOR) {
+            r = e / RB;
+            c = e % RB;
+        } else {
+            c = e / kb;
+            r = e % kb;
+        }
+        C2 v = zero;
+        if (c < nc) v = B_ROWMAJOR ? B[(int64_t)(r0 + r) * ldb + cb + c] : B[(int64_t)(cb + c) * ldb + r0 + r];
+        xs[c * XP + r] = v;
+    }
+    const int nsb = (kb + TS - 1) / TS;
+    for (int step = 0; step < nsb; step++) {
+        const int sb = UPPER ? nsb - 1 - step : step;
+        const int s0 = sb * TS, ts = min(TS, kb - s0);
+        for (int e = threadIdx.x; e < TS * TS; e += blockDim.x) {
+            const int i = e / TS, j = e % TS;
+            sT[i][j] = (i < ts && j < ts) ? T[(int64_t)(r0 + s0 + i) * ldt + r0 + s0 + j] : zero;
+        }
+        __syncthreads();
+        if (threadIdx.x < RB) {
+            const int c = threadIdx.x;
+            C2 x[TS];
+#pragma unroll
+            for (int i = 0; i < TS; i++) x[i] = i < ts ? xs[c * XP + s0 + i] : zero;
+            if (!UPPER) {
+#pragma unroll
+                for (int i = 1; i < TS; i++) {
+                    C2 acc = x[i];
+#pragma unroll
+                    for (int k = 0; k < i; k++) {
+                        const C2 l = sT[i][k];
+                        acc.x -= l.x * x[k].x - l.y * x[k].y;
+                        acc.y -= l.x * x[k].y + l.y * x[k].x;
+                    }
+                    x[i] = acc;
+                }
+            } else {
+#pragma unroll
+                for (int ii = TS - 1; ii >= 0; ii--) {
+                    if (ii >= ts) continue;
+                    C2 acc = x[ii];
+#pragma unroll
+                    for (int k = ii + 1; k < TS; k++) {
+                        const C2 u = sT[ii][k];
+                        acc.x -= u.x * x[k].x - u.y * x[k].y;
+                        acc.y -= u.x * x[k].y + u.y * x[k].x;
+                    }
+                    const C2 d = sT[ii][ii];
+                    const R den = d.x * d.x + d.y * d.y;
+                    C2 q;
+                    q.x = (acc.x * d.x + acc.y * d.y) / den;
+                    q.y = (acc.y * d.x - acc.x * d.y) / den;
+                    x[ii] = q;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < TS; i++)
+                if (i < ts) xs[c * XP + s0 + i] = x[i];
+        }
+        __syncthreads();
+        const int r = threadIdx.x;
+        const bool active = UPPER ? (r < s0) : (r >= s0 + ts && r < kb);
+        if (active) {
+            C2 t[TS];
+#pragma unroll
+            for (int m = 0; m < TS; m++) t[m] = m < ts ? T[(int64_t)(r0 + r) * ldt + r0 + s0 + m] : zero;
+#pragma unroll 4
+            for (int c = 0; c < RB; c++) {
+                C2 acc = xs[c * XP + r];
+#pragma unroll
+                for (int m = 0; m < TS; m++) {
+                    const C2 y = xs[c * XP + s0 + m];
+                    acc.x -= t[m].x * y.x - t[m].y * y.y;
+                    acc.y -= t[m].x * y.y + t[m].y * y.x;
+                }
+                xs[c * XP + r] = acc;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kb * RB; e += blockDim.x) {
+        int r, c;
+        if (B_ROWMAJOR) {
+            r = e / RB;
+            c = e % RB;
+        } else {
+            c = e / kb;
+            r = e % kb;
+        }
+        if (c < nc) {
+            if (B_ROWMAJOR) B[(int64_t)(r0 + r) * ldb + cb + c] = xs[c * XP + r];
+            else B[(int64_t)(cb + c) * ldb + r0 + r] = xs[c * XP + r];
+        }
+    }
+}
+
+// Column-block width of the block TRSM: the factor's U12 rows are wide
+// (many columns per CTA amortise the serial sub-block solves), the solves'
+// right-hand sides are fewer (more CTAs).  64 KB of shared memory at most.
+template <typename R> struct TrsmRB {
+    static constexpr int rows_major = sizeof(R) == 4 ? 32 : 16;
+    static constexpr int col_major = sizeof(R) == 4 ? 16 : 8;
+};
+
+template <typename R, bool UPPER, bool B_ROWMAJOR>
+int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0, int kb,
+               typename C2T<R>::type* B, int64_t ldb, int c0, int c1) {
+    using C2 = typename C2T<R>::type;
+    constexpr int RB = B_ROWMAJOR ? TrsmRB<R>::rows_major : TrsmRB<R>::col_major;
+    if (c1 <= c0 || kb <= 0) return BEM_OK;
+    if (kb > TRSM_KB) return fail(ctx, BEM_ERR_INVALID, "block TRSM: %d rows > %d", kb, TRSM_KB);
+    const size_t smem = (size_t)RB * TRSM_PITCH * sizeof(C2);
+    static_assert(RB * TRSM_PITCH * sizeof(C2) <= 66 * 1024, "block TRSM shared memory");
+    // the attribute is per device: one bit per device id, set once
+    static std::atomic<unsigned long long> attr_set{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_set.load() & bit)) {
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set.fetch_or(bit);
+    }
+    const int grid = (c1 - c0 + RB - 1) / RB;
+    trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB><<<grid, TRSM_KB, smem, ctx->stream>>>(T, ldt, r0, kb, B, ldb, c0,
+                                                                                     c1);
+    BEM_LAUNCHED(ctx);
+    return BEM_OK;
+}
+
 // Unit-lower TRSM on rows [r0, r0+kb) of the row-major matrix itself, for
 // columns [c0, c1): the U12 step of the factorisation.
 template <typename R>
 int trsm_rows_lower_unit(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int r0, int kb,
                          int c0, int c1) {
-    using C2 = typename C2T<R>::type;
-    constexpr int TB = TBsel<R>::v;
-    int nc = c1 - c0;
-    if (nc <= 0 || kb <= 0) return BEM_OK;
-    for (int b = 0; b < kb; b += TB) {
-        int tb = std::min(TB, kb - b);
-        trsm_small_kernel<R, TB, false, true><<<(nc + 127) / 128, 128, 0, ctx->stream>>>(
-            A, lda, r0 + b, tb, A, lda, c0, c1);
-        BEM_LAUNCHED(ctx);
-        int rest = kb - b - tb;
-        if (rest > 0)
-            BEM_TRY(cgemm<R>(ctx, rest, nc, tb, A + (int64_t)(r0 + b + tb) * lda + r0 + b, lda,
-                             A + (int64_t)(r0 + b) * lda + c0, lda, false,
-                             A + (int64_t)(r0 + b + tb) * lda + c0, lda, false, mk<C2>(-1, 0),
-                             mk<C2>(1, 0)));
-    }
-    return BEM_OK;
+    return trsm_block<R, false, true>(ctx, A, lda, r0, kb, A, lda, c0, c1);
 }
 
 // ------------------------------------------------------------------ getrf
@@ -509,7 +652,6 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
           const typename C2T<R>::type* B, int64_t ldb, typename C2T<R>::type* X, int64_t ldx,
           int nrhs, const TrailingUpdate<R>* tc) {
     using C2 = typename C2T<R>::type;
-    constexpr int TB = TBsel<R>::v;
     const int NB = 256;
     if (nrhs <= 0) return BEM_OK;
     int64_t tot = (int64_t)n * nrhs;
@@ -519,17 +661,7 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
     // forward: L Y = P B
     for (int j0 = 0; j0 < n; j0 += NB) {
         int jb = std::min(NB, n - j0);
-        for (int b = 0; b < jb; b += TB) {
-            int tb = std::min(TB, jb - b);
-            trsm_small_kernel<R, TB, false, false><<<(nrhs + 127) / 128, 128, 0, ctx->stream>>>(
-                LU, lda, j0 + b, tb, X, ldx, 0, nrhs);
-            BEM_LAUNCHED(ctx);
-            int rest = jb - b - tb;
-            if (rest > 0)
-                BEM_TRY(cgemm<R>(ctx, rest, nrhs, tb, LU + (int64_t)(j0 + b + tb) * lda + j0 + b, lda,
-                                 X + j0 + b, ldx, true, X + j0 + b + tb, ldx, true, mk<C2>(-1, 0),
-                                 mk<C2>(1, 0)));
-        }
+        BEM_TRY((trsm_block<R, false, false>(ctx, LU, lda, j0, jb, X, ldx, 0, nrhs)));
         int below = n - j0 - jb;
         if (below > 0) {
             if (tc && tc->fn_solve)
@@ -544,16 +676,7 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
     int nblk = (n + NB - 1) / NB;
     for (int bi = nblk - 1; bi >= 0; bi--) {
         int j0 = bi * NB, jb = std::min(NB, n - j0);
-        int nsub = (jb + TB - 1) / TB;
-        for (int s = nsub - 1; s >= 0; s--) {
-            int b = s * TB, tb = std::min(TB, jb - b);
-            trsm_small_kernel<R, TB, true, false><<<(nrhs + 127) / 128, 128, 0, ctx->stream>>>(
-                LU, lda, j0 + b, tb, X, ldx, 0, nrhs);
-            BEM_LAUNCHED(ctx);
-            if (b > 0)
-                BEM_TRY(cgemm<R>(ctx, b, nrhs, tb, LU + (int64_t)j0 * lda + j0 + b, lda, X + j0 + b, ldx, true,
-                                 X + j0, ldx, true, mk<C2>(-1, 0), mk<C2>(1, 0)));
-        }
+        BEM_TRY((trsm_block<R, true, false>(ctx, LU, lda, j0, jb, X, ldx, 0, nrhs)));
         if (j0 > 0) {
             if (tc && tc->fn_solve)
                 BEM_TRY(tc->fn_solve(ctx, tc->state, j0, nrhs, jb, LU + j0, lda, X + j0, ldx, X, ldx));

@@ -255,10 +255,24 @@ residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
         }
     } else {
         const int q = warp & 3;
+        // R of the next tile is prefetched into L2 while the current one is
+        // multiplied (one column segment of 128 rows per thread)
+        auto prefetch_r = [&](int u) {
+            if (u >= ntiles) return;
+            int mt, ntl;
+            unit_tile(u, mt, ntl);
+            const int j = ntl * (BN / 2) + q * 32 + lane, r0 = mt * BM;
+            if (j >= nrhs || r0 >= n) return;
+            const char* p = reinterpret_cast<const char*>(&R[(int64_t)j * ldr + r0]);
+            const int bytes = min(BM, n - r0) * (int)sizeof(double2);
+            for (int o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + o));
+        };
+        prefetch_r(blockIdx.x);
         int lt = 0;
         bool stop = false;
         for (int u = blockIdx.x; u < ntiles && !stop; u += gridDim.x)
         for (int gr = 0; gr < G.ng; gr++, lt++) {
+            if (gr == 0) prefetch_r(u + gridDim.x);
             const int b = lt & 1;
             bool ok = mbar_wait(smem_u32(&tfull[b]), (lt >> 1) & 1, status, &abort_flag);
             ok = __all_sync(0xffffffffu, ok);
@@ -333,13 +347,31 @@ __global__ void row_exp_kernel(const double2* __restrict__ Z, int64_t ldz, int n
     if (threadIdx.x == 0) e[blockIdx.x] = s[0] > 0.0 ? ilogb(s[0]) + 2 : 0;
 }
 
+// The right-hand operand: X itself (complex128), or a refinement correction
+// held as complex64 D with a per-column FP64 scale, X[:, j] = scale[j] D[:, j]
+// (the product rounded to FP64, as the refinement adds it to the iterate).
+struct ColSrc {
+    const double2* X;
+    const float2* D;
+    const double* scale;
+    int64_t ld;
+    __device__ __forceinline__ double2 get(int j, int k) const {
+        if (X) return X[(int64_t)j * ld + k];
+        const double sc = scale[j];
+        const float2 d = D[(int64_t)j * ld + k];
+        return make_double2(sc * (double)d.x, sc * (double)d.y);
+    }
+};
+
 // f[j] for column j of X (column-major): both X' rows 2j, 2j+1 hold the same
 // magnitudes, so one exponent per complex column.
-__global__ void col_exp_kernel(const double2* __restrict__ X, int64_t ldx, int n, int* __restrict__ f) {
+__global__ void col_exp_kernel(ColSrc src, int n, int* __restrict__ f) {
     __shared__ double s[256];
-    const double2* col = X + (int64_t)blockIdx.x * ldx;
     double m = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) m = fmax(m, fmax(fabs(col[k].x), fabs(col[k].y)));
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const double2 v = src.get(blockIdx.x, k);
+        m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
     s[threadIdx.x] = m;
     __syncthreads();
     for (int o = 128; o > 0; o >>= 1) {
@@ -381,14 +413,13 @@ __global__ void slice_rows_kernel(const double2* __restrict__ Z, int64_t ldz, in
 }
 
 // B digit planes: B[t][2j + p][k'] for X' rows (Re, -Im) / (Im, Re).
-__global__ void slice_cols_kernel(const double2* __restrict__ X, int64_t ldx, int n, int nrhs,
-                                  const int* __restrict__ f, int8_t* __restrict__ B, int64_t ldk, int64_t plane,
-                                  int S) {
+__global__ void slice_cols_kernel(ColSrc src, int n, int nrhs, const int* __restrict__ f, int8_t* __restrict__ B,
+                                  int64_t ldk, int64_t plane, int S) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t kc = ldk / 2;
     if (t >= (int64_t)nrhs * kc) return;
     const int j = (int)(t / kc), k = (int)(t % kc);
-    double2 x = k < n ? X[(int64_t)j * ldx + k] : make_double2(0.0, 0.0);
+    double2 x = k < n ? src.get(j, k) : make_double2(0.0, 0.0);
     const int ex = f[j];
     int8_t qr[S_MAX], qi[S_MAX];
     const double sc = pow2i(-ex);
@@ -462,10 +493,10 @@ void ozaki_free(OzakiZ* oz_) {
     oz_->e = nullptr;
 }
 
-// R -= Z X (R already holds B).  X, R: column-major n x nrhs complex128.
-int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ldx, double2* R, int64_t ldr,
-                   int nrhs) {
-    const int n = oz_->n, S = oz_->S;
+// R -= Z X with the first S digits of Z and of X (S <= the digits of Z).
+static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2* R, int64_t ldr, int nrhs, int S) {
+    const int n = oz_->n;
+    if (S < 2 || S > oz_->S) return fail(ctx, BEM_ERR_INVALID, "ozaki residual: %d digits of %d", S, oz_->S);
     const int64_t ldk = oz_->ldk;
     const int64_t bplane = (int64_t)2 * nrhs * ldk;
     size_t need = (size_t)S * bplane + (size_t)nrhs * sizeof(int) + 512;
@@ -486,14 +517,14 @@ int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ld
     int8_t* Bd = (int8_t*)ctx->oz_buf;
     int* f = (int*)((char*)ctx->oz_buf + (((size_t)S * bplane + 255) & ~(size_t)255));
     cudaEvent_t ev = ctx->prof_begin(PROF_RESIDUAL);
-    oz::col_exp_kernel<<<nrhs, 256, 0, ctx->stream>>>(X, ldx, n, f);
+    oz::col_exp_kernel<<<nrhs, 256, 0, ctx->stream>>>(src, n, f);
     BEM_LAUNCHED(ctx);
     int64_t tot = (int64_t)nrhs * (ldk / 2);
-    oz::slice_cols_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(X, ldx, n, nrhs, f, Bd, ldk, bplane,
+    oz::slice_cols_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(src, n, nrhs, f, Bd, ldk, bplane,
                                                                                   S);
     BEM_LAUNCHED(ctx);
     CUtensorMap tA, tB;
-    BEM_TRY(encode_i8(ctx, &tA, oz_->A, (int64_t)S * n, ldk, oz::BM));
+    BEM_TRY(encode_i8(ctx, &tA, oz_->A, (int64_t)oz_->S * n, ldk, oz::BM));
     BEM_TRY(encode_i8(ctx, &tB, Bd, (int64_t)S * 2 * nrhs, ldk, oz::BN));
     // digit pairs s + t <= S + 1 (1-based), grouped by d = s + t, <= MAXP per group
     // int32 safety: maxp pairs of |q q| <= 2^12 over ldk terms stay below 2^31
@@ -535,6 +566,23 @@ int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ld
         ctx->prof_end(PROF_RESIDUAL, ev, ops, bytes);
     }
     return BEM_OK;
+}
+
+// R -= Z X (R already holds B).  X, R: column-major n x nrhs complex128.
+int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ldx, double2* R, int64_t ldr,
+                   int nrhs) {
+    oz::ColSrc src{X, nullptr, nullptr, ldx};
+    return ozaki_apply(ctx, oz_, src, R, ldr, nrhs, oz_->S);
+}
+
+// R -= Z (scale D): the residual of the next refinement iterate from the
+// current one (r_{k+1} = r_k - Z d_k), with `digits` digits for the correction
+// (it is small against the iterate, so fewer digits reach the same absolute
+// accuracy).
+int ozaki_residual_update(bem_ctx* ctx, const OzakiZ* oz_, const float2* D, int64_t ldd, const double* scale,
+                          double2* R, int64_t ldr, int nrhs, int digits) {
+    oz::ColSrc src{nullptr, D, scale, ldd};
+    return ozaki_apply(ctx, oz_, src, R, ldr, nrhs, digits);
 }
 
 }  // namespace bem

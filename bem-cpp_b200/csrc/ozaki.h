@@ -26,4 +26,8 @@ void ozaki_free(OzakiZ* oz);
 // R -= Z X with FP64 accuracy (R holds B on entry).
 int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz, const double2* X, int64_t ldx, double2* R, int64_t ldr,
                    int nrhs);
+// R -= Z (scale[j] D[:, j]) with `digits` (<= oz->S) digits: the update form
+// r_{k+1} = r_k - Z d_k of the refinement residual.
+int ozaki_residual_update(bem_ctx* ctx, const OzakiZ* oz, const float2* D, int64_t ldd, const double* scale,
+                          double2* R, int64_t ldr, int nrhs, int digits);
 }  // namespace bem
