@@ -37,6 +37,12 @@ for _p in (REPO, os.path.join(REPO, "bem-cpp_b200")):
 
 METRIC = "s/solve at 2N=61440: FP32+refine vs FP64 LU on one B200 at 1e-9 rel err"
 FP64_PEAK_TFS = 37.0
+# DRAM traffic per algorithmic byte of a kernel class, from one ncu capture of a
+# smaller launch of the same kernel whose traffic grows with the same units
+TRAFFIC_RATIO = {
+    "lu_update": (1.49, "ncu dram__bytes_read+write / algorithmic bytes of the 3xTF32 update at "
+                        "M=N=15104, K=256 (5.52 GB / 3.71 GB), scaled to the average launch"),
+}
 
 
 def parse():
@@ -303,9 +309,14 @@ def run_bem(a):
         peak = FP64_PEAK_TFS
         pbasis = ("FP64: 37.0 TF/s measured on this pool (cuBLAS ZGEMM 8192^3; DFMA and m8n8k4 DMMA "
                   "throughput probes 36-37 TF/s); MEASURED_PEAKS.json has no FP64 figure")
+    traffic, tbasis = None, None
+    if name in TRAFFIC_RATIO:
+        ratio, tbasis = TRAFFIC_RATIO[name]
+        traffic = ratio * by / max(nl, 1)
     roof = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": None, "launches": nl, "ms_per_launch": ms_launch,
-            "peak_basis": pbasis,
+            "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes per launch",
+            "traffic_basis": tbasis, "algorithmic_bytes_per_launch": by / max(nl, 1),
+            "launches": nl, "ms_per_launch": ms_launch, "peak_basis": pbasis,
             "share": {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()}}
 
     # free the step buffers before the end-to-end pipeline
