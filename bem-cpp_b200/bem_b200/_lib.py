@@ -36,7 +36,8 @@ class SolveStats(C.Structure):
                 ("max_rel_update", C.c_double), ("max_rel_residual", C.c_double),
                 ("est_rel_error", C.c_double),
                 ("t_factor_ms", C.c_double), ("t_solve_ms", C.c_double),
-                ("t_refine_ms", C.c_double), ("update_hist", C.c_double * 12)]
+                ("t_refine_ms", C.c_double), ("update_hist", C.c_double * 12),
+                ("factorization", C.c_int)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_}
@@ -80,6 +81,7 @@ SIGNATURES = {
     "bem_ctx_profile": (_I, [_P, _I]),
     "bem_ctx_set_tensor_cores": (_I, [_P, _I]),
     "bem_ctx_set_residual_digits": (_I, [_P, _I]),
+    "bem_ctx_set_symmetric": (_I, [_P, _I]),
     "bem_lu_residual_dev": (_I, [_P, _P, _P, _L, _P, _L, _P, _L, _I, _I]),
     "bem_cgemm_tf32x3": (_I, [_P, _I, _I, _I, _P, _L, _P, _L, _I, _P, _L, _I]),
     "bem_ctx_profile_read": (_I, [_P, _I, C.POINTER(_L), C.POINTER(_D), C.POINTER(_D),
@@ -117,6 +119,7 @@ SIGNATURES = {
     "bem_farfield_mueller_noalloc": (_I, [_P, _P, _P, _L, _P, _P, _I, _D, _D, _D, _I, _I, _P]),
     "bem_amplitude_to_mueller": (_I, [_P, _P, _P, _P, _I, _P]),
     "bem_dense_run": (_I, [_P, C.POINTER(Problem), C.POINTER(Result)]),
+    "bem_batch_run": (_I, [_P, C.POINTER(Problem), _I, C.POINTER(Result), C.POINTER(_I)]),
 }
 
 _lib = None

@@ -457,6 +457,20 @@ def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=Fals
               ntheta=181, precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False):
     """The --solver dense pipeline (main.cpp:660-854) through bem_dense_run.
     Returns (mueller (4,4,ntheta), info dict)."""
+    p, _keep = _problem(verts, tris, ka, m, quad_order, single, orient, orient_sym, gamma_mirror,
+                        orient_range, ntheta, precision, refine_tol, max_refine, exact_gsmooth)
+    M = np.zeros((4, 4, ntheta))
+    r = Result(mueller=M.ctypes.data)
+    ctx.check(lib().bem_dense_run(ctx.h, C.byref(p), C.byref(r)))
+    info = {"N": r.N, "n_orient": r.n_orient, "t_assembly_s": r.t_assembly_s,
+            "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s, "t_total_s": r.t_total_s,
+            "stats": r.stats.as_dict()}
+    return M, info
+
+
+def _problem(verts, tris, ka, m=1.3116, quad_order=7, single=False, orient=(8, 8, 1),
+             orient_sym=(1, 1), gamma_mirror=False, orient_range=None, ntheta=181,
+             precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False):
     v, t = _f64(verts), _i32(tris)
     m = complex(m)
     i0, i1 = orient_range if orient_range is not None else (-1, -1)
@@ -467,13 +481,55 @@ def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=Fals
                 gamma_mirror=int(bool(gamma_mirror)), orient_i0=int(i0), orient_i1=int(i1),
                 ntheta=int(ntheta), precision=int(precision), refine_tol=float(refine_tol),
                 max_refine=int(max_refine), asm_flags=ASM_GSMOOTH_EXACT if exact_gsmooth else 0)
-    M = np.zeros((4, 4, ntheta))
-    r = Result(mueller=M.ctypes.data)
-    ctx.check(lib().bem_dense_run(ctx.h, C.byref(p), C.byref(r)))
-    info = {"N": r.N, "n_orient": r.n_orient, "t_assembly_s": r.t_assembly_s,
-            "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s, "t_total_s": r.t_total_s,
-            "stats": r.stats.as_dict()}
-    return M, info
+    return p, (v, t)
+
+
+def batch_run(ctx: Context, particles, raise_on_error=True):
+    """Many particles through bem_batch_run.  `particles`: list of dicts with
+    the keyword arguments of dense_run (verts, tris, ka, m, orient, ...; a
+    "meta" entry is ignored).
+    Returns a list of (mueller (4,4,ntheta), info) with info["status"] per
+    particle (0 = OK)."""
+    n = len(particles)
+    probs = (Problem * max(n, 1))()
+    res = (Result * max(n, 1))()
+    keep, outs = [], []
+    for i, kw in enumerate(particles):
+        p, arrays = _problem(**{k: v for k, v in kw.items() if k != "meta"})
+        keep.append(arrays)
+        probs[i] = p
+        M = np.zeros((4, 4, p.ntheta))
+        outs.append(M)
+        res[i].mueller = M.ctypes.data
+    st = (C.c_int * max(n, 1))()
+    s = lib().bem_batch_run(ctx.h, probs, n, res, st)
+    if s != 0 and raise_on_error:
+        ctx.check(s)
+    out = []
+    for i in range(n):
+        r = res[i]
+        out.append((outs[i], {"status": st[i], "N": r.N, "n_orient": r.n_orient,
+                              "t_assembly_s": r.t_assembly_s, "t_solve_s": r.t_solve_s,
+                              "t_farfield_s": r.t_farfield_s, "t_total_s": r.t_total_s,
+                              "stats": r.stats.as_dict()}))
+    return out
+
+
+def c4_particles(seed, count=64, orient=(4, 4, 1), ntheta=181, precision=PREC_FP64):
+    """The seeded batched-particle workload: hex prisms with aspect ratio
+    U[0.5, 2], refinement 2 or 3 (2N = 1152 / 4608), ka U[1, 5], Re m
+    U[1.30, 1.60], Im m log-uniform in [1e-6, 1e-2], 4 x 4 x 1 orientations."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        ar = rng.uniform(0.5, 2.0)
+        ref = int(rng.integers(2, 4))
+        ka = rng.uniform(1.0, 5.0)
+        m = complex(rng.uniform(1.30, 1.60), 10.0 ** rng.uniform(-6.0, -2.0))
+        v, t = hex_prism(ar, ref)
+        out.append(dict(verts=v, tris=t, ka=ka, m=m, orient=orient, ntheta=ntheta, precision=precision,
+                        meta={"aspect_ratio": ar, "refinements": ref}))
+    return out
 
 
 def cgemm_tf32x3(ctx: Context, A, B, C, b_rowmajor=True, c_colmajor=False):
@@ -493,6 +549,12 @@ def cgemm_tf32x3(ctx: Context, A, B, C, b_rowmajor=True, c_colmajor=False):
 
 def set_tensor_cores(ctx: Context, enable: bool):
     ctx.check(lib().bem_ctx_set_tensor_cores(ctx.h, int(bool(enable))))
+
+
+def set_symmetric(ctx: Context, mode: int):
+    """1 (default): FP32 L D L^T without pivoting for symmetric-structured Z
+    (PMCHWT); 0: always LU with partial pivoting."""
+    ctx.check(lib().bem_ctx_set_symmetric(ctx.h, int(mode)))
 
 
 def set_residual_digits(ctx: Context, digits: int):

@@ -423,7 +423,11 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
         cplx t1 = cmul(ik, Lv[e]), t2 = cmul(iok, Ls[e]);
         Lf[e] = {t1.re - t2.re, t1.im - t2.im};
     }
-    const bool mirror = (bi != bj);
+    // L and K are symmetric: in a diagonal tile only the thread of the upper
+    // entry writes, to both positions, so the stored blocks are exactly
+    // symmetric (as after the reference's (X + X^T)/2, assembly.cu:494-502)
+    if (bi == bj && n < mm) return;
+    const bool mirror = (n != mm);
     if (NMED == 2) {
         cplx TL = {a.eta_e * Lf[0].re + a.eta_i * Lf[1].re, a.eta_e * Lf[0].im + a.eta_i * Lf[1].im};
         cplx BR = {Lf[0].re / a.eta_e + Lf[1].re / a.eta_i, Lf[0].im / a.eta_e + Lf[1].im / a.eta_i};

@@ -134,6 +134,7 @@ struct bem_ctx {
     size_t tc_bytes = 0;
     bool tc_attr = false;
     bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)
+    int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)
     int oz_digits = 7;           // int8 digits of the Ozaki residual (0: FP64 DMMA residual)
     void* oz_buf = nullptr;      // digit planes of X for the residual
     size_t oz_bytes = 0;

@@ -149,6 +149,13 @@ const char* bem_last_error(const bem_ctx* ctx) { return ctx ? ctx->last_error.c_
 
 int64_t bem_ctx_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int bem_ctx_set_symmetric(bem_ctx* ctx, int mode) {
+    if (!ctx) return BEM_ERR_INVALID;
+    if (mode != 0 && mode != 1) return bem::fail(ctx, BEM_ERR_INVALID, "symmetric mode must be 0 or 1");
+    ctx->sym_mode = mode;
+    return BEM_OK;
+}
+
 int bem_ctx_set_residual_digits(bem_ctx* ctx, int digits) {
     if (!ctx) return BEM_ERR_INVALID;
     if (digits != 0 && (digits < 2 || digits > bem::oz::S_MAX))

@@ -266,6 +266,8 @@ constexpr uint32_t TMEM_COLS2 = 512;
 
 struct TileMap {
     int num_m, num_n;
+    int lower;  // square C, only tiles on or below the diagonal (BM rows == BN / 2 complex columns)
+    __device__ __forceinline__ bool skip(int mt, int nt) const { return lower && nt > mt; }
     __device__ __forceinline__ void tile(int t, int& mt, int& nt) const {
         const int per_group = GROUP_M * num_n;
         const int g = t / per_group, first_m = g * GROUP_M;
@@ -283,7 +285,8 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 __global__ void __launch_bounds__(192, 1)
 gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                        const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
-                       float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int* status) {
+                       float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int lower,
+                       int* status) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
@@ -300,6 +303,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     TileMap tm;
     tm.num_m = (M + BM - 1) / BM;
     tm.num_n = (2 * Nc + BN - 1) / BN;
+    tm.lower = lower;
     const int ntiles = tm.num_m * tm.num_n;
 
     if (threadIdx.x == 0) {
@@ -331,6 +335,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
             for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
                 int mt, ntl;
                 tm.tile(t, mt, ntl);
+                if (tm.skip(mt, ntl)) continue;
                 for (int kt = 0; kt < nk; kt++, it++) {
                     const int s = it % STAGES;
                     if (!mbar_wait(smem_u32(&empty[s]), ((it / STAGES) & 1) ^ 1, status, &abort_flag)) break;
@@ -348,9 +353,15 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     } else if (warp == 1) {
         if (lane == 0) {
             int it = 0, lt = 0;
-            for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, lt++) {
+            for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+                {
+                    int mt, ntl;
+                    tm.tile(t, mt, ntl);
+                    if (tm.skip(mt, ntl)) continue;
+                }
                 const int b = lt & 1;
-                if (!mbar_wait(smem_u32(&tempty[b]), ((lt >> 1) & 1) ^ 1, status, &abort_flag)) break;
+                lt++;  // accumulator buffers alternate over the tiles this CTA computes
+                if (!mbar_wait(smem_u32(&tempty[b]), (((lt - 1) >> 1) & 1) ^ 1, status, &abort_flag)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t acc = tmem + (uint32_t)(b * 256);
                 bool ok = true;
@@ -389,6 +400,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
             if (t >= ntiles) return;
             int mt, ntl;
             tm.tile(t, mt, ntl);
+            if (tm.skip(mt, ntl)) return;
             const int i = q * 32 + lane;  // 128 threads: one row (row-major C) or one column (column-major C)
             const int c0 = ntl * (BN / 2);
             if (!c_colmajor) {
@@ -407,10 +419,17 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
         };
         prefetch_c(blockIdx.x);
         int lt = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            {
+                int mt, ntl;
+                tm.tile(t, mt, ntl);
+                if (tm.skip(mt, ntl)) continue;
+            }
             const int b = lt & 1;
+            const int ph = (lt >> 1) & 1;
+            lt++;
             prefetch_c(t + gridDim.x);
-            bool ok = mbar_wait(smem_u32(&tfull[b]), (lt >> 1) & 1, status, &abort_flag);
+            bool ok = mbar_wait(smem_u32(&tfull[b]), ph, status, &abort_flag);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -507,14 +526,43 @@ __global__ void pack_a_kernel(const float2* __restrict__ A, int64_t lda, int M, 
     reinterpret_cast<float2*>(lo + (int64_t)i * ld)[k] = make_float2(l0, l1);
 }
 
+// A given as its transpose (At: K x M row-major, A[i][k] = At[k*lda + i]),
+// transposed through shared memory into the K-major hi / lo planes.
+__global__ void pack_a_trans_kernel(const float2* __restrict__ At, int64_t lda, int M, int K, float* __restrict__ hi,
+                                    float* __restrict__ lo, int ld) {
+    __shared__ float2 tile[32][33];
+    const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 256 threads: 8 rows per pass
+    for (int r = ty; r < 32; r += 8) {
+        int k = k0 + r, i = i0 + tx;
+        tile[r][tx] = (k < K && i < M) ? At[(int64_t)k * lda + i] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        int i = i0 + r, k = k0 + tx;
+        if (i >= M || k >= ld / 2) continue;
+        float2 a = tile[tx][r];
+        float h0 = to_tf32(a.x), h1 = to_tf32(a.y);
+        float l0 = to_tf32(a.x - h0), l1 = to_tf32(a.y - h1);
+        reinterpret_cast<float2*>(hi + (int64_t)i * ld)[k] = make_float2(h0, h1);
+        reinterpret_cast<float2*>(lo + (int64_t)i * ld)[k] = make_float2(l0, l1);
+    }
+}
+
 // B given column-major (B[j*ldb + k], K contiguous): rows 2j, 2j+1 of B'.
+// With `dsc`, B[k][j] is multiplied by the complex factor dsc[k * dstride]
+// first (the D of an L D L^T update, read from the factor's diagonal).
 __global__ void pack_b_col_kernel(const float2* __restrict__ B, int64_t ldb, int N, int K, float* __restrict__ hi,
-                                  float* __restrict__ lo, int ld) {
+                                  float* __restrict__ lo, int ld, const float2* __restrict__ dsc, int64_t dstride) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t tot = (int64_t)N * (ld / 2);
     if (t >= tot) return;
     int j = (int)(t / (ld / 2)), k = (int)(t % (ld / 2));
     float2 b = k < K ? B[(int64_t)j * ldb + k] : make_float2(0.f, 0.f);
+    if (dsc && k < K) {
+        const float2 d = dsc[(int64_t)k * dstride];
+        b = make_float2(b.x * d.x - b.y * d.y, b.x * d.y + b.y * d.x);
+    }
     float hr = to_tf32(b.x), hi_ = to_tf32(b.y);
     float lr = to_tf32(b.x - hr), li = to_tf32(b.y - hi_);
     float2* r0h = reinterpret_cast<float2*>(hi + (int64_t)(2 * j) * ld);
@@ -581,9 +629,13 @@ static int make_map(bem_ctx* ctx, CUtensorMap* map, float* base, int rows, int l
 
 // C -= A * B on the tensor cores.  b_rowmajor: B[k*ldb + j] (U12 block),
 // else B[j*ldb + k].  c_colmajor: C[j*ldc + i], else C[i*ldc + j].
-static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, const float2* B, int64_t ldb,
-                   bool b_rowmajor, float2* C, int64_t ldc, bool c_colmajor, int prof_cls) {
+int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, const float2* B, int64_t ldb,
+               float2* C, int64_t ldc, const TcOpts& o) {
+    const bool b_rowmajor = o.b_rowmajor, c_colmajor = o.c_colmajor;
+    const int prof_cls = o.prof_cls;
     if (M <= 0 || N <= 0 || K <= 0) return BEM_OK;
+    if (o.lower && (M != N || c_colmajor)) return fail(ctx, BEM_ERR_INVALID, "tc gemm: lower needs square row-major C");
+    if (o.bscale && b_rowmajor) return fail(ctx, BEM_ERR_INVALID, "tc gemm: B scaling needs column-major B");
     BEM_TRY(tc_encode_init(ctx));
     // K-major operand rows padded to a multiple of 32 floats (128 B)
     const int ld = ((2 * K + tc::BK - 1) / tc::BK) * tc::BK;
@@ -604,7 +656,11 @@ static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t l
     float* b_hi = a_lo + a_elems;
     float* b_lo = b_hi + b_elems;
     cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
-    {
+    if (o.a_trans) {
+        dim3 g((M + 31) / 32, (ld / 2 + 31) / 32);
+        tc::pack_a_trans_kernel<<<g, 256, 0, ctx->stream>>>(A, lda, M, K, a_hi, a_lo, ld);
+        BEM_LAUNCHED(ctx);
+    } else {
         int64_t tot = (int64_t)M * (ld / 2);
         tc::pack_a_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, M, K, a_hi, a_lo, ld);
         BEM_LAUNCHED(ctx);
@@ -614,7 +670,8 @@ static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t l
         tc::pack_b_row_kernel<<<g, 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld);
     } else {
         int64_t tot = (int64_t)N * (ld / 2);
-        tc::pack_b_col_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld);
+        tc::pack_b_col_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld,
+                                                                                     o.bscale, o.bscale_stride);
     }
     BEM_LAUNCHED(ctx);
     CUtensorMap mah, mal, mbh, mbl;
@@ -634,18 +691,29 @@ static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t l
         const int grid = std::min(ntiles, ctx->sm_count);
         tc::gemm_persistent_kernel<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc,
                                                                                 c_colmajor ? 1 : 0, M, N, ld,
-                                                                                ctx->d_status);
+                                                                                o.lower ? 1 : 0, ctx->d_status);
     } else {
         dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
         if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");
+        if (o.lower) return fail(ctx, BEM_ERR_INVALID, "tc gemm: lower needs the persistent kernel");
         tc::gemm_kernel<<<grid, 128, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc, c_colmajor ? 1 : 0,
                                                                      M, N, ld, ctx->d_status);
     }
     BEM_LAUNCHED(ctx);
-    if (ev)
-        ctx->prof_end(prof_cls, ev, 8.0 * M * (double)N * K,
-                      8.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
+    if (ev) {
+        const double mn = o.lower ? 0.5 * (double)M * (M + 1) : (double)M * N;  // the lower triangle of C
+        ctx->prof_end(prof_cls, ev, 8.0 * mn * K, 8.0 * ((double)M * K + (double)K * N + 2.0 * mn));
+    }
     return BEM_OK;
+}
+
+static int tc_gemm(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, const float2* B, int64_t ldb,
+                   bool b_rowmajor, float2* C, int64_t ldc, bool c_colmajor, int prof_cls) {
+    TcOpts o;
+    o.b_rowmajor = b_rowmajor;
+    o.c_colmajor = c_colmajor;
+    o.prof_cls = prof_cls;
+    return tc_gemm_ex(ctx, M, N, K, A, lda, B, ldb, C, ldc, o);
 }
 
 static int tc_lu_update(bem_ctx* ctx, void*, int M, int N, int K, const float2* A, int64_t lda, const float2* B,

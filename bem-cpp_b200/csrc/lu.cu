@@ -308,7 +308,7 @@ __global__ void permute_rows_kernel(const typename C2T<R>::type* __restrict__ B,
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)n * nrhs) return;
     int r = (int)(i % n), c = (int)(i / n);
-    X[(int64_t)c * ldx + r] = B[(int64_t)c * ldb + perm[r]];
+    X[(int64_t)c * ldx + r] = B[(int64_t)c * ldb + (perm ? perm[r] : r)];
 }
 
 // ------------------------------------------------------------ small TRSM
@@ -389,12 +389,31 @@ template <typename R> struct TBsel { static constexpr int v = 16; };
 // thread updates the one row it owns with the sub-block's 16 solved rows
 // (T's row segment in registers, the solved values broadcast from shared
 // memory).  This replaces a TRSM + GEMM launch pair per 16 rows.
+//
+// MODE bits: TRSM_TRANS reads T transposed (T[i][j] = A[r0+j][r0+i], the L^T
+// of an L D L^T factor), TRSM_UNIT makes an upper T unit-diagonal, and
+// TRSM_DIVDIAG divides the solution of a unit-lower T by T's diagonal (the D
+// of L D L^T) when it is stored.
 constexpr int TRSM_KB = 256, TRSM_TS = 16, TRSM_PITCH = TRSM_KB + 1;
+constexpr int TRSM_TRANS = 1, TRSM_UNIT = 2, TRSM_DIVDIAG = 4;
 
-template <typename R, bool UPPER, bool B_ROWMAJOR, int RB>
+template <typename C2> __device__ __forceinline__ C2 cdiv(C2 a, C2 d) {
+    const auto den = d.x * d.x + d.y * d.y;
+    C2 q;
+    q.x = (a.x * d.x + a.y * d.y) / den;
+    q.y = (a.y * d.x - a.x * d.y) / den;
+    return q;
+}
+
+template <typename R, bool UPPER, bool B_ROWMAJOR, int RB, int MODE = 0>
 __global__ void __launch_bounds__(TRSM_KB)
 trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int r0, int kb,
                   typename C2T<R>::type* __restrict__ B, int64_t ldb, int c0, int c1) {
+    constexpr bool TRANS = (MODE & TRSM_TRANS) != 0, UNIT = (MODE & TRSM_UNIT) != 0,
+                   DIVDIAG = (MODE & TRSM_DIVDIAG) != 0;
+    auto tel = [&](int i, int j) {  // element (i, j) of the triangle, block-relative
+        return TRANS ? T[(int64_t)(r0 + j) * ldt + r0 + i] : T[(int64_t)(r0 + i) * ldt + r0 + j];
+    };
     using C2 = typename C2T<R>::type;
     constexpr int TS = TRSM_TS, XP = TRSM_PITCH;
     extern __shared__ __align__(16) unsigned char trsm_smem[];
@@ -424,7 +443,7 @@ trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
         const int s0 = sb * TS, ts = min(TS, kb - s0);
         for (int e = threadIdx.x; e < TS * TS; e += blockDim.x) {
             const int i = e / TS, j = e % TS;
-            sT[i][j] = (i < ts && j < ts) ? T[(int64_t)(r0 + s0 + i) * ldt + r0 + s0 + j] : zero;
+            sT[i][j] = (i < ts && j < ts) ? tel(s0 + i, s0 + j) : zero;
         }
         __syncthreads();
         if (threadIdx.x < RB) {
@@ -455,12 +474,7 @@ trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
                         acc.x -= u.x * x[k].x - u.y * x[k].y;
                         acc.y -= u.x * x[k].y + u.y * x[k].x;
                     }
-                    const C2 d = sT[ii][ii];
-                    const R den = d.x * d.x + d.y * d.y;
-                    C2 q;
-                    q.x = (acc.x * d.x + acc.y * d.y) / den;
-                    q.y = (acc.y * d.x - acc.x * d.y) / den;
-                    x[ii] = q;
+                    x[ii] = UNIT ? acc : cdiv(acc, sT[ii][ii]);
                 }
             }
 #pragma unroll
@@ -473,7 +487,7 @@ trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
         if (active) {
             C2 t[TS];
 #pragma unroll
-            for (int m = 0; m < TS; m++) t[m] = m < ts ? T[(int64_t)(r0 + r) * ldt + r0 + s0 + m] : zero;
+            for (int m = 0; m < TS; m++) t[m] = m < ts ? tel(r, s0 + m) : zero;
 #pragma unroll 4
             for (int c = 0; c < RB; c++) {
                 C2 acc = xs[c * XP + r];
@@ -498,8 +512,10 @@ trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
             r = e % kb;
         }
         if (c < nc) {
-            if (B_ROWMAJOR) B[(int64_t)(r0 + r) * ldb + cb + c] = xs[c * XP + r];
-            else B[(int64_t)(cb + c) * ldb + r0 + r] = xs[c * XP + r];
+            C2 v = xs[c * XP + r];
+            if (DIVDIAG) v = cdiv(v, T[(int64_t)(r0 + r) * ldt + r0 + r]);
+            if (B_ROWMAJOR) B[(int64_t)(r0 + r) * ldb + cb + c] = v;
+            else B[(int64_t)(cb + c) * ldb + r0 + r] = v;
         }
     }
 }
@@ -512,7 +528,7 @@ template <typename R> struct TrsmRB {
     static constexpr int col_major = sizeof(R) == 4 ? 16 : 8;
 };
 
-template <typename R, bool UPPER, bool B_ROWMAJOR>
+template <typename R, bool UPPER, bool B_ROWMAJOR, int MODE = 0>
 int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0, int kb,
                typename C2T<R>::type* B, int64_t ldb, int c0, int c1) {
     using C2 = typename C2T<R>::type;
@@ -525,13 +541,13 @@ int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0
     static std::atomic<unsigned long long> attr_set{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);
     if (!(attr_set.load() & bit)) {
-        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB>,
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB, MODE>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set.fetch_or(bit);
     }
     const int grid = (c1 - c0 + RB - 1) / RB;
-    trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB><<<grid, TRSM_KB, smem, ctx->stream>>>(T, ldt, r0, kb, B, ldb, c0,
-                                                                                     c1);
+    trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB, MODE><<<grid, TRSM_KB, smem, ctx->stream>>>(T, ldt, r0, kb, B, ldb,
+                                                                                           c0, c1);
     BEM_LAUNCHED(ctx);
     return BEM_OK;
 }
@@ -698,6 +714,245 @@ template int cgemm<double>(bem_ctx*, int, int, int, const double2*, int64_t, con
                            double2*, int64_t, bool, double2, double2, int);
 template int cgemm<float>(bem_ctx*, int, int, int, const float2*, int64_t, const float2*, int64_t, bool,
                           float2*, int64_t, bool, float2, float2, int);
+
+// ============================================================ L D L^T
+// Complex-symmetric factorisation without pivoting, S = L D L^T, for the
+// FP32 + refinement solve of matrices with S = Z diag(s) symmetric: the
+// PMCHWT matrix is [[A, -K], [K, C]] with A, C and K symmetric (the Galerkin
+// L and K operators are), so Z diag(I, -I) = [[A, K], [K, -C]] is symmetric.
+// Its diagonal blocks dominate enough that elimination without pivoting
+// stays as accurate as partial pivoting on these systems (pivot growth below
+// 5 at 2N = 960..3840); the refinement residual uses the original FP64 Z, and
+// a factorisation that hits a zero pivot or does not let the refinement
+// converge is redone with partial pivoting by the caller.  Half the flops of
+// LU (the trailing update touches only the lower triangle) and no pivot
+// search, so no grid-wide barrier per column.
+
+// Exact (bitwise) symmetry tests of Z and of Z diag(I, -I), 32 x 32 tiles of
+// the lower triangle against the mirrored tiles.  flags bit 0: Z is not
+// symmetric; bit 1: Z diag(I, -I) is not (n odd counts as not).
+__global__ void sym_check_kernel(const double2* __restrict__ Z, int64_t ldz, int n, unsigned* __restrict__ flags) {
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bj > bi) return;
+    __shared__ double2 tt[32][33];
+    __shared__ int done;
+    if (threadIdx.x == 0) done = *(volatile unsigned*)flags == 3u;  // both tests already failed
+    __syncthreads();
+    if (done) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 256 threads
+    const int half = (n % 2 == 0) ? n / 2 : -1;
+    // tile (bj, bi) transposed into shared memory
+    for (int r = ty; r < 32; r += 8) {
+        const int i = bj * 32 + r, j = bi * 32 + tx;
+        tt[r][tx] = (i < n && j < n) ? Z[(int64_t)i * ldz + j] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    unsigned bad = 0;
+    for (int r = ty; r < 32; r += 8) {
+        const int i = bi * 32 + r, j = bj * 32 + tx;
+        if (i >= n || j >= n || j >= i) continue;
+        const double2 a = Z[(int64_t)i * ldz + j];  // Z[i][j]
+        const double2 b = tt[tx][r];                // Z[j][i]
+        if (a.x != b.x || a.y != b.y) bad |= 1u;
+        // (Z D)[i][j] = Z[i][j] s_j  vs  (Z D)[j][i] = Z[j][i] s_i
+        const double si = (half >= 0 && i >= half) ? -1.0 : 1.0, sj = (half >= 0 && j >= half) ? -1.0 : 1.0;
+        if (half < 0 || a.x * sj != b.x * si || a.y * sj != b.y * si) bad |= 2u;
+    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bad) atomicOr(flags, bad);
+}
+
+// Factors the jb x jb diagonal block at (j0, j0) in place: the strict lower
+// triangle receives L, the diagonal D (the upper triangle is not touched).
+// One CTA of 1024 threads; 32-column sub-panels of the block's rows are
+// eliminated column by column in shared memory, then the rest of the block's
+// lower triangle is updated with them.  *info: first zero pivot (1-based).
+constexpr int LDLT_SP = 32, LDLT_PITCH = LDLT_SP + 1;
+
+template <typename R>
+__global__ void __launch_bounds__(1024)
+ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int jb, int* __restrict__ info) {
+    using C2 = typename C2T<R>::type;
+    extern __shared__ __align__(16) unsigned char ldlt_smem[];
+    C2* P = reinterpret_cast<C2*>(ldlt_smem);  // [jb][LDLT_PITCH]: rows c0.. of the block, sub-panel columns
+    const int tid = threadIdx.x, nth = blockDim.x;
+    C2 zero;
+    zero.x = 0;
+    zero.y = 0;
+    for (int c0 = 0; c0 < jb; c0 += LDLT_SP) {
+        const int w = min(LDLT_SP, jb - c0), rows = jb - c0;
+        for (int e = tid; e < rows * w; e += nth) {
+            const int i = e / w, c = e % w;
+            P[i * LDLT_PITCH + c] = A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + c];
+        }
+        __syncthreads();
+        for (int jj = 0; jj < w; jj++) {
+            const C2 d = P[jj * LDLT_PITCH + jj];
+            const bool zp = (d.x == 0 && d.y == 0);
+            if (zp && tid == 0) atomicCAS(info, 0, j0 + c0 + jj + 1);
+            // rank-1 update of the sub-panel's remaining columns (lower part)
+            const int wr = w - jj - 1;
+            if (!zp && wr > 0) {
+                for (int e = tid; e < (rows - jj - 1) * wr; e += nth) {
+                    const int i = jj + 1 + e / wr, c = jj + 1 + e % wr;
+                    if (c > i) continue;
+                    const C2 wi = P[i * LDLT_PITCH + jj], wc = P[c * LDLT_PITCH + jj];
+                    const C2 l = cdiv(wi, d);
+                    C2 x = P[i * LDLT_PITCH + c];
+                    x.x -= l.x * wc.x - l.y * wc.y;
+                    x.y -= l.x * wc.y + l.y * wc.x;
+                    P[i * LDLT_PITCH + c] = x;
+                }
+            }
+            __syncthreads();
+            for (int i = jj + 1 + tid; i < rows; i += nth)
+                P[i * LDLT_PITCH + jj] = zp ? zero : cdiv(P[i * LDLT_PITCH + jj], d);
+            __syncthreads();
+        }
+        for (int e = tid; e < rows * w; e += nth) {
+            const int i = e / w, c = e % w;
+            if (c <= i) A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + c] = P[i * LDLT_PITCH + c];
+        }
+        // the block's remaining lower triangle: A[i][c] -= sum_k L[i][k] d_k L[c][k]
+        const int rest = rows - w;
+        if (rest > 0) {
+            for (int e = tid; e < rest * rest; e += nth) {
+                const int ii = w + e / rest, cc = w + e % rest;
+                if (cc > ii) continue;
+                C2 acc = A[(int64_t)(j0 + c0 + ii) * lda + j0 + c0 + cc];
+                for (int k = 0; k < w; k++) {
+                    const C2 dk = P[k * LDLT_PITCH + k], li = P[ii * LDLT_PITCH + k], lc = P[cc * LDLT_PITCH + k];
+                    C2 t;  // d_k * l_c
+                    t.x = dk.x * lc.x - dk.y * lc.y;
+                    t.y = dk.x * lc.y + dk.y * lc.x;
+                    acc.x -= li.x * t.x - li.y * t.y;
+                    acc.y -= li.x * t.y + li.y * t.x;
+                }
+                A[(int64_t)(j0 + c0 + ii) * lda + j0 + c0 + cc] = acc;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+int sym_structure(bem_ctx* ctx, const double2* Z, int64_t ldz, int n, bool* sym, bool* sym_half) {
+    unsigned* d_flags = nullptr;
+    BEM_TRY_CUDA(ctx, cudaMalloc(&d_flags, sizeof(unsigned)));
+    int s = BEM_OK;
+    unsigned h = 3;
+    do {
+        if (cudaMemsetAsync(d_flags, 0, sizeof(unsigned), ctx->stream) != cudaSuccess) {
+            s = fail(ctx, BEM_ERR_CUDA, "symmetry check");
+            break;
+        }
+        const int T = (n + 31) / 32;
+        if (T > 65535) {
+            s = fail(ctx, BEM_ERR_INVALID, "symmetry check: n too large");
+            break;
+        }
+        sym_check_kernel<<<dim3(T, T), 256, 0, ctx->stream>>>(Z, ldz, n, d_flags);
+        ctx->launches++;
+        if (cudaMemcpyAsync(&h, d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            s = fail(ctx, BEM_ERR_CUDA, "symmetry check: %s", cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+    } while (0);
+    cudaFree(d_flags);
+    *sym = s == BEM_OK && !(h & 1u);
+    *sym_half = s == BEM_OK && !(h & 2u);
+    return s;
+}
+
+// Blocked right-looking L D L^T of the row-major complex64 S (lower triangle).
+int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
+    using C2 = float2;
+    const int NB = TRSM_KB;
+    const size_t smem = (size_t)NB * LDLT_PITCH * sizeof(C2);
+    BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(ldlt_diag_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = std::min(NB, n - j0);
+        cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
+        ldlt_diag_kernel<float><<<1, 1024, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
+        BEM_LAUNCHED(ctx);
+        const int below = n - j0 - jb;
+        if (below > 0) {
+            // L21 = S21 L11^-T D^-1: every row of the panel solves L11 D y = s
+            BEM_TRY((trsm_block<float, false, false, TRSM_DIVDIAG>(ctx, A, lda, j0, jb, A + (int64_t)(j0 + jb) * lda,
+                                                                   lda, 0, below)));
+        }
+        if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3 + 8.0 * below * (double)jb * jb / 2,
+                              8.0 * (double)(jb + below) * jb * 2);
+        if (below > 0) {
+            // S22 -= L21 D L21^T, lower triangle
+            TcOpts o;
+            o.lower = true;
+            o.bscale = A + (int64_t)j0 * lda + j0;
+            o.bscale_stride = lda + 1;
+            o.prof_cls = PROF_LU_UPDATE;
+            const float2* L21 = A + (int64_t)(j0 + jb) * lda + j0;
+            BEM_TRY(tc_gemm_ex(ctx, below, below, jb, L21, lda, L21, lda, A + (int64_t)(j0 + jb) * lda + j0 + jb, lda,
+                               o));
+        }
+    }
+    return BEM_OK;
+}
+
+// X[i][c] /= D_i
+__global__ void diag_div_kernel(const float2* __restrict__ A, int64_t lda, float2* __restrict__ X, int64_t ldx, int n,
+                                int nrhs) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)n * nrhs) return;
+    const int r = (int)(t % n), c = (int)(t / n);
+    X[(int64_t)c * ldx + r] = cdiv(X[(int64_t)c * ldx + r], A[(int64_t)r * lda + r]);
+}
+
+// X = S^-1 B with S = L D L^T (B, X column-major complex64; X may alias B).
+int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2* B, int64_t ldb, float2* X,
+                int64_t ldx, int nrhs) {
+    const int NB = TRSM_KB;
+    if (nrhs <= 0) return BEM_OK;
+    int64_t tot = (int64_t)n * nrhs;
+    if (B != X || ldb != ldx) {
+        permute_rows_kernel<float><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, X, ldx, nullptr, n,
+                                                                                         nrhs);
+        BEM_LAUNCHED(ctx);
+    }
+    // L z = b
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = std::min(NB, n - j0);
+        BEM_TRY((trsm_block<float, false, false>(ctx, A, lda, j0, jb, X, ldx, 0, nrhs)));
+        const int below = n - j0 - jb;
+        if (below > 0) {
+            TcOpts o;
+            o.c_colmajor = true;
+            o.prof_cls = PROF_SOLVE_UPDATE;
+            BEM_TRY(tc_gemm_ex(ctx, below, nrhs, jb, A + (int64_t)(j0 + jb) * lda + j0, lda, X + j0, ldx, X + j0 + jb,
+                               ldx, o));
+        }
+    }
+    // y = D^-1 z
+    diag_div_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, X, ldx, n, nrhs);
+    BEM_LAUNCHED(ctx);
+    // L^T x = y
+    const int nblk = (n + NB - 1) / NB;
+    for (int bi = nblk - 1; bi >= 0; bi--) {
+        const int j0 = bi * NB, jb = std::min(NB, n - j0);
+        BEM_TRY((trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, j0, jb, X, ldx, 0, nrhs)));
+        if (j0 > 0) {
+            // X[0:j0] -= (L[j0:j0+jb, 0:j0])^T X[j0:j0+jb]
+            TcOpts o;
+            o.c_colmajor = true;
+            o.a_trans = true;
+            o.prof_cls = PROF_SOLVE_UPDATE;
+            BEM_TRY(tc_gemm_ex(ctx, j0, nrhs, jb, A + (int64_t)j0 * lda, lda, X + j0, ldx, X, ldx, o));
+        }
+    }
+    return BEM_OK;
+}
 
 // Row pivots (LAPACK interchange sequence, 0-based) -> gather permutation.
 void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm) {

@@ -22,6 +22,19 @@ struct PanelWS {
 // Optional replacement of the CUDA-core GEMM for the big updates
 // C -= A * B (A: M x K, K contiguous; B: K x N).  fn: B row-major (the U12
 // block of the factor), C row-major.  fn_solve: B and C column-major.
+// Options of the 3xTF32 tensor-core GEMM C -= op(A) op(B) (complex64).
+struct TcOpts {
+    bool b_rowmajor = false;  // B is K x N row-major (else given as N x K row-major, "column-major")
+    bool c_colmajor = false;  // C column-major
+    bool a_trans = false;     // A given as its transpose: K x M row-major
+    bool lower = false;       // square row-major C: only the tiles on or below the diagonal
+    const float2* bscale = nullptr;  // column-major B: B[k][j] *= bscale[k * bscale_stride]
+    int64_t bscale_stride = 0;
+    int prof_cls = -1;
+};
+int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, const float2* B, int64_t ldb,
+               float2* C, int64_t ldc, const TcOpts& o);
+
 template <typename R> struct TrailingUpdate {
     using C2 = typename C2T<R>::type;
     int (*fn)(bem_ctx*, void*, int M, int N, int K, const C2* A, int64_t lda, const C2* B,
@@ -47,6 +60,12 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
           int nrhs, const TrailingUpdate<R>* tc);
 
 void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm);
+// Complex-symmetric S = L D L^T without pivoting (complex64, lower triangle,
+// 3xTF32 tensor-core updates) and its multi-RHS solve.
+int sym_structure(bem_ctx* ctx, const double2* Z, int64_t ldz, int n, bool* sym, bool* sym_half);
+int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info);
+int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2* B, int64_t ldb, float2* X,
+                int64_t ldx, int nrhs);
 
 // 3xTF32 tensor-core updates (gemm_tc.cu); nullptr hooks when unavailable.
 TrailingUpdate<float> tc_update_fp32(bem_ctx* ctx);

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "bem_internal.h"
@@ -152,6 +153,26 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
     r->n_orient = no;
     bem_geom_free(g);
     return s;
+}
+
+// Batched particles: every problem through the dense pipeline in turn on the
+// context's stream (device buffers are sized per particle and released before
+// the next).  statuses[i] (optional) receives each problem's status; a failing
+// particle does not stop the batch.  Returns BEM_OK, or the first failure.
+int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_result* results, int* statuses) {
+    if (!ctx || count < 0 || (count > 0 && (!problems || !results))) return BEM_ERR_INVALID;
+    int first = BEM_OK;
+    std::string first_msg;
+    for (int i = 0; i < count; i++) {
+        int s = bem_dense_run(ctx, &problems[i], &results[i]);
+        if (statuses) statuses[i] = s;
+        if (s != BEM_OK && first == BEM_OK) {
+            first = s;
+            first_msg = "particle " + std::to_string(i) + ": " + ctx->last_error;
+        }
+    }
+    if (first != BEM_OK) ctx->last_error = first_msg;
+    return first;
 }
 
 }  // extern "C"

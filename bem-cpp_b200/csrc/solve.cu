@@ -26,13 +26,16 @@ struct bem_lu {
     std::vector<int> ipiv;  // 0-based interchange rows
     double znorm = 0.0;     // ||Z||_F
     double t_factor_ms = 0.0;
+    bool ldlt = false;      // FP32 factors are L D L^T of Z diag(s) (no pivoting)
+    bool dhalf = false;     // s = (I, -I) (else s = 1)
     bem::OzakiZ oz;         // int8 digit planes of Z for the refinement residual (oz.A null: FP64 GEMM)
 };
 
 namespace bem {
 
+// A = complex64(Z), columns >= flip_from negated (flip_from = n: none).
 __global__ void z_to_c_kernel(const double2* __restrict__ Z, int64_t ldz, float2* __restrict__ A,
-                              int64_t lda, int n, double* __restrict__ fro_part) {
+                              int64_t lda, int n, double* __restrict__ fro_part, int flip_from) {
     // one CTA row-block: converts and accumulates |z|^2 into fro_part[blockIdx.x]
     __shared__ double s[256];
     double acc = 0.0;
@@ -42,7 +45,10 @@ __global__ void z_to_c_kernel(const double2* __restrict__ Z, int64_t ldz, float2
         int r = (int)(i / n), c = (int)(i % n);
         double2 z = Z[(int64_t)r * ldz + c];
         acc += z.x * z.x + z.y * z.y;
-        if (A) A[(int64_t)r * lda + c] = make_float2((float)z.x, (float)z.y);
+        if (A) {
+            const float sg = c >= flip_from ? -1.f : 1.f;
+            A[(int64_t)r * lda + c] = make_float2(sg * (float)z.x, sg * (float)z.y);
+        }
     }
     s[threadIdx.x] = acc;
     __syncthreads();
@@ -126,6 +132,32 @@ static int finish_factor(bem_ctx* ctx, bem_lu* lu, int* d_info, int* info) {
     return BEM_OK;
 }
 
+// X[r][c] = -X[r][c] for r >= r0 (x = diag(I, -I) y)
+__global__ void negate_rows_kernel(float2* __restrict__ X, int64_t ldx, int r0, int n, int nrhs) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = n - r0;
+    if (t >= (int64_t)m * nrhs) return;
+    const int r = r0 + (int)(t % m), c = (int)(t / m);
+    float2 v = X[(int64_t)c * ldx + r];
+    X[(int64_t)c * ldx + r] = make_float2(-v.x, -v.y);
+}
+
+// D = (FP32 factors)^-1 S for the correction solves.
+static int solve32(bem_ctx* ctx, bem_lu* lu, const float2* S, float2* D, int nrhs, const TrailingUpdate<float>* tc) {
+    const int n = lu->n;
+    if (!lu->ldlt) return getrs<float>(ctx, lu->A32, n, n, lu->d_perm, S, n, D, n, nrhs, tc);
+    BEM_TRY(sytrs_nopiv(ctx, lu->A32, n, n, S, n, D, n, nrhs));
+    if (lu->dhalf) {
+        const int64_t tot = (int64_t)(n - n / 2) * nrhs;
+        negate_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(D, n, n / 2, n, nrhs);
+        BEM_LAUNCHED(ctx);
+    }
+    return BEM_OK;
+}
+
+// FP32 LU with partial pivoting of Z into lu->A32 (also the fallback of L D L^T).
+static int factor_lu32(bem_ctx* ctx, bem_lu* lu, int* d_info, double* fro, int* info);
+
 static void lu_release(bem_lu* lu) {
     if (!lu) return;
     cudaSetDevice(lu->device);
@@ -134,6 +166,15 @@ static void lu_release(bem_lu* lu) {
     if (lu->d_perm) cudaFree(lu->d_perm);
     bem::ozaki_free(&lu->oz);
     delete lu;
+}
+
+static int factor_lu32(bem_ctx* ctx, bem_lu* lu, int* d_info, double* fro, int* info) {
+    const int n = lu->n;
+    z_to_c_kernel<<<1024, 256, 0, ctx->stream>>>(lu->Z, lu->ldz, lu->A32, n, n, fro, n);
+    BEM_LAUNCHED(ctx);
+    TrailingUpdate<float> tc = tc_update_fp32(ctx);
+    BEM_TRY(getrf<float>(ctx, lu->A32, n, n, lu->d_ipiv, d_info, &tc));
+    return finish_factor(ctx, lu, d_info, info);
 }
 
 int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu** out, int* info) {
@@ -169,7 +210,16 @@ int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu**
                 break;
             }
         }
-        z_to_c_kernel<<<1024, 256, 0, ctx->stream>>>(lu->Z, ldz, lu->A32, n, n, fro);
+        // symmetric structure: L D L^T without pivoting on Z diag(s)
+        if (precision == BEM_PREC_FP32_REFINE && ctx->sym_mode && ctx->use_tc) {
+            bool sym = false, sym_half = false;
+            s = sym_structure(ctx, lu->Z, ldz, n, &sym, &sym_half);
+            if (s != BEM_OK) break;
+            lu->ldlt = sym || sym_half;
+            lu->dhalf = !sym && sym_half;
+        }
+        const int flip_from = lu->dhalf ? n / 2 : n;
+        z_to_c_kernel<<<1024, 256, 0, ctx->stream>>>(lu->Z, ldz, lu->A32, n, n, fro, flip_from);
         ctx->launches++;
         std::vector<double> hf(1024);
         if (cudaMemcpyAsync(hf.data(), fro, 1024 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
@@ -187,8 +237,32 @@ int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu**
             // refinement keeps the FP64 tensor-core GEMM
             if (ctx->oz_digits > 0 && ozaki_prepare_z(ctx, &lu->oz, lu->Z, ldz, n, ctx->oz_digits) != BEM_OK)
                 ozaki_free(&lu->oz);
-            TrailingUpdate<float> tc = tc_update_fp32(ctx);
-            s = getrf<float>(ctx, lu->A32, n, n, lu->d_ipiv, d_info, &tc);
+            if (lu->ldlt) {
+                s = sytrf_nopiv(ctx, lu->A32, n, n, d_info);
+                if (s != BEM_OK) break;
+                int h[2] = {0, 0};
+                if (cudaMemcpyAsync(&h[0], d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+                    cudaMemcpyAsync(&h[1], ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) !=
+                        cudaSuccess ||
+                    cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+                    s = fail(ctx, BEM_ERR_CUDA, "L D L^T: %s", cudaGetErrorString(cudaGetLastError()));
+                    break;
+                }
+                if (h[1] != 0) {
+                    s = fail(ctx, h[1], "device-side wait in the L D L^T factorisation gave up");
+                    break;
+                }
+                if (h[0] == 0) {
+                    lu->ipiv.resize(n);
+                    for (int i = 0; i < n; i++) lu->ipiv[i] = i;
+                    if (info) *info = 0;
+                    break;
+                }
+                // a zero pivot without pivoting: partial pivoting instead
+                lu->ldlt = lu->dhalf = false;
+            }
+            s = factor_lu32(ctx, lu, d_info, fro, info);
+            break;
         }
         if (s != BEM_OK) break;
         s = finish_factor(ctx, lu, d_info, info);
@@ -215,6 +289,7 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
     bem_solve_stats stats;
     std::memset(&stats, 0, sizeof stats);
     stats.t_factor_ms = lu->t_factor_ms;
+    stats.factorization = lu->precision == BEM_PREC_FP64 ? -1 : lu->ldlt ? (lu->dhalf ? 2 : 1) : 0;
     auto t0 = std::chrono::steady_clock::now();
     if (nrhs == 0) {
         if (st) *st = stats;
@@ -275,7 +350,7 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
     BEM_LAUNCHED(ctx);
     scale_down_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, S, n, scale, n, nrhs);
     BEM_LAUNCHED(ctx);
-    BEM_TRY(getrs<float>(ctx, lu->A32, n, n, lu->d_perm, S, n, D, n, nrhs, &tc));
+    BEM_TRY(solve32(ctx, lu, S, D, nrhs, &tc));
     scale_up_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(D, n, X, ldx, scale, n, nrhs, 0);
     BEM_LAUNCHED(ctx);
     BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -290,9 +365,9 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         // iterate by the last relative update, so 7 bits fewer per factor of
         // 128 keep the same absolute accuracy.
         int rs = BEM_ERR_OOM;
-        if (lu->oz.A && it > 1) {
+        if (lu->oz.A && it > 1 && prev_upd < 0.5) {
             const double lg = prev_upd > 0 ? -std::log2(prev_upd) : 1e9;
-            const int digits = std::max(2, lu->oz.S - (int)std::min(64.0, std::floor(lg / 7.0)));
+            const int digits = std::min(lu->oz.S, std::max(2, lu->oz.S - (int)std::min(64.0, std::floor(lg / 7.0))));
             rs = ozaki_residual_update(ctx, &lu->oz, D, n, scale, R, n, nrhs, digits);
         } else if (lu->oz.A) {
             copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, R, n, n, nrhs);
@@ -311,7 +386,7 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         BEM_LAUNCHED(ctx);
         scale_down_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(R, n, S, n, scale, n, nrhs);
         BEM_LAUNCHED(ctx);
-        BEM_TRY(getrs<float>(ctx, lu->A32, n, n, lu->d_perm, S, n, D, n, nrhs, &tc));
+        BEM_TRY(solve32(ctx, lu, S, D, nrhs, &tc));
         colmax_kernel<float2><<<nrhs, 256, 0, ctx->stream>>>(D, n, n, dmax);
         BEM_LAUNCHED(ctx);
         scale_up_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(D, n, X, ldx, scale, n, nrhs, 1);
@@ -346,6 +421,31 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         }
     }
     stats.t_refine_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    if (!stats.converged && lu->ldlt) {
+        // the factorisation without pivoting was not good enough: partial pivoting, and solve again
+        if (alias) {
+            copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, X, ldx, n, nrhs);
+            BEM_LAUNCHED(ctx);
+            BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+        int* d_info = nullptr;
+        double* fro = nullptr;
+        if (cudaMalloc(&d_info, sizeof(int)) != cudaSuccess || cudaMalloc(&fro, 1024 * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            if (d_info) cudaFree(d_info);
+            return fail(ctx, BEM_ERR_OOM, "lu workspace");
+        }
+        lu->ldlt = lu->dhalf = false;
+        auto tf = std::chrono::steady_clock::now();
+        int info = 0;
+        int fs = factor_lu32(ctx, lu, d_info, fro, &info);
+        cudaFree(d_info);
+        cudaFree(fro);
+        BEM_TRY(fs);
+        if (info > 0) return fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+        lu->t_factor_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf).count();
+        return lu_solve(ctx, lu, alias ? (const void*)X : Bv, alias ? ldx : ldb, Xv, ldx, nrhs, tol, max_iter, st);
+    }
     if (st) *st = stats;
     if (!stats.converged)
         return fail(ctx, BEM_ERR_NOCONV, "refinement stopped after %d sweeps at relative update %.3e",

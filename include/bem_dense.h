@@ -78,6 +78,13 @@ int bem_ctx_set_tensor_cores(bem_ctx* ctx, int enable);
  * digits per entry (default 7, 49 bits; needs 2 digits x n^2 x digits bytes
  * more device memory, and falls back to the FP64 GEMM when that is short). */
 int bem_ctx_set_residual_digits(bem_ctx* ctx, int digits);
+/* FP32 factorisation of BEM_PREC_FP32_REFINE systems whose Z, or Z diag(I, -I)
+ * (the PMCHWT structure: symmetric L and K blocks), is exactly symmetric:
+ * mode 1 (default) factors that matrix as L D L^T without pivoting (half the
+ * flops of LU, checked bitwise at factor time), falling back to partial
+ * pivoting on a zero pivot or when the refinement does not converge; mode 0
+ * always uses LU with partial pivoting. */
+int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
 const char* bem_version(void);
@@ -182,6 +189,8 @@ typedef struct bem_solve_stats {
     double est_rel_error;    /* estimated max-column relative error of the returned X */
     double t_factor_ms, t_solve_ms, t_refine_ms;
     double update_hist[12];  /* max relative update of sweeps 1..12 */
+    int factorization;       /* FP32 factors used: 0 LU with partial pivoting, 1 L D L^T of Z,
+                                2 L D L^T of Z diag(I, -I); -1 FP64 */
 } bem_solve_stats;
 
 /* Factorises the row-major n x n complex128 matrix Z_dev (leading dimension
@@ -302,6 +311,14 @@ typedef struct bem_result {
 /* The dense branch of main.cpp (:660-854) end to end on the device: assemble,
  * factor, solve every orientation x polarisation at once, far field, Mueller. */
 int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r);
+
+/* Batched particles (many small scatterers, e.g. the seeded hex-prism sets
+ * that cluster_bem.py farms out one process per particle): bem_dense_run for
+ * problems[0..count) on this context, results[i] for each; statuses[i]
+ * (optional) gets each particle's status and a failure does not stop the
+ * batch.  Returns BEM_OK or the first particle's failure. */
+int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_result* results,
+                  int* statuses);
 
 #ifdef __cplusplus
 }

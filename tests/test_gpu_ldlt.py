@@ -1,0 +1,126 @@
+"""FP32 L D L^T without pivoting for symmetric-structured systems.
+
+The PMCHWT Z is [[A, -K], [K, C]] with A, C, K symmetric, so Z diag(I, -I)
+is symmetric; the FP32 + refinement solve factors it as L D L^T (half the
+flops of LU) and must give the FP64 solution.  Plain symmetric matrices use
+the same path with s = 1; a zero pivot, or a factorisation too inaccurate for
+the refinement to converge, falls back to LU with partial pivoting."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import bem_b200 as bb
+    c = bb.Context(0)
+    yield c
+    bb.set_symmetric(c, 1)
+    c.close()
+
+
+def _solve(ctx, Z, B, sym=1, tol=1e-12):
+    import torch
+    import bem_b200 as bb
+    bb.set_symmetric(ctx, sym)
+    try:
+        Zt = torch.from_numpy(np.ascontiguousarray(Z)).cuda()
+        lu = bb.LU(ctx, Zt, bb.PREC_FP32_REFINE)
+        X, st = lu.solve(B, tol=tol, max_iter=12)
+        lu.close()
+    finally:
+        bb.set_symmetric(ctx, 1)
+    return X.cpu().numpy().T, st
+
+
+def _cplx(rng, *shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+@pytest.fixture(scope="module")
+def pmchwt():
+    import bem_b200 as bb
+    c = bb.Context(0)
+    v, t = bb.icosphere(1.0, 3)
+    kx, ki, ee, ei = bb.physics(5.0, complex(1.3116, 1e-4))
+    g = bb.Geometry(c, v, t, 7)
+    Z = bb.assemble_pmchwt_dev(g, kx, ki, ee, ei).cpu().numpy()
+    RT, w = bb.generate_orientations(4, 3, 1)
+    B = bb.rhs_planewave_dev(g, kx, ee, RT).cpu().numpy().T
+    g.close()
+    c.close()
+    return Z, B
+
+
+def test_pmchwt_structure_is_symmetric_after_sign_flip(pmchwt):
+    Z, _ = pmchwt
+    n = Z.shape[0]
+    S = Z.copy()
+    S[:, n // 2:] *= -1
+    assert np.array_equal(S, S.T)
+    assert not np.array_equal(Z, Z.T)
+
+
+def test_pmchwt_ldlt_matches_fp64(ctx, pmchwt):
+    import scipy.linalg as sl
+    Z, B = pmchwt
+    X1, st1 = _solve(ctx, Z, B, sym=1)
+    X0, st0 = _solve(ctx, Z, B, sym=0)
+    assert st1["factorization"] == 2 and st0["factorization"] == 0
+    assert st1["converged"] and st0["converged"]
+    Xr = sl.lu_solve(sl.lu_factor(Z), B)
+    for X in (X1, X0):
+        err = np.linalg.norm(X - Xr, axis=0) / np.linalg.norm(Xr, axis=0)
+        assert err.max() < 1e-10
+    # the no-pivot factors are about as good a preconditioner as partial pivoting
+    assert st1["update_hist"][0] < 20 * st0["update_hist"][0]
+
+
+@pytest.mark.parametrize("n", [1, 7, 256, 300, 700])
+def test_symmetric_random_uses_ldlt(ctx, n):
+    rng = np.random.default_rng(n)
+    A = _cplx(rng, n, n)
+    Z = A + A.T + 4 * np.sqrt(n) * np.eye(n)   # complex symmetric, well conditioned
+    B = _cplx(rng, n, 5)
+    X, st = _solve(ctx, Z, B)
+    assert st["factorization"] == 1 and st["converged"]
+    assert rel(X, np.linalg.solve(Z, B)) < 1e-11
+
+
+def test_zero_pivot_falls_back_to_lu(ctx):
+    rng = np.random.default_rng(2)
+    n = 300
+    A = _cplx(rng, n, n)
+    Z = A + A.T
+    Z[0, 0] = 0.0                               # no pivoting cannot start
+    B = _cplx(rng, n, 3)
+    X, st = _solve(ctx, Z, B)
+    assert st["factorization"] == 0 and st["converged"]
+    assert rel(X, np.linalg.solve(Z, B)) < 1e-10
+
+
+def test_hard_symmetric_matrix_still_solves(ctx):
+    # an indefinite symmetric matrix with tiny leading pivots: whichever
+    # factorisation ends up used, the refined solution is the FP64 one
+    rng = np.random.default_rng(9)
+    n = 400
+    A = _cplx(rng, n, n)
+    Z = A + A.T
+    Z[:8, :8] *= 1e-6
+    B = _cplx(rng, n, 4)
+    X, st = _solve(ctx, Z, B)
+    assert st["converged"]
+    assert rel(X, np.linalg.solve(Z, B)) < 1e-9
+
+
+def test_nonsymmetric_matrix_uses_lu(ctx):
+    rng = np.random.default_rng(4)
+    n = 257
+    Z = _cplx(rng, n, n) + 10 * np.eye(n)
+    B = _cplx(rng, n, 2)
+    X, st = _solve(ctx, Z, B)
+    assert st["factorization"] == 0
+    assert rel(X, np.linalg.solve(Z, B)) < 1e-11
