@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(192, 1)
 gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                        const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
                        float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int lower,
-                       int* status) {
+                       int store, int* status) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
@@ -397,7 +397,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
         // C of the tile after the current one is prefetched into L2 while the
         // tensor cores work on it, so the read-modify-write below hits L2
         auto prefetch_c = [&](int t) {
-            if (t >= ntiles) return;
+            if (t >= ntiles || store) return;
             int mt, ntl;
             tm.tile(t, mt, ntl);
             if (tm.skip(mt, ntl)) return;
@@ -451,7 +451,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                             float4* p4 = reinterpret_cast<float4*>(p);
                             float4 c[8];
 #pragma unroll
-                            for (int j = 0; j < 8; j++) c[j] = p4[j];
+                            for (int j = 0; j < 8; j++) c[j] = store ? make_float4(0.f, 0.f, 0.f, 0.f) : p4[j];
 #pragma unroll
                             for (int j = 0; j < 8; j++) {
                                 c[j].x -= v[4 * j];
@@ -464,7 +464,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
 #pragma unroll
                             for (int j = 0; j < 16; j++)
                                 if (c0 + j < Nc) {
-                                    float2 c = p[j];
+                                    float2 c = store ? make_float2(0.f, 0.f) : p[j];
                                     c.x -= v[2 * j];
                                     c.y -= v[2 * j + 1];
                                     p[j] = c;
@@ -477,7 +477,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                         float2 c[16];
 #pragma unroll
                         for (int j = 0; j < 16; j++)
-                            if (j < nj) c[j] = C[(int64_t)(c0 + j) * ldc + row];
+                            if (j < nj) c[j] = store ? make_float2(0.f, 0.f) : C[(int64_t)(c0 + j) * ldc + row];
 #pragma unroll
                         for (int j = 0; j < 16; j++)
                             if (j < nj) {
@@ -691,11 +691,12 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
         const int grid = std::min(ntiles, ctx->sm_count);
         tc::gemm_persistent_kernel<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc,
                                                                                 c_colmajor ? 1 : 0, M, N, ld,
-                                                                                o.lower ? 1 : 0, ctx->d_status);
+                                                                                o.lower ? 1 : 0, o.store ? 1 : 0,
+                                                                                ctx->d_status);
     } else {
         dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
         if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");
-        if (o.lower) return fail(ctx, BEM_ERR_INVALID, "tc gemm: lower needs the persistent kernel");
+        if (o.lower || o.store) return fail(ctx, BEM_ERR_INVALID, "tc gemm: lower / store need the persistent kernel");
         tc::gemm_kernel<<<grid, 128, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc, c_colmajor ? 1 : 0,
                                                                      M, N, ld, ctx->d_status);
     }

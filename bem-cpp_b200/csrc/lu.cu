@@ -864,7 +864,19 @@ int sym_structure(bem_ctx* ctx, const double2* Z, int64_t ldz, int n, bool* sym,
     return s;
 }
 
+// W[c][r] (column-major, ld 256) = -1 on the diagonal, 0 elsewhere.
+__global__ void neg_eye_kernel(float2* __restrict__ W, int jb) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= jb * TRSM_KB) return;
+    const int c = t / TRSM_KB, r = t % TRSM_KB;
+    W[t] = make_float2(r == c ? -1.f : 0.f, 0.f);
+}
+
 // Blocked right-looking L D L^T of the row-major complex64 S (lower triangle).
+// Per 256-column block: the diagonal block is factored in one CTA; its
+// inverse factor W = L11^-T D^-1 comes from a block TRSM on -I; the panel
+// below becomes L21 = S21 W in one tensor-core GEMM (in place: the operands
+// are packed before the product is written); then the lower-triangle update.
 int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
     using C2 = float2;
     const int NB = TRSM_KB;
@@ -873,6 +885,13 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
                                            (int)smem));
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    struct Buf {
+        float2* p = nullptr;
+        ~Buf() {
+            if (p) cudaFree(p);
+        }
+    } W;
+    BEM_TRY_CUDA(ctx, cudaMalloc(&W.p, (size_t)NB * NB * sizeof(float2)));
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = std::min(NB, n - j0);
         cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
@@ -880,9 +899,19 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
         BEM_LAUNCHED(ctx);
         const int below = n - j0 - jb;
         if (below > 0) {
-            // L21 = S21 L11^-T D^-1: every row of the panel solves L11 D y = s
-            BEM_TRY((trsm_block<float, false, false, TRSM_DIVDIAG>(ctx, A, lda, j0, jb, A + (int64_t)(j0 + jb) * lda,
-                                                                   lda, 0, below)));
+            // column c of W.p solves L11 x = -e_c, then x_r /= d_r:
+            // W.p[c * 256 + r] = -L11^-1[r][c] / d_r.  (The kernel indexes the
+            // right-hand side rows from r0 = j0, hence the base W.p - j0.)
+            neg_eye_kernel<<<(jb * NB + 255) / 256, 256, 0, ctx->stream>>>(W.p, jb);
+            BEM_LAUNCHED(ctx);
+            BEM_TRY((trsm_block<float, false, false, TRSM_DIVDIAG>(ctx, A, lda, j0, jb, W.p - j0, NB, 0, jb)));
+            // L21 = S21 L11^-T D^-1: B given row-major (K x N) is
+            // B[k][j] = W.p[k * 256 + j] = -(L11^-T D^-1)[k][j]; the store mode writes C = -A B
+            TcOpts o;
+            o.b_rowmajor = true;
+            o.store = true;
+            float2* S21 = A + (int64_t)(j0 + jb) * lda + j0;
+            BEM_TRY(tc_gemm_ex(ctx, below, jb, jb, S21, lda, W.p, NB, S21, lda, o));
         }
         if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3 + 8.0 * below * (double)jb * jb / 2,
                               8.0 * (double)(jb + below) * jb * 2);

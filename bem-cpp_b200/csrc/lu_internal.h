@@ -28,6 +28,7 @@ struct TcOpts {
     bool c_colmajor = false;  // C column-major
     bool a_trans = false;     // A given as its transpose: K x M row-major
     bool lower = false;       // square row-major C: only the tiles on or below the diagonal
+    bool store = false;       // C = -op(A) op(B) (C is not read)
     const float2* bscale = nullptr;  // column-major B: B[k][j] *= bscale[k * bscale_stride]
     int64_t bscale_stride = 0;
     int prof_cls = -1;
