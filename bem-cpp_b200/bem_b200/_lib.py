@@ -82,6 +82,7 @@ SIGNATURES = {
     "bem_ctx_set_tensor_cores": (_I, [_P, _I]),
     "bem_ctx_set_residual_digits": (_I, [_P, _I]),
     "bem_ctx_set_symmetric": (_I, [_P, _I]),
+    "bem_ctx_set_option": (_I, [_P, C.c_char_p, _I]),
     "bem_lu_residual_dev": (_I, [_P, _P, _P, _L, _P, _L, _P, _L, _I, _I]),
     "bem_cgemm_tf32x3": (_I, [_P, _I, _I, _I, _P, _L, _P, _L, _I, _P, _L, _I]),
     "bem_ctx_profile_read": (_I, [_P, _I, C.POINTER(_L), C.POINTER(_D), C.POINTER(_D),

@@ -557,6 +557,11 @@ def set_symmetric(ctx: Context, mode: int):
     ctx.check(lib().bem_ctx_set_symmetric(ctx.h, int(mode)))
 
 
+def set_option(ctx: Context, name: str, value: int):
+    """Kernel-shape switches: "residual_pairs", "persistent_gemm"."""
+    ctx.check(lib().bem_ctx_set_option(ctx.h, name.encode(), int(value)))
+
+
 def set_residual_digits(ctx: Context, digits: int):
     """Digits of the int8 refinement residual (0: FP64 GEMM residual)."""
     ctx.check(lib().bem_ctx_set_residual_digits(ctx.h, int(digits)))

@@ -149,6 +149,18 @@ const char* bem_last_error(const bem_ctx* ctx) { return ctx ? ctx->last_error.c_
 
 int64_t bem_ctx_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
+    if (!ctx || !name) return BEM_ERR_INVALID;
+    if (!std::strcmp(name, "residual_pairs")) {
+        ctx->oz_pair = value != 0;
+    } else if (!std::strcmp(name, "persistent_gemm")) {
+        ctx->tc_persistent = value != 0;
+    } else {
+        return bem::fail(ctx, BEM_ERR_INVALID, "unknown option '%s'", name);
+    }
+    return BEM_OK;
+}
+
 int bem_ctx_set_symmetric(bem_ctx* ctx, int mode) {
     if (!ctx) return BEM_ERR_INVALID;
     if (mode != 0 && mode != 1) return bem::fail(ctx, BEM_ERR_INVALID, "symmetric mode must be 0 or 1");

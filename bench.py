@@ -59,6 +59,8 @@ def parse():
                     help="refinement target: estimated max-column relative error")
     ap.add_argument("--residual-digits", type=int, default=7,
                     help="int8 digits of the refinement residual (0: FP64 DMMA GEMM)")
+    ap.add_argument("--residual-pairs", type=int, default=0,
+                    help="int8 residual on 2-CTA clusters (1) or one CTA per tile (0)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -248,6 +250,7 @@ def run_bem(a):
         torch.cuda.empty_cache()
 
     bb.set_residual_digits(ctx, a.residual_digits)
+    bb.set_option(ctx, "residual_pairs", a.residual_pairs)
     X = torch.empty_like(B)
     times, stats = [], []
     launches0 = None

@@ -85,6 +85,11 @@ int bem_ctx_set_residual_digits(bem_ctx* ctx, int digits);
  * pivoting on a zero pivot or when the refinement does not converge; mode 0
  * always uses LU with partial pivoting. */
 int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
+/* Kernel-shape switches, mainly for measurement: "residual_pairs" (0, default:
+ * one CTA per tile; 1: the int8 residual on 2-CTA clusters, cta_group::2),
+ * "persistent_gemm" (1, default: persistent tensor-core GEMM; 0: one CTA per
+ * tile).  Unknown names give BEM_ERR_INVALID. */
+int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
 const char* bem_version(void);

@@ -166,3 +166,30 @@ def test_residual_method_needs_digit_planes(ctx):
         bb.set_residual_digits(ctx, 7)
     with pytest.raises(bb.BemError):
         bb.set_residual_digits(ctx, 9)
+
+
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (300, 129), (700, 300)])
+def test_cta_pair_kernel_matches_single_cta(ctx, n, nrhs):
+    # the 2-CTA (cta_group::2) residual computes the same integer sums and
+    # applies the groups in the same order: bitwise identical to one CTA per tile
+    import torch
+    import bem_b200 as bb
+    rng = np.random.default_rng(77 + n)
+    Z = _cplx(rng, n, n) + 3 * np.eye(n)
+    X = _cplx(rng, nrhs, n)
+    B = _cplx(rng, nrhs, n)
+    Zt = torch.from_numpy(Z.copy()).cuda()
+    lu = bb.LU(ctx, Zt, bb.PREC_FP32_REFINE)
+    Bt = torch.from_numpy(B.copy()).cuda()
+    Xt = torch.from_numpy(X.copy()).cuda()
+    try:
+        bb.set_option(ctx, "residual_pairs", 1)
+        R2 = lu.residual(Bt, Xt, method=1).cpu().numpy()
+        bb.set_option(ctx, "residual_pairs", 0)
+        R1 = lu.residual(Bt, Xt, method=1).cpu().numpy()
+    finally:
+        bb.set_option(ctx, "residual_pairs", 0)
+        lu.close()
+    assert np.array_equal(R1, R2)
+    with pytest.raises(bb.BemError):
+        bb.set_option(ctx, "no_such_option", 1)
