@@ -121,6 +121,7 @@ SIGNATURES = {
     "bem_amplitude_to_mueller": (_I, [_P, _P, _P, _P, _I, _P]),
     "bem_dense_run": (_I, [_P, C.POINTER(Problem), C.POINTER(Result)]),
     "bem_batch_run": (_I, [_P, C.POINTER(Problem), _I, C.POINTER(Result), C.POINTER(_I)]),
+    "bem_adjoint_grad": (_I, [_P, C.POINTER(Problem), _P, _P, C.POINTER(_D), _P, _P]),
 }
 
 _lib = None

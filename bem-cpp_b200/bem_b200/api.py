@@ -515,6 +515,23 @@ def batch_run(ctx: Context, particles, raise_on_error=True):
     return out
 
 
+def adjoint_grad(ctx: Context, verts, tris, ka, m, target, wt=None, **kw):
+    """Adjoint gradient of sum_t wt_t (M11(theta_t) - target_t)^2 with respect to
+    (Re m, Im m).  `target` has one value per scattering angle (ntheta = len).
+    Returns (loss, grad (2,), mueller (4, 4, ntheta))."""
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    nt = len(target)
+    p, keep = _problem(verts, tris, ka, m, ntheta=nt, **kw)
+    wtv = None if wt is None else np.ascontiguousarray(wt, dtype=np.float64)
+    loss = C.c_double()
+    grad = np.zeros(2)
+    M = np.zeros((4, 4, nt))
+    ctx.check(lib().bem_adjoint_grad(ctx.h, C.byref(p), target.ctypes.data,
+                                     None if wtv is None else wtv.ctypes.data, C.byref(loss),
+                                     grad.ctypes.data, M.ctypes.data))
+    return loss.value, grad, M
+
+
 def c4_particles(seed, count=64, orient=(4, 4, 1), ntheta=181, precision=PREC_FP64):
     """The seeded batched-particle workload: hex prisms with aspect ratio
     U[0.5, 2], refinement 2 or 3 (2N = 1152 / 4608), ka U[1, 5], Re m

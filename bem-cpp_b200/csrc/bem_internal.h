@@ -191,5 +191,6 @@ int farfield_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, in
                  int n_orient, int ndir, double k_re, double k_im, double eta, double* Fv_host);
 int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, const double* RT,
                 const double* w, int n_orient, double k_re, double k_im, double eta,
-                int ntheta, int gamma_mirror, double* M_avg, double* M_orient_dev);
+                int ntheta, int gamma_mirror, double* M_avg, double* M_orient_dev,
+                double* Fv_host = nullptr);
 }  // namespace bem

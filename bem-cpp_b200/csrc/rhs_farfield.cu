@@ -392,13 +392,14 @@ int farfield_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, in
 
 int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, const double* RT,
                 const double* w, int n_orient, double k_re, double k_im, double eta, int ntheta,
-                int gamma_mirror, double* M_avg, double* M_orient_dev) {
+                int gamma_mirror, double* M_avg, double* M_orient_dev, double* Fv_host) {
     const int N = g->N;
     size_t rtb = (size_t)n_orient * 9 * 8, wb = (size_t)n_orient * 8, tb = (size_t)ntheta * 8,
-           mob = M_orient_dev ? 0 : (size_t)n_orient * 16 * ntheta * 8, mab = (size_t)16 * ntheta * 8;
+           mob = M_orient_dev ? 0 : (size_t)n_orient * 16 * ntheta * 8, mab = (size_t)16 * ntheta * 8,
+           fvb = Fv_host ? (size_t)2 * n_orient * ntheta * 3 * 16 : 0;
     size_t off = 0;
     auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
-    size_t oRT = take(rtb), oW = take(wb), oT = take(tb), oMo = take(mob), oMa = take(mab);
+    size_t oRT = take(rtb), oW = take(wb), oT = take(tb), oMo = take(mob), oMa = take(mab), oFv = take(fvb);
     BEM_TRY(ctx->ensure_ws(off));
     char* ws = (char*)ctx->ws;
     std::vector<double> th(ntheta);
@@ -424,11 +425,13 @@ int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, con
     a.w = (const double*)(ws + oW);
     a.Mo = M_orient_dev ? M_orient_dev : (double*)(ws + oMo);
     a.gamma_mirror = gamma_mirror;
+    a.Fv = Fv_host ? (double2*)(ws + oFv) : nullptr;
     BEM_TRY(launch_ff(ctx, a));
     int nel = 16 * ntheta;
     mueller_sum_kernel<<<(nel + 255) / 256, 256, 0, ctx->stream>>>(a.Mo, n_orient, nel, (double*)(ws + oMa));
     BEM_LAUNCHED(ctx);
     BEM_TRY_CUDA(ctx, cudaMemcpyAsync(M_avg, ws + oMa, mab, cudaMemcpyDeviceToHost, ctx->stream));
+    if (Fv_host) BEM_TRY_CUDA(ctx, cudaMemcpyAsync(Fv_host, ws + oFv, fvb, cudaMemcpyDeviceToHost, ctx->stream));
     BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return BEM_OK;
 }

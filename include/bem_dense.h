@@ -317,6 +317,17 @@ typedef struct bem_result {
  * factor, solve every orientation x polarisation at once, far field, Mueller. */
 int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r);
 
+/* Adjoint gradient of an orientation-averaged M11 misfit,
+ *   loss = sum_t wt[t] (M11(theta_t) - target[t])^2   (wt NULL: 1),
+ * with respect to the relative refractive index (grad[0] = dloss/dRe m,
+ * grad[1] = dloss/dIm m), for the problem p (mesh, ka, m, orientations,
+ * ntheta; its precision is ignored: FP64 forward and adjoint solves).
+ * mueller (optional, 16 ntheta) receives the forward Mueller matrix.  The
+ * reference has no gradient code; the result is checked against central
+ * differences of the forward path. */
+int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
+                     double* loss, double* grad, double* mueller);
+
 /* Batched particles (many small scatterers, e.g. the seeded hex-prism sets
  * that cluster_bem.py farms out one process per particle): bem_dense_run for
  * problems[0..count) on this context, results[i] for each; statuses[i]
