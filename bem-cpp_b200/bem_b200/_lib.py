@@ -53,14 +53,15 @@ class Problem(C.Structure):
                 ("beta_sym", C.c_int), ("gamma_sym", C.c_int), ("gamma_mirror", C.c_int),
                 ("orient_i0", C.c_int), ("orient_i1", C.c_int), ("ntheta", C.c_int),
                 ("precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
-                ("asm_flags", C.c_uint)]
+                ("asm_flags", C.c_uint), ("orient_tol", C.c_double)]
 
 
 class Result(C.Structure):
     _fields_ = [("mueller", C.c_void_p), ("t_assembly_s", C.c_double),
                 ("t_solve_s", C.c_double), ("t_farfield_s", C.c_double),
                 ("t_total_s", C.c_double), ("N", C.c_int), ("n_orient", C.c_int),
-                ("stats", SolveStats)]
+                ("stats", SolveStats), ("per_orient_mueller", C.c_void_p),
+                ("per_orient_weight", C.c_void_p), ("n_computed", C.c_int)]
 
 
 _P = C.c_void_p

@@ -454,23 +454,38 @@ def amplitude_to_mueller(S1, S2, S3, S4):
 # ------------------------------------------------------------ whole pipeline
 def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=False,
               orient=(8, 8, 1), orient_sym=(1, 1), gamma_mirror=False, orient_range=None,
-              ntheta=181, precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False):
+              ntheta=181, precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False,
+              orient_tol=0.0, per_orient=False):
     """The --solver dense pipeline (main.cpp:660-854) through bem_dense_run.
-    Returns (mueller (4,4,ntheta), info dict)."""
+    Returns (mueller (4,4,ntheta), info dict).  orient_tol > 0: adaptive
+    orientation stopping (main.cpp:477-636); per_orient=True adds the
+    per-orientation Mueller matrices and weights of the solved orientations to
+    info ("per_orient_mueller" (n,4,4,ntheta), "per_orient_weight" (n,))."""
     p, _keep = _problem(verts, tris, ka, m, quad_order, single, orient, orient_sym, gamma_mirror,
-                        orient_range, ntheta, precision, refine_tol, max_refine, exact_gsmooth)
+                        orient_range, ntheta, precision, refine_tol, max_refine, exact_gsmooth, orient_tol)
     M = np.zeros((4, 4, ntheta))
     r = Result(mueller=M.ctypes.data)
+    po_M = po_w = None
+    if per_orient:
+        cnt = 1 if single else len(generate_orientations(orient[0], orient[1], orient[2], orient_sym[0],
+                                                         orient_sym[1], gamma_mirror)[1])
+        po_M = np.zeros((cnt, 4, 4, ntheta))
+        po_w = np.zeros(cnt)
+        r.per_orient_mueller = po_M.ctypes.data
+        r.per_orient_weight = po_w.ctypes.data
     ctx.check(lib().bem_dense_run(ctx.h, C.byref(p), C.byref(r)))
-    info = {"N": r.N, "n_orient": r.n_orient, "t_assembly_s": r.t_assembly_s,
-            "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s, "t_total_s": r.t_total_s,
-            "stats": r.stats.as_dict()}
+    info = {"N": r.N, "n_orient": r.n_orient, "n_computed": r.n_computed,
+            "t_assembly_s": r.t_assembly_s, "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s,
+            "t_total_s": r.t_total_s, "stats": r.stats.as_dict()}
+    if per_orient:
+        info["per_orient_mueller"] = po_M[:r.n_computed]
+        info["per_orient_weight"] = po_w[:r.n_computed]
     return M, info
 
 
 def _problem(verts, tris, ka, m=1.3116, quad_order=7, single=False, orient=(8, 8, 1),
              orient_sym=(1, 1), gamma_mirror=False, orient_range=None, ntheta=181,
-             precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False):
+             precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False, orient_tol=0.0):
     v, t = _f64(verts), _i32(tris)
     m = complex(m)
     i0, i1 = orient_range if orient_range is not None else (-1, -1)
@@ -480,7 +495,8 @@ def _problem(verts, tris, ka, m=1.3116, quad_order=7, single=False, orient=(8, 8
                 beta_sym=int(orient_sym[0]), gamma_sym=int(orient_sym[1]),
                 gamma_mirror=int(bool(gamma_mirror)), orient_i0=int(i0), orient_i1=int(i1),
                 ntheta=int(ntheta), precision=int(precision), refine_tol=float(refine_tol),
-                max_refine=int(max_refine), asm_flags=ASM_GSMOOTH_EXACT if exact_gsmooth else 0)
+                max_refine=int(max_refine), asm_flags=ASM_GSMOOTH_EXACT if exact_gsmooth else 0,
+                orient_tol=float(orient_tol))
     return p, (v, t)
 
 

@@ -43,6 +43,7 @@ static void usage(const char* prog) {
 int main(int argc, char** argv) {
     setbuf(stdout, NULL);
     double ka = 0, n_re = 1.3116, n_im = 0.0, hex_ar = 1.0, refine_tol = 0.0, orient_auto_R = 4.0;
+    double orient_tol = 0.0;
     int ref = 3, na = 8, nb = 8, ng = 1, ntheta = 181, quad = 7, bsym = 1, gsym = 1, i0 = -1, i1 = -1, subdiv = 0;
     bool single = false, mirror = false, orient_auto = false;
     int precision = BEM_PREC_FP64;
@@ -81,9 +82,9 @@ int main(int argc, char** argv) {
             else if (std::strcmp(p, "fp32-refine") == 0) precision = BEM_PREC_FP32_REFINE;
             else { std::fprintf(stderr, "Unknown precision: %s\n", p); return 1; }
         } else if (is("--refine-tol", 1)) refine_tol = std::atof(argv[++i]);
+        else if (is("--orient-tol", 1)) orient_tol = std::atof(argv[++i]);
         else if (is("--digits", 1) || is("--gmres-tol", 1) || is("--gmres-restart", 1) || is("--max-leaf", 1) ||
-                 is("--prec", 1) || is("--prec-r", 1) || is("--prec-bs", 1) || is("--prec-overlap", 1) ||
-                 is("--orient-tol", 1)) {
+                 is("--prec", 1) || is("--prec-r", 1) || is("--prec-bs", 1) || is("--prec-overlap", 1)) {
             std::fprintf(stderr, "Warning: %s applies to the iterative solvers; ignored\n", argv[i]);
             ++i;
         } else if (std::strcmp(argv[i], "--goi") == 0) {
@@ -159,11 +160,22 @@ int main(int argc, char** argv) {
     p.ntheta = ntheta;
     p.precision = precision;
     p.refine_tol = refine_tol;
+    p.orient_tol = orient_tol;
     std::vector<double> M(16 * (size_t)ntheta), theta(ntheta);
     for (int t = 0; t < ntheta; t++) theta[t] = M_PI * t / (ntheta - 1);
     bem_result r;
     std::memset(&r, 0, sizeof r);
     r.mueller = M.data();
+    // per-orientation stream of the adaptive mode (main.cpp:640-653)
+    std::vector<double> po_M, po_w;
+    if (orient_tol > 0 && !single) {
+        int count = 0;
+        bem_orientations(na, nb, ng, bsym, gsym, mirror, 1, &count, nullptr, nullptr);
+        po_M.resize((size_t)count * 16 * ntheta);
+        po_w.resize(count);
+        r.per_orient_mueller = po_M.data();
+        r.per_orient_weight = po_w.data();
+    }
     s = bem_dense_run(ctx, &p, &r);
     if (s != BEM_OK) {
         std::fprintf(stderr, "Dense solve failed (status %d): %s\n", s, bem_last_error(ctx));
@@ -171,6 +183,19 @@ int main(int argc, char** argv) {
         return 1;
     }
     std::printf("  RWG: %d basis functions, %d orientations\n", r.N, r.n_orient);
+    if (orient_tol > 0 && !single) {
+        std::printf("  Averaged over %d/%d orientations.\n", r.n_computed, r.n_orient);
+        std::string po_path = std::string(out) + ".per_orient";
+        if (FILE* pf = std::fopen(po_path.c_str(), "wb")) {
+            int header[4] = {r.n_computed, ntheta, na, nb};
+            std::fwrite(header, sizeof(int), 4, pf);
+            std::fwrite(po_w.data(), sizeof(double), r.n_computed, pf);
+            std::fwrite(po_M.data(), sizeof(double), (size_t)r.n_computed * 16 * ntheta, pf);
+            std::fclose(pf);
+            std::printf("  Per-orient Mueller saved: %s (%d orient x 16 x %d)\n", po_path.c_str(), r.n_computed,
+                        ntheta);
+        }
+    }
     if (precision == BEM_PREC_FP32_REFINE)
         std::printf("  FP32 + refinement: %d sweeps, estimated rel. error %.2e\n", r.stats.iterations,
                     r.stats.est_rel_error);

@@ -2,6 +2,7 @@
 // of main.cpp:660-854) over the device kernels.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -118,14 +119,21 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         w = std::vector<double>(w.begin() + i0, w.begin() + i1);
     }
     const int no = (int)w.size();
-    const int nrhs = 2 * no;
-    DevBuf dZ, dB, dX;
+    const int nt = p->ntheta;
+    // orientation batches: the whole set at once, or the reference's check
+    // interval for adaptive stopping (main.cpp:478)
+    const bool adaptive = p->orient_tol > 0 && !p->single;
+    const int batch = adaptive ? std::max(20, no / 20) : no;
+    const int nrhs_max = 2 * std::min(batch, no);
+    DevBuf dZ, dB, dX, dMo;
     int s = BEM_OK;
-    if (cudaMalloc(&dZ.p, (size_t)n * n * 16) != cudaSuccess || cudaMalloc(&dB.p, (size_t)n * nrhs * 16) != cudaSuccess ||
-        cudaMalloc(&dX.p, (size_t)n * nrhs * 16) != cudaSuccess) {
+    if (cudaMalloc(&dZ.p, (size_t)n * n * 16) != cudaSuccess ||
+        cudaMalloc(&dB.p, (size_t)n * nrhs_max * 16) != cudaSuccess ||
+        cudaMalloc(&dX.p, (size_t)n * nrhs_max * 16) != cudaSuccess ||
+        cudaMalloc(&dMo.p, (size_t)std::min(batch, no) * 16 * nt * 8) != cudaSuccess) {
         cudaGetLastError();
         bem_geom_free(g);
-        return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs);
+        return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs_max);
     }
     auto t0 = std::chrono::steady_clock::now();
     s = assemble_dev(ctx, g, kext.real(), kext.imag(), kint.real(), kint.imag(), eta_e, eta_i, p->asm_flags, 2,
@@ -134,20 +142,87 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         s = fail(ctx, BEM_ERR_CUDA, "assembly: %s", cudaGetErrorString(cudaGetLastError()));
     r->t_assembly_s = secs(t0);
     auto t1 = std::chrono::steady_clock::now();
-    if (s == BEM_OK) s = rhs_dev(ctx, g, kext.real(), kext.imag(), eta_e, RT.data(), nullptr, nullptr, no, dB.p, n);
     bem_lu* lu = nullptr;
     int info = 0;
     if (s == BEM_OK) s = bem_lu_factor_dev(ctx, dZ.p, n, n, p->precision, &lu, &info);
     if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
-    if (s == BEM_OK)
-        s = bem_lu_solve_dev(ctx, lu, dB.p, n, dX.p, n, nrhs, p->refine_tol, p->max_refine, &r->stats);
-    if (lu) bem_lu_free(lu);
     r->t_solve_s = secs(t1);
-    auto t2 = std::chrono::steady_clock::now();
-    if (s == BEM_OK)
-        s = mueller_dev(ctx, g, dX.p, n, RT.data(), w.data(), no, kext.real(), kext.imag(), eta_e, p->ntheta,
-                        p->gamma_mirror, r->mueller, nullptr);
-    r->t_farfield_s = secs(t2);
+    r->t_farfield_s = 0.0;
+    // streamed multi-RHS solve and far field per batch
+    std::vector<double> Mavg((size_t)16 * nt, 0.0), Mb((size_t)16 * nt), Mo;
+    const double k2 = std::norm(kext);
+    double w_sum = 0.0, w_total = 0.0, prev_csca = 0.0;
+    for (double x : w) w_total += x;
+    bool has_prev = false, converged = false;
+    int consecutive_ok = 0, done = 0;
+    std::memset(&r->stats, 0, sizeof r->stats);
+    for (int o0 = 0; s == BEM_OK && o0 < no; o0 += batch) {
+        const int nb = std::min(batch, no - o0), nrhs = 2 * nb;
+        auto ts = std::chrono::steady_clock::now();
+        s = rhs_dev(ctx, g, kext.real(), kext.imag(), eta_e, RT.data() + 9 * (size_t)o0, nullptr, nullptr, nb, dB.p,
+                    n);
+        bem_solve_stats st;
+        if (s == BEM_OK) s = bem_lu_solve_dev(ctx, lu, dB.p, n, dX.p, n, nrhs, p->refine_tol, p->max_refine, &st);
+        if (s != BEM_OK) break;
+        r->stats.iterations = std::max(r->stats.iterations, st.iterations);
+        r->stats.converged = o0 == 0 ? st.converged : (r->stats.converged && st.converged);
+        r->stats.max_rel_update = std::max(r->stats.max_rel_update, st.max_rel_update);
+        r->stats.max_rel_residual = std::max(r->stats.max_rel_residual, st.max_rel_residual);
+        r->stats.est_rel_error = std::max(r->stats.est_rel_error, st.est_rel_error);
+        r->stats.t_factor_ms = st.t_factor_ms;
+        r->stats.t_solve_ms += st.t_solve_ms;
+        r->stats.t_refine_ms += st.t_refine_ms;
+        r->stats.factorization = st.factorization;
+        for (int i = 0; i < 12; i++) r->stats.update_hist[i] = std::max(r->stats.update_hist[i], st.update_hist[i]);
+        r->t_solve_s += secs(ts);
+        auto tf = std::chrono::steady_clock::now();
+        s = mueller_dev(ctx, g, dX.p, n, RT.data() + 9 * (size_t)o0, w.data() + o0, nb, kext.real(), kext.imag(),
+                        eta_e, nt, p->gamma_mirror, Mb.data(), (double*)dMo.p);
+        if (s != BEM_OK) break;
+        for (size_t i = 0; i < Mb.size(); i++) Mavg[i] += Mb[i];
+        if (r->per_orient_mueller || r->per_orient_weight) {
+            Mo.resize((size_t)nb * 16 * nt);
+            if (cudaMemcpy(Mo.data(), dMo.p, Mo.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                s = fail(ctx, BEM_ERR_CUDA, "per-orientation Mueller download");
+                break;
+            }
+            for (int o = 0; o < nb; o++) {
+                const double wo = w[o0 + o];
+                if (r->per_orient_weight) r->per_orient_weight[o0 + o] = wo;
+                if (r->per_orient_mueller)
+                    for (int i = 0; i < 16 * nt; i++)
+                        r->per_orient_mueller[(size_t)(o0 + o) * 16 * nt + i] =
+                            wo != 0.0 ? Mo[(size_t)o * 16 * nt + i] * k2 / wo : 0.0;
+            }
+        }
+        r->t_farfield_s += secs(tf);
+        done += nb;
+        for (int o = 0; o < nb; o++) w_sum += w[o0 + o];
+        // adaptive check (main.cpp:579-620)
+        if (adaptive && done >= 40 && done % batch == 0) {
+            double csca = 0.0;
+            for (int it = 3; it < nt - 3; it++) csca += (Mavg[it] / w_sum) * std::sin(M_PI * it / (nt - 1));
+            if (!has_prev) {
+                prev_csca = csca;
+                has_prev = true;
+            } else {
+                const double rel = std::abs(prev_csca) > 1e-30 ? std::abs(csca - prev_csca) / std::abs(prev_csca) : 0;
+                consecutive_ok = rel < p->orient_tol ? consecutive_ok + 1 : 0;
+                prev_csca = csca;
+                if (consecutive_ok >= 2) {
+                    converged = true;
+                    break;
+                }
+            }
+        }
+    }
+    if (lu) bem_lu_free(lu);
+    if (s == BEM_OK) {
+        // rescale to the full weight after an early stop (main.cpp:624-636)
+        const double scale = converged && done < no && w_sum > 0 ? w_total / w_sum : 1.0;
+        for (size_t i = 0; i < Mavg.size(); i++) r->mueller[i] = Mavg[i] * scale;
+    }
+    r->n_computed = done;
     r->t_total_s = secs(t_all);
     r->N = N;
     r->n_orient = no;

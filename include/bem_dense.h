@@ -304,6 +304,13 @@ typedef struct bem_problem {
     double refine_tol;     /* <= 0: 1e-12 */
     int max_refine;        /* <= 0: 10 */
     unsigned asm_flags;
+    /* Adaptive orientation stopping (main.cpp:477-636): orientations are solved
+     * in batches of max(20, n/20) with the one factorisation; after each batch
+     * from 40 orientations on, the scattering-cross-section proxy
+     * sum_{t=3}^{ntheta-4} M11(t) sin(theta_t) / w_sum is compared with the
+     * previous batch's; two consecutive relative changes below orient_tol stop
+     * the loop and the average is rescaled to the full weight.  0 = off. */
+    double orient_tol;
 } bem_problem;
 
 typedef struct bem_result {
@@ -311,6 +318,13 @@ typedef struct bem_result {
     double t_assembly_s, t_solve_s, t_farfield_s, t_total_s;
     int N, n_orient;
     bem_solve_stats stats;
+    /* optional per-orientation stream (the .per_orient file of main.cpp:640-653):
+     * per_orient_mueller[o*16*ntheta + i*ntheta + t] = M_o (amplitude_to_mueller,
+     * no weight, no 1/|k|^2) and per_orient_weight[o], for the n_computed first
+     * orientations; caller buffers sized for n_orient orientations, or NULL. */
+    double* per_orient_mueller;
+    double* per_orient_weight;
+    int n_computed;        /* orientations solved (< n_orient after an adaptive stop) */
 } bem_result;
 
 /* The dense branch of main.cpp (:660-854) end to end on the device: assemble,
