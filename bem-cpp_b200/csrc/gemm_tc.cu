@@ -261,7 +261,10 @@ gemm_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ C
 // accumulator into C, so the read-modify-write of tile i overlaps the MMAs of
 // tile i+1.  Barriers: full/empty per smem stage, tfull/tempty per
 // accumulator (tempty counts the four epilogue warps).
-constexpr int GROUP_M = 8;
+// Raster: groups of GROUP_M row tiles x all column tiles; a wave of 148 tiles
+// then spans ~16 row x ~9 column tiles (8 MB of A and 9 MB of B panels in L2),
+// which halves the B-panel re-reads against groups of 8.
+constexpr int GROUP_M = 16;
 constexpr uint32_t TMEM_COLS2 = 512;
 
 struct TileMap {

@@ -786,27 +786,33 @@ ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int
             P[i * LDLT_PITCH + c] = A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + c];
         }
         __syncthreads();
+        __shared__ C2 wcol[LDLT_SP];  // the unscaled column jj of the sub-block's rows
         for (int jj = 0; jj < w; jj++) {
             const C2 d = P[jj * LDLT_PITCH + jj];
             const bool zp = (d.x == 0 && d.y == 0);
             if (zp && tid == 0) atomicCAS(info, 0, j0 + c0 + jj + 1);
-            // rank-1 update of the sub-panel's remaining columns (lower part)
+            // column jj: keep the sub-block rows' unscaled values, then scale to L
+            // (one division per row)
+            for (int i = jj + 1 + tid; i < rows; i += nth) {
+                const C2 v = P[i * LDLT_PITCH + jj];
+                if (i < w) wcol[i] = v;
+                P[i * LDLT_PITCH + jj] = zp ? zero : cdiv(v, d);
+            }
+            __syncthreads();
+            // rank-1 update of the sub-panel's remaining columns (lower part):
+            // a[i][c] -= l_i (d l_c), d l_c being the unscaled a[c][jj]
             const int wr = w - jj - 1;
             if (!zp && wr > 0) {
                 for (int e = tid; e < (rows - jj - 1) * wr; e += nth) {
                     const int i = jj + 1 + e / wr, c = jj + 1 + e % wr;
                     if (c > i) continue;
-                    const C2 wi = P[i * LDLT_PITCH + jj], wc = P[c * LDLT_PITCH + jj];
-                    const C2 l = cdiv(wi, d);
+                    const C2 l = P[i * LDLT_PITCH + jj], wc = wcol[c];
                     C2 x = P[i * LDLT_PITCH + c];
                     x.x -= l.x * wc.x - l.y * wc.y;
                     x.y -= l.x * wc.y + l.y * wc.x;
                     P[i * LDLT_PITCH + c] = x;
                 }
             }
-            __syncthreads();
-            for (int i = jj + 1 + tid; i < rows; i += nth)
-                P[i * LDLT_PITCH + jj] = zp ? zero : cdiv(P[i * LDLT_PITCH + jj], d);
             __syncthreads();
         }
         for (int e = tid; e < rows * w; e += nth) {
