@@ -61,7 +61,8 @@ class Result(C.Structure):
                 ("t_solve_s", C.c_double), ("t_farfield_s", C.c_double),
                 ("t_total_s", C.c_double), ("N", C.c_int), ("n_orient", C.c_int),
                 ("stats", SolveStats), ("per_orient_mueller", C.c_void_p),
-                ("per_orient_weight", C.c_void_p), ("n_computed", C.c_int)]
+                ("per_orient_weight", C.c_void_p), ("n_computed", C.c_int),
+                ("t_setup_s", C.c_double), ("t_release_s", C.c_double)]
 
 
 _P = C.c_void_p

@@ -476,7 +476,8 @@ def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=Fals
     ctx.check(lib().bem_dense_run(ctx.h, C.byref(p), C.byref(r)))
     info = {"N": r.N, "n_orient": r.n_orient, "n_computed": r.n_computed,
             "t_assembly_s": r.t_assembly_s, "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s,
-            "t_total_s": r.t_total_s, "stats": r.stats.as_dict()}
+            "t_total_s": r.t_total_s, "t_setup_s": r.t_setup_s, "t_release_s": r.t_release_s,
+            "stats": r.stats.as_dict()}
     if per_orient:
         info["per_orient_mueller"] = po_M[:r.n_computed]
         info["per_orient_weight"] = po_w[:r.n_computed]

@@ -18,9 +18,11 @@ namespace {
 
 struct DevBuf {
     void* p = nullptr;
-    ~DevBuf() {
+    void release() {
         if (p) cudaFree(p);
+        p = nullptr;
     }
+    ~DevBuf() { release(); }
 };
 
 double secs(std::chrono::steady_clock::time_point a) {
@@ -136,6 +138,7 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs_max);
     }
     auto t0 = std::chrono::steady_clock::now();
+    r->t_setup_s = std::chrono::duration<double>(t0 - t_all).count();
     s = assemble_dev(ctx, g, kext.real(), kext.imag(), kint.real(), kint.imag(), eta_e, eta_i, p->asm_flags, 2,
                      dZ.p, n, nullptr, nullptr);
     if (s == BEM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
@@ -216,13 +219,25 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
             }
         }
     }
+    auto tr = std::chrono::steady_clock::now();
     if (lu) bem_lu_free(lu);
+    r->t_release_s = secs(tr);
     if (s == BEM_OK) {
         // rescale to the full weight after an early stop (main.cpp:624-636)
         const double scale = converged && done < no && w_sum > 0 ? w_total / w_sum : 1.0;
         for (size_t i = 0; i < Mavg.size(); i++) r->mueller[i] = Mavg[i] * scale;
     }
     r->n_computed = done;
+    {
+        auto tf = std::chrono::steady_clock::now();
+        dZ.release();
+        dB.release();
+        dX.release();
+        dMo.release();
+        bem_geom_free(g);
+        g = nullptr;
+        r->t_release_s += secs(tf);
+    }
     r->t_total_s = secs(t_all);
     r->N = N;
     r->n_orient = no;

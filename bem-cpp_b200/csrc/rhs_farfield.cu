@@ -154,11 +154,6 @@ __device__ __forceinline__ double theta_of(const FFArgs& a, int d) {
 constexpr int FF_LANES = 4;
 constexpr int FF_CHUNK = 256;  // points staged per step
 
-__device__ __forceinline__ void cmac(double* acc, double cr, double ci, double tr, double ti) {
-    acc[0] += cr * tr - ci * ti;
-    acc[1] += cr * ti + ci * tr;
-}
-
 // Block: dpb directions x FF_LANES point lanes; grid (direction chunks, orientations).
 __global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
     extern __shared__ double sm[];
@@ -217,12 +212,18 @@ __global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
             sincos(a.kr * rd, &sn, &cs);
             double ea = a.ki != 0.0 ? exp(a.ki * rd) : 1.0;
             double phr = cs * ea, phi = -sn * ea;  // exp(-i k r.r')
-            double t[3][2] = {{q[3] * phr, q[3] * phi}, {q[4] * phr, q[4] * phi}, {q[5] * phr, q[5] * phi}};
             const double2* cc = s_c + e * 4;
+            // u_k = c_k exp(-i k r.r') once per coefficient, then the real
+            // weighted basis vector: 40 FP64 operations per point instead of 54
 #pragma unroll
-            for (int k = 0; k < 4; k++)
+            for (int k = 0; k < 4; k++) {
+                const double ur = cc[k].x * phr - cc[k].y * phi, ui = cc[k].x * phi + cc[k].y * phr;
 #pragma unroll
-                for (int x = 0; x < 3; x++) cmac(acc[3 * k + x], cc[k].x, cc[k].y, t[x][0], t[x][1]);
+                for (int x = 0; x < 3; x++) {
+                    acc[3 * k + x][0] += q[3 + x] * ur;
+                    acc[3 * k + x][1] += q[3 + x] * ui;
+                }
+            }
         }
     }
     // reduce the FF_LANES lanes of each direction

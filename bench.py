@@ -342,7 +342,9 @@ def run_bem(a):
                    "d2h_bytes_per_step": int(M.nbytes),
                    "scope": "bem_dense_run: host mesh -> assembly, FP32 LU + refinement, far field -> host Mueller",
                    "t_assembly_s": info["t_assembly_s"], "t_solve_s": info["t_solve_s"],
-                   "t_farfield_s": info["t_farfield_s"], "refine": info["stats"]["iterations"]}
+                   "t_farfield_s": info["t_farfield_s"], "t_setup_s": info["t_setup_s"],
+                   "t_release_s": info["t_release_s"], "t_total_s": info["t_total_s"],
+                   "refine": info["stats"]["iterations"]}
         except bb.BemError as ex:
             e2e = {"value": None, "unit": "s/solve", "error": str(ex)}
 

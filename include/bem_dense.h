@@ -325,6 +325,8 @@ typedef struct bem_result {
     double* per_orient_mueller;
     double* per_orient_weight;
     int n_computed;        /* orientations solved (< n_orient after an adaptive stop) */
+    double t_setup_s;      /* geometry upload, orientations and device buffers */
+    double t_release_s;    /* freeing the device buffers */
 } bem_result;
 
 /* The dense branch of main.cpp (:660-854) end to end on the device: assemble,
