@@ -124,6 +124,7 @@ SIGNATURES = {
     "bem_dense_run": (_I, [_P, C.POINTER(Problem), C.POINTER(Result)]),
     "bem_batch_run": (_I, [_P, C.POINTER(Problem), _I, C.POINTER(Result), C.POINTER(_I)]),
     "bem_adjoint_grad": (_I, [_P, C.POINTER(Problem), _P, _P, C.POINTER(_D), _P, _P]),
+    "bem_adjoint_grad_vertices": (_I, [_P, C.POINTER(Problem), _P, _P, C.POINTER(_D), _P, _P]),
 }
 
 _lib = None

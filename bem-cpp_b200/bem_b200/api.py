@@ -549,6 +549,44 @@ def adjoint_grad(ctx: Context, verts, tris, ka, m, target, wt=None, **kw):
     return loss.value, grad, M
 
 
+def adjoint_grad_vertices(ctx: Context, verts, tris, ka, m, target, wt=None, **kw):
+    """Gradient of sum_t wt_t (M11(theta_t) - target_t)^2 with respect to the
+    vertex coordinates.  Returns (loss, grad (nv, 3), mueller (4, 4, ntheta))."""
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    nt = len(target)
+    p, keep = _problem(verts, tris, ka, m, ntheta=nt, **kw)
+    wtv = None if wt is None else np.ascontiguousarray(wt, dtype=np.float64)
+    loss = C.c_double()
+    grad = np.zeros((len(keep[0]), 3))
+    M = np.zeros((4, 4, nt))
+    ctx.check(lib().bem_adjoint_grad_vertices(ctx.h, C.byref(p), target.ctypes.data,
+                                              None if wtv is None else wtv.ctypes.data, C.byref(loss),
+                                              grad.ctypes.data, M.ctypes.data))
+    return loss.value, grad, M
+
+
+def c5_mesh(seed, refinements=3, rms=0.05, lmax=6, slope=2.0):
+    """The seeded shape-gradient workload: an icosphere with a radial
+    displacement r -> r (1 + g(rhat)), g a Gaussian random field of real
+    spherical harmonics of degree 1..lmax (i.i.d. normal coefficients with
+    variance (l + 1)^-slope), scaled to RMS `rms` over the vertices."""
+    from scipy.special import sph_harm_y
+    v, t = icosphere(1.0, refinements)
+    rng = np.random.default_rng(seed)
+    r = np.linalg.norm(v, axis=1)
+    th = np.arccos(np.clip(v[:, 2] / r, -1.0, 1.0))
+    ph = np.arctan2(v[:, 1], v[:, 0])
+    g = np.zeros(len(v))
+    for ell in range(1, lmax + 1):
+        sd = (ell + 1.0) ** (-slope / 2.0)
+        for mm in range(-ell, ell + 1):
+            y = sph_harm_y(ell, abs(mm), th, ph)
+            yr = y.real if mm == 0 else np.sqrt(2.0) * (y.real if mm > 0 else y.imag)
+            g += rng.standard_normal() * sd * yr
+    g *= rms / np.sqrt(np.mean(g ** 2))
+    return v * (1.0 + g)[:, None], t
+
+
 def c4_particles(seed, count=64, orient=(4, 4, 1), ntheta=181, precision=PREC_FP64):
     """The seeded batched-particle workload: hex prisms with aspect ratio
     U[0.5, 2], refinement 2 or 3 (2N = 1152 / 4608), ka U[1, 5], Re m

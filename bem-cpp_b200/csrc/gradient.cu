@@ -151,9 +151,15 @@ unsigned blocks_for(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 
 
 using namespace bem;
 
-extern "C" int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
-                                double* loss_out, double* grad_out, double* mueller_out) {
-    if (!ctx || !p || !target || !loss_out || !grad_out) return BEM_ERR_INVALID;
+// Forward solve, adjoint solve, then the requested gradients: with respect to
+// (Re m, Im m) (grad_m, 2 values) and/or the vertex coordinates (grad_v, 3 nv
+// values).  The vertex derivatives use, per coordinate, the operator, the
+// right-hand sides and the far field (at fixed coefficients) assembled on
+// the geometry moved by +-h:
+//   dloss/dv = Re sum_c lambda_c^T (dB_c/dv - dZ/dv x_c) + dloss/dv|_x
+static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
+                        double* loss_out, double* grad_out, double* grad_v, double* mueller_out) {
+    if (!ctx || !p || !target || !loss_out || (!grad_out && !grad_v)) return BEM_ERR_INVALID;
     if (!(p->ka > 0) || p->ntheta < 2) return fail(ctx, BEM_ERR_INVALID, "ka must be > 0, ntheta >= 2");
     BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     const std::complex<double> m(p->m_re, p->m_im), kext(p->ka, 0.0);
@@ -204,13 +210,17 @@ extern "C" int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double
     std::vector<double> M(16 * (size_t)nt), Fv((size_t)nc * nt * 3 * 2);
     BEM_TRY(mueller_dev(ctx, g, dX.p, n, RT.data(), w.data(), no, kext.real(), kext.imag(), eta_e, nt,
                         p->gamma_mirror, M.data(), nullptr, Fv.data()));
-    double loss = 0.0;
+    auto misfit = [&](const double* MM) {
+        double l = 0.0;
+        for (int t = 0; t < nt; t++) {
+            const double wtt = wt ? wt[t] : 1.0, r = MM[t] - target[t];
+            l += wtt * r * r;
+        }
+        return l;
+    };
+    const double loss = misfit(M.data());
     std::vector<double> coef(nt);
-    for (int t = 0; t < nt; t++) {
-        const double wtt = wt ? wt[t] : 1.0, r = M[t] - target[t];
-        loss += wtt * r * r;
-        coef[t] = 2.0 * wtt * r;
-    }
+    for (int t = 0; t < nt; t++) coef[t] = 2.0 * (wt ? wt[t] : 1.0) * (M[t] - target[t]);
     // adjoint weights: h_c(theta) = coef w_o sum_{e in (e_par, e_perp)} conj(F.e) e, and rhat x h
     std::vector<double> hp((size_t)nc * nt * 3 * 2), rh((size_t)nc * nt * 3 * 2);
     for (int c = 0; c < nc; c++) {
@@ -278,9 +288,22 @@ extern "C" int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double
     BEM_TRY(bem_lu_solve_dev(ctx, lu, dY.p, n, dL.p, n, nc, 0.0, 0, nullptr));
     flip_rows_kernel<<<blocks_for(half), 256, 0, ctx->stream>>>((double2*)dL.p, n, N, n, nc);
     BEM_LAUNCHED(ctx);
+    // sum over all entries of lambda . Y (complex, no conjugate)
+    std::vector<double> part(2048);
+    auto dot_lambda = [&](const void* Y, double* re) {
+        cdot_kernel<<<1024, 256, 0, ctx->stream>>>((const double2*)dL.p, (const double2*)Y, (int64_t)n * nc,
+                                                  (double2*)dPart.p);
+        BEM_LAUNCHED(ctx);
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(part.data(), dPart.p, 1024 * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        double tr = 0;
+        for (int i = 0; i < 1024; i++) tr += part[2 * i];
+        *re = tr;
+        return (int)BEM_OK;
+    };
     // dZ/dp by central differences in m, contracted with lambda and x
     const double delta = 1e-5;
-    for (int comp = 0; comp < 2; comp++) {
+    for (int comp = 0; grad_out && comp < 2; comp++) {
         const std::complex<double> dm = comp == 0 ? std::complex<double>(delta, 0) : std::complex<double>(0, delta);
         BEM_TRY(assemble_m(m + dm, dZ.p));
         BEM_TRY(assemble_m(m - dm, dZp.p));
@@ -292,17 +315,83 @@ extern "C" int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double
         BEM_TRY_CUDA(ctx, cudaMemsetAsync(dY.p, 0, xb, ctx->stream));
         BEM_TRY(cgemm<double>(ctx, n, nc, n, (const double2*)dZ.p, n, (const double2*)dX.p, n, true, (double2*)dY.p,
                               n, true, make_double2(-1, 0), make_double2(1, 0)));
-        cdot_kernel<<<1024, 256, 0, ctx->stream>>>((const double2*)dL.p, (const double2*)dY.p, (int64_t)n * nc,
-                                                  (double2*)dPart.p);
-        BEM_LAUNCHED(ctx);
-        std::vector<double> part(2048);
-        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(part.data(), dPart.p, 1024 * 16, cudaMemcpyDeviceToHost, ctx->stream));
-        BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         double tr = 0;
-        for (int i = 0; i < 1024; i++) tr += part[2 * i];
+        BEM_TRY(dot_lambda(dY.p, &tr));
         grad_out[comp] = tr;  // Re(-sum lambda^T dZ x)
+    }
+    if (grad_v) {
+        // per vertex coordinate: Z, B and the far field on the geometry moved by +-h
+        const double h = 1e-6;
+        std::vector<double> vp(p->verts, p->verts + 3 * (size_t)p->nv);
+        std::vector<double> Mp(16 * (size_t)nt), Mm(16 * (size_t)nt);
+        DevMem dBm;
+        if (cudaMalloc(&dBm.p, xb) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, BEM_ERR_OOM, "gradient buffers");
+        }
+        const std::complex<double> ki = kext * m;
+        for (int iv = 0; iv < p->nv; iv++)
+            for (int comp = 0; comp < 3; comp++) {
+                const double v0 = vp[3 * iv + comp];
+                double lpm[2] = {0, 0};
+                void* Zs[2] = {dZ.p, dZp.p};
+                void* Bs[2] = {dB.p, dBm.p};
+                double* Ms[2] = {Mp.data(), Mm.data()};
+                for (int sgn = 0; sgn < 2; sgn++) {
+                    vp[3 * iv + comp] = v0 + (sgn == 0 ? h : -h);
+                    bem_geom* gs = nullptr;
+                    int Ns = 0;
+                    int st = bem_geom_create(ctx, vp.data(), p->nv, p->tris, p->nt, p->quad_order, &gs, &Ns);
+                    if (st == BEM_OK && Ns != N) st = fail(ctx, BEM_ERR_INVALID, "moved mesh changed its RWG count");
+                    if (st == BEM_OK)
+                        st = assemble_dev(ctx, gs, kext.real(), kext.imag(), ki.real(), ki.imag(), eta_e,
+                                          1.0 / std::abs(m), p->asm_flags, 2, Zs[sgn], n, nullptr, nullptr);
+                    if (st == BEM_OK)
+                        st = rhs_dev(ctx, gs, kext.real(), kext.imag(), eta_e, RT.data(), nullptr, nullptr, no,
+                                     Bs[sgn], n);
+                    if (st == BEM_OK)
+                        st = mueller_dev(ctx, gs, dX.p, n, RT.data(), w.data(), no, kext.real(), kext.imag(), eta_e,
+                                         nt, p->gamma_mirror, Ms[sgn], nullptr);
+                    bem_geom_free(gs);
+                    if (st != BEM_OK) {
+                        vp[3 * iv + comp] = v0;
+                        return st;
+                    }
+                    lpm[sgn] = misfit(Ms[sgn]);
+                }
+                vp[3 * iv + comp] = v0;
+                const double inv2h = 0.5 / h;
+                const int64_t nn = (int64_t)n * n, nx = (int64_t)n * nc;
+                // -dZ/dv x
+                diff_scale_kernel<<<blocks_for(nn), 256, 0, ctx->stream>>>((const double2*)dZ.p, (const double2*)dZp.p,
+                                                                          inv2h, (double2*)dZ.p, nn);
+                BEM_LAUNCHED(ctx);
+                BEM_TRY_CUDA(ctx, cudaMemsetAsync(dY.p, 0, xb, ctx->stream));
+                BEM_TRY(cgemm<double>(ctx, n, nc, n, (const double2*)dZ.p, n, (const double2*)dX.p, n, true,
+                                      (double2*)dY.p, n, true, make_double2(-1, 0), make_double2(1, 0)));
+                double t_z = 0, t_b = 0;
+                BEM_TRY(dot_lambda(dY.p, &t_z));
+                // dB/dv
+                diff_scale_kernel<<<blocks_for(nx), 256, 0, ctx->stream>>>((const double2*)dB.p, (const double2*)dBm.p,
+                                                                          inv2h, (double2*)dY.p, nx);
+                BEM_LAUNCHED(ctx);
+                BEM_TRY(dot_lambda(dY.p, &t_b));
+                grad_v[3 * iv + comp] = t_z + t_b + (lpm[0] - lpm[1]) * inv2h;
+            }
     }
     *loss_out = loss;
     if (mueller_out) std::memcpy(mueller_out, M.data(), M.size() * 8);
     return BEM_OK;
+}
+
+extern "C" int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
+                                double* loss, double* grad, double* mueller) {
+    if (!grad) return BEM_ERR_INVALID;
+    return adjoint_core(ctx, p, target, wt, loss, grad, nullptr, mueller);
+}
+
+extern "C" int bem_adjoint_grad_vertices(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
+                                         double* loss, double* grad_verts, double* mueller) {
+    if (!grad_verts) return BEM_ERR_INVALID;
+    return adjoint_core(ctx, p, target, wt, loss, nullptr, grad_verts, mueller);
 }

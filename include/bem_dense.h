@@ -343,6 +343,13 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r);
  * differences of the forward path. */
 int bem_adjoint_grad(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
                      double* loss, double* grad, double* mueller);
+/* The same misfit's gradient with respect to the vertex coordinates of the
+ * mesh (grad_verts: 3 nv doubles, x y z per vertex): the adjoint vectors of
+ * one forward and one adjoint solve, contracted per coordinate with the
+ * central differences (h = 1e-6) of the operator, the right-hand sides and
+ * the far field assembled on the moved geometry (no re-solve). */
+int bem_adjoint_grad_vertices(bem_ctx* ctx, const bem_problem* p, const double* target, const double* wt,
+                              double* loss, double* grad_verts, double* mueller);
 
 /* Batched particles (many small scatterers, e.g. the seeded hex-prism sets
  * that cluster_bem.py farms out one process per particle): bem_dense_run for

@@ -50,3 +50,31 @@ def test_zero_misfit_has_zero_gradient(ctx):
     loss, grad, _ = bb.adjoint_grad(ctx, v, t, 1.0, 1.4, M[0, 0], orient=(2, 2, 1))
     assert loss < 1e-28
     assert np.abs(grad).max() < 1e-12
+
+
+def test_vertex_gradient_matches_central_differences(ctx):
+    import bem_b200 as bb
+    v, t = bb.c5_mesh(3, refinements=1, rms=0.05)
+    nt = 13
+    theta = np.linspace(0, np.pi, nt)
+    target = 0.04 * (1 + np.cos(theta) ** 2)
+    kw = dict(orient=(2, 2, 1))
+    ka, m = 1.5, complex(1.33, 0.01)
+    loss, grad, M = bb.adjoint_grad_vertices(ctx, v, t, ka, m, target, **kw)
+    assert grad.shape == v.shape and np.all(np.isfinite(grad))
+    l2, _, M2 = bb.adjoint_grad(ctx, v, t, ka, m, target, **kw)
+    assert abs(loss - l2) <= 1e-15 * abs(loss) and np.array_equal(M, M2)
+    rng = np.random.default_rng(0)
+    h = 1e-5
+    scale = np.abs(grad).max()
+    for _ in range(4):
+        i, c = int(rng.integers(len(v))), int(rng.integers(3))
+        lp = bb.adjoint_grad(ctx, v + h * np.eye(1, v.size, 3 * i + c).reshape(v.shape), t, ka, m, target,
+                             **kw)[0]
+        lm = bb.adjoint_grad(ctx, v - h * np.eye(1, v.size, 3 * i + c).reshape(v.shape), t, ka, m, target,
+                             **kw)[0]
+        fd = (lp - lm) / (2 * h)
+        assert abs(grad[i, c] - fd) <= 1e-5 * scale, (i, c, grad[i, c], fd)
+    # a rigid translation changes only phases common to the incident and the
+    # scattered field: the orientation-averaged M11 (and the misfit) is invariant
+    assert np.abs(grad.sum(axis=0)).max() <= 1e-6 * scale
