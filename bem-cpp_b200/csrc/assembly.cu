@@ -268,6 +268,7 @@ struct Medium {
 
 // ------------------------------------------------------------ main assembly
 constexpr int TILE = 16;
+static_assert(TILE == ASM_TILE, "assembly band width");
 constexpr int MAXQ = 13;
 
 struct AsmArgs {
@@ -283,6 +284,8 @@ struct AsmArgs {
     double2* L;      // row-major N x N (nmed == 1)
     double2* K;
     int64_t ld;
+    // optional: only tiles whose row or column band is flagged are computed
+    const unsigned char* band;
 };
 
 // G_smooth = (exp(ikR) - 1)/(4 pi R) without cancellation (limit ik/(4 pi)).
@@ -311,6 +314,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
 
     const int N = a.N, Nq = a.Nq;
     const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
+    if (a.band && !a.band[bi] && !a.band[bj]) return;  // a tile the caller keeps
     const int m0 = bi * TILE, n0 = bj * TILE;
 
     // source data of the tile's columns: [half][q][col]
@@ -467,6 +471,7 @@ struct FixArgs {
     int64_t ldz;
     double2* L;
     int64_t ld;
+    const unsigned char* band;  // as AsmArgs::band (bands of TILE RWGs)
 };
 
 // One thread per unordered RWG pair {m, n} sharing a triangle.  For every
@@ -480,6 +485,7 @@ __global__ void singular_fixup_kernel(FixArgs a) {
     if (p >= a.s.npairs) return;
     const int N = a.N, Nq = a.Nq;
     int m = a.s.pair_mn[2 * p], n = a.s.pair_mn[2 * p + 1];
+    if (a.band && !a.band[m / TILE] && !a.band[n / TILE]) return;
     double SA = 0.0, SB = 0.0;
     for (int it = a.s.item_ptr[p]; it < a.s.item_ptr[p + 1]; it++) {
         int t = a.s.item[3 * it], ha = a.s.item[3 * it + 1], hb = a.s.item[3 * it + 2];
@@ -539,7 +545,7 @@ __global__ void singular_fixup_kernel(FixArgs a) {
 // mode 2: PMCHWT into Z; mode 1: L and K of medium 0 into L, K.
 int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
                  double ki_im, double eta_e, double eta_i, unsigned flags, int mode, void* Z,
-                 int64_t ldz, void* L, void* K) {
+                 int64_t ldz, void* L, void* K, const unsigned char* band) {
     const int N = g->N;
     if (N < 1) return fail(ctx, BEM_ERR_INVALID, "empty basis");
     if (mode == 2 && (!Z || ldz < 2 * N)) return fail(ctx, BEM_ERR_INVALID, "bad Z / ldz");
@@ -572,6 +578,7 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
     a.L = (double2*)L;
     a.K = (double2*)K;
     a.ld = ldz;
+    a.band = band;
     int64_t ntiles = (int64_t)a.ntile * (a.ntile + 1) / 2;
     if (ntiles > 0x7fffffffLL) return fail(ctx, BEM_ERR_INVALID, "too many tiles");
     cudaEvent_t ev = ctx->prof_begin(PROF_ASSEMBLY);
@@ -603,6 +610,7 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
         f.ldz = ldz;
         f.L = (double2*)L;
         f.ld = ldz;
+        f.band = band;
         singular_fixup_kernel<<<(g->sing.npairs + 127) / 128, 128, 0, st>>>(f);
         BEM_LAUNCHED(ctx);
     }

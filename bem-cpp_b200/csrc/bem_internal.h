@@ -178,9 +178,12 @@ struct bem_geom {
 
 namespace bem {
 // assembly.cu
+// band (device, optional): one flag per band of 16 RWGs; only the tiles of
+// flagged row or column bands are written (the others keep their values).
 int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
                  double ki_im, double eta_e, double eta_i, unsigned flags, int mode,
-                 void* Z, int64_t ldz, void* L, void* K);
+                 void* Z, int64_t ldz, void* L, void* K, const unsigned char* band = nullptr);
+constexpr int ASM_TILE = 16;  // RWGs per assembly band
 int geom_upload(bem_ctx* ctx, bem_geom* g);
 // rhs / farfield
 int rhs_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im, double eta,

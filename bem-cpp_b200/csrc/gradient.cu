@@ -197,6 +197,16 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
     // forward solve (FP64)
     BEM_TRY(assemble_m(m, dZ.p));
     BEM_TRY(rhs_dev(ctx, g, kext.real(), kext.imag(), eta_e, RT.data(), nullptr, nullptr, no, dB.p, n));
+    // the vertex derivatives reassemble only the tiles around a moved vertex
+    // into a copy of the unperturbed operator
+    DevMem dZbase;
+    if (grad_v) {
+        if (cudaMalloc(&dZbase.p, zb) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, BEM_ERR_OOM, "gradient buffers for n=%d", n);
+        }
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dZbase.p, dZ.p, zb, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
     bem_lu* lu = nullptr;
     int info = 0;
     BEM_TRY(bem_lu_factor_dev(ctx, dZ.p, n, n, BEM_PREC_FP64, &lu, &info));
@@ -330,7 +340,26 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
             return fail(ctx, BEM_ERR_OOM, "gradient buffers");
         }
         const std::complex<double> ki = kext * m;
-        for (int iv = 0; iv < p->nv; iv++)
+        // RWGs around each vertex (the RWGs of its triangles) -> bands of ASM_TILE
+        const int nband = (N + ASM_TILE - 1) / ASM_TILE;
+        std::vector<std::vector<int>> vbands(p->nv);
+        for (int mm = 0; mm < N; mm++)
+            for (int tri : {g->rwg.tri_p[mm], g->rwg.tri_m[mm]})
+                for (int k = 0; k < 3; k++) {
+                    auto& vb = vbands[p->tris[3 * tri + k]];
+                    const int b = mm / ASM_TILE;
+                    if (std::find(vb.begin(), vb.end(), b) == vb.end()) vb.push_back(b);
+                }
+        DevMem dBand;
+        if (cudaMalloc(&dBand.p, nband) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, BEM_ERR_OOM, "gradient buffers");
+        }
+        std::vector<unsigned char> band(nband);
+        for (int iv = 0; iv < p->nv; iv++) {
+            std::fill(band.begin(), band.end(), 0);
+            for (int b : vbands[iv]) band[b] = 1;
+            BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dBand.p, band.data(), nband, cudaMemcpyHostToDevice, ctx->stream));
             for (int comp = 0; comp < 3; comp++) {
                 const double v0 = vp[3 * iv + comp];
                 double lpm[2] = {0, 0};
@@ -343,9 +372,13 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
                     int Ns = 0;
                     int st = bem_geom_create(ctx, vp.data(), p->nv, p->tris, p->nt, p->quad_order, &gs, &Ns);
                     if (st == BEM_OK && Ns != N) st = fail(ctx, BEM_ERR_INVALID, "moved mesh changed its RWG count");
+                    if (st == BEM_OK && cudaMemcpyAsync(Zs[sgn], dZbase.p, zb, cudaMemcpyDeviceToDevice,
+                                                        ctx->stream) != cudaSuccess)
+                        st = fail(ctx, BEM_ERR_CUDA, "operator copy");
                     if (st == BEM_OK)
                         st = assemble_dev(ctx, gs, kext.real(), kext.imag(), ki.real(), ki.imag(), eta_e,
-                                          1.0 / std::abs(m), p->asm_flags, 2, Zs[sgn], n, nullptr, nullptr);
+                                          1.0 / std::abs(m), p->asm_flags, 2, Zs[sgn], n, nullptr, nullptr,
+                                          (const unsigned char*)dBand.p);
                     if (st == BEM_OK)
                         st = rhs_dev(ctx, gs, kext.real(), kext.imag(), eta_e, RT.data(), nullptr, nullptr, no,
                                      Bs[sgn], n);
@@ -378,6 +411,7 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
                 BEM_TRY(dot_lambda(dY.p, &t_b));
                 grad_v[3 * iv + comp] = t_z + t_b + (lpm[0] - lpm[1]) * inv2h;
             }
+        }
     }
     *loss_out = loss;
     if (mueller_out) std::memcpy(mueller_out, M.data(), M.size() * 8);

@@ -49,16 +49,18 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
     cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
     if (sizeof(R) == 8) {
         // FP64: the m8n8k4 f64 tensor path (zgemm_dmma.cuh)
-        static bool attr[4] = {false, false, false, false};
+        // the attribute is per device: one bit per (kernel variant, device id)
+        static std::atomic<unsigned long long> attr[4];
         const double2* Ad = reinterpret_cast<const double2*>(A);
         const double2* Bd = reinterpret_cast<const double2*>(B);
         double2* Cd = reinterpret_cast<double2*>(C);
         double2 al = make_double2(alpha.x, alpha.y), be = make_double2(beta.x, beta.y);
         auto go = [&](auto kern, int slot) -> int {
-            if (!attr[slot]) {
+            const unsigned long long bit = 1ull << (ctx->device & 63);
+            if (!(attr[slot].load() & bit)) {
                 BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        dmma::SMEM_BYTES));
-                attr[slot] = true;
+                attr[slot].fetch_or(bit);
             }
             kern<<<grid, 128, dmma::SMEM_BYTES, ctx->stream>>>(M, N, K, Ad, lda, Bd, ldb, Cd, ldc, al, be);
             return BEM_OK;
@@ -408,7 +410,7 @@ template <typename C2> __device__ __forceinline__ C2 cdiv(C2 a, C2 d) {
 template <typename R, bool UPPER, bool B_ROWMAJOR, int RB, int MODE = 0>
 __global__ void __launch_bounds__(TRSM_KB)
 trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int r0, int kb,
-                  typename C2T<R>::type* __restrict__ B, int64_t ldb, int c0, int c1) {
+                  typename C2T<R>::type* __restrict__ B, int64_t ldb, int br0, int c0, int c1) {
     constexpr bool TRANS = (MODE & TRSM_TRANS) != 0, UNIT = (MODE & TRSM_UNIT) != 0,
                    DIVDIAG = (MODE & TRSM_DIVDIAG) != 0;
     auto tel = [&](int i, int j) {  // element (i, j) of the triangle, block-relative
@@ -434,7 +436,7 @@ trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
             r = e % kb;
         }
         C2 v = zero;
-        if (c < nc) v = B_ROWMAJOR ? B[(int64_t)(r0 + r) * ldb + cb + c] : B[(int64_t)(cb + c) * ldb + r0 + r];
+        if (c < nc) v = B_ROWMAJOR ? B[(int64_t)(br0 + r) * ldb + cb + c] : B[(int64_t)(cb + c) * ldb + br0 + r];
         xs[c * XP + r] = v;
     }
     const int nsb = (kb + TS - 1) / TS;
@@ -514,8 +516,8 @@ trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int 
         if (c < nc) {
             C2 v = xs[c * XP + r];
             if (DIVDIAG) v = cdiv(v, T[(int64_t)(r0 + r) * ldt + r0 + r]);
-            if (B_ROWMAJOR) B[(int64_t)(r0 + r) * ldb + cb + c] = v;
-            else B[(int64_t)(cb + c) * ldb + r0 + r] = v;
+            if (B_ROWMAJOR) B[(int64_t)(br0 + r) * ldb + cb + c] = v;
+            else B[(int64_t)(cb + c) * ldb + br0 + r] = v;
         }
     }
 }
@@ -528,9 +530,11 @@ template <typename R> struct TrsmRB {
     static constexpr int col_major = sizeof(R) == 4 ? 16 : 8;
 };
 
+// B's rows of the block start at br0 (at r0, the block's own rows, when br0 < 0).
 template <typename R, bool UPPER, bool B_ROWMAJOR, int MODE = 0>
 int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0, int kb,
-               typename C2T<R>::type* B, int64_t ldb, int c0, int c1) {
+               typename C2T<R>::type* B, int64_t ldb, int c0, int c1, int br0 = -1) {
+    if (br0 < 0) br0 = r0;
     using C2 = typename C2T<R>::type;
     constexpr int RB = B_ROWMAJOR ? TrsmRB<R>::rows_major : TrsmRB<R>::col_major;
     if (c1 <= c0 || kb <= 0) return BEM_OK;
@@ -547,7 +551,7 @@ int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0
     }
     const int grid = (c1 - c0 + RB - 1) / RB;
     trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB, MODE><<<grid, TRSM_KB, smem, ctx->stream>>>(T, ldt, r0, kb, B, ldb,
-                                                                                           c0, c1);
+                                                                                           br0, c0, c1);
     BEM_LAUNCHED(ctx);
     return BEM_OK;
 }
@@ -906,11 +910,10 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
         const int below = n - j0 - jb;
         if (below > 0) {
             // column c of W.p solves L11 x = -e_c, then x_r /= d_r:
-            // W.p[c * 256 + r] = -L11^-1[r][c] / d_r.  (The kernel indexes the
-            // right-hand side rows from r0 = j0, hence the base W.p - j0.)
+            // W.p[c * 256 + r] = -L11^-1[r][c] / d_r
             neg_eye_kernel<<<(jb * NB + 255) / 256, 256, 0, ctx->stream>>>(W.p, jb);
             BEM_LAUNCHED(ctx);
-            BEM_TRY((trsm_block<float, false, false, TRSM_DIVDIAG>(ctx, A, lda, j0, jb, W.p - j0, NB, 0, jb)));
+            BEM_TRY((trsm_block<float, false, false, TRSM_DIVDIAG>(ctx, A, lda, j0, jb, W.p, NB, 0, jb, 0)));
             // L21 = S21 L11^-T D^-1: B given row-major (K x N) is
             // B[k][j] = W.p[k * 256 + j] = -(L11^-T D^-1)[k][j]; the store mode writes C = -A B
             TcOpts o;
