@@ -270,15 +270,47 @@ constexpr uint32_t TMEM_COLS2 = 512;
 struct TileMap {
     int num_m, num_n;
     int lower;  // square C, only tiles on or below the diagonal (BM rows == BN / 2 complex columns)
-    __device__ __forceinline__ bool skip(int mt, int nt) const { return lower && nt > mt; }
-    __device__ __forceinline__ void tile(int t, int& mt, int& nt) const {
-        const int per_group = GROUP_M * num_n;
-        const int g = t / per_group, first_m = g * GROUP_M;
-        const int gsize = min(GROUP_M, num_m - first_m);
-        const int r = t % per_group;
-        mt = first_m + r % gsize;
-        nt = r / gsize;
+    __device__ __forceinline__ int count() const {
+        return lower ? num_m * (num_m + 1) / 2 : num_m * num_n;
     }
+    // Grouped raster: GROUP_M row tiles at a time, column by column.  For the
+    // lower triangle only the tiles on or below the diagonal are enumerated
+    // (row group g starts at tile S(g) = G g (G g + 1) / 2), so consecutive
+    // CTAs stay on neighbouring tiles and share their operand panels in L2.
+    __device__ __forceinline__ void tile(int t, int& mt, int& nt) const {
+        if (!lower) {
+            const int per_group = GROUP_M * num_n;
+            const int g = t / per_group, first_m = g * GROUP_M;
+            const int gsize = min(GROUP_M, num_m - first_m);
+            const int r = t % per_group;
+            mt = first_m + r % gsize;
+            nt = r / gsize;
+            return;
+        }
+        // largest y with y (y + 1) / 2 <= t, then the group of row y
+        long long y = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while (y > 0 && y * (y + 1) / 2 > t) y--;
+        while ((y + 1) * (y + 2) / 2 <= t) y++;
+        const int g = (int)(y / GROUP_M), first_m = g * GROUP_M;
+        const int gsize = min(GROUP_M, num_m - first_m);
+        int r = t - (int)((long long)first_m * (first_m + 1) / 2);
+        if (r < gsize * first_m) {  // columns left of the group's diagonal block
+            nt = r / gsize;
+            mt = first_m + r % gsize;
+            return;
+        }
+        r -= gsize * first_m;
+        for (int c = 0; c < gsize; c++) {  // the diagonal block, column by column
+            if (r < gsize - c) {
+                nt = first_m + c;
+                mt = first_m + c + r;
+                return;
+            }
+            r -= gsize - c;
+        }
+        mt = nt = num_m - 1;  // not reached for t < count()
+    }
+    __device__ __forceinline__ bool skip(int, int) const { return false; }
 };
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
@@ -307,7 +339,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     tm.num_m = (M + BM - 1) / BM;
     tm.num_n = (2 * Nc + BN - 1) / BN;
     tm.lower = lower;
-    const int ntiles = tm.num_m * tm.num_n;
+    const int ntiles = tm.count();
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -690,7 +722,8 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
         ctx->tc_attr = true;
     }
     if (ctx->tc_persistent) {
-        const int ntiles = ((M + tc::BM - 1) / tc::BM) * ((2 * N + tc::BN - 1) / tc::BN);
+        const int nm = (M + tc::BM - 1) / tc::BM;
+        const int ntiles = o.lower ? nm * (nm + 1) / 2 : nm * ((2 * N + tc::BN - 1) / tc::BN);
         const int grid = std::min(ntiles, ctx->sm_count);
         tc::gemm_persistent_kernel<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc,
                                                                                 c_colmajor ? 1 : 0, M, N, ld,

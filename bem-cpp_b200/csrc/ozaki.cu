@@ -176,7 +176,7 @@ __device__ __forceinline__ void drain_tile(uint32_t base, double2* __restrict__ 
 __global__ void __launch_bounds__(192, 1)
 residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
                 const __grid_constant__ Groups G, double2* __restrict__ R, int64_t ldr, const int* __restrict__ e_row,
-                const int* __restrict__ f_col, int n, int nrhs, int K2p, int* status) {
+                const int* __restrict__ f_col, int n, int nrhs, int K2p, unsigned* __restrict__ pace, int* status) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
@@ -230,6 +230,19 @@ residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
 
     if (warp == 0) {
         if (lane == 0) {
+            // Pacing: the CTAs of a wave share the digit rows of their tiles
+            // through L2 only while they stream the same K slabs at about the
+            // same time (K = 2n is ~1000 slabs per digit pair).  Every EPOCH
+            // slabs the producer adds one to a grid-wide counter and lets at
+            // most LEAD epochs of lead over the grid average build up; the
+            // wait is soft (it gives up after PACE_CYCLES), so it cannot hang.
+            constexpr int EPOCH = 32, LEAD = 2;
+            constexpr long long PACE_CYCLES = 200000;
+            int np_total = 0;
+            for (int gr = 0; gr < G.ng; gr++) np_total += G.g[gr].np;
+            const long long max_epochs =
+                ((long long)((ntiles + gridDim.x - 1) / gridDim.x) * np_total * nk + EPOCH - 1) / EPOCH;
+            long long my_epochs = 0;
             int it = 0;
             for (int gr = 0; gr < G.ng && !abort_flag; gr++)
             for (int u = blockIdx.x; u < ntiles && !abort_flag; u += gridDim.x) {
@@ -247,9 +260,21 @@ residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
                         tma_load_2d(smem_u32(st), &tA, kt * BKB, ya, fb);
                         tma_load_2d(smem_u32(st + A_BYTES), &tB, kt * BKB, yb, fb);
                         issued_total = it + 1;
+                        if ((it + 1) % EPOCH == 0) {
+                            my_epochs++;
+                            atomicAdd(pace, 1u);
+                            const long long t0 = clock64();
+                            while (!abort_flag && clock64() - t0 < PACE_CYCLES) {
+                                const long long tot = *(volatile unsigned*)pace;
+                                if (my_epochs * gridDim.x <= tot + (long long)LEAD * gridDim.x) break;
+                                __nanosleep(256);
+                            }
+                        }
                     }
                 }
             }
+            // finished: count as at the end, so the others are not held back
+            if (max_epochs > my_epochs) atomicAdd(pace, (unsigned)(max_epochs - my_epochs));
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -829,8 +854,10 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
     if (!done) {
         const int ntiles = ((n + oz::BM - 1) / oz::BM) * ((2 * nrhs + oz::BN - 1) / oz::BN);
         const int grid = std::min(ntiles, ctx->sm_count);
+        unsigned* pace = (unsigned*)(ctx->d_status + 32);  // a spare word of the context's status block
+        BEM_TRY_CUDA(ctx, cudaMemsetAsync(pace, 0, sizeof(unsigned), ctx->stream));
         oz::residual_kernel<<<grid, 192, oz::SMEM_BYTES, ctx->stream>>>(tA, tB, G, R, ldr, oz_->e, f, n, nrhs,
-                                                                        (int)ldk, ctx->d_status);
+                                                                        (int)ldk, pace, ctx->d_status);
         BEM_LAUNCHED(ctx);
     }
     if (ev) {
