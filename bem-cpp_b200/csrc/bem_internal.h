@@ -139,6 +139,8 @@ struct bem_ctx {
     void* oz_buf = nullptr;      // digit planes of X for the residual
     size_t oz_bytes = 0;
     bool oz_attr = false;
+    int oz_pace_epoch = 32;      // int8 residual: K slabs per pacing epoch (0: no pacing)
+    int oz_pace_lead = 2;        // epochs of lead over the grid average before a CTA waits
     bool oz_pair = false;        // int8 residual on CTA pairs (cta_group::2); off: the pairs draw
                                  // more power and more DRAM traffic than they save under the 1 kW cap
     bool prof = false;

@@ -153,6 +153,12 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
     if (!ctx || !name) return BEM_ERR_INVALID;
     if (!std::strcmp(name, "residual_pairs")) {
         ctx->oz_pair = value != 0;
+    } else if (!std::strcmp(name, "residual_pace_epoch")) {
+        if (value < 0) return bem::fail(ctx, BEM_ERR_INVALID, "residual_pace_epoch must be >= 0");
+        ctx->oz_pace_epoch = value;
+    } else if (!std::strcmp(name, "residual_pace_lead")) {
+        if (value < 0) return bem::fail(ctx, BEM_ERR_INVALID, "residual_pace_lead must be >= 0");
+        ctx->oz_pace_lead = value;
     } else if (!std::strcmp(name, "persistent_gemm")) {
         ctx->tc_persistent = value != 0;
     } else {

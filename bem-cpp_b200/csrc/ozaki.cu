@@ -176,7 +176,8 @@ __device__ __forceinline__ void drain_tile(uint32_t base, double2* __restrict__ 
 __global__ void __launch_bounds__(192, 1)
 residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
                 const __grid_constant__ Groups G, double2* __restrict__ R, int64_t ldr, const int* __restrict__ e_row,
-                const int* __restrict__ f_col, int n, int nrhs, int K2p, unsigned* __restrict__ pace, int* status) {
+                const int* __restrict__ f_col, int n, int nrhs, int K2p, unsigned* __restrict__ pace, int pace_epoch,
+                int pace_lead, int* status) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
@@ -236,7 +237,7 @@ residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
             // slabs the producer adds one to a grid-wide counter and lets at
             // most LEAD epochs of lead over the grid average build up; the
             // wait is soft (it gives up after PACE_CYCLES), so it cannot hang.
-            constexpr int EPOCH = 32, LEAD = 2;
+            const int EPOCH = pace_epoch > 0 ? pace_epoch : 1 << 30, LEAD = pace_lead;
             constexpr long long PACE_CYCLES = 200000;
             int np_total = 0;
             for (int gr = 0; gr < G.ng; gr++) np_total += G.g[gr].np;
@@ -857,7 +858,8 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
         unsigned* pace = (unsigned*)(ctx->d_status + 32);  // a spare word of the context's status block
         BEM_TRY_CUDA(ctx, cudaMemsetAsync(pace, 0, sizeof(unsigned), ctx->stream));
         oz::residual_kernel<<<grid, 192, oz::SMEM_BYTES, ctx->stream>>>(tA, tB, G, R, ldr, oz_->e, f, n, nrhs,
-                                                                        (int)ldk, pace, ctx->d_status);
+                                                                        (int)ldk, pace, ctx->oz_pace_epoch,
+                                                                        ctx->oz_pace_lead, ctx->d_status);
         BEM_LAUNCHED(ctx);
     }
     if (ev) {

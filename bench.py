@@ -39,11 +39,16 @@ for _p in (REPO, os.path.join(REPO, "bem-cpp_b200")):
 
 METRIC = "s/solve at 2N=61440: FP32+refine vs FP64 LU on one B200 at 1e-9 rel err"
 FP64_PEAK_TFS = 37.0
-# DRAM traffic per algorithmic byte of a kernel class, from one ncu capture of a
-# smaller launch of the same kernel whose traffic grows with the same units
-TRAFFIC_RATIO = {
-    "lu_update": (1.49, "ncu dram__bytes_read+write / algorithmic bytes of the 3xTF32 update at "
-                        "M=N=15104, K=256 (5.52 GB / 3.71 GB), scaled to the average launch"),
+# DRAM traffic of a kernel class from ncu captures of the full-size launches
+# (one-pass dram__bytes_read/write): per algorithmic byte for the trailing
+# update, per int8 digit-pair GEMM for the residual
+TRAFFIC_MODEL = {
+    "lu_update": ("per_byte", 1.52, "ncu dram__bytes_read+write of the first 2N=61440 lower-triangle update "
+                                    "(45.75 GB) / its algorithmic bytes (30.1 GB), times the average launch's "
+                                    "algorithmic bytes"),
+    "residual": ("per_pair", 75.6e9, "ncu dram__bytes_read+write of the two 2N=61440 residuals (2.105 TB for 28 "
+                                     "digit pairs, 1.142 TB for 15) = 75.6 GB per digit-pair GEMM, times the "
+                                     "average launch's pairs"),
 }
 
 
@@ -318,9 +323,13 @@ def run_bem(a):
         pbasis = ("FP64: 37.0 TF/s measured on this pool (cuBLAS ZGEMM 8192^3; DFMA and m8n8k4 DMMA "
                   "throughput probes 36-37 TF/s); MEASURED_PEAKS.json has no FP64 figure")
     traffic, tbasis = None, None
-    if name in TRAFFIC_RATIO:
-        ratio, tbasis = TRAFFIC_RATIO[name]
-        traffic = ratio * by / max(nl, 1)
+    if name in TRAFFIC_MODEL and (name != "residual" or a.residual_digits > 0):
+        kind, f, tbasis = TRAFFIC_MODEL[name]
+        if kind == "per_byte":
+            traffic = f * by / max(nl, 1)
+        else:
+            pair_ops = 2.0 * n * (2.0 * nrhs) * (2.0 * n)
+            traffic = f * (fl / max(nl, 1)) / pair_ops
     roof = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": traffic, "traffic_unit": "bytes per launch",
             "traffic_basis": tbasis, "algorithmic_bytes_per_launch": by / max(nl, 1),

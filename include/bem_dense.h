@@ -88,7 +88,10 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
 /* Kernel-shape switches, mainly for measurement: "residual_pairs" (0, default:
  * one CTA per tile; 1: the int8 residual on 2-CTA clusters, cta_group::2),
  * "persistent_gemm" (1, default: persistent tensor-core GEMM; 0: one CTA per
- * tile).  Unknown names give BEM_ERR_INVALID. */
+ * tile), "residual_pace_epoch" / "residual_pace_lead" (32 / 2: the int8
+ * residual's CTAs report every 32 K slabs and wait, softly, when more than 2
+ * epochs ahead of the grid average, so a wave shares its digit rows in L2;
+ * epoch 0 turns the pacing off).  Unknown names give BEM_ERR_INVALID. */
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
