@@ -902,8 +902,9 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
         }
     } W;
     BEM_TRY_CUDA(ctx, cudaMalloc(&W.p, (size_t)NB * NB * sizeof(float2)));
-    for (int j0 = 0; j0 < n; j0 += NB) {
-        const int jb = std::min(NB, n - j0);
+    // the diagonal block at j0 and its panel below: L D L^T of the block,
+    // then L21 = S21 L11^-T D^-1 for the rows [j0 + jb, n)
+    auto factor_block = [&](int j0, int jb) -> int {
         cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
         ldlt_diag_kernel<float><<<1, 1024, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
         BEM_LAUNCHED(ctx);
@@ -924,15 +925,37 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
         }
         if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3 + 8.0 * below * (double)jb * jb / 2,
                               8.0 * (double)(jb + below) * jb * 2);
-        if (below > 0) {
-            // S22 -= L21 D L21^T, lower triangle
+        return (int)BEM_OK;
+    };
+    // Super-blocks of two 256-column blocks: block 1 is factored and updates
+    // block column 2 alone (a thin GEMM), block 2 is factored, and the
+    // lower-triangle update of the rest takes both (K = 512: half the launches
+    // and half the read-modify-write of the trailing matrix).
+    const int SB = (ctx->factor_sb == 2 ? 2 : 1) * NB;
+    for (int J0 = 0; J0 < n; J0 += SB) {
+        const int JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
+        BEM_TRY(factor_block(J0, jb1));
+        if (jb2 > 0) {
+            // S[J0+jb1:, J0+jb1:J0+JB] -= L21 D1 (rows J0+jb1.. of L21)^T
             TcOpts o;
-            o.lower = true;
-            o.bscale = A + (int64_t)j0 * lda + j0;
+            o.bscale = A + (int64_t)J0 * lda + J0;
             o.bscale_stride = lda + 1;
             o.prof_cls = PROF_LU_UPDATE;
-            const float2* L21 = A + (int64_t)(j0 + jb) * lda + j0;
-            BEM_TRY(tc_gemm_ex(ctx, below, below, jb, L21, lda, L21, lda, A + (int64_t)(j0 + jb) * lda + j0 + jb, lda,
+            const float2* L21 = A + (int64_t)(J0 + jb1) * lda + J0;
+            BEM_TRY(tc_gemm_ex(ctx, n - J0 - jb1, jb2, jb1, L21, lda, L21, lda,
+                               A + (int64_t)(J0 + jb1) * lda + J0 + jb1, lda, o));
+            BEM_TRY(factor_block(J0 + jb1, jb2));
+        }
+        const int below = n - J0 - JB;
+        if (below > 0) {
+            // S22 -= L21 D L21^T over both blocks, lower triangle
+            TcOpts o;
+            o.lower = true;
+            o.bscale = A + (int64_t)J0 * lda + J0;
+            o.bscale_stride = lda + 1;
+            o.prof_cls = PROF_LU_UPDATE;
+            const float2* L21 = A + (int64_t)(J0 + JB) * lda + J0;
+            BEM_TRY(tc_gemm_ex(ctx, below, below, JB, L21, lda, L21, lda, A + (int64_t)(J0 + JB) * lda + J0 + JB, lda,
                                o));
         }
     }
@@ -959,35 +982,45 @@ int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2*
                                                                                          nrhs);
         BEM_LAUNCHED(ctx);
     }
+    // Super-blocks of two 256-row diagonal blocks (ctx->solve_sb = 2): the
+    // second block is updated by the first with a thin GEMM, so the update of
+    // all rows below runs with K = 512 (half the launches and half the
+    // read-modify-write of X).
+    const int SB = (ctx->solve_sb == 2 ? 2 : 1) * NB;
+    auto update = [&](int M, int K, const float2* Ablk, bool trans, float2* Bx, float2* Cx) {
+        TcOpts o;
+        o.c_colmajor = true;
+        o.a_trans = trans;
+        o.prof_cls = PROF_SOLVE_UPDATE;
+        return tc_gemm_ex(ctx, M, nrhs, K, Ablk, lda, Bx, ldx, Cx, ldx, o);
+    };
     // L z = b
-    for (int j0 = 0; j0 < n; j0 += NB) {
-        const int jb = std::min(NB, n - j0);
-        BEM_TRY((trsm_block<float, false, false>(ctx, A, lda, j0, jb, X, ldx, 0, nrhs)));
-        const int below = n - j0 - jb;
-        if (below > 0) {
-            TcOpts o;
-            o.c_colmajor = true;
-            o.prof_cls = PROF_SOLVE_UPDATE;
-            BEM_TRY(tc_gemm_ex(ctx, below, nrhs, jb, A + (int64_t)(j0 + jb) * lda + j0, lda, X + j0, ldx, X + j0 + jb,
-                               ldx, o));
+    for (int J0 = 0; J0 < n; J0 += SB) {
+        const int JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
+        BEM_TRY((trsm_block<float, false, false>(ctx, A, lda, J0, jb1, X, ldx, 0, nrhs)));
+        if (jb2 > 0) {
+            BEM_TRY(update(jb2, jb1, A + (int64_t)(J0 + jb1) * lda + J0, false, X + J0, X + J0 + jb1));
+            BEM_TRY((trsm_block<float, false, false>(ctx, A, lda, J0 + jb1, jb2, X, ldx, 0, nrhs)));
         }
+        const int below = n - J0 - JB;
+        if (below > 0) BEM_TRY(update(below, JB, A + (int64_t)(J0 + JB) * lda + J0, false, X + J0, X + J0 + JB));
     }
     // y = D^-1 z
     diag_div_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, X, ldx, n, nrhs);
     BEM_LAUNCHED(ctx);
-    // L^T x = y
-    const int nblk = (n + NB - 1) / NB;
-    for (int bi = nblk - 1; bi >= 0; bi--) {
-        const int j0 = bi * NB, jb = std::min(NB, n - j0);
-        BEM_TRY((trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, j0, jb, X, ldx, 0, nrhs)));
-        if (j0 > 0) {
-            // X[0:j0] -= (L[j0:j0+jb, 0:j0])^T X[j0:j0+jb]
-            TcOpts o;
-            o.c_colmajor = true;
-            o.a_trans = true;
-            o.prof_cls = PROF_SOLVE_UPDATE;
-            BEM_TRY(tc_gemm_ex(ctx, j0, nrhs, jb, A + (int64_t)j0 * lda, lda, X + j0, ldx, X, ldx, o));
+    // L^T x = y, super-blocks from the last
+    const int nsb = (n + SB - 1) / SB;
+    for (int bi = nsb - 1; bi >= 0; bi--) {
+        const int J0 = bi * SB, JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
+        if (jb2 > 0) {
+            BEM_TRY((trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, J0 + jb1, jb2, X, ldx, 0,
+                                                                           nrhs)));
+            // X[J0:J0+jb1] -= (L[J0+jb1:J0+JB, J0:J0+jb1])^T X[J0+jb1:J0+JB]
+            BEM_TRY(update(jb1, jb2, A + (int64_t)(J0 + jb1) * lda + J0, true, X + J0 + jb1, X + J0));
         }
+        BEM_TRY((trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, J0, jb1, X, ldx, 0, nrhs)));
+        // X[0:J0] -= (L[J0:J0+JB, 0:J0])^T X[J0:J0+JB]
+        if (J0 > 0) BEM_TRY(update(J0, JB, A + (int64_t)J0 * lda, true, X + J0, X));
     }
     return BEM_OK;
 }

@@ -363,10 +363,13 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         // after the first update the previous residual instead,
         // r_k = r_{k-1} - Z d_{k-1}: the correction d is smaller than the
         // iterate by the last relative update, so 7 bits fewer per factor of
-        // 128 keep the same absolute accuracy.
+        // 128 keep the same absolute accuracy.  One bit of slack: the update
+        // form may truncate up to twice as much as the full S-digit product
+        // (2^(5-7S) of max|Z| max|x| instead of 2^(4-7S)), still far below
+        // the rounding of an FP64 dot product of length n.
         int rs = BEM_ERR_OOM;
         if (lu->oz.A && it > 1 && prev_upd < 0.5) {
-            const double lg = prev_upd > 0 ? -std::log2(prev_upd) : 1e9;
+            const double lg = prev_upd > 0 ? -std::log2(prev_upd) + 1.0 : 1e9;
             const int digits = std::min(lu->oz.S, std::max(2, lu->oz.S - (int)std::min(64.0, std::floor(lg / 7.0))));
             rs = ozaki_residual_update(ctx, &lu->oz, D, n, scale, R, n, nrhs, digits);
         } else if (lu->oz.A) {

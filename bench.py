@@ -68,6 +68,10 @@ def parse():
                     help="int8 digits of the refinement residual (0: FP64 DMMA GEMM)")
     ap.add_argument("--residual-pairs", type=int, default=0,
                     help="int8 residual on 2-CTA clusters (1) or one CTA per tile (0)")
+    ap.add_argument("--factor-superblock", type=int, default=2, choices=[1, 2],
+                    help="256-column blocks per L D L^T trailing update")
+    ap.add_argument("--solve-superblock", type=int, default=2, choices=[1, 2],
+                    help="256-row blocks per L D L^T solve update")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -258,6 +262,8 @@ def run_bem(a):
 
     bb.set_residual_digits(ctx, a.residual_digits)
     bb.set_option(ctx, "residual_pairs", a.residual_pairs)
+    bb.set_option(ctx, "factor_superblock", a.factor_superblock)
+    bb.set_option(ctx, "solve_superblock", a.solve_superblock)
     X = torch.empty_like(B)
     def step():
         lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
