@@ -65,6 +65,18 @@ class Result(C.Structure):
                 ("t_setup_s", C.c_double), ("t_release_s", C.c_double)]
 
 
+class GmresStats(C.Structure):
+    _fields_ = [("converged", C.c_int), ("n_unconverged", C.c_int),
+                ("max_iterations", C.c_int), ("total_iterations", C.c_int),
+                ("max_cycles", C.c_int), ("matvecs", C.c_int),
+                ("max_rel_residual", C.c_double), ("t_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+PRECOND_NONE, PRECOND_DIAG, PRECOND_BLOCK_DIAG, PRECOND_LU = 0, 1, 2, 3
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -107,6 +119,11 @@ SIGNATURES = {
     "bem_geom_size": (_I, [_P]),
     "bem_assemble_pmchwt_dev": (_I, [_P, _P, _D, _D, _D, _D, _D, _D, C.c_uint, _P, _L]),
     "bem_assemble_LK_dev": (_I, [_P, _P, _D, _D, C.c_uint, _P, _P, _L]),
+    "bem_assemble_aext_dev": (_I, [_P, _P, _D, _D, _D, C.c_uint, _P, _L]),
+    "bem_precond_create": (_I, [_P, _I, _P, _I, _L, _I, _P, C.POINTER(_P)]),
+    "bem_precond_free": (_I, [_P]),
+    "bem_gmres_solve_dev": (_I, [_P, _P, _I, _L, _P, _P, _L, _P, _L, _I, _I, _D, _I, _P, _P,
+                                 C.POINTER(GmresStats)]),
     "bem_assemble_L_K": (_I, [_P, _P, _I, _P, _I, _D, _D, _I, _P, _P]),
     "bem_assemble_pmchwt": (_I, [_P, _P, _I, _P, _I, _D, _D, _D, _D, _D, _D, _I, _P, _P, _P]),
     "bem_rhs_planewave_dev": (_I, [_P, _P, _D, _D, _D, _P, _I, _P, _L]),

@@ -15,8 +15,9 @@ import math
 
 import numpy as np
 
-from ._lib import (ASM_GSMOOTH_EXACT, PREC_FP32_REFINE, PREC_FP64, BemError, Problem, Result,
-                   SolveStats, check, lib)
+from ._lib import (ASM_GSMOOTH_EXACT, PRECOND_BLOCK_DIAG, PRECOND_DIAG, PRECOND_LU,  # noqa: F401
+                   PRECOND_NONE, PREC_FP32_REFINE, PREC_FP64, BemError, GmresStats, Problem,
+                   Result, SolveStats, check, lib)
 
 
 def _ptr(a):
@@ -226,6 +227,31 @@ class Geometry:
         self.n = 2 * self.N
         self.quad_order = quad_order
 
+    @classmethod
+    def from_rwg(cls, ctx: Context, verts, tris, rwg, quad_order=7):
+        """Geometry with an explicit RWG basis (dict of build_rwg arrays: tri_p,
+        tri_m, free_p, free_m, length, area_p, area_m), e.g. the reference
+        Python build_rwg's order (bem_core.py:397-421)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.verts = _f64(verts)
+        self.tris = _i32(tris)
+        arr = {k: (_i32(rwg[k]) if k in ("tri_p", "tri_m") else _f64(rwg[k]))
+               for k in ("tri_p", "tri_m", "free_p", "free_m", "length", "area_p", "area_m")}
+        self._rwg = arr
+        N = len(arr["tri_p"])
+        h = C.c_void_p()
+        ctx.check(lib().bem_geom_create_rwg(
+            ctx.h, _ptr(self.verts), len(self.verts), _ptr(self.tris), len(self.tris), N,
+            _ptr(arr["tri_p"]), _ptr(arr["tri_m"]), _ptr(arr["free_p"]), _ptr(arr["free_m"]),
+            _ptr(arr["length"]), _ptr(arr["area_p"]), _ptr(arr["area_m"]), int(quad_order),
+            C.byref(h)))
+        self.h = h
+        self.N = N
+        self.n = 2 * N
+        self.quad_order = quad_order
+        return self
+
     def close(self):
         if self.h:
             lib().bem_geom_free(self.h)
@@ -382,6 +408,134 @@ def lu_solve_full(ctx: Context, Z, B, precision=PREC_FP64):
 
 
 # --------------------------------------------------------------- excitation
+# ------------------------------------------------------------------- GMRES
+def assemble_aext_dev(geom: Geometry, k_ext, eta_ext, Z=None, exact_gsmooth=False):
+    """Device A_ext = [[eta L_ext, -K_ext], [K_ext, L_ext / eta]] (torch complex128,
+    row-major 2N x 2N) -- the matrix of build_aext_preconditioner, bem_core.py:1071-1090."""
+    import torch
+    n = geom.n
+    if Z is None:
+        Z = _empty((n, n), torch.complex128, geom.ctx.device)
+    assert Z.dtype == torch.complex128 and Z.is_contiguous() and Z.shape[0] == n
+    k_ext = complex(k_ext)
+    geom.ctx.check(lib().bem_assemble_aext_dev(
+        geom.ctx.h, geom.h, k_ext.real, k_ext.imag, float(eta_ext),
+        ASM_GSMOOTH_EXACT if exact_gsmooth else 0, _dptr(Z), Z.stride(0)))
+    return Z
+
+
+_PRECOND = {None: PRECOND_NONE, "none": PRECOND_NONE, "diag": PRECOND_DIAG,
+            "block_diag": PRECOND_BLOCK_DIAG, "aext": PRECOND_LU, "lu": PRECOND_LU}
+
+
+class Preconditioner:
+    """bem_precond: kind None / 'diag' / 'block_diag' built from Z (torch
+    complex128, kept alive here), or 'aext' / 'lu' from an LU object (the
+    factorisation of A_ext; kept alive here)."""
+
+    def __init__(self, ctx: Context, kind, Z=None, n=None, precision=PREC_FP64, lu=None):
+        if kind not in _PRECOND:
+            raise ValueError(f"unknown preconditioner {kind!r}")
+        self.ctx, self.kind, self.Z, self.lu = ctx, kind, Z, lu
+        self.n = n if n is not None else (Z.shape[0] if Z is not None else lu.n)
+        h = C.c_void_p()
+        ctx.check(lib().bem_precond_create(ctx.h, _PRECOND[kind], _dptr(Z) if Z is not None else None,
+                                           self.n, Z.stride(0) if Z is not None else self.n,
+                                           int(precision), lu.h if lu is not None else None,
+                                           C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().bem_precond_free(self.h)
+            self.h = None
+        if self.lu is not None and getattr(self, "_own_lu", False):
+            self.lu.close()
+        self.Z = self.lu = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build_aext_preconditioner(geom: Geometry, k_ext, eta_ext, precision=PREC_FP64, keep_matrix=False):
+    """build_aext_preconditioner (bem_core.py:1071-1090): A_ext assembled on the
+    device and factored.  Returns (Z_ext_lu, Z_ext) like the reference, where
+    Z_ext_lu is a Preconditioner of kind 'aext' and Z_ext the unfactored matrix
+    when keep_matrix (an FP64 factorisation overwrites its input, so keeping it
+    costs a copy), else None.  precision PREC_FP32_REFINE factors A_ext in FP32
+    (applied once per step, no refinement)."""
+    A = assemble_aext_dev(geom, k_ext, eta_ext)
+    Z_ext = A.clone() if keep_matrix else None
+    lu = LU(geom.ctx, A, precision)
+    M = Preconditioner(geom.ctx, "aext", lu=lu)
+    M._own_lu = True
+    return M, Z_ext
+
+
+def gmres(ctx: Context, Z, B, M=None, tol=1e-5, restart=20, maxiter=None):
+    """GMRES(restart) for Z X = B on the device, all columns of B at once (the
+    algorithm of scipy.sparse.linalg.gmres that the reference calls).  Z: torch
+    complex128 (n, n) on the device.  B: numpy (n,) / (n, nrhs), or torch
+    (nrhs, n) on the device.  M: a Preconditioner (None: identity).  maxiter:
+    restart cycles (default 10 n, scipy's).  Returns (X in B's form, info dict:
+    'iters' and 'info' per column as scipy's callback count and info, and the
+    batch statistics)."""
+    import torch
+    n = Z.shape[0]
+    as_numpy = isinstance(B, np.ndarray)
+    one = as_numpy and B.ndim == 1
+    Bt = _as_cols(B, n, ctx.device)
+    nrhs = Bt.shape[0]
+    X = torch.empty_like(Bt)
+    own = M is None
+    if own:
+        M = Preconditioner(ctx, None, n=n)
+    iters = np.zeros(nrhs, dtype=np.int32)
+    info = np.zeros(nrhs, dtype=np.int32)
+    st = GmresStats()
+    try:
+        ctx.check(lib().bem_gmres_solve_dev(
+            ctx.h, _dptr(Z), n, Z.stride(0), M.h, _dptr(Bt), n, _dptr(X), n, nrhs, int(restart),
+            float(tol), int(maxiter if maxiter is not None else 10 * n), _ptr(iters), _ptr(info),
+            C.byref(st)))
+    finally:
+        if own:
+            M.close()
+    d = st.as_dict()
+    d["iters"], d["info"] = iters, info
+    if as_numpy:
+        Xh = X.cpu().numpy().T
+        return (Xh[:, 0] if one else Xh), d
+    return X, d
+
+
+def solve_gmres_aext(ctx: Context, Z, b, Z_ext_lu, tol=1e-5, maxiter=200):
+    """solve_gmres_aext (bem_core.py:1093-1123): GMRES with the A_ext
+    preconditioner, restart min(200, n).  Returns x in b's form."""
+    x, _ = gmres(ctx, Z, b, Z_ext_lu, tol=tol, restart=min(200, Z.shape[0]), maxiter=maxiter)
+    return x
+
+
+def solve_gmres(ctx: Context, Z, b, tol=1e-4, maxiter=500, precond="block_diag", Z_ext_lu=None,
+                precision=PREC_FP64):
+    """solve_gmres (bem_core.py:1126-1183): precond 'aext' (needs Z_ext_lu),
+    'block_diag' (LU of Z11 and Z22), 'diag' or None; restart 20 (scipy's
+    default) except for 'aext'.  precision: of the block factorisations."""
+    if precond == "aext":
+        if Z_ext_lu is None:
+            raise ValueError("precond='aext' requires Z_ext_lu from build_aext_preconditioner()")
+        return solve_gmres_aext(ctx, Z, b, Z_ext_lu, tol=tol, maxiter=maxiter)
+    M = Preconditioner(ctx, precond, Z=Z, precision=precision)
+    try:
+        x, _ = gmres(ctx, Z, b, M, tol=tol, restart=20, maxiter=maxiter)
+    finally:
+        M.close()
+    return x
+
+
 def rhs_planewave_dev(geom: Geometry, k_ext, eta_ext, RT, B=None):
     """Right-hand sides for orientations RT (n,3,3): torch (2n_orient, 2N) whose
     row 2o is par (E0 = RT x), 2o+1 perp (E0 = RT y), k_hat = RT z

@@ -279,9 +279,9 @@ struct AsmArgs {
     double eta_e, eta_i;
     unsigned flags;
     // outputs
-    double2* Z;      // row-major 2N x 2N (nmed == 2)
+    double2* Z;      // row-major 2N x 2N: PMCHWT (nmed == 2) or A_ext (nmed == 1)
     int64_t ldz;
-    double2* L;      // row-major N x N (nmed == 1)
+    double2* L;      // row-major N x N (nmed == 1, Z null)
     double2* K;
     int64_t ld;
     // optional: only tiles whose row or column band is flagged are computed
@@ -432,10 +432,19 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
     // symmetric (as after the reference's (X + X^T)/2, assembly.cu:494-502)
     if (bi == bj && n < mm) return;
     const bool mirror = (n != mm);
-    if (NMED == 2) {
-        cplx TL = {a.eta_e * Lf[0].re + a.eta_i * Lf[1].re, a.eta_e * Lf[0].im + a.eta_i * Lf[1].im};
-        cplx BR = {Lf[0].re / a.eta_e + Lf[1].re / a.eta_i, Lf[0].im / a.eta_e + Lf[1].im / a.eta_i};
-        cplx Ks = {Kk[0].re + Kk[1].re, Kk[0].im + Kk[1].im};
+    if (a.Z) {
+        // PMCHWT blocks; with one medium the exterior-only A_ext
+        // [[eta_e L_e, -K_e], [K_e, L_e / eta_e]] (bem_core.py:1071-1090)
+        cplx TL, BR, Ks;
+        if constexpr (NMED == 2) {
+            TL = {a.eta_e * Lf[0].re + a.eta_i * Lf[1].re, a.eta_e * Lf[0].im + a.eta_i * Lf[1].im};
+            BR = {Lf[0].re / a.eta_e + Lf[1].re / a.eta_i, Lf[0].im / a.eta_e + Lf[1].im / a.eta_i};
+            Ks = {Kk[0].re + Kk[1].re, Kk[0].im + Kk[1].im};
+        } else {
+            TL = {a.eta_e * Lf[0].re, a.eta_e * Lf[0].im};
+            BR = {Lf[0].re / a.eta_e, Lf[0].im / a.eta_e};
+            Ks = Kk[0];
+        }
         double2* Z = a.Z;
         int64_t ld = a.ldz;
         Z[(int64_t)mm * ld + n] = make_double2(TL.re, TL.im);
@@ -518,9 +527,15 @@ __global__ void singular_fixup_kernel(FixArgs a) {
         cplx ik = {-k.ki, k.kr};
         dL[e] = {-iok.re * SA + ik.re * SB, -iok.im * SA + ik.im * SB};
     }
-    if (a.nmed == 2) {
-        cplx TL = {a.eta_e * dL[0].re + a.eta_i * dL[1].re, a.eta_e * dL[0].im + a.eta_i * dL[1].im};
-        cplx BR = {dL[0].re / a.eta_e + dL[1].re / a.eta_i, dL[0].im / a.eta_e + dL[1].im / a.eta_i};
+    if (a.Z) {
+        cplx TL, BR;
+        if (a.nmed == 2) {
+            TL = {a.eta_e * dL[0].re + a.eta_i * dL[1].re, a.eta_e * dL[0].im + a.eta_i * dL[1].im};
+            BR = {dL[0].re / a.eta_e + dL[1].re / a.eta_i, dL[0].im / a.eta_e + dL[1].im / a.eta_i};
+        } else {
+            TL = {a.eta_e * dL[0].re, a.eta_e * dL[0].im};
+            BR = {dL[0].re / a.eta_e, dL[0].im / a.eta_e};
+        }
         double2* z;
         z = &a.Z[(int64_t)m * a.ldz + n];
         z->x += TL.re, z->y += TL.im;
@@ -542,17 +557,20 @@ __global__ void singular_fixup_kernel(FixArgs a) {
     }
 }
 
-// mode 2: PMCHWT into Z; mode 1: L and K of medium 0 into L, K.
+// mode 2: PMCHWT into Z; mode 1: L and K of medium 0 into L, K; mode 3: the
+// exterior-only PMCHWT A_ext of medium 0 into Z.
 int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
                  double ki_im, double eta_e, double eta_i, unsigned flags, int mode, void* Z,
                  int64_t ldz, void* L, void* K, const unsigned char* band) {
     const int N = g->N;
     if (N < 1) return fail(ctx, BEM_ERR_INVALID, "empty basis");
-    if (mode == 2 && (!Z || ldz < 2 * N)) return fail(ctx, BEM_ERR_INVALID, "bad Z / ldz");
+    if ((mode == 2 || mode == 3) && (!Z || ldz < 2 * N)) return fail(ctx, BEM_ERR_INVALID, "bad Z / ldz");
     if (mode == 1 && (!L || !K || ldz < N)) return fail(ctx, BEM_ERR_INVALID, "bad L/K / ld");
     if (!(ke_re != 0.0 || ke_im != 0.0) || (mode == 2 && !(ki_re != 0.0 || ki_im != 0.0)))
         return fail(ctx, BEM_ERR_INVALID, "zero wavenumber");
     if (mode == 2 && (!(eta_e > 0) || !(eta_i > 0))) return fail(ctx, BEM_ERR_INVALID, "eta <= 0");
+    if (mode == 3 && !(eta_e > 0)) return fail(ctx, BEM_ERR_INVALID, "eta <= 0");
+    const int nmed = mode == 2 ? 2 : 1;
     BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     // 1. Graglia P, V per (triangle, point)
@@ -573,7 +591,7 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
     a.eta_e = eta_e;
     a.eta_i = eta_i;
     a.flags = flags;
-    a.Z = (double2*)Z;
+    a.Z = mode == 1 ? nullptr : (double2*)Z;
     a.ldz = ldz;
     a.L = (double2*)L;
     a.K = (double2*)K;
@@ -590,8 +608,8 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
     // algorithmic unit: one quadrature-pair evaluation per medium, every
     // ordered RWG pair (no symmetry credit): 64 flop + sincos + exp each
     if (ev)
-        ctx->prof_end(PROF_ASSEMBLY, ev, 64.0 * mode * 4.0 * N * (double)N * g->Nq * g->Nq,
-                      (mode == 2 ? 64.0 : 32.0) * (double)N * N);
+        ctx->prof_end(PROF_ASSEMBLY, ev, 64.0 * nmed * 4.0 * N * (double)N * g->Nq * g->Nq,
+                      (mode == 1 ? 32.0 : 64.0) * (double)N * N);
     // 3. singular correction
     if (g->sing.npairs > 0) {
         FixArgs f;
@@ -601,12 +619,12 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
         f.fr = g->sing_free;
         f.N = N;
         f.Nq = g->Nq;
-        f.nmed = mode;
+        f.nmed = nmed;
         f.med[0] = {ke_re, ke_im};
         f.med[1] = {ki_re, ki_im};
         f.eta_e = eta_e;
         f.eta_i = eta_i;
-        f.Z = (double2*)Z;
+        f.Z = a.Z;
         f.ldz = ldz;
         f.L = (double2*)L;
         f.ld = ldz;
@@ -723,6 +741,12 @@ int bem_assemble_pmchwt_dev(bem_ctx* ctx, const bem_geom* g, double kext_re, dou
     if (!ctx || !g) return BEM_ERR_INVALID;
     return assemble_dev(ctx, g, kext_re, kext_im, kint_re, kint_im, eta_ext, eta_int, flags, 2,
                         Z_dev, ldz, nullptr, nullptr);
+}
+
+int bem_assemble_aext_dev(bem_ctx* ctx, const bem_geom* g, double kext_re, double kext_im, double eta_ext,
+                          unsigned flags, void* Z_dev, int64_t ldz) {
+    if (!ctx || !g) return BEM_ERR_INVALID;
+    return assemble_dev(ctx, g, kext_re, kext_im, 0, 0, eta_ext, 1, flags, 3, Z_dev, ldz, nullptr, nullptr);
 }
 
 int bem_assemble_LK_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,

@@ -139,6 +139,7 @@ struct bem_ctx {
     void* oz_buf = nullptr;      // digit planes of X for the residual
     size_t oz_bytes = 0;
     bool oz_attr = false;
+    int gmres_digits = 0;        // GMRES products with Z: 0 FP64 DMMA GEMM, 2..8 int8 Ozaki digits
     int factor_sb = 2;           // L D L^T: 256-column blocks per trailing update (1 or 2)
     int solve_sb = 2;            // L D L^T solves: 256-row blocks per update (1 or 2)
     int oz_pace_epoch = 32;      // int8 residual: K slabs per pacing epoch (0: no pacing)

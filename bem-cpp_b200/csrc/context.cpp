@@ -159,6 +159,10 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
     } else if (!std::strcmp(name, "residual_pace_lead")) {
         if (value < 0) return bem::fail(ctx, BEM_ERR_INVALID, "residual_pace_lead must be >= 0");
         ctx->oz_pace_lead = value;
+    } else if (!std::strcmp(name, "gmres_digits")) {
+        if (value != 0 && (value < 2 || value > bem::oz::S_MAX))
+            return bem::fail(ctx, BEM_ERR_INVALID, "gmres_digits must be 0 or 2..%d", bem::oz::S_MAX);
+        ctx->gmres_digits = value;
     } else if (!std::strcmp(name, "factor_superblock") || !std::strcmp(name, "solve_superblock")) {
         if (value != 1 && value != 2) return bem::fail(ctx, BEM_ERR_INVALID, "%s must be 1 or 2", name);
         (name[0] == 'f' ? ctx->factor_sb : ctx->solve_sb) = value;

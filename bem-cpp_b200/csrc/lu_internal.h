@@ -68,6 +68,14 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info);
 int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2* B, int64_t ldb, float2* X,
                 int64_t ldx, int nrhs);
 
+// Factorisation without the int8 digit planes of Z (residual_digits false:
+// a factorisation used only as a preconditioner), its order, and one
+// application of the factors without refinement (B, X distinct; uses ctx->ws).
+int lu_factor_ex(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bool residual_digits, bem_lu** out,
+                 int* info);
+int lu_order(const bem_lu* lu);
+int lu_apply(bem_ctx* ctx, bem_lu* lu, const double2* B, int64_t ldb, double2* X, int64_t ldx, int nrhs);
+
 // 3xTF32 tensor-core updates (gemm_tc.cu); nullptr hooks when unavailable.
 TrailingUpdate<float> tc_update_fp32(bem_ctx* ctx);
 

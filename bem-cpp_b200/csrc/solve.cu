@@ -177,7 +177,8 @@ static int factor_lu32(bem_ctx* ctx, bem_lu* lu, int* d_info, double* fro, int* 
     return finish_factor(ctx, lu, d_info, info);
 }
 
-int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu** out, int* info) {
+int lu_factor_ex(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bool residual_digits, bem_lu** out,
+                 int* info) {
     if (!ctx || !Z || !out || n < 1 || ldz < n) return fail(ctx, BEM_ERR_INVALID, "bad lu_factor args");
     if (precision != BEM_PREC_FP64 && precision != BEM_PREC_FP32_REFINE)
         return fail(ctx, BEM_ERR_INVALID, "unknown precision %d", precision);
@@ -235,7 +236,8 @@ int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu**
         } else {
             // digit planes of Z for the int8 residual; without room for them the
             // refinement keeps the FP64 tensor-core GEMM
-            if (ctx->oz_digits > 0 && ozaki_prepare_z(ctx, &lu->oz, lu->Z, ldz, n, ctx->oz_digits) != BEM_OK)
+            if (residual_digits && ctx->oz_digits > 0 &&
+                ozaki_prepare_z(ctx, &lu->oz, lu->Z, ldz, n, ctx->oz_digits) != BEM_OK)
                 ozaki_free(&lu->oz);
             if (lu->ldlt) {
                 s = sytrf_nopiv(ctx, lu->A32, n, n, d_info);
@@ -275,6 +277,40 @@ int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu**
     }
     lu->t_factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     *out = lu;
+    return BEM_OK;
+}
+
+int lu_factor(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bem_lu** out, int* info) {
+    return lu_factor_ex(ctx, Z, n, ldz, precision, true, out, info);
+}
+
+int lu_order(const bem_lu* lu) { return lu ? lu->n : 0; }
+
+// X = (factors)^-1 B once, without refinement: the FP64 factors' solve, or
+// the FP32 factors' solve of B scaled per column by a power of two (the
+// first step of the refinement).  B and X distinct.  Uses ctx->ws.
+int lu_apply(bem_ctx* ctx, bem_lu* lu, const double2* B, int64_t ldb, double2* X, int64_t ldx, int nrhs) {
+    const int n = lu->n;
+    if (nrhs <= 0) return BEM_OK;
+    if (lu->precision == BEM_PREC_FP64)
+        return getrs<double>(ctx, lu->Z, lu->ldz, n, lu->d_perm, B, ldb, X, ldx, nrhs, nullptr);
+    const size_t nn = (size_t)n * nrhs;
+    size_t off = 0;
+    auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~(size_t)255; return o; };
+    size_t o_S = take(nn * sizeof(float2)), o_D = take(nn * sizeof(float2)), o_sc = take(nrhs * sizeof(double));
+    BEM_TRY(ctx->ensure_ws(off));
+    char* ws = (char*)ctx->ws;
+    float2* S = (float2*)(ws + o_S);
+    float2* D = (float2*)(ws + o_D);
+    double* scale = (double*)(ws + o_sc);
+    TrailingUpdate<float> tc = tc_update_fp32(ctx);
+    colmax_kernel<double2><<<nrhs, 256, 0, ctx->stream>>>(B, ldb, n, scale);
+    BEM_LAUNCHED(ctx);
+    scale_down_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, S, n, scale, n, nrhs);
+    BEM_LAUNCHED(ctx);
+    BEM_TRY(solve32(ctx, lu, S, D, nrhs, &tc));
+    scale_up_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(D, n, X, ldx, scale, n, nrhs, 0);
+    BEM_LAUNCHED(ctx);
     return BEM_OK;
 }
 

@@ -91,7 +91,11 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * tile), "residual_pace_epoch" / "residual_pace_lead" (32 / 2: the int8
  * residual's CTAs report every 32 K slabs and wait, softly, when more than 2
  * epochs ahead of the grid average, so a wave shares its digit rows in L2;
- * epoch 0 turns the pacing off).  Unknown names give BEM_ERR_INVALID. */
+ * epoch 0 turns the pacing off), "factor_superblock" / "solve_superblock"
+ * (2, default: the L D L^T factorisation and solves update with two 256-wide
+ * blocks at once, K = 512; 1: one block), "gmres_digits" (0, default: GMRES
+ * products with Z on the FP64 GEMM; 2..8: int8 Ozaki digits).  Unknown names
+ * give BEM_ERR_INVALID. */
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
@@ -165,6 +169,12 @@ int bem_assemble_pmchwt_dev(bem_ctx* ctx, const bem_geom* g,
  * row-major N x N complex128, leading dimension ld. */
 int bem_assemble_LK_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
                         unsigned flags, void* L_dev, void* K_dev, int64_t ld);
+/* Exterior-only PMCHWT (build_aext_preconditioner, bem_core.py:1071-1090):
+ *   A_ext = [[eta_e L_e, -K_e], [K_e, L_e/eta_e]]
+ * the preconditioner of the A_ext GMRES (A_ext^-1 Z = I + A_ext^-1 A_int with
+ * A_int compact).  Z_dev: row-major 2N x 2N complex128, leading dimension ldz. */
+int bem_assemble_aext_dev(bem_ctx* ctx, const bem_geom* g, double kext_re, double kext_im,
+                          double eta_ext, unsigned flags, void* Z_dev, int64_t ldz);
 /* Host-buffer mirrors: assemble_L_K_cuda (assembly.h:11-13) and assemble_pmchwt
  * (pmchwt.h:12-18).  L_ext / K_ext of the latter may be NULL. */
 int bem_assemble_L_K(bem_ctx* ctx, const double* verts, int nv, const int* tris, int nt,
@@ -235,6 +245,58 @@ int bem_lu_factorize(bem_ctx* ctx, double* Z, int n, int* ipiv, int* info);
 int bem_lu_solve(bem_ctx* ctx, const double* Z_lu, const int* ipiv, int n, double* B, int nrhs);
 int bem_lu_solve_full(bem_ctx* ctx, double* Z, int n, double* B, int nrhs, int precision,
                       bem_solve_stats* stats);
+
+/* ------------------------------------------------------------------ GMRES */
+
+/* Preconditioners of the reference's iterative dense solves (solve_gmres,
+ * bem_core.py:1126-1183, and solve_gmres_aext, :1093-1123). */
+typedef struct bem_precond bem_precond;
+typedef enum bem_precond_kind {
+    BEM_PRECOND_NONE = 0,        /* identity (precond=None) */
+    BEM_PRECOND_DIAG = 1,        /* x / diag(Z) ('diag') */
+    BEM_PRECOND_BLOCK_DIAG = 2,  /* LU of Z11 and of Z22 separately ('block_diag') */
+    BEM_PRECOND_LU = 3           /* a factorisation made by the caller, e.g. of A_ext ('aext') */
+} bem_precond_kind;
+
+/* DIAG and BLOCK_DIAG are built from Z_dev (row-major n x n, leading dimension
+ * ldz; BLOCK_DIAG needs n even), which must stay valid while the
+ * preconditioner is used.  precision: of the BLOCK_DIAG factorisations
+ * (BEM_PREC_FP64: exact solves of copies of the blocks; FP32_REFINE: FP32
+ * factors, applied once without refinement).  LU: `lu`, a factorisation of
+ * order n owned by the caller that must outlive the preconditioner (FP64
+ * factors solve exactly; FP32 factors are applied once without refinement).
+ * NONE: only n is used. */
+int bem_precond_create(bem_ctx* ctx, int kind, const void* Z_dev, int n, int64_t ldz, int precision,
+                       bem_lu* lu, bem_precond** out);
+int bem_precond_free(bem_precond* M);
+
+typedef struct bem_gmres_stats {
+    int converged;            /* 1 when every column met ||b - Z x||_2 <= tol ||b||_2 */
+    int n_unconverged;        /* columns that did not */
+    int max_iterations;       /* max over columns of inner (Arnoldi) iterations */
+    int total_iterations;     /* sum over columns */
+    int max_cycles;           /* max over columns of restart cycles */
+    int matvecs;              /* batched products with Z (each over the columns still active) */
+    double max_rel_residual;  /* max over columns of ||b - Z x||_2 / ||b||_2 (FP64) */
+    double t_ms;
+} bem_gmres_stats;
+
+/* GMRES(restart) for Z X = B, nrhs columns (column-major, leading dimensions
+ * ldb / ldx; X distinct from B), with the algorithm of
+ * scipy.sparse.linalg.gmres that the reference calls (SciPy 1.18.1): x0 = 0,
+ * left preconditioning by M, modified Gram-Schmidt Arnoldi, Givens
+ * rotations, an inner loop that ends when the preconditioned residual
+ * estimate is below its adaptive tolerance, and restart cycles until
+ * ||b - Z x||_2 <= tol ||b||_2 (recomputed in FP64) or `maxiter` cycles.  Each
+ * column runs its own Krylov space; the columns share every product with Z
+ * (the FP64 tensor-core GEMM, or the int8 Ozaki product with
+ * bem_ctx_set_option(ctx, "gmres_digits", 2..8)).  iters / info (optional,
+ * nrhs ints): inner iterations, and 0 or maxiter as scipy's info.  Columns
+ * that do not converge leave stats->converged = 0 (not an error status). */
+int bem_gmres_solve_dev(bem_ctx* ctx, const void* Z_dev, int n, int64_t ldz, bem_precond* M,
+                        const void* B_dev, int64_t ldb, void* X_dev, int64_t ldx, int nrhs,
+                        int restart, double tol, int maxiter, int* iters, int* info,
+                        bem_gmres_stats* stats);
 
 /* ------------------------------------------------------ far field, Mueller */
 

@@ -591,6 +591,146 @@ def lu_solve_dense(Z, B):
 
 
 # ---------------------------------------------------------------------------
+# f4. GMRES on the dense Z with the reference's preconditioners
+# ---------------------------------------------------------------------------
+
+def aext_matrix(L_ext, K_ext, eta_ext):
+    """A_ext = [[eta L_ext, -K_ext], [K_ext, L_ext / eta]]
+    (build_aext_preconditioner, bem_core.py:1071-1090)."""
+    N = L_ext.shape[0]
+    A = np.zeros((2 * N, 2 * N), dtype=complex)
+    A[:N, :N] = eta_ext * L_ext
+    A[:N, N:] = -K_ext
+    A[N:, :N] = K_ext
+    A[N:, N:] = L_ext / eta_ext
+    return A
+
+
+def precond_solver(Z, kind, A_ext=None):
+    """x -> M^-1 x for the preconditioners of solve_gmres (bem_core.py:1141-1166):
+    'aext' (LU of A_ext), 'block_diag' (LU of Z11 and Z22), 'diag', None."""
+    from scipy.linalg import lu_factor, lu_solve
+    n = Z.shape[0]
+    if kind == "aext":
+        lu = lu_factor(A_ext)
+        return lambda x: lu_solve(lu, x)
+    if kind == "block_diag":
+        N = n // 2
+        lu11, lu22 = lu_factor(Z[:N, :N]), lu_factor(Z[N:, N:])
+
+        def apply(x):
+            y = np.empty(n, dtype=complex)
+            y[:N] = lu_solve(lu11, x[:N])
+            y[N:] = lu_solve(lu22, x[N:])
+            return y
+        return apply
+    if kind == "diag":
+        d = np.diag(Z).copy()
+        return lambda x: x / d
+    return lambda x: np.array(x, dtype=complex, copy=True)
+
+
+def _zlartg(f, g):
+    """LAPACK zlartg: c real, s complex, [c s; -conj(s) c] [f; g] = [r; 0],
+    r with the phase of f."""
+    if g == 0:
+        return 1.0, 0j, f
+    if f == 0:
+        ag = abs(g)
+        return 0.0, np.conj(g) / ag, complex(ag)
+    af, ag = abs(f), abs(g)
+    d = math.hypot(af, ag)
+    ph = f / af
+    return af / d, ph * np.conj(g) / d, ph * d
+
+
+def gmres(A, b, psolve, rtol=1e-5, restart=20, maxiter=None):
+    """scipy.sparse.linalg.gmres as the reference calls it (solve_gmres_aext,
+    bem_core.py:1093-1123; solve_gmres :1126-1183), restated from SciPy 1.18.1
+    scipy/sparse/linalg/_isolve/iterative.py (gmres): x0 = 0, left
+    preconditioning (the preconditioned residual is minimised), modified
+    Gram-Schmidt, Givens rotations by LAPACK lartg, inner loop ended by the
+    adaptive ptol of gh-8400, restart cycles until ||b - A x|| <= rtol ||b||.
+    Returns (x, info, inner_iterations)."""
+    n = len(b)
+    bnrm2 = np.linalg.norm(b)
+    atol = rtol * bnrm2
+    x = np.zeros(n, dtype=complex)
+    if bnrm2 == 0:
+        return np.array(b, dtype=complex), 0, 0
+    eps = np.finfo(np.float64).eps
+    maxiter = n * 10 if maxiter is None else maxiter
+    restart = min(restart, n)
+    Mb_nrm2 = np.linalg.norm(psolve(b))
+    ptol_max_factor = 1.0
+    ptol = Mb_nrm2 * min(ptol_max_factor, atol / bnrm2)
+    presid = 0.0
+    v = np.empty((restart + 1, n), dtype=complex)
+    h = np.zeros((restart, restart + 1), dtype=complex)
+    givens = np.zeros((restart, 2), dtype=complex)
+    inner = 0
+    rnorm = bnrm2
+    r = np.array(b, dtype=complex)
+    if np.linalg.norm(r) < atol:
+        return x, 0, 0
+    for _ in range(maxiter):
+        v[0] = psolve(r)
+        tmp = np.linalg.norm(v[0])
+        v[0] *= 1 / tmp
+        S = np.zeros(restart + 1, dtype=complex)
+        S[0] = tmp
+        breakdown = False
+        for col in range(restart):
+            w = psolve(A @ v[col])
+            h0 = np.linalg.norm(w)
+            for k in range(col + 1):
+                t = np.vdot(v[k], w)
+                h[col, k] = t
+                w -= t * v[k]
+            h1 = np.linalg.norm(w)
+            h[col, col + 1] = h1
+            v[col + 1] = w
+            if h1 <= eps * h0:
+                h[col, col + 1] = 0
+                breakdown = True
+            else:
+                v[col + 1] *= 1 / h1
+            for k in range(col):
+                c, s = givens[k, 0], givens[k, 1]
+                n0, n1 = h[col, k], h[col, k + 1]
+                h[col, k], h[col, k + 1] = c * n0 + s * n1, -np.conj(s) * n0 + c * n1
+            c, s, mag = _zlartg(h[col, col], h[col, col + 1])
+            givens[col] = c, s
+            h[col, col], h[col, col + 1] = mag, 0
+            t = -np.conj(s) * S[col]
+            S[col], S[col + 1] = c * S[col], t
+            presid = abs(t)
+            inner += 1
+            if presid <= ptol or breakdown:
+                break
+        if h[col, col] == 0:
+            S[col] = 0
+        y = np.array(S[:col + 1])
+        for k in range(col, 0, -1):
+            if y[k] != 0:
+                y[k] /= h[k, k]
+                y[:k] -= y[k] * h[k, :k]
+        if y[0] != 0:
+            y[0] /= h[0, 0]
+        x += y @ v[:col + 1]
+        r = b - A @ x
+        rnorm = np.linalg.norm(r)
+        if rnorm <= atol or breakdown:
+            break
+        if presid <= ptol:
+            ptol_max_factor = max(eps, 0.25 * ptol_max_factor)
+        else:
+            ptol_max_factor = min(1.0, 1.5 * ptol_max_factor)
+        ptol = presid * min(ptol_max_factor, atol / rnorm)
+    return x, (0 if rnorm <= atol else maxiter), inner
+
+
+# ---------------------------------------------------------------------------
 # a12-a14. Far field and Mueller matrix
 # ---------------------------------------------------------------------------
 

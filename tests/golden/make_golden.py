@@ -10,9 +10,13 @@ on small seeded cases, and stores inputs and outputs as ``.npz`` files:
   c1_single.npz   ico ref 2, ka=1, m=1.3116 (n=960), --single: Z probes, b, X, Mueller
   ico1_orient.npz ico ref 1, ka=2, m=1.3116+0.001i, 3x4x2 orientations: <M>
   hex1_probe.npz  hex prism AR=0.7 ref 1 from the C++ mesher (C++ RWG order): Z probes
+  c1_gmres.npz    C1 system solved by the reference's GMRES: solve_gmres_aext (both
+                  columns) and solve_gmres with 'block_diag', 'diag' and None
+                  (column 0); solutions and the inner iteration counts it prints
 
 "Z probes" are Z @ v for a seeded complex vector v, diag(Z), ||Z||_F and
 Z[::s, ::s].  Usage:  python tests/golden/make_golden.py --ref /root/reference
+[--only gmres]
 """
 from __future__ import annotations
 
@@ -43,6 +47,7 @@ def rwg_arrays(rwg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", choices=["gmres"], default=None)
     a = ap.parse_args()
     os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(REPO, "_work", "numba_cache"))
     sys.path.insert(0, os.path.join(a.ref, "python"))
@@ -51,6 +56,9 @@ def main():
     from oracle import ref_host  # noqa: E402
 
     quiet = contextlib.redirect_stdout(io.StringIO())
+    if a.only == "gmres":
+        gmres_golden(bc)
+        return
 
     # 1. icosahedron, full Z
     v, t = bc.icosphere(1.0, 0)
@@ -127,6 +135,41 @@ def main():
         np.savez_compressed(os.path.join(HERE, "hex1_probe.npz"), **out)
     else:
         print("oracle/_ref/libref_host.so missing: run `make -C oracle` first; hex1 skipped")
+    gmres_golden(bc)
+
+
+def gmres_golden(bc):
+    """6. C1 solved by the reference's GMRES paths (bem_core.py:1071-1183)."""
+    import re
+    v, t = bc.icosphere(1.0, 2)
+    rwg = bc.build_rwg(v, t)
+    N = len(rwg["length"])
+    m = 1.3116
+    with contextlib.redirect_stdout(io.StringIO()):
+        Z, Lext, Kext = bc.assemble_pmchwt(rwg, v, t, 1.0, 1.0 * m, 1.0, 1.0 / abs(m),
+                                           quad_order=7, parallel=False)
+        Zext_lu, _ = bc.build_aext_preconditioner(Lext, Kext, 1.0, N)
+    B = np.stack([bc.compute_rhs_planewave(rwg, v, t, 1.0, 1.0, E0=np.array(e),
+                                           k_hat=np.array([0, 0, 1.0]), quad_order=7)
+                  for e in ([1.0, 0, 0], [0, 1.0, 0])], 1)
+    out = {"verts": v, "tris": t, **rwg_arrays(rwg), "ka": 1.0, "m": m, "B": B,
+           "tol_aext": 1e-5, "maxiter_aext": 200, "tol": 1e-4, "maxiter": 500}
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        xs = [bc.solve_gmres_aext(Z, B[:, c], Zext_lu) for c in range(2)]
+    out["x_aext"] = np.stack(xs, 1)
+    out["it_aext"] = np.array([int(i) for i in re.findall(r"GMRES\(A_ext\): (\d+) iter", buf.getvalue())])
+    assert len(out["it_aext"]) == 2, buf.getvalue()
+    for tag, pc in (("block_diag", "block_diag"), ("diag", "diag"), ("none", None)):
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            x = bc.solve_gmres(Z, B[:, 0], precond=pc)
+        it = re.findall(r"(\d+) iterations", buf.getvalue())
+        assert len(it) == 1, buf.getvalue()
+        out[f"x_{tag}"] = x
+        out[f"it_{tag}"] = int(it[0])
+        out[f"conv_{tag}"] = "did not converge" not in buf.getvalue()
+    np.savez_compressed(os.path.join(HERE, "c1_gmres.npz"), **out)
 
 
 if __name__ == "__main__":
