@@ -45,26 +45,6 @@ class SolveStats(C.Structure):
         return d
 
 
-class Problem(C.Structure):
-    _fields_ = [("verts", C.c_void_p), ("nv", C.c_int), ("tris", C.c_void_p), ("nt", C.c_int),
-                ("ka", C.c_double), ("m_re", C.c_double), ("m_im", C.c_double),
-                ("quad_order", C.c_int), ("single", C.c_int),
-                ("n_alpha", C.c_int), ("n_beta", C.c_int), ("n_gamma", C.c_int),
-                ("beta_sym", C.c_int), ("gamma_sym", C.c_int), ("gamma_mirror", C.c_int),
-                ("orient_i0", C.c_int), ("orient_i1", C.c_int), ("ntheta", C.c_int),
-                ("precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
-                ("asm_flags", C.c_uint), ("orient_tol", C.c_double)]
-
-
-class Result(C.Structure):
-    _fields_ = [("mueller", C.c_void_p), ("t_assembly_s", C.c_double),
-                ("t_solve_s", C.c_double), ("t_farfield_s", C.c_double),
-                ("t_total_s", C.c_double), ("N", C.c_int), ("n_orient", C.c_int),
-                ("stats", SolveStats), ("per_orient_mueller", C.c_void_p),
-                ("per_orient_weight", C.c_void_p), ("n_computed", C.c_int),
-                ("t_setup_s", C.c_double), ("t_release_s", C.c_double)]
-
-
 class GmresStats(C.Structure):
     _fields_ = [("converged", C.c_int), ("n_unconverged", C.c_int),
                 ("max_iterations", C.c_int), ("total_iterations", C.c_int),
@@ -76,6 +56,32 @@ class GmresStats(C.Structure):
 
 
 PRECOND_NONE, PRECOND_DIAG, PRECOND_BLOCK_DIAG, PRECOND_LU = 0, 1, 2, 3
+
+SOLVER_LU, SOLVER_GMRES_AEXT = 0, 1
+
+
+class Problem(C.Structure):
+    _fields_ = [("verts", C.c_void_p), ("nv", C.c_int), ("tris", C.c_void_p), ("nt", C.c_int),
+                ("ka", C.c_double), ("m_re", C.c_double), ("m_im", C.c_double),
+                ("quad_order", C.c_int), ("single", C.c_int),
+                ("n_alpha", C.c_int), ("n_beta", C.c_int), ("n_gamma", C.c_int),
+                ("beta_sym", C.c_int), ("gamma_sym", C.c_int), ("gamma_mirror", C.c_int),
+                ("orient_i0", C.c_int), ("orient_i1", C.c_int), ("ntheta", C.c_int),
+                ("precision", C.c_int), ("refine_tol", C.c_double), ("max_refine", C.c_int),
+                ("asm_flags", C.c_uint), ("orient_tol", C.c_double),
+                ("solver", C.c_int), ("gmres_tol", C.c_double), ("gmres_restart", C.c_int),
+                ("gmres_maxiter", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("mueller", C.c_void_p), ("t_assembly_s", C.c_double),
+                ("t_solve_s", C.c_double), ("t_farfield_s", C.c_double),
+                ("t_total_s", C.c_double), ("N", C.c_int), ("n_orient", C.c_int),
+                ("stats", SolveStats), ("per_orient_mueller", C.c_void_p),
+                ("per_orient_weight", C.c_void_p), ("n_computed", C.c_int),
+                ("t_setup_s", C.c_double), ("t_release_s", C.c_double),
+                ("gmres", GmresStats)]
+
 
 _P = C.c_void_p
 _I = C.c_int

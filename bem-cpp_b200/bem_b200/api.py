@@ -16,8 +16,8 @@ import math
 import numpy as np
 
 from ._lib import (ASM_GSMOOTH_EXACT, PRECOND_BLOCK_DIAG, PRECOND_DIAG, PRECOND_LU,  # noqa: F401
-                   PRECOND_NONE, PREC_FP32_REFINE, PREC_FP64, BemError, GmresStats, Problem,
-                   Result, SolveStats, check, lib)
+                   PRECOND_NONE, PREC_FP32_REFINE, PREC_FP64, SOLVER_GMRES_AEXT, SOLVER_LU, BemError,
+                   GmresStats, Problem, Result, SolveStats, check, lib)
 
 
 def _ptr(a):
@@ -609,14 +609,18 @@ def amplitude_to_mueller(S1, S2, S3, S4):
 def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=False,
               orient=(8, 8, 1), orient_sym=(1, 1), gamma_mirror=False, orient_range=None,
               ntheta=181, precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False,
-              orient_tol=0.0, per_orient=False):
+              orient_tol=0.0, per_orient=False, solver="lu", gmres_tol=0.0, gmres_restart=0,
+              gmres_maxiter=0):
     """The --solver dense pipeline (main.cpp:660-854) through bem_dense_run.
     Returns (mueller (4,4,ntheta), info dict).  orient_tol > 0: adaptive
     orientation stopping (main.cpp:477-636); per_orient=True adds the
     per-orientation Mueller matrices and weights of the solved orientations to
-    info ("per_orient_mueller" (n,4,4,ntheta), "per_orient_weight" (n,))."""
+    info ("per_orient_mueller" (n,4,4,ntheta), "per_orient_weight" (n,)).
+    solver "gmres_aext": GMRES with the A_ext LU preconditioner instead of
+    the LU of Z (bem_core.py:1703-1709); info["gmres"] has its statistics."""
     p, _keep = _problem(verts, tris, ka, m, quad_order, single, orient, orient_sym, gamma_mirror,
-                        orient_range, ntheta, precision, refine_tol, max_refine, exact_gsmooth, orient_tol)
+                        orient_range, ntheta, precision, refine_tol, max_refine, exact_gsmooth, orient_tol,
+                        solver, gmres_tol, gmres_restart, gmres_maxiter)
     M = np.zeros((4, 4, ntheta))
     r = Result(mueller=M.ctypes.data)
     po_M = po_w = None
@@ -631,7 +635,7 @@ def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=Fals
     info = {"N": r.N, "n_orient": r.n_orient, "n_computed": r.n_computed,
             "t_assembly_s": r.t_assembly_s, "t_solve_s": r.t_solve_s, "t_farfield_s": r.t_farfield_s,
             "t_total_s": r.t_total_s, "t_setup_s": r.t_setup_s, "t_release_s": r.t_release_s,
-            "stats": r.stats.as_dict()}
+            "stats": r.stats.as_dict(), "gmres": r.gmres.as_dict()}
     if per_orient:
         info["per_orient_mueller"] = po_M[:r.n_computed]
         info["per_orient_weight"] = po_w[:r.n_computed]
@@ -640,7 +644,11 @@ def dense_run(ctx: Context, verts, tris, ka, m=1.3116, quad_order=7, single=Fals
 
 def _problem(verts, tris, ka, m=1.3116, quad_order=7, single=False, orient=(8, 8, 1),
              orient_sym=(1, 1), gamma_mirror=False, orient_range=None, ntheta=181,
-             precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False, orient_tol=0.0):
+             precision=PREC_FP64, refine_tol=0.0, max_refine=0, exact_gsmooth=False, orient_tol=0.0,
+             solver="lu", gmres_tol=0.0, gmres_restart=0, gmres_maxiter=0):
+    solvers = {"lu": SOLVER_LU, "gmres_aext": SOLVER_GMRES_AEXT}
+    if solver not in solvers:
+        raise ValueError(f"unknown solver {solver!r} (lu, gmres_aext)")
     v, t = _f64(verts), _i32(tris)
     m = complex(m)
     i0, i1 = orient_range if orient_range is not None else (-1, -1)
@@ -651,7 +659,8 @@ def _problem(verts, tris, ka, m=1.3116, quad_order=7, single=False, orient=(8, 8
                 gamma_mirror=int(bool(gamma_mirror)), orient_i0=int(i0), orient_i1=int(i1),
                 ntheta=int(ntheta), precision=int(precision), refine_tol=float(refine_tol),
                 max_refine=int(max_refine), asm_flags=ASM_GSMOOTH_EXACT if exact_gsmooth else 0,
-                orient_tol=float(orient_tol))
+                orient_tol=float(orient_tol), solver=solvers[solver], gmres_tol=float(gmres_tol),
+                gmres_restart=int(gmres_restart), gmres_maxiter=int(gmres_maxiter))
     return p, (v, t)
 
 

@@ -38,12 +38,17 @@ static void usage(const char* prog) {
     std::printf("  --orient-auto [R]  Orientation count from ka and D_max (default R=4)\n");
     std::printf("  --precision P      fp64 (default) or fp32-refine\n");
     std::printf("  --refine-tol F     FP32+refinement error target (default 1e-11)\n");
+    std::printf("  --dense-solver S   lu (default) or gmres-aext: GMRES on Z preconditioned by\n");
+    std::printf("                     the LU of the exterior-only A_ext (bem_core.py:1093)\n");
+    std::printf("  --gmres-tol F      gmres-aext relative tolerance (default 1e-5)\n");
+    std::printf("  --gmres-restart N  gmres-aext restart (default min(200, 2N))\n");
 }
 
 int main(int argc, char** argv) {
     setbuf(stdout, NULL);
     double ka = 0, n_re = 1.3116, n_im = 0.0, hex_ar = 1.0, refine_tol = 0.0, orient_auto_R = 4.0;
-    double orient_tol = 0.0;
+    double orient_tol = 0.0, gmres_tol = 0.0;
+    int gmres_restart = 0, dense_solver = BEM_SOLVER_LU;
     int ref = 3, na = 8, nb = 8, ng = 1, ntheta = 181, quad = 7, bsym = 1, gsym = 1, i0 = -1, i1 = -1, subdiv = 0;
     bool single = false, mirror = false, orient_auto = false;
     int precision = BEM_PREC_FP64;
@@ -83,7 +88,14 @@ int main(int argc, char** argv) {
             else { std::fprintf(stderr, "Unknown precision: %s\n", p); return 1; }
         } else if (is("--refine-tol", 1)) refine_tol = std::atof(argv[++i]);
         else if (is("--orient-tol", 1)) orient_tol = std::atof(argv[++i]);
-        else if (is("--digits", 1) || is("--gmres-tol", 1) || is("--gmres-restart", 1) || is("--max-leaf", 1) ||
+        else if (is("--dense-solver", 1)) {
+            const char* d = argv[++i];
+            if (std::strcmp(d, "lu") == 0) dense_solver = BEM_SOLVER_LU;
+            else if (std::strcmp(d, "gmres-aext") == 0) dense_solver = BEM_SOLVER_GMRES_AEXT;
+            else { std::fprintf(stderr, "Unknown dense solver: %s\n", d); return 1; }
+        } else if (is("--gmres-tol", 1)) gmres_tol = std::atof(argv[++i]);
+        else if (is("--gmres-restart", 1)) gmres_restart = std::atoi(argv[++i]);
+        else if (is("--digits", 1) || is("--max-leaf", 1) ||
                  is("--prec", 1) || is("--prec-r", 1) || is("--prec-bs", 1) || is("--prec-overlap", 1)) {
             std::fprintf(stderr, "Warning: %s applies to the iterative solvers; ignored\n", argv[i]);
             ++i;
@@ -161,6 +173,9 @@ int main(int argc, char** argv) {
     p.precision = precision;
     p.refine_tol = refine_tol;
     p.orient_tol = orient_tol;
+    p.solver = dense_solver;
+    p.gmres_tol = gmres_tol;
+    p.gmres_restart = gmres_restart;
     std::vector<double> M(16 * (size_t)ntheta), theta(ntheta);
     for (int t = 0; t < ntheta; t++) theta[t] = M_PI * t / (ntheta - 1);
     bem_result r;
@@ -196,7 +211,10 @@ int main(int argc, char** argv) {
                         ntheta);
         }
     }
-    if (precision == BEM_PREC_FP32_REFINE)
+    if (dense_solver == BEM_SOLVER_GMRES_AEXT)
+        std::printf("  GMRES(A_ext): max %d iter per column, %d columns unconverged, max rel. residual %.2e\n",
+                    r.gmres.max_iterations, r.gmres.n_unconverged, r.gmres.max_rel_residual);
+    else if (precision == BEM_PREC_FP32_REFINE)
         std::printf("  FP32 + refinement: %d sweeps, estimated rel. error %.2e\n", r.stats.iterations,
                     r.stats.est_rel_error);
     write_json(out, M.data(), theta.data(), ntheta, ka, n_re, n_im, ref, na, nb, ng, r.t_assembly_s, r.t_solve_s,

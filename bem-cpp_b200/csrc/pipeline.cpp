@@ -127,12 +127,18 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
     const bool adaptive = p->orient_tol > 0 && !p->single;
     const int batch = adaptive ? std::max(20, no / 20) : no;
     const int nrhs_max = 2 * std::min(batch, no);
-    DevBuf dZ, dB, dX, dMo;
+    const bool gm = p->solver == BEM_SOLVER_GMRES_AEXT;
+    if (p->solver != BEM_SOLVER_LU && !gm) {
+        bem_geom_free(g);
+        return fail(ctx, BEM_ERR_INVALID, "unknown solver %d", p->solver);
+    }
+    DevBuf dZ, dB, dX, dMo, dA;
     int s = BEM_OK;
     if (cudaMalloc(&dZ.p, (size_t)n * n * 16) != cudaSuccess ||
         cudaMalloc(&dB.p, (size_t)n * nrhs_max * 16) != cudaSuccess ||
         cudaMalloc(&dX.p, (size_t)n * nrhs_max * 16) != cudaSuccess ||
-        cudaMalloc(&dMo.p, (size_t)std::min(batch, no) * 16 * nt * 8) != cudaSuccess) {
+        cudaMalloc(&dMo.p, (size_t)std::min(batch, no) * 16 * nt * 8) != cudaSuccess ||
+        (gm && cudaMalloc(&dA.p, (size_t)n * n * 16) != cudaSuccess)) {
         cudaGetLastError();
         bem_geom_free(g);
         return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs_max);
@@ -145,10 +151,31 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         s = fail(ctx, BEM_ERR_CUDA, "assembly: %s", cudaGetErrorString(cudaGetLastError()));
     r->t_assembly_s = secs(t0);
     auto t1 = std::chrono::steady_clock::now();
-    bem_lu* lu = nullptr;
+    bem_lu* lu = nullptr;       // LU of Z, or of A_ext (GMRES preconditioner)
+    bem_precond* M = nullptr;
     int info = 0;
-    if (s == BEM_OK) s = bem_lu_factor_dev(ctx, dZ.p, n, n, p->precision, &lu, &info);
-    if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+    if (gm) {
+        // A_ext = [[eta L_ext, -K_ext], [K_ext, L_ext/eta]] and its LU
+        // (build_aext_preconditioner, bem_core.py:1071-1090); the
+        // preconditioner's factorisation needs no int8 digit planes
+        if (s == BEM_OK)
+            s = assemble_dev(ctx, g, kext.real(), kext.imag(), 0, 0, eta_e, 1, p->asm_flags, 3, dA.p, n, nullptr,
+                             nullptr);
+        const int digits = ctx->oz_digits;
+        ctx->oz_digits = 0;
+        if (s == BEM_OK) s = bem_lu_factor_dev(ctx, dA.p, n, n, p->precision, &lu, &info);
+        ctx->oz_digits = digits;
+        if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "A_ext: zero pivot at %d", info);
+        if (s == BEM_OK) s = bem_precond_create(ctx, BEM_PRECOND_LU, nullptr, n, n, p->precision, lu, &M);
+    } else {
+        if (s == BEM_OK) s = bem_lu_factor_dev(ctx, dZ.p, n, n, p->precision, &lu, &info);
+        if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+    }
+    const double gtol = p->gmres_tol > 0 ? p->gmres_tol : 1e-5;
+    const int grestart = p->gmres_restart > 0 ? p->gmres_restart : std::min(200, n);
+    const int gmaxiter = p->gmres_maxiter > 0 ? p->gmres_maxiter : 200;
+    std::memset(&r->gmres, 0, sizeof r->gmres);
+    r->gmres.converged = 1;
     r->t_solve_s = secs(t1);
     r->t_farfield_s = 0.0;
     // streamed multi-RHS solve and far field per batch
@@ -165,7 +192,30 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         s = rhs_dev(ctx, g, kext.real(), kext.imag(), eta_e, RT.data() + 9 * (size_t)o0, nullptr, nullptr, nb, dB.p,
                     n);
         bem_solve_stats st;
-        if (s == BEM_OK) s = bem_lu_solve_dev(ctx, lu, dB.p, n, dX.p, n, nrhs, p->refine_tol, p->max_refine, &st);
+        std::memset(&st, 0, sizeof st);
+        if (gm) {
+            bem_gmres_stats gs;
+            if (s == BEM_OK)
+                s = bem_gmres_solve_dev(ctx, dZ.p, n, n, M, dB.p, n, dX.p, n, nrhs, grestart, gtol, gmaxiter, nullptr,
+                                        nullptr, &gs);
+            if (s != BEM_OK) break;
+            bem_gmres_stats& a = r->gmres;
+            a.converged = a.converged && gs.converged;
+            a.n_unconverged += gs.n_unconverged;
+            a.max_iterations = std::max(a.max_iterations, gs.max_iterations);
+            a.total_iterations += gs.total_iterations;
+            a.max_cycles = std::max(a.max_cycles, gs.max_cycles);
+            a.matvecs += gs.matvecs;
+            a.max_rel_residual = std::max(a.max_rel_residual, gs.max_rel_residual);
+            a.t_ms += gs.t_ms;
+            st.iterations = gs.max_iterations;
+            st.converged = gs.converged;
+            st.max_rel_residual = gs.max_rel_residual;
+            st.t_factor_ms = 0;
+            st.factorization = -1;
+        } else if (s == BEM_OK) {
+            s = bem_lu_solve_dev(ctx, lu, dB.p, n, dX.p, n, nrhs, p->refine_tol, p->max_refine, &st);
+        }
         if (s != BEM_OK) break;
         r->stats.iterations = std::max(r->stats.iterations, st.iterations);
         r->stats.converged = o0 == 0 ? st.converged : (r->stats.converged && st.converged);
@@ -220,6 +270,7 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         }
     }
     auto tr = std::chrono::steady_clock::now();
+    if (M) bem_precond_free(M);
     if (lu) bem_lu_free(lu);
     r->t_release_s = secs(tr);
     if (s == BEM_OK) {
@@ -234,6 +285,7 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         dB.release();
         dX.release();
         dMo.release();
+        dA.release();
         bem_geom_free(g);
         g = nullptr;
         r->t_release_s += secs(tf);

@@ -376,7 +376,21 @@ typedef struct bem_problem {
      * previous batch's; two consecutive relative changes below orient_tol stop
      * the loop and the average is rescaled to the full weight.  0 = off. */
     double orient_tol;
+    /* Solver of the orientation columns: BEM_SOLVER_LU (the LU of Z, default)
+     * or BEM_SOLVER_GMRES_AEXT (GMRES on Z with the LU of the exterior-only
+     * A_ext as preconditioner, per column as the reference's
+     * orientation-averaging functions do when given Z_ext_lu,
+     * bem_core.py:1703-1709; `precision` then applies to A_ext's LU).
+     * gmres_tol <= 0: 1e-5; gmres_restart <= 0: min(200, 2N);
+     * gmres_maxiter <= 0: 200 (solve_gmres_aext's defaults). */
+    int solver;
+    double gmres_tol;
+    int gmres_restart;
+    int gmres_maxiter;
 } bem_problem;
+
+#define BEM_SOLVER_LU 0
+#define BEM_SOLVER_GMRES_AEXT 1
 
 typedef struct bem_result {
     double* mueller;       /* caller buffer, 16 * ntheta doubles */
@@ -392,6 +406,7 @@ typedef struct bem_result {
     int n_computed;        /* orientations solved (< n_orient after an adaptive stop) */
     double t_setup_s;      /* geometry upload, orientations and device buffers */
     double t_release_s;    /* freeing the device buffers */
+    bem_gmres_stats gmres; /* BEM_SOLVER_GMRES_AEXT: over all batches */
 } bem_result;
 
 /* The dense branch of main.cpp (:660-854) end to end on the device: assemble,

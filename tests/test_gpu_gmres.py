@@ -169,3 +169,41 @@ def test_bad_arguments(ctx, c1):
         bb.Preconditioner(ctx, "diag", Z=Zodd)              # zero diagonal
     with pytest.raises(bb.BemError):
         bb.gmres(ctx, Z, g["B"], bb.Preconditioner(ctx, None, n=4))   # order mismatch
+
+
+def test_dense_run_with_gmres_aext(ctx):
+    # orientation averaging solved column by column with GMRES(A_ext), as the
+    # reference's orientation functions do when given Z_ext_lu
+    # (bem_core.py:1703-1709): the Mueller matrix agrees with the LU path to
+    # the GMRES tolerance
+    import bem_b200 as bb
+    v, t = bb.icosphere(1.0, 2)
+    kw = dict(orient=(3, 4, 1), ntheta=37)
+    M_lu, _ = bb.dense_run(ctx, v, t, 2.0, complex(1.4, 0.01), **kw)
+    M_gm, info = bb.dense_run(ctx, v, t, 2.0, complex(1.4, 0.01), solver="gmres_aext", gmres_tol=1e-8, **kw)
+    g = info["gmres"]
+    assert g["converged"] == 1 and g["n_unconverged"] == 0 and 0 < g["max_iterations"] <= 30
+    assert g["max_rel_residual"] <= 1e-8
+    assert rel(M_gm, M_lu) < 1e-6
+    M32, i32 = bb.dense_run(ctx, v, t, 2.0, complex(1.4, 0.01), solver="gmres_aext", gmres_tol=1e-8,
+                            precision=bb.PREC_FP32_REFINE, **kw)
+    assert i32["gmres"]["converged"] == 1 and rel(M32, M_lu) < 1e-6
+
+
+def test_cli_dense_solver_gmres_aext(tmp_path):
+    import json
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "bem-cpp_b200", "bin",
+                       "bem_cuda")
+    if not os.path.exists(cli):
+        pytest.skip("bem_cuda not built")
+    base = [cli, "--ka", "1.5", "--ref", "2", "--ri", "1.33", "0.0", "--orient", "2", "3", "1", "--ntheta", "19"]
+    out = {}
+    for tag, extra in (("lu", []), ("gm", ["--dense-solver", "gmres-aext", "--gmres-tol", "1e-9"])):
+        f = tmp_path / f"{tag}.json"
+        run = subprocess.run(base + extra + ["--out", str(f)], check=True, capture_output=True, text=True,
+                             timeout=300)
+        out[tag] = (np.array(json.loads(f.read_text())["mueller"]), run.stdout)
+    assert "GMRES(A_ext)" in out["gm"][1]
+    assert rel(out["gm"][0], out["lu"][0]) < 1e-6
