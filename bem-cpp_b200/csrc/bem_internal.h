@@ -107,6 +107,17 @@ struct DevSingular {
     double* tv;         // (nt*9) triangle vertices
 };
 
+// Device-memory cache for the large per-factorisation blocks (FP32 factors,
+// int8 digit planes of Z).  While enabled for a device (the
+// "cache_factor_memory" option), blocks freed there are kept and handed to
+// the next request of exactly the same size, so a loop of factorisations of
+// one size allocates once.  Per device and process-wide, so a factorisation
+// may outlive the context that made it.  Disabling frees the kept blocks; an
+// allocation that fails frees them and retries once.
+void* devmem_alloc(int device, size_t bytes);  // nullptr when out of memory
+void devmem_free(int device, void* p, size_t bytes);
+void devmem_cache_enable(int device, bool on);
+
 }  // namespace bem
 
 // Per-kernel-class timing (CUDA events around the launches of one class on

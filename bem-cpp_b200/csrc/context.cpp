@@ -1,6 +1,7 @@
 // Context: device, stream, error reporting, workspace.
 #include <cstdarg>
 #include <cstring>
+#include <mutex>
 
 #include "bem_internal.h"
 #include "ozaki.h"
@@ -68,6 +69,80 @@ int bem_ctx::prof_collect() {
     prof_pending.clear();
     return BEM_OK;
 }
+
+namespace bem {
+namespace {
+struct DevCache {
+    bool on = false;
+    std::vector<std::pair<void*, size_t>> blocks;
+};
+std::mutex g_cache_mu;
+DevCache g_cache[64];
+
+void trim_locked(int device) {
+    DevCache& c = g_cache[device];
+    if (c.blocks.empty()) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    for (auto& b : c.blocks) cudaFree(b.first);
+    c.blocks.clear();
+    cudaSetDevice(prev);
+}
+}  // namespace
+
+void* devmem_alloc(int device, size_t bytes) {
+    if (device >= 0 && device < 64) {
+        std::lock_guard<std::mutex> g(g_cache_mu);
+        auto& bl = g_cache[device].blocks;
+        for (size_t i = 0; i < bl.size(); i++)
+            if (bl[i].second == bytes) {
+                void* p = bl[i].first;
+                bl.erase(bl.begin() + i);
+                return p;
+            }
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    cudaGetLastError();
+    if (device < 0 || device >= 64) return nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_cache_mu);
+        if (g_cache[device].blocks.empty()) return nullptr;
+        trim_locked(device);
+    }
+    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    cudaGetLastError();
+    return nullptr;
+}
+
+void devmem_free(int device, void* p, size_t bytes) {
+    if (!p) return;
+    if (device >= 0 && device < 64) {
+        std::lock_guard<std::mutex> g(g_cache_mu);
+        if (g_cache[device].on) {
+            // work queued on any stream of this device that still reads the
+            // block must finish before another factorisation reuses it
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(device);
+            cudaDeviceSynchronize();
+            cudaSetDevice(prev);
+            g_cache[device].blocks.push_back({p, bytes});
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
+void devmem_cache_enable(int device, bool on) {
+    if (device < 0 || device >= 64) return;
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    g_cache[device].on = on;
+    if (!on) trim_locked(device);
+}
+
+}  // namespace bem
 
 int bem_ctx::ensure_ws(size_t bytes) {
     if (bytes <= ws_bytes) return BEM_OK;
@@ -166,6 +241,8 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
     } else if (!std::strcmp(name, "factor_superblock") || !std::strcmp(name, "solve_superblock")) {
         if (value != 1 && value != 2) return bem::fail(ctx, BEM_ERR_INVALID, "%s must be 1 or 2", name);
         (name[0] == 'f' ? ctx->factor_sb : ctx->solve_sb) = value;
+    } else if (!std::strcmp(name, "cache_factor_memory")) {
+        bem::devmem_cache_enable(ctx->device, value != 0);
     } else if (!std::strcmp(name, "persistent_gemm")) {
         ctx->tc_persistent = value != 0;
     } else {

@@ -753,8 +753,10 @@ int ozaki_prepare_z(bem_ctx* ctx, OzakiZ* oz_, const double2* Z, int64_t ldz, in
     oz_->ldk = ((int64_t)2 * n + oz::BKB - 1) / oz::BKB * oz::BKB;
     oz_->plane = (int64_t)n * oz_->ldk;
     size_t bytes = (size_t)S * oz_->plane;
-    if (cudaMalloc(&oz_->A, bytes) != cudaSuccess || cudaMalloc(&oz_->e, (size_t)n * sizeof(int)) != cudaSuccess) {
-        cudaGetLastError();
+    oz_->device = ctx->device;
+    oz_->A = (int8_t*)devmem_alloc(ctx->device, bytes);
+    oz_->e = oz_->A ? (int*)devmem_alloc(ctx->device, (size_t)n * sizeof(int)) : nullptr;
+    if (!oz_->A || !oz_->e) {
         ozaki_free(oz_);
         return fail(ctx, BEM_ERR_OOM, "ozaki digit planes (%zu bytes)", bytes);
     }
@@ -768,8 +770,8 @@ int ozaki_prepare_z(bem_ctx* ctx, OzakiZ* oz_, const double2* Z, int64_t ldz, in
 }
 
 void ozaki_free(OzakiZ* oz_) {
-    if (oz_->A) cudaFree(oz_->A);
-    if (oz_->e) cudaFree(oz_->e);
+    devmem_free(oz_->device, oz_->A, (size_t)oz_->S * oz_->plane);
+    devmem_free(oz_->device, oz_->e, (size_t)oz_->n * sizeof(int));
     oz_->A = nullptr;
     oz_->e = nullptr;
 }

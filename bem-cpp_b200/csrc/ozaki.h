@@ -18,6 +18,7 @@ struct OzakiZ {
     int64_t plane = 0;  // bytes per digit plane (n * ldk)
     int8_t* A = nullptr;
     int* e = nullptr;   // per-row power-of-two exponents
+    int device = -1;    // where A and e live
 };
 
 size_t ozaki_z_bytes(int n, int S);

@@ -72,6 +72,8 @@ def parse():
                     help="256-column blocks per L D L^T trailing update")
     ap.add_argument("--solve-superblock", type=int, default=2, choices=[1, 2],
                     help="256-row blocks per L D L^T solve update")
+    ap.add_argument("--no-factor-cache", action="store_true",
+                    help="free the FP32 factors and digit planes after every step instead of reusing them")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -264,6 +266,8 @@ def run_bem(a):
     bb.set_option(ctx, "residual_pairs", a.residual_pairs)
     bb.set_option(ctx, "factor_superblock", a.factor_superblock)
     bb.set_option(ctx, "solve_superblock", a.solve_superblock)
+    # a loop of solves of one size keeps its factor / digit-plane memory
+    bb.set_option(ctx, "cache_factor_memory", 0 if a.no_factor_cache else 1)
     X = torch.empty_like(B)
     def step():
         lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
@@ -289,6 +293,7 @@ def run_bem(a):
     prof = ctx.profile_read()
     ctx.profile(False)
     clocks = sampler.stop()
+    bb.set_option(ctx, "cache_factor_memory", 0)
     launches = ctx.launches - launches0
     times = [evs[i].elapsed_time(evs[i + 1]) / 1e3 for i in range(a.steps)]
     t_total = evs[0].elapsed_time(evs[-1]) / 1e3
@@ -347,21 +352,38 @@ def run_bem(a):
     torch.cuda.empty_cache()
     e2e = None
     if not a.no_e2e:
+        from bem_b200.parallel import allreduce_max, allreduce_sum
+        # N > 1: every rank runs the pipeline on its orientation range
+        # (--orient-range, main.cpp:118-121) and one all-reduce sums the
+        # partial Mueller matrices (the cluster_bem.py JSON sum).  Every rank
+        # takes the same collectives whether or not its pipeline failed.
+        dev = f"cuda:{local}"
+        barrier()
+        t0 = time.perf_counter()
+        err_e2e, info = None, None
+        M = np.zeros((4, 4, 181))
         try:
-            t0 = time.perf_counter()
             M, info = bb.dense_run(ctx, verts, tris, a.ka, a.m, orient=tuple(a.orient), ntheta=181,
-                                   precision=bb.PREC_FP32_REFINE, refine_tol=a.tol, max_refine=12)
-            t_e2e = time.perf_counter() - t0
+                                   precision=bb.PREC_FP32_REFINE, refine_tol=a.tol, max_refine=12,
+                                   orient_range=(o0, o1) if world > 1 else None)
+        except bb.BemError as ex:
+            err_e2e = str(ex)
+        if world > 1:
+            M = allreduce_sum(M, device=dev).reshape(M.shape)
+        t_e2e = allreduce_max(time.perf_counter() - t0, device=dev)
+        failed = allreduce_max(1.0 if err_e2e else 0.0, device=dev) > 0
+        if failed:
+            e2e = {"value": None, "unit": "s/solve", "error": err_e2e or "the pipeline failed on another rank"}
+        else:
             h2d = verts.nbytes + tris.astype(np.int32).nbytes + 9 * 8 * no_all + 8 * no_all
             e2e = {"value": t_e2e, "unit": "s/solve", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(M.nbytes),
-                   "scope": "bem_dense_run: host mesh -> assembly, FP32 LU + refinement, far field -> host Mueller",
+                   "scope": "bem_dense_run: host mesh -> assembly, FP32 LU + refinement, far field -> host Mueller"
+                            + (f"; orientations split over {world} ranks, Mueller all-reduced" if world > 1 else ""),
                    "t_assembly_s": info["t_assembly_s"], "t_solve_s": info["t_solve_s"],
                    "t_farfield_s": info["t_farfield_s"], "t_setup_s": info["t_setup_s"],
                    "t_release_s": info["t_release_s"], "t_total_s": info["t_total_s"],
                    "refine": info["stats"]["iterations"]}
-        except bb.BemError as ex:
-            e2e = {"value": None, "unit": "s/solve", "error": str(ex)}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -377,7 +399,10 @@ def run_bem(a):
                          (f" (int8 Ozaki residual, {a.residual_digits} digits)" if a.residual_digits else
                           " (FP64 DMMA residual)"),
                 "data": "synthetic (generated icosphere mesh and plane waves)",
-                "config": {**workload(a, n), "parallelism": f"rhs-split x{world}" if world > 1 else "single"},
+                "config": {**workload(a, n), "parallelism": f"rhs-split x{world}" if world > 1 else "single",
+                           "factor_memory": ("allocated and freed by every step" if a.no_factor_cache else
+                                             "FP32 factors and digit planes allocated once, reused by every step "
+                                             "(cache_factor_memory)")},
                 "step_times_s": times, "max_step_s": t_max,
                 "fp64_s_per_solve": t64m or None,
                 "speedup_vs_fp64": (t64m / t_step) if t64m else None,

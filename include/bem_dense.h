@@ -94,8 +94,14 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * epoch 0 turns the pacing off), "factor_superblock" / "solve_superblock"
  * (2, default: the L D L^T factorisation and solves update with two 256-wide
  * blocks at once, K = 512; 1: one block), "gmres_digits" (0, default: GMRES
- * products with Z on the FP64 GEMM; 2..8: int8 Ozaki digits).  Unknown names
- * give BEM_ERR_INVALID. */
+ * products with Z on the FP64 GEMM; 2..8: int8 Ozaki digits),
+ * "cache_factor_memory" (0, default; 1: the FP32 factors and int8 digit planes
+ * of a freed factorisation stay allocated on this context's device and are
+ * reused by the next factorisation of the same order, so a loop of solves of
+ * one size allocates them once; the kept memory counts against the device
+ * until the option is set back to 0, which frees it, or until an allocation
+ * of this library fails, which frees it and retries).  Unknown names give
+ * BEM_ERR_INVALID. */
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);

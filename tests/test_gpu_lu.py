@@ -105,3 +105,37 @@ def test_pmchwt_fp64_and_fp32_refine(ctx):
     assert rel(X64, Xr) < 1e-12
     col = np.linalg.norm(X32 - X64, axis=0) / np.linalg.norm(X64, axis=0)
     assert col.max() < 1e-9, (col.max(), st)
+
+
+def test_factor_memory_cache_reuses_blocks_bitwise(ctx):
+    # cache_factor_memory: a loop of factorisations of one order reuses the
+    # FP32 factor and digit-plane blocks; results are bitwise those of fresh
+    # allocations, and switching the option off returns the memory
+    import torch
+    import bem_b200 as bb
+    rng = np.random.default_rng(17)
+    n = 640
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 4 * np.sqrt(n) * np.eye(n)
+    Z = torch.from_numpy(A).cuda()
+    B = torch.from_numpy(np.ascontiguousarray((rng.standard_normal((n, 6)) + 0j).T)).cuda()
+
+    def run():
+        lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+        X, st = lu.solve(B, tol=1e-12)
+        lu.close()
+        torch.cuda.synchronize()
+        return X.cpu().numpy(), st
+
+    X0, _ = run()
+    bb.set_option(ctx, "cache_factor_memory", 1)
+    try:
+        free0 = torch.cuda.mem_get_info()[0]
+        X1, _ = run()
+        held = free0 - torch.cuda.mem_get_info()[0]
+        X2, _ = run()
+        assert held >= n * n * 8                     # the FP32 factors stay allocated
+        assert free0 - torch.cuda.mem_get_info()[0] <= held + (2 << 20)   # and are reused
+    finally:
+        bb.set_option(ctx, "cache_factor_memory", 0)
+    assert torch.cuda.mem_get_info()[0] >= free0 - (2 << 20)
+    assert np.array_equal(X0, X1) and np.array_equal(X1, X2)
