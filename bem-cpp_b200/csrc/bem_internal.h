@@ -144,6 +144,7 @@ struct bem_ctx {
     float* tc_buf = nullptr;  // packed hi/lo operands of the tensor-core GEMM
     size_t tc_bytes = 0;
     bool tc_attr = false;
+    int tc_group_m = 16;         // row tiles per raster group of the persistent tensor-core GEMM
     bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)
     int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)
     int oz_digits = 7;           // int8 digits of the Ozaki residual (0: FP64 DMMA residual)

@@ -261,27 +261,28 @@ gemm_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ C
 // accumulator into C, so the read-modify-write of tile i overlaps the MMAs of
 // tile i+1.  Barriers: full/empty per smem stage, tfull/tempty per
 // accumulator (tempty counts the four epilogue warps).
-// Raster: groups of GROUP_M row tiles x all column tiles; a wave of 148 tiles
-// then spans ~16 row x ~9 column tiles (8 MB of A and 9 MB of B panels in L2),
-// which halves the B-panel re-reads against groups of 8.
-constexpr int GROUP_M = 16;
+// Raster: groups of gm row tiles x all column tiles (gm = 16 by default,
+// bem_ctx_set_option "gemm_group_m"); a wave of 148 tiles then spans ~16 row x
+// ~9 column tiles (8 MB of A and 9 MB of B panels in L2 at K = 256), which
+// halves the B-panel re-reads against groups of 8.
 constexpr uint32_t TMEM_COLS2 = 512;
 
 struct TileMap {
     int num_m, num_n;
+    int gm;     // row tiles per raster group
     int lower;  // square C, only tiles on or below the diagonal (BM rows == BN / 2 complex columns)
     __device__ __forceinline__ int count() const {
         return lower ? num_m * (num_m + 1) / 2 : num_m * num_n;
     }
-    // Grouped raster: GROUP_M row tiles at a time, column by column.  For the
+    // Grouped raster: gm row tiles at a time, column by column.  For the
     // lower triangle only the tiles on or below the diagonal are enumerated
     // (row group g starts at tile S(g) = G g (G g + 1) / 2), so consecutive
     // CTAs stay on neighbouring tiles and share their operand panels in L2.
     __device__ __forceinline__ void tile(int t, int& mt, int& nt) const {
         if (!lower) {
-            const int per_group = GROUP_M * num_n;
-            const int g = t / per_group, first_m = g * GROUP_M;
-            const int gsize = min(GROUP_M, num_m - first_m);
+            const int per_group = gm * num_n;
+            const int g = t / per_group, first_m = g * gm;
+            const int gsize = min(gm, num_m - first_m);
             const int r = t % per_group;
             mt = first_m + r % gsize;
             nt = r / gsize;
@@ -291,8 +292,8 @@ struct TileMap {
         long long y = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
         while (y > 0 && y * (y + 1) / 2 > t) y--;
         while ((y + 1) * (y + 2) / 2 <= t) y++;
-        const int g = (int)(y / GROUP_M), first_m = g * GROUP_M;
-        const int gsize = min(GROUP_M, num_m - first_m);
+        const int g = (int)(y / gm), first_m = g * gm;
+        const int gsize = min(gm, num_m - first_m);
         int r = t - (int)((long long)first_m * (first_m + 1) / 2);
         if (r < gsize * first_m) {  // columns left of the group's diagonal block
             nt = r / gsize;
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(192, 1)
 gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                        const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
                        float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int lower,
-                       int store, int* status) {
+                       int store, int group_m, int* status) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
@@ -339,6 +340,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     tm.num_m = (M + BM - 1) / BM;
     tm.num_n = (2 * Nc + BN - 1) / BN;
     tm.lower = lower;
+    tm.gm = group_m > 0 ? group_m : 16;
     const int ntiles = tm.count();
 
     if (threadIdx.x == 0) {
@@ -728,7 +730,7 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
         tc::gemm_persistent_kernel<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc,
                                                                                 c_colmajor ? 1 : 0, M, N, ld,
                                                                                 o.lower ? 1 : 0, o.store ? 1 : 0,
-                                                                                ctx->d_status);
+                                                                                ctx->tc_group_m, ctx->d_status);
     } else {
         dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
         if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");

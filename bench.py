@@ -72,6 +72,8 @@ def parse():
                     help="256-column blocks per L D L^T trailing update")
     ap.add_argument("--solve-superblock", type=int, default=2, choices=[1, 2],
                     help="256-row blocks per L D L^T solve update")
+    ap.add_argument("--gemm-group-m", type=int, default=16,
+                    help="row tiles per raster group of the tensor-core GEMM")
     ap.add_argument("--no-factor-cache", action="store_true",
                     help="free the FP32 factors and digit planes after every step instead of reusing them")
     ap.add_argument("--no-fp64", action="store_true")
@@ -266,6 +268,7 @@ def run_bem(a):
     bb.set_option(ctx, "residual_pairs", a.residual_pairs)
     bb.set_option(ctx, "factor_superblock", a.factor_superblock)
     bb.set_option(ctx, "solve_superblock", a.solve_superblock)
+    bb.set_option(ctx, "gemm_group_m", a.gemm_group_m)
     # a loop of solves of one size keeps its factor / digit-plane memory
     bb.set_option(ctx, "cache_factor_memory", 0 if a.no_factor_cache else 1)
     X = torch.empty_like(B)
