@@ -13,6 +13,7 @@
 //                            mirrored (L and K are symmetric).
 //   3. singular_fixup     -- per RWG pair sharing a triangle: the symmetrised
 //                            same-triangle correction (S[m,n] + S[n,m])/2.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -99,6 +100,92 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     g->sing.npairs = (int)pair_mn.size() / 2;
     g->sing.nitems = (int)item.size() / 3;
 
+    // triangle-pair assembly data: per triangle the centroid, the quadrature
+    // points relative to it (the same points as the halves') and area x
+    // weight; per half the free vertex relative to its triangle's centroid
+    std::vector<double> tc(3 * (size_t)nt), tu(3 * (size_t)nt * Nq), tjw((size_t)nt * Nq), hpi(3 * (size_t)2 * N);
+    std::vector<double> tarea(nt, -1.0);
+    for (int h = 0; h < 2; h++)
+        for (int n = 0; n < N; n++) {
+            const int t = h == 0 ? r.tri_p[n] : r.tri_m[n];
+            if (tarea[t] < 0) tarea[t] = h == 0 ? r.area_p[n] : r.area_m[n];
+        }
+    for (int t = 0; t < nt; t++) {
+        V3 v0 = m.verts[m.tris[3 * t]], v1 = m.verts[m.tris[3 * t + 1]], v2 = m.verts[m.tris[3 * t + 2]];
+        const double cx0 = (v0.x + v1.x + v2.x) / 3.0, cy0 = (v0.y + v1.y + v2.y) / 3.0,
+                     cz0 = (v0.z + v1.z + v2.z) / 3.0;
+        tc[3 * t] = cx0, tc[3 * t + 1] = cy0, tc[3 * t + 2] = cz0;
+        for (int k = 0; k < Nq; k++) {
+            double l1 = q.l1[k], l2 = q.l2[k], l0 = 1.0 - l1 - l2;
+            double rx = (v0.x * l0 + v1.x * l1) + v2.x * l2;
+            double ry = (v0.y * l0 + v1.y * l1) + v2.y * l2;
+            double rz = (v0.z * l0 + v1.z * l1) + v2.z * l2;
+            size_t i = ((size_t)t * Nq + k) * 3;
+            tu[i] = rx - cx0, tu[i + 1] = ry - cy0, tu[i + 2] = rz - cz0;
+            tjw[(size_t)t * Nq + k] = (tarea[t] > 0 ? tarea[t] : 0.0) * q.w[k];
+        }
+    }
+    for (int h = 0; h < 2; h++)
+        for (int n = 0; n < N; n++) {
+            const int t = h == 0 ? r.tri_p[n] : r.tri_m[n];
+            const V3 fr = h == 0 ? r.free_p[n] : r.free_m[n];
+            size_t i = ((size_t)h * N + n) * 3;
+            hpi[i] = fr.x - tc[3 * t], hpi[i + 1] = fr.y - tc[3 * t + 1], hpi[i + 2] = fr.z - tc[3 * t + 2];
+        }
+    // RWGs in the Morton order of their triangles' centroids: each triangle
+    // in turn appends its RWGs not placed yet, so a tile of 16 consecutive
+    // RWGs touches ~17 distinct triangles instead of ~21-32
+    std::vector<int> torder(nt);
+    {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int t = 0; t < nt; t++)
+            for (int j = 0; j < 3; j++) lo[j] = std::min(lo[j], tc[3 * t + j]), hi[j] = std::max(hi[j], tc[3 * t + j]);
+        const double span = std::max(std::max(hi[0] - lo[0], hi[1] - lo[1]), std::max(hi[2] - lo[2], 1e-300));
+        std::vector<uint64_t> key(nt);
+        for (int t = 0; t < nt; t++) {
+            uint64_t code = 0;
+            uint64_t c3[3];
+            for (int j = 0; j < 3; j++) {
+                double f = (tc[3 * t + j] - lo[j]) / span;
+                c3[j] = (uint64_t)std::min(2097151.0, std::max(0.0, f * 2097151.0));
+            }
+            for (int b = 20; b >= 0; b--)
+                for (int j = 0; j < 3; j++) code = (code << 1) | ((c3[j] >> b) & 1u);
+            key[t] = code;
+        }
+        for (int t = 0; t < nt; t++) torder[t] = t;
+        std::stable_sort(torder.begin(), torder.end(), [&](int x, int y) { return key[x] < key[y]; });
+    }
+    std::vector<std::vector<int>> rwg_of_tri(nt);
+    for (int n = 0; n < N; n++) rwg_of_tri[r.tri_p[n]].push_back(n), rwg_of_tri[r.tri_m[n]].push_back(n);
+    const int ntile = (N + ASM_TILE - 1) / ASM_TILE;
+    std::vector<int> perm, pos(N, -1);
+    perm.reserve(N);
+    for (int t : torder)
+        for (int n : rwg_of_tri[t])
+            if (pos[n] < 0) pos[n] = (int)perm.size(), perm.push_back(n);
+    std::vector<int> tile_rwg((size_t)ntile * ASM_TILE, -1), tile_tri((size_t)ntile * ASM_TRI_MAX, -1), tile_ntri(ntile, 0);
+    std::vector<unsigned char> tile_ent((size_t)ntile * ASM_TRI_MAX * 3, 0xff);
+    for (int tl = 0; tl < ntile; tl++) {
+        int cnt = 0;
+        for (int sl = 0; sl < ASM_TILE && tl * ASM_TILE + sl < N; sl++) {
+            const int n = perm[tl * ASM_TILE + sl];
+            tile_rwg[(size_t)tl * ASM_TILE + sl] = n;
+            for (int h = 0; h < 2; h++) {
+                const int t = h == 0 ? r.tri_p[n] : r.tri_m[n];
+                int li = 0;
+                while (li < cnt && tile_tri[(size_t)tl * ASM_TRI_MAX + li] != t) li++;
+                if (li == cnt) tile_tri[(size_t)tl * ASM_TRI_MAX + cnt++] = t;
+                unsigned char* e = &tile_ent[((size_t)tl * ASM_TRI_MAX + li) * 3];
+                int j = 0;
+                while (j < 3 && e[j] != 0xff) j++;
+                if (j == 3) return fail(ctx, BEM_ERR_INVALID, "triangle %d carries more than 3 RWG halves", t);
+                e[j] = (unsigned char)(sl * 2 + h);
+            }
+        }
+        tile_ntri[tl] = cnt;
+    }
+
     // one device allocation, 256-byte aligned sub-arrays
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -114,6 +201,10 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
            o_item = take(item.size() * 4);
     size_t o_P = take((size_t)nt * Nq * 8), o_V = take((size_t)nt * Nq * 3 * 8),
            o_tv = take(tv.size() * 8);
+    size_t o_tc = take(tc.size() * 8), o_tu = take(tu.size() * 8), o_tjw = take(tjw.size() * 8),
+           o_hpi = take(hpi.size() * 8), o_trwg = take(tile_rwg.size() * 4), o_pos = take((size_t)N * 4),
+           o_ttri = take(tile_tri.size() * 4), o_tntri = take((size_t)ntile * 4), o_tent = take(tile_ent.size()),
+           o_tflag = take((size_t)ntile), o_rrec = take((size_t)N);
     BEM_TRY_CUDA(ctx, cudaMalloc(&g->dmem, off));
     char* base = (char*)g->dmem;
     double** pts[10] = {&g->half.px, &g->half.py, &g->half.pz, &g->half.fx, &g->half.fy,
@@ -143,6 +234,28 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.item_ptr, item_ptr.data(), item_ptr.size() * 4, cudaMemcpyHostToDevice));
     BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.item, item.data(), item.size() * 4, cudaMemcpyHostToDevice));
     BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.tv, tv.data(), tv.size() * 8, cudaMemcpyHostToDevice));
+    DevTriAsm& ta = g->tri;
+    ta.c = (double*)(base + o_tc);
+    ta.u = (double*)(base + o_tu);
+    ta.jw = (double*)(base + o_tjw);
+    ta.pi = (double*)(base + o_hpi);
+    ta.tile_rwg = (int*)(base + o_trwg);
+    ta.pos = (int*)(base + o_pos);
+    ta.tile_tri = (int*)(base + o_ttri);
+    ta.tile_ntri = (int*)(base + o_tntri);
+    ta.tile_ent = (unsigned char*)(base + o_tent);
+    ta.tile_flag = (unsigned char*)(base + o_tflag);
+    ta.rwg_rec = (unsigned char*)(base + o_rrec);
+    ta.ntile = ntile;
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.c, tc.data(), tc.size() * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.u, tu.data(), tu.size() * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.jw, tjw.data(), tjw.size() * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.pi, hpi.data(), hpi.size() * 8, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_rwg, tile_rwg.data(), tile_rwg.size() * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.pos, pos.data(), (size_t)N * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_tri, tile_tri.data(), tile_tri.size() * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_ntri, tile_ntri.data(), (size_t)ntile * 4, cudaMemcpyHostToDevice));
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_ent, tile_ent.data(), tile_ent.size(), cudaMemcpyHostToDevice));
     // half coefficient and free vertex live right after div (see fixup kernel)
     (void)d_coef;
     (void)d_fr;
@@ -284,9 +397,16 @@ struct AsmArgs {
     double2* L;      // row-major N x N (nmed == 1, Z null)
     double2* K;
     int64_t ld;
-    // optional: only tiles whose row or column band is flagged are computed
-    const unsigned char* band;
+    // optional: only tile pairs with a flagged row or column tile are computed
+    const unsigned char* tile_flag;
+    const double* coef;  // (2N) sign*l/(2A) per half (triangle-pair kernel)
 };
+
+// e^-x for x >= 0.  Below 2^-54 the correctly rounded value is exactly 1;
+// the literal G_smooth at coincident points (R_s = 1e-15) subtracts
+// 1/(4 pi R_s) from e^-x cos(k R_s)/(4 pi R_s), so one unit in the last
+// place of e^-x there would become 0.0156 in G.
+__device__ __forceinline__ double exp_decay(double x) { return x < 5.551115123125783e-17 ? 1.0 : exp(-x); }
 
 // G_smooth = (exp(ikR) - 1)/(4 pi R) without cancellation (limit ik/(4 pi)).
 __device__ __forceinline__ cplx g_smooth_exact(Medium k, double R) {
@@ -314,7 +434,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
 
     const int N = a.N, Nq = a.Nq;
     const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
-    if (a.band && !a.band[bi] && !a.band[bj]) return;  // a tile the caller keeps
+    if (a.tile_flag && !a.tile_flag[bi] && !a.tile_flag[bj]) return;  // a tile the caller keeps
     const int m0 = bi * TILE, n0 = bj * TILE;
 
     // source data of the tile's columns: [half][q][col]
@@ -374,7 +494,10 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
                     double R = sqrt(dx * dx + dy * dy + dz * dz);
                     double Rs = fmax(R, 1e-15);
                     double invR = 1.0 / Rs;
-                    double i4R = INV4PI_D * invR;
+                    // rounded on its own: the literal G_smooth subtracts it
+                    // from G, and a multiply-add fused across the two would
+                    // leave its rounding error (~0.01 at R_s = 1e-15)
+                    double i4R = __dmul_rn(INV4PI_D, invR);
                     double jwp = tjw * s_jw[sh][qs][tx];
                     double fdot = tfx * s_fx[sh][qs][tx] + tfy * s_fy[sh][qs][tx] + tfz * s_fz[sh][qs][tx];
                     // f_t . ((r_t - r_s) x f_s) = (f_t x r_t).f_s + f_t.(f_s x r_s)
@@ -386,7 +509,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
                         const Medium k = a.med[e];
                         double s, c;
                         sincos(k.kr * Rs, &s, &c);
-                        double ea = (k.ki != 0.0) ? exp(-k.ki * Rs) : 1.0;
+                        double ea = (k.ki != 0.0) ? exp_decay(k.ki * Rs) : 1.0;
                         cplx G = {ea * c * i4R, ea * s * i4R};
                         cplx Gu = G;
                         if (sing) {
@@ -467,6 +590,267 @@ __global__ void __launch_bounds__(256) assemble_kernel(AsmArgs a) {
     }
 }
 
+
+// ------------------------------------------------- triangle-pair assembly
+// The same quadrature sums as assemble_kernel, organised by triangle pairs:
+// every RWG half on triangle a paired with every half on triangle b uses the
+// same 7 x 7 Green's function values, so each (a, b) of a tile pair computes
+// them once and keeps moments in coordinates relative to the centroids
+// (u = r - c_a, v = r' - c_b, D = c_a - c_b, d = r - r' = D + u - v):
+//   L: M0 = sum G, Mu = sum G u, Mv = sum G v, Muv = sum G u.v
+//   K: S0 = sum g, A = sum g u, B = sum g v, C = sum g u x v, from which
+//      (D being constant over the pair) P1 = sum g u.(D x v) = -D.C,
+//      Q2 = sum g (u x D - u x v) = A x D - C, Q3 = sum g (D x v + u x v)
+//      = D x B + C and Q4 = sum g d = D S0 + A - B
+// (G, g with the weights jw jw').  With f_m = s_m (r - p_m) = s_m (u - pi_m),
+// f_n = s_n (v - nu_n):
+//   sum G f_m.f_n  = s_m s_n (Muv - pi.Mv - nu.Mu + pi.nu M0)
+//   sum g f_m.(d x f_n) = s_m s_n (P1 - nu.Q2 - pi.Q3 + pi.(Q4 x nu))
+// Each (RWG pair, half pair) term lands in its own shared-memory slot and the
+// four half pairs of an entry are summed in a fixed order, so the result does
+// not depend on the tiling.  RWGs are tiled in the Morton order of their
+// triangles (geom_upload), ~17 distinct triangles per 16 RWGs: ~3.5x fewer
+// Green's function evaluations than per RWG pair.
+constexpr size_t tri_smem_bytes(int nmed) {
+    return (size_t)2 * nmed * 1024 * sizeof(double2) +
+           sizeof(double) * (2 * ASM_TRI_MAX * 3 + 2 * ASM_TRI_MAX * MAXQ * 3 + 2 * ASM_TRI_MAX * MAXQ +
+                             2 * TILE * 2 * 5) +
+           sizeof(int) * (2 * ASM_TRI_MAX + 2) + 2 * ASM_TRI_MAX * 3;
+}
+
+template <int NMED>
+__global__ void __launch_bounds__(256, 2) assemble_tri_kernel(AsmArgs a, DevTriAsm ta) {
+    int64_t lin = blockIdx.x;
+    const int T = a.ntile;
+    int bi = (int)floor((2.0 * T + 1.0 - sqrt((2.0 * T + 1.0) * (2.0 * T + 1.0) - 8.0 * (double)lin)) * 0.5);
+    if (bi < 0) bi = 0;
+    while (bi > 0 && (int64_t)bi * T - (int64_t)bi * (bi - 1) / 2 > lin) bi--;
+    while ((int64_t)(bi + 1) * T - (int64_t)(bi + 1) * bi / 2 <= lin) bi++;
+    const int bj = bi + (int)(lin - ((int64_t)bi * T - (int64_t)bi * (bi - 1) / 2));
+    if (a.tile_flag && !a.tile_flag[bi] && !a.tile_flag[bj]) return;  // a tile the caller keeps
+    const int N = a.N, Nq = a.Nq, tid = threadIdx.x;
+
+    extern __shared__ __align__(16) unsigned char tri_smem[];
+    double2* sL = reinterpret_cast<double2*>(tri_smem);  // [NMED][256 entries][4 half pairs]
+    double2* sK = sL + NMED * 1024;
+    double* sc = reinterpret_cast<double*>(sK + NMED * 1024);  // [2][TRI_MAX][3]
+    double* su = sc + 2 * ASM_TRI_MAX * 3;                      // [2][TRI_MAX][MAXQ][3]
+    double* sjw = su + 2 * ASM_TRI_MAX * MAXQ * 3;              // [2][TRI_MAX][MAXQ]
+    double* ssig = sjw + 2 * ASM_TRI_MAX * MAXQ;                // [2][TILE][2]
+    double* sdiv = ssig + 2 * TILE * 2;                         // [2][TILE][2]
+    double* spi = sdiv + 2 * TILE * 2;                          // [2][TILE][2][3]
+    int* stri = reinterpret_cast<int*>(spi + 2 * TILE * 2 * 3);  // [2][TRI_MAX]
+    int* sntri = stri + 2 * ASM_TRI_MAX;                         // [2]
+    unsigned char* sent = reinterpret_cast<unsigned char*>(sntri + 2);  // [2][TRI_MAX][3]
+
+    for (int i = tid; i < 2 * ASM_TRI_MAX; i += blockDim.x) {
+        const int side = i / ASM_TRI_MAX, li = i % ASM_TRI_MAX;
+        const int t = ta.tile_tri[(size_t)(side ? bj : bi) * ASM_TRI_MAX + li];
+        stri[i] = t;
+        for (int j = 0; j < 3; j++) sc[i * 3 + j] = t >= 0 ? ta.c[(size_t)t * 3 + j] : 0.0;
+    }
+    for (int i = tid; i < 2 * ASM_TRI_MAX * Nq; i += blockDim.x) {
+        const int q = i % Nq, sl = i / Nq;  // sl = side * TRI_MAX + li
+        const int t = ta.tile_tri[(size_t)(sl >= ASM_TRI_MAX ? bj : bi) * ASM_TRI_MAX + sl % ASM_TRI_MAX];
+        for (int j = 0; j < 3; j++) su[(sl * MAXQ + q) * 3 + j] = t >= 0 ? ta.u[((size_t)t * Nq + q) * 3 + j] : 0.0;
+        sjw[sl * MAXQ + q] = t >= 0 ? ta.jw[(size_t)t * Nq + q] : 0.0;
+    }
+    for (int i = tid; i < 2 * ASM_TRI_MAX * 3; i += blockDim.x) {
+        const int side = i / (ASM_TRI_MAX * 3);
+        sent[i] = ta.tile_ent[(size_t)(side ? bj : bi) * ASM_TRI_MAX * 3 + i % (ASM_TRI_MAX * 3)];
+    }
+    for (int i = tid; i < 2 * TILE * 2; i += blockDim.x) {
+        const int side = i / (TILE * 2), slot = (i / 2) % TILE, h = i % 2;
+        const int n = ta.tile_rwg[(size_t)(side ? bj : bi) * TILE + slot];
+        const int hn = h * N + (n >= 0 ? n : 0);
+        ssig[i] = n >= 0 ? a.coef[hn] : 0.0;
+        sdiv[i] = n >= 0 ? a.h.div[hn] : 0.0;
+        for (int j = 0; j < 3; j++) spi[i * 3 + j] = n >= 0 ? ta.pi[(size_t)hn * 3 + j] : 0.0;
+    }
+    if (tid < 2) sntri[tid] = ta.tile_ntri[tid ? bj : bi];
+    __syncthreads();
+
+    const int na = sntri[0], nb = sntri[1];
+    const bool exact = (a.flags & BEM_ASM_GSMOOTH_EXACT) != 0;
+    const int items = na * nb * NMED;
+    for (int it = tid; it < items; it += blockDim.x) {
+        // medium-major: the lanes of a warp take the same branches (the
+        // exterior medium is lossless, the interior one takes exp)
+        const int e = it / (na * nb), pr = it % (na * nb), ia = pr / nb, ib = ASM_TRI_MAX + pr % nb;
+        const bool same = stri[ia] == stri[ib];
+        const Medium k = a.med[e];
+        const double Dx = sc[ia * 3] - sc[ib * 3], Dy = sc[ia * 3 + 1] - sc[ib * 3 + 1],
+                     Dz = sc[ia * 3 + 2] - sc[ib * 3 + 2];
+        cplx M0 = {0, 0}, Muv = {0, 0}, S0 = {0, 0};
+        cplx Mu[3], Mv[3], A[3], B[3], C[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) Mu[j] = Mv[j] = A[j] = B[j] = C[j] = {0, 0};
+        for (int qa = 0; qa < Nq; qa++) {
+            const double* up = &su[(ia * MAXQ + qa) * 3];
+            const double ux = up[0], uy = up[1], uz = up[2], wa = sjw[ia * MAXQ + qa];
+            for (int qb = 0; qb < Nq; qb++) {
+                const double* vp = &su[(ib * MAXQ + qb) * 3];
+                const double vx = vp[0], vy = vp[1], vz = vp[2], w = wa * sjw[ib * MAXQ + qb];
+                const double dx = Dx + (ux - vx), dy = Dy + (uy - vy), dz = Dz + (uz - vz);
+                const double R = sqrt(dx * dx + dy * dy + dz * dz);
+                const double Rs = fmax(R, 1e-15), invR = 1.0 / Rs;
+                const double i4R = __dmul_rn(INV4PI_D, invR);  // rounded alone, as in assemble_kernel
+                double sn, cs;
+                sincos(k.kr * Rs, &sn, &cs);
+                const double ea = (k.ki != 0.0) ? exp_decay(k.ki * Rs) : 1.0;
+                const cplx G = {ea * cs * i4R, ea * sn * i4R};
+                cplx Gu = G;
+                if (same) {
+                    if (exact) Gu = g_smooth_exact(k, R);
+                    else Gu.re -= i4R;
+                }
+                const cplx Gj = {Gu.re * w, Gu.im * w};
+                const double uv = ux * vx + uy * vy + uz * vz;
+                M0.re += Gj.re, M0.im += Gj.im;
+                Muv.re += Gj.re * uv, Muv.im += Gj.im * uv;
+                Mu[0].re += Gj.re * ux, Mu[0].im += Gj.im * ux;
+                Mu[1].re += Gj.re * uy, Mu[1].im += Gj.im * uy;
+                Mu[2].re += Gj.re * uz, Mu[2].im += Gj.im * uz;
+                Mv[0].re += Gj.re * vx, Mv[0].im += Gj.im * vx;
+                Mv[1].re += Gj.re * vy, Mv[1].im += Gj.im * vy;
+                Mv[2].re += Gj.re * vz, Mv[2].im += Gj.im * vz;
+                if (!same && R > 1e-12) {
+                    const cplx gc = cmul(G, cplx{(-k.ki - invR) * invR, k.kr * invR});
+                    const cplx gw = {gc.re * w, gc.im * w};
+                    const double uu[3] = {ux, uy, uz}, vv[3] = {vx, vy, vz};
+                    const double cr[3] = {uy * vz - uz * vy, uz * vx - ux * vz, ux * vy - uy * vx};
+                    S0.re += gw.re, S0.im += gw.im;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        A[j].re += gw.re * uu[j], A[j].im += gw.im * uu[j];
+                        B[j].re += gw.re * vv[j], B[j].im += gw.im * vv[j];
+                        C[j].re += gw.re * cr[j], C[j].im += gw.im * cr[j];
+                    }
+                }
+            }
+        }
+        // P1 = -D.C, Q2 = A x D - C, Q3 = D x B + C, Q4 = D S0 + A - B
+        const double DD[3] = {Dx, Dy, Dz};
+        cplx P1 = {0, 0}, Q2[3], Q3[3], Q4[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            P1.re -= DD[j] * C[j].re, P1.im -= DD[j] * C[j].im;
+            Q2[j] = {A[j1].re * DD[j2] - A[j2].re * DD[j1] - C[j].re, A[j1].im * DD[j2] - A[j2].im * DD[j1] - C[j].im};
+            Q3[j] = {DD[j1] * B[j2].re - DD[j2] * B[j1].re + C[j].re, DD[j1] * B[j2].im - DD[j2] * B[j1].im + C[j].im};
+            Q4[j] = {DD[j] * S0.re + A[j].re - B[j].re, DD[j] * S0.im + A[j].im - B[j].im};
+        }
+        const cplx ik = {-k.ki, k.kr};
+        const double k2 = k.kr * k.kr + k.ki * k.ki;
+        const cplx iok = {k.ki / k2, k.kr / k2};  // i/k
+        for (int x = 0; x < 3; x++) {
+            const int er = sent[ia * 3 + x];
+            if (er == 0xff) break;
+            const int r = er >> 1, hr = er & 1;
+            const double sr = ssig[(r)*2 + hr], dr = sdiv[(r)*2 + hr];
+            const double* pp = &spi[((r)*2 + hr) * 3];
+            for (int y = 0; y < 3; y++) {
+                const int ec = sent[ib * 3 + y];
+                if (ec == 0xff) break;
+                const int c = ec >> 1, hc = ec & 1;
+                const double scn = ssig[(TILE + c) * 2 + hc], dc = sdiv[(TILE + c) * 2 + hc];
+                const double* nn = &spi[((TILE + c) * 2 + hc) * 3];
+                const double ss = sr * scn, pn = pp[0] * nn[0] + pp[1] * nn[1] + pp[2] * nn[2];
+                cplx lv = {Muv.re + pn * M0.re, Muv.im + pn * M0.im};
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    lv.re -= pp[j] * Mv[j].re + nn[j] * Mu[j].re;
+                    lv.im -= pp[j] * Mv[j].im + nn[j] * Mu[j].im;
+                }
+                lv.re *= ss, lv.im *= ss;
+                const double dd = dr * dc;
+                const cplx ls = {dd * M0.re, dd * M0.im};
+                const cplx t1 = cmul(ik, lv), t2 = cmul(iok, ls);
+                cplx kv = P1;
+                // pi . (Q4 x nu)
+                const cplx qx[3] = {{Q4[1].re * nn[2] - Q4[2].re * nn[1], Q4[1].im * nn[2] - Q4[2].im * nn[1]},
+                                    {Q4[2].re * nn[0] - Q4[0].re * nn[2], Q4[2].im * nn[0] - Q4[0].im * nn[2]},
+                                    {Q4[0].re * nn[1] - Q4[1].re * nn[0], Q4[0].im * nn[1] - Q4[1].im * nn[0]}};
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    kv.re += pp[j] * qx[j].re - nn[j] * Q2[j].re - pp[j] * Q3[j].re;
+                    kv.im += pp[j] * qx[j].im - nn[j] * Q2[j].im - pp[j] * Q3[j].im;
+                }
+                const int slot = (r * TILE + c) * 4 + hr * 2 + hc;
+                sL[e * 1024 + slot] = make_double2(t1.re - t2.re, t1.im - t2.im);
+                sK[e * 1024 + slot] = make_double2(ss * kv.re, ss * kv.im);
+            }
+        }
+    }
+    __syncthreads();
+
+    const int r = tid / TILE, c = tid % TILE;
+    const int mm = ta.tile_rwg[(size_t)bi * TILE + r], n = ta.tile_rwg[(size_t)bj * TILE + c];
+    if (mm < 0 || n < 0) return;
+    if (bi == bj && c < r) return;  // diagonal tile pair: the upper entry writes both positions
+    cplx Lf[NMED], Kk[NMED];
+#pragma unroll
+    for (int e = 0; e < NMED; e++) {
+        const double2* l = &sL[e * 1024 + (r * TILE + c) * 4];
+        const double2* kk = &sK[e * 1024 + (r * TILE + c) * 4];
+        Lf[e] = {((l[0].x + l[1].x) + l[2].x) + l[3].x, ((l[0].y + l[1].y) + l[2].y) + l[3].y};
+        Kk[e] = {((kk[0].x + kk[1].x) + kk[2].x) + kk[3].x, ((kk[0].y + kk[1].y) + kk[2].y) + kk[3].y};
+    }
+    const bool mirror = (n != mm);
+    if (a.Z) {
+        cplx TL, BR, Ks;
+        if constexpr (NMED == 2) {
+            TL = {a.eta_e * Lf[0].re + a.eta_i * Lf[1].re, a.eta_e * Lf[0].im + a.eta_i * Lf[1].im};
+            BR = {Lf[0].re / a.eta_e + Lf[1].re / a.eta_i, Lf[0].im / a.eta_e + Lf[1].im / a.eta_i};
+            Ks = {Kk[0].re + Kk[1].re, Kk[0].im + Kk[1].im};
+        } else {
+            TL = {a.eta_e * Lf[0].re, a.eta_e * Lf[0].im};
+            BR = {Lf[0].re / a.eta_e, Lf[0].im / a.eta_e};
+            Ks = Kk[0];
+        }
+        double2* Z = a.Z;
+        const int64_t ld = a.ldz;
+        Z[(int64_t)mm * ld + n] = make_double2(TL.re, TL.im);
+        Z[(int64_t)mm * ld + N + n] = make_double2(-Ks.re, -Ks.im);
+        Z[(int64_t)(N + mm) * ld + n] = make_double2(Ks.re, Ks.im);
+        Z[(int64_t)(N + mm) * ld + N + n] = make_double2(BR.re, BR.im);
+        if (mirror) {
+            Z[(int64_t)n * ld + mm] = make_double2(TL.re, TL.im);
+            Z[(int64_t)n * ld + N + mm] = make_double2(-Ks.re, -Ks.im);
+            Z[(int64_t)(N + n) * ld + mm] = make_double2(Ks.re, Ks.im);
+            Z[(int64_t)(N + n) * ld + N + mm] = make_double2(BR.re, BR.im);
+        }
+    } else {
+        a.L[(int64_t)mm * a.ld + n] = make_double2(Lf[0].re, Lf[0].im);
+        a.K[(int64_t)mm * a.ld + n] = make_double2(Kk[0].re, Kk[0].im);
+        if (mirror) {
+            a.L[(int64_t)n * a.ld + mm] = make_double2(Lf[0].re, Lf[0].im);
+            a.K[(int64_t)n * a.ld + mm] = make_double2(Kk[0].re, Kk[0].im);
+        }
+    }
+}
+
+// Tiles to recompute from an RWG mask (tile_rwg null: tiles of 16
+// consecutive RWGs), and per RWG whether its tile is recomputed.
+__global__ void mask_tiles_kernel(const unsigned char* __restrict__ mask, const int* __restrict__ tile_rwg, int N,
+                                  int ntile, unsigned char* __restrict__ flag) {
+    const int tl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tl >= ntile) return;
+    unsigned char f = 0;
+    for (int sl = 0; sl < TILE; sl++) {
+        const int n = tile_rwg ? tile_rwg[(size_t)tl * TILE + sl] : tl * TILE + sl;
+        if (n >= 0 && n < N && mask[n]) f = 1;
+    }
+    flag[tl] = f;
+}
+
+__global__ void mask_rec_kernel(const unsigned char* __restrict__ flag, const int* __restrict__ pos, int N,
+                                unsigned char* __restrict__ rec) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    rec[n] = flag[(pos ? pos[n] : n) / TILE];
+}
+
 // ------------------------------------------------------------ singular fixup
 struct FixArgs {
     DevHalf h;
@@ -480,7 +864,7 @@ struct FixArgs {
     int64_t ldz;
     double2* L;
     int64_t ld;
-    const unsigned char* band;  // as AsmArgs::band (bands of TILE RWGs)
+    const unsigned char* rec;   // optional: RWGs whose assembly tiles were recomputed
 };
 
 // One thread per unordered RWG pair {m, n} sharing a triangle.  For every
@@ -494,7 +878,7 @@ __global__ void singular_fixup_kernel(FixArgs a) {
     if (p >= a.s.npairs) return;
     const int N = a.N, Nq = a.Nq;
     int m = a.s.pair_mn[2 * p], n = a.s.pair_mn[2 * p + 1];
-    if (a.band && !a.band[m / TILE] && !a.band[n / TILE]) return;
+    if (a.rec && !a.rec[m] && !a.rec[n]) return;
     double SA = 0.0, SB = 0.0;
     for (int it = a.s.item_ptr[p]; it < a.s.item_ptr[p + 1]; it++) {
         int t = a.s.item[3 * it], ha = a.s.item[3 * it + 1], hb = a.s.item[3 * it + 2];
@@ -561,7 +945,7 @@ __global__ void singular_fixup_kernel(FixArgs a) {
 // exterior-only PMCHWT A_ext of medium 0 into Z.
 int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
                  double ki_im, double eta_e, double eta_i, unsigned flags, int mode, void* Z,
-                 int64_t ldz, void* L, void* K, const unsigned char* band) {
+                 int64_t ldz, void* L, void* K, const unsigned char* rwg_mask) {
     const int N = g->N;
     if (N < 1) return fail(ctx, BEM_ERR_INVALID, "empty basis");
     if ((mode == 2 || mode == 3) && (!Z || ldz < 2 * N)) return fail(ctx, BEM_ERR_INVALID, "bad Z / ldz");
@@ -596,14 +980,45 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
     a.L = (double2*)L;
     a.K = (double2*)K;
     a.ld = ldz;
-    a.band = band;
+    a.coef = g->sing_coef;
+    a.tile_flag = nullptr;
+    const bool tri = ctx->asm_kernel == 0;
+    const unsigned char* rec = nullptr;
+    if (rwg_mask) {
+        // tiles holding a flagged RWG, and the RWGs of those tiles
+        mask_tiles_kernel<<<(a.ntile + 127) / 128, 128, 0, st>>>(rwg_mask, tri ? g->tri.tile_rwg : nullptr, N,
+                                                                 a.ntile, g->tri.tile_flag);
+        BEM_LAUNCHED(ctx);
+        mask_rec_kernel<<<(N + 255) / 256, 256, 0, st>>>(g->tri.tile_flag, tri ? g->tri.pos : nullptr, N,
+                                                         g->tri.rwg_rec);
+        BEM_LAUNCHED(ctx);
+        a.tile_flag = g->tri.tile_flag;
+        rec = g->tri.rwg_rec;
+    }
     int64_t ntiles = (int64_t)a.ntile * (a.ntile + 1) / 2;
     if (ntiles > 0x7fffffffLL) return fail(ctx, BEM_ERR_INVALID, "too many tiles");
+    if (g->Nq > MAXQ) return fail(ctx, BEM_ERR_INVALID, "quadrature of %d points (at most %d)", g->Nq, MAXQ);
     cudaEvent_t ev = ctx->prof_begin(PROF_ASSEMBLY);
-    if (mode == 2)
+    if (tri) {
+        // dynamic shared memory beyond 48 KB: set once per device
+        static unsigned attr_done = 0;
+        const unsigned bit = 1u << (ctx->device & 31);
+        if (!(__atomic_load_n(&attr_done, __ATOMIC_ACQUIRE) & bit)) {
+            BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(assemble_tri_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)tri_smem_bytes(2)));
+            BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(assemble_tri_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)tri_smem_bytes(1)));
+            __atomic_fetch_or(&attr_done, bit, __ATOMIC_RELEASE);
+        }
+        if (mode == 2)
+            assemble_tri_kernel<2><<<(unsigned)ntiles, 256, tri_smem_bytes(2), st>>>(a, g->tri);
+        else
+            assemble_tri_kernel<1><<<(unsigned)ntiles, 256, tri_smem_bytes(1), st>>>(a, g->tri);
+    } else if (mode == 2) {
         assemble_kernel<2><<<(unsigned)ntiles, 256, 0, st>>>(a);
-    else
+    } else {
         assemble_kernel<1><<<(unsigned)ntiles, 256, 0, st>>>(a);
+    }
     BEM_LAUNCHED(ctx);
     // algorithmic unit: one quadrature-pair evaluation per medium, every
     // ordered RWG pair (no symmetry credit): 64 flop + sincos + exp each
@@ -628,7 +1043,7 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
         f.ldz = ldz;
         f.L = (double2*)L;
         f.ld = ldz;
-        f.band = band;
+        f.rec = rec;
         singular_fixup_kernel<<<(g->sing.npairs + 127) / 128, 128, 0, st>>>(f);
         BEM_LAUNCHED(ctx);
     }

@@ -118,6 +118,25 @@ void* devmem_alloc(int device, size_t bytes);  // nullptr when out of memory
 void devmem_free(int device, void* p, size_t bytes);
 void devmem_cache_enable(int device, bool on);
 
+// Triangle-pair assembly: per-triangle quadrature data relative to the
+// centroid, and the RWGs in tiles of ASM_TILE ordered along a Morton curve of
+// their triangles' centroids, so that the RWGs of a tile share triangles.
+constexpr int ASM_TRI_MAX = 32;  // distinct triangles of one tile (2 halves x 16 RWGs at most)
+struct DevTriAsm {
+    double* c = nullptr;          // (nt, 3) centroids
+    double* u = nullptr;          // (nt, Nq, 3) quadrature points minus the centroid
+    double* jw = nullptr;         // (nt, Nq) area x weight
+    double* pi = nullptr;         // (2N, 3) free vertex of half h*N+n minus its triangle's centroid
+    int* tile_rwg = nullptr;      // (ntile, 16) RWG of each tile slot, -1 past N
+    int* pos = nullptr;           // (N) slot of each RWG: tile = pos / 16
+    int* tile_tri = nullptr;      // (ntile, ASM_TRI_MAX) distinct triangles of the tile, -1 padded
+    int* tile_ntri = nullptr;     // (ntile)
+    unsigned char* tile_ent = nullptr;  // (ntile, ASM_TRI_MAX, 3): slot * 2 + half on the triangle, 0xff none
+    unsigned char* tile_flag = nullptr; // (ntile) scratch: tiles to recompute
+    unsigned char* rwg_rec = nullptr;   // (N) scratch: RWGs whose tile is recomputed
+    int ntile = 0;
+};
+
 }  // namespace bem
 
 // Per-kernel-class timing (CUDA events around the launches of one class on
@@ -144,6 +163,7 @@ struct bem_ctx {
     float* tc_buf = nullptr;  // packed hi/lo operands of the tensor-core GEMM
     size_t tc_bytes = 0;
     bool tc_attr = false;
+    int asm_kernel = 0;          // assembly: 0 triangle-pair moments (Morton tiles), 1 per RWG pair
     int tc_group_m = 16;         // row tiles per raster group of the persistent tensor-core GEMM
     bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)
     int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)
@@ -190,16 +210,19 @@ struct bem_geom {
     bem::DevSingular sing{};
     double* sing_coef = nullptr;  // (2N) sign*l/(2A) per half
     double* sing_free = nullptr;  // (3*2N) free vertex per half, x | y | z blocks
+    bem::DevTriAsm tri{};         // triangle-pair assembly data (Morton-ordered tiles)
     void* dmem = nullptr;  // one allocation backing every device array
 };
 
 namespace bem {
 // assembly.cu
-// band (device, optional): one flag per band of 16 RWGs; only the tiles of
-// flagged row or column bands are written (the others keep their values).
+// rwg_mask (device, optional): one flag per RWG; only the tiles holding a
+// flagged RWG in their rows or columns are written (every entry of a flagged
+// RWG among them; the other tiles keep their values, and entries recomputed
+// without a flagged RWG come out bitwise as before).
 int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, double ki_re,
                  double ki_im, double eta_e, double eta_i, unsigned flags, int mode,
-                 void* Z, int64_t ldz, void* L, void* K, const unsigned char* band = nullptr);
+                 void* Z, int64_t ldz, void* L, void* K, const unsigned char* rwg_mask = nullptr);
 constexpr int ASM_TILE = 16;  // RWGs per assembly band
 int geom_upload(bem_ctx* ctx, bem_geom* g);
 // rhs / farfield

@@ -340,26 +340,25 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
             return fail(ctx, BEM_ERR_OOM, "gradient buffers");
         }
         const std::complex<double> ki = kext * m;
-        // RWGs around each vertex (the RWGs of its triangles) -> bands of ASM_TILE
-        const int nband = (N + ASM_TILE - 1) / ASM_TILE;
-        std::vector<std::vector<int>> vbands(p->nv);
+        // RWGs around each vertex (the RWGs with a triangle on it): the
+        // entries the vertex moves; assembly recomputes only their tiles
+        std::vector<std::vector<int>> vrwg(p->nv);
         for (int mm = 0; mm < N; mm++)
             for (int tri : {g->rwg.tri_p[mm], g->rwg.tri_m[mm]})
                 for (int k = 0; k < 3; k++) {
-                    auto& vb = vbands[p->tris[3 * tri + k]];
-                    const int b = mm / ASM_TILE;
-                    if (std::find(vb.begin(), vb.end(), b) == vb.end()) vb.push_back(b);
+                    auto& vr = vrwg[p->tris[3 * tri + k]];
+                    if (vr.empty() || vr.back() != mm) vr.push_back(mm);
                 }
-        DevMem dBand;
-        if (cudaMalloc(&dBand.p, nband) != cudaSuccess) {
+        DevMem dMask;
+        if (cudaMalloc(&dMask.p, N) != cudaSuccess) {
             cudaGetLastError();
             return fail(ctx, BEM_ERR_OOM, "gradient buffers");
         }
-        std::vector<unsigned char> band(nband);
+        std::vector<unsigned char> mask(N);
         for (int iv = 0; iv < p->nv; iv++) {
-            std::fill(band.begin(), band.end(), 0);
-            for (int b : vbands[iv]) band[b] = 1;
-            BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dBand.p, band.data(), nband, cudaMemcpyHostToDevice, ctx->stream));
+            std::fill(mask.begin(), mask.end(), 0);
+            for (int mm : vrwg[iv]) mask[mm] = 1;
+            BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dMask.p, mask.data(), N, cudaMemcpyHostToDevice, ctx->stream));
             for (int comp = 0; comp < 3; comp++) {
                 const double v0 = vp[3 * iv + comp];
                 double lpm[2] = {0, 0};
@@ -378,7 +377,7 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
                     if (st == BEM_OK)
                         st = assemble_dev(ctx, gs, kext.real(), kext.imag(), ki.real(), ki.imag(), eta_e,
                                           1.0 / std::abs(m), p->asm_flags, 2, Zs[sgn], n, nullptr, nullptr,
-                                          (const unsigned char*)dBand.p);
+                                          (const unsigned char*)dMask.p);
                     if (st == BEM_OK)
                         st = rhs_dev(ctx, gs, kext.real(), kext.imag(), eta_e, RT.data(), nullptr, nullptr, no,
                                      Bs[sgn], n);
