@@ -156,6 +156,15 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
         for (int t = 0; t < nt; t++) torder[t] = t;
         std::stable_sort(torder.begin(), torder.end(), [&](int x, int y) { return key[x] < key[y]; });
     }
+    std::vector<int> tri_half(3 * (size_t)nt, -1);
+    for (int h = 0; h < 2; h++)
+        for (int n = 0; n < N; n++) {
+            const int t = h == 0 ? r.tri_p[n] : r.tri_m[n];
+            int j = 0;
+            while (j < 3 && tri_half[3 * (size_t)t + j] >= 0) j++;
+            if (j == 3) return fail(ctx, BEM_ERR_INVALID, "triangle %d carries more than 3 RWG halves", t);
+            tri_half[3 * (size_t)t + j] = h * N + n;
+        }
     std::vector<std::vector<int>> rwg_of_tri(nt);
     for (int n = 0; n < N; n++) rwg_of_tri[r.tri_p[n]].push_back(n), rwg_of_tri[r.tri_m[n]].push_back(n);
     const int ntile = (N + ASM_TILE - 1) / ASM_TILE;
@@ -204,7 +213,7 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     size_t o_tc = take(tc.size() * 8), o_tu = take(tu.size() * 8), o_tjw = take(tjw.size() * 8),
            o_hpi = take(hpi.size() * 8), o_trwg = take(tile_rwg.size() * 4), o_pos = take((size_t)N * 4),
            o_ttri = take(tile_tri.size() * 4), o_tntri = take((size_t)ntile * 4), o_tent = take(tile_ent.size()),
-           o_tflag = take((size_t)ntile), o_rrec = take((size_t)N);
+           o_tflag = take((size_t)ntile), o_rrec = take((size_t)N), o_thalf = take(tri_half.size() * 4);
     BEM_TRY_CUDA(ctx, cudaMalloc(&g->dmem, off));
     char* base = (char*)g->dmem;
     double** pts[10] = {&g->half.px, &g->half.py, &g->half.pz, &g->half.fx, &g->half.fy,
@@ -247,6 +256,8 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     ta.tile_flag = (unsigned char*)(base + o_tflag);
     ta.rwg_rec = (unsigned char*)(base + o_rrec);
     ta.ntile = ntile;
+    ta.tri_half = (int*)(base + o_thalf);
+    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tri_half, tri_half.data(), tri_half.size() * 4, cudaMemcpyHostToDevice));
     BEM_TRY_CUDA(ctx, cudaMemcpy(ta.c, tc.data(), tc.size() * 8, cudaMemcpyHostToDevice));
     BEM_TRY_CUDA(ctx, cudaMemcpy(ta.u, tu.data(), tu.size() * 8, cudaMemcpyHostToDevice));
     BEM_TRY_CUDA(ctx, cudaMemcpy(ta.jw, tjw.data(), tjw.size() * 8, cudaMemcpyHostToDevice));

@@ -132,6 +132,7 @@ struct DevTriAsm {
     int* tile_tri = nullptr;      // (ntile, ASM_TRI_MAX) distinct triangles of the tile, -1 padded
     int* tile_ntri = nullptr;     // (ntile)
     unsigned char* tile_ent = nullptr;  // (ntile, ASM_TRI_MAX, 3): slot * 2 + half on the triangle, 0xff none
+    int* tri_half = nullptr;      // (nt, 3) RWG halves h*N+n on each triangle, -1 padded
     unsigned char* tile_flag = nullptr; // (ntile) scratch: tiles to recompute
     unsigned char* rwg_rec = nullptr;   // (N) scratch: RWGs whose tile is recomputed
     int ntile = 0;
@@ -163,6 +164,7 @@ struct bem_ctx {
     float* tc_buf = nullptr;  // packed hi/lo operands of the tensor-core GEMM
     size_t tc_bytes = 0;
     bool tc_attr = false;
+    int ff_kernel = 0;           // far field: 0 by triangles (shared phases), 1 per RWG-half point
     int asm_kernel = 0;          // assembly: 0 triangle-pair moments (Morton tiles), 1 per RWG pair
     int tc_group_m = 16;         // row tiles per raster group of the persistent tensor-core GEMM
     bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)

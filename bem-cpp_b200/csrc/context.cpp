@@ -243,6 +243,9 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
         (name[0] == 'f' ? ctx->factor_sb : ctx->solve_sb) = value;
     } else if (!std::strcmp(name, "cache_factor_memory")) {
         bem::devmem_cache_enable(ctx->device, value != 0);
+    } else if (!std::strcmp(name, "farfield_kernel")) {
+        if (value != 0 && value != 1) return bem::fail(ctx, BEM_ERR_INVALID, "farfield_kernel must be 0 or 1");
+        ctx->ff_kernel = value;
     } else if (!std::strcmp(name, "assembly_kernel")) {
         if (value != 0 && value != 1) return bem::fail(ctx, BEM_ERR_INVALID, "assembly_kernel must be 0 or 1");
         ctx->asm_kernel = value;

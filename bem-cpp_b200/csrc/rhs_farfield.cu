@@ -151,92 +151,10 @@ __device__ __forceinline__ double theta_of(const FFArgs& a, int d) {
     return a.theta ? a.theta[d] : (a.ndir > 1 ? M_PI * d / (a.ndir - 1) : 0.0);
 }
 
-constexpr int FF_LANES = 4;
-constexpr int FF_CHUNK = 256;  // points staged per step
-
-// Block: dpb directions x FF_LANES point lanes; grid (direction chunks, orientations).
-__global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
-    extern __shared__ double sm[];
-    double* s_p = sm;                   // FF_CHUNK * 6 : x y z wfx wfy wfz
-    double2* s_c = (double2*)(sm + FF_CHUNK * 6);  // FF_CHUNK * 4 : cJ0 cM0 cJ1 cM1
-    const int o = blockIdx.y;
-    const int dl = threadIdx.x / FF_LANES, lane = threadIdx.x % FF_LANES;
-    const int d = blockIdx.x * dpb + dl;
-    const bool active = dl < dpb && d < a.ndir;
-    const int c0 = 2 * o, c1 = 2 * o + 1;
-    const bool has1 = c1 < a.n_calls;
-    double r[3] = {0, 0, 1};
-    if (active) {
-        if (a.rhat) {
-            const double* rr = a.rhat + ((size_t)o * a.ndir + d) * 3;
-            r[0] = rr[0], r[1] = rr[1], r[2] = rr[2];
-        } else {
-            double st, ct;
-            sincos(theta_of(a, d), &st, &ct);
-            const double* R = a.RT + 9 * o;
-            for (int i = 0; i < 3; i++) r[i] = R[3 * i] * st + R[3 * i + 2] * ct;
-        }
-    }
-    double acc[12][2];
-    for (int i = 0; i < 12; i++) acc[i][0] = acc[i][1] = 0.0;
-    const int P = 2 * a.N * a.Nq;
-    for (int base = 0; base < P; base += FF_CHUNK) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < FF_CHUNK; e += blockDim.x) {
-            int p = base + e;
-            if (p < P) {
-                double w = a.h.jw[p];
-                s_p[e * 6 + 0] = a.h.px[p];
-                s_p[e * 6 + 1] = a.h.py[p];
-                s_p[e * 6 + 2] = a.h.pz[p];
-                s_p[e * 6 + 3] = a.h.fx[p] * w;
-                s_p[e * 6 + 4] = a.h.fy[p] * w;
-                s_p[e * 6 + 5] = a.h.fz[p] * w;
-                int n = (p / a.Nq) % a.N;
-                s_c[e * 4 + 0] = a.cJ[(int64_t)c0 * a.cs + n];
-                s_c[e * 4 + 1] = a.cM[(int64_t)c0 * a.cs + n];
-                s_c[e * 4 + 2] = has1 ? a.cJ[(int64_t)c1 * a.cs + n] : make_double2(0, 0);
-                s_c[e * 4 + 3] = has1 ? a.cM[(int64_t)c1 * a.cs + n] : make_double2(0, 0);
-            } else {
-                for (int k = 0; k < 6; k++) s_p[e * 6 + k] = 0.0;
-                for (int k = 0; k < 4; k++) s_c[e * 4 + k] = make_double2(0, 0);
-            }
-        }
-        __syncthreads();
-        if (!active) continue;
-        const int lim = min(FF_CHUNK, P - base);
-        for (int e = lane; e < lim; e += FF_LANES) {
-            const double* q = s_p + e * 6;
-            double rd = r[0] * q[0] + r[1] * q[1] + r[2] * q[2];
-            double sn, cs;
-            sincos(a.kr * rd, &sn, &cs);
-            double ea = a.ki != 0.0 ? exp(a.ki * rd) : 1.0;
-            double phr = cs * ea, phi = -sn * ea;  // exp(-i k r.r')
-            const double2* cc = s_c + e * 4;
-            // u_k = c_k exp(-i k r.r') once per coefficient, then the real
-            // weighted basis vector: 40 FP64 operations per point instead of 54
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const double ur = cc[k].x * phr - cc[k].y * phi, ui = cc[k].x * phi + cc[k].y * phr;
-#pragma unroll
-                for (int x = 0; x < 3; x++) {
-                    acc[3 * k + x][0] += q[3 + x] * ur;
-                    acc[3 * k + x][1] += q[3 + x] * ui;
-                }
-            }
-        }
-    }
-    // reduce the FF_LANES lanes of each direction
-    __syncthreads();
-    double* red = sm;  // blockDim.x * 24
-    for (int i = 0; i < 12; i++) {
-        red[threadIdx.x * 24 + 2 * i] = acc[i][0];
-        red[threadIdx.x * 24 + 2 * i + 1] = acc[i][1];
-    }
-    __syncthreads();
-    if (!active || lane != 0) return;
-    for (int l = 1; l < FF_LANES; l++)
-        for (int i = 0; i < 24; i++) (&acc[0][0])[i] += red[(threadIdx.x + l) * 24 + i];
+// Far-field vectors of both polarisations from the accumulated J and M
+// sums, then the S matrix and the weighted Mueller matrix of the direction
+// (main.cpp:785-845, amplitude_to_mueller farfield.cu:464-508).
+__device__ void ff_epilogue(const FFArgs& a, int o, int d, const double* r, double (*acc)[2]) {
     // F = -ik/(4 pi) (eta (J - r (r.J)) - r x M)   (sM = -1)
     const double pfr = a.ki * INV4PI_FF, pfi = -a.kr * INV4PI_FF;
     double F[2][3][2];
@@ -324,6 +242,209 @@ __global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
     }
 }
 
+constexpr int FF_LANES = 4;
+constexpr int FF_CHUNK = 256;  // points staged per step
+
+// Block: dpb directions x FF_LANES point lanes; grid (direction chunks, orientations).
+__global__ void __launch_bounds__(256) farfield_kernel(FFArgs a, int dpb) {
+    extern __shared__ double sm[];
+    double* s_p = sm;                   // FF_CHUNK * 6 : x y z wfx wfy wfz
+    double2* s_c = (double2*)(sm + FF_CHUNK * 6);  // FF_CHUNK * 4 : cJ0 cM0 cJ1 cM1
+    const int o = blockIdx.y;
+    const int dl = threadIdx.x / FF_LANES, lane = threadIdx.x % FF_LANES;
+    const int d = blockIdx.x * dpb + dl;
+    const bool active = dl < dpb && d < a.ndir;
+    const int c0 = 2 * o, c1 = 2 * o + 1;
+    const bool has1 = c1 < a.n_calls;
+    double r[3] = {0, 0, 1};
+    if (active) {
+        if (a.rhat) {
+            const double* rr = a.rhat + ((size_t)o * a.ndir + d) * 3;
+            r[0] = rr[0], r[1] = rr[1], r[2] = rr[2];
+        } else {
+            double st, ct;
+            sincos(theta_of(a, d), &st, &ct);
+            const double* R = a.RT + 9 * o;
+            for (int i = 0; i < 3; i++) r[i] = R[3 * i] * st + R[3 * i + 2] * ct;
+        }
+    }
+    double acc[12][2];
+    for (int i = 0; i < 12; i++) acc[i][0] = acc[i][1] = 0.0;
+    const int P = 2 * a.N * a.Nq;
+    for (int base = 0; base < P; base += FF_CHUNK) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < FF_CHUNK; e += blockDim.x) {
+            int p = base + e;
+            if (p < P) {
+                double w = a.h.jw[p];
+                s_p[e * 6 + 0] = a.h.px[p];
+                s_p[e * 6 + 1] = a.h.py[p];
+                s_p[e * 6 + 2] = a.h.pz[p];
+                s_p[e * 6 + 3] = a.h.fx[p] * w;
+                s_p[e * 6 + 4] = a.h.fy[p] * w;
+                s_p[e * 6 + 5] = a.h.fz[p] * w;
+                int n = (p / a.Nq) % a.N;
+                s_c[e * 4 + 0] = a.cJ[(int64_t)c0 * a.cs + n];
+                s_c[e * 4 + 1] = a.cM[(int64_t)c0 * a.cs + n];
+                s_c[e * 4 + 2] = has1 ? a.cJ[(int64_t)c1 * a.cs + n] : make_double2(0, 0);
+                s_c[e * 4 + 3] = has1 ? a.cM[(int64_t)c1 * a.cs + n] : make_double2(0, 0);
+            } else {
+                for (int k = 0; k < 6; k++) s_p[e * 6 + k] = 0.0;
+                for (int k = 0; k < 4; k++) s_c[e * 4 + k] = make_double2(0, 0);
+            }
+        }
+        __syncthreads();
+        if (!active) continue;
+        const int lim = min(FF_CHUNK, P - base);
+        for (int e = lane; e < lim; e += FF_LANES) {
+            const double* q = s_p + e * 6;
+            double rd = r[0] * q[0] + r[1] * q[1] + r[2] * q[2];
+            double sn, cs;
+            sincos(a.kr * rd, &sn, &cs);
+            double ea = a.ki != 0.0 ? exp(a.ki * rd) : 1.0;
+            double phr = cs * ea, phi = -sn * ea;  // exp(-i k r.r')
+            const double2* cc = s_c + e * 4;
+            // u_k = c_k exp(-i k r.r') once per coefficient, then the real
+            // weighted basis vector: 40 FP64 operations per point instead of 54
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const double ur = cc[k].x * phr - cc[k].y * phi, ui = cc[k].x * phi + cc[k].y * phr;
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                    acc[3 * k + x][0] += q[3 + x] * ur;
+                    acc[3 * k + x][1] += q[3 + x] * ui;
+                }
+            }
+        }
+    }
+    // reduce the FF_LANES lanes of each direction
+    __syncthreads();
+    double* red = sm;  // blockDim.x * 24
+    for (int i = 0; i < 12; i++) {
+        red[threadIdx.x * 24 + 2 * i] = acc[i][0];
+        red[threadIdx.x * 24 + 2 * i + 1] = acc[i][1];
+    }
+    __syncthreads();
+    if (!active || lane != 0) return;
+    for (int l = 1; l < FF_LANES; l++)
+        for (int i = 0; i < 24; i++) (&acc[0][0])[i] += red[(threadIdx.x + l) * 24 + i];
+    ff_epilogue(a, o, d, r, acc);
+}
+
+
+// The same far field by triangles: the phase exp(-ik rhat.r_q) at a
+// triangle's quadrature point is shared by the (up to three) RWG halves on
+// it, whose basis is f_h = s_h (u - pi_h) with u = r - c_t.  Per (direction,
+// triangle): E0 = sum_q ph_q w_q and Eu = sum_q ph_q w_q u_q, then for each
+// coefficient column k the triangle adds alpha_k Eu + gamma_k E0 with
+// alpha_k = sum_h c_kh s_h and gamma_k = -sum_h c_kh s_h pi_h (direction
+// independent, formed once per block and staged chunk).  One sincos per
+// triangle point instead of per RWG-half point, ~4x fewer operations.
+constexpr int FT_CHUNK = 64;  // triangles staged per step
+constexpr int FF_MAXQ = 13;
+
+__global__ void __launch_bounds__(256) farfield_tri_kernel(FFArgs a, DevTriAsm ta, int nt, const double* coef,
+                                                           int dpb) {
+    extern __shared__ double sm[];
+    double* s_c = sm;                                     // FT_CHUNK * 3 centroids
+    double* s_u = s_c + FT_CHUNK * 3;                     // FT_CHUNK * FF_MAXQ * 3
+    double* s_w = s_u + FT_CHUNK * FF_MAXQ * 3;           // FT_CHUNK * FF_MAXQ
+    double2* s_al = (double2*)(s_w + FT_CHUNK * FF_MAXQ);  // FT_CHUNK * 4
+    double2* s_ga = s_al + FT_CHUNK * 4;                  // FT_CHUNK * 4 * 3
+    const int o = blockIdx.y, tid = threadIdx.x;
+    const int dl = tid / FF_LANES, lane = tid % FF_LANES;
+    const int d = blockIdx.x * dpb + dl;
+    const bool active = dl < dpb && d < a.ndir;
+    const int c0 = 2 * o, c1 = 2 * o + 1;
+    const bool has1 = c1 < a.n_calls;
+    const int N = a.N, Nq = a.Nq;
+    double r[3] = {0, 0, 1};
+    if (active) {
+        if (a.rhat) {
+            const double* rr = a.rhat + ((size_t)o * a.ndir + d) * 3;
+            r[0] = rr[0], r[1] = rr[1], r[2] = rr[2];
+        } else {
+            double st, ct;
+            sincos(theta_of(a, d), &st, &ct);
+            const double* R = a.RT + 9 * o;
+            for (int i = 0; i < 3; i++) r[i] = R[3 * i] * st + R[3 * i + 2] * ct;
+        }
+    }
+    double acc[12][2];
+    for (int i = 0; i < 12; i++) acc[i][0] = acc[i][1] = 0.0;
+    for (int t0 = 0; t0 < nt; t0 += FT_CHUNK) {
+        const int cnt = min(FT_CHUNK, nt - t0);
+        __syncthreads();
+        for (int e = tid; e < cnt * 3; e += blockDim.x) s_c[e] = ta.c[(size_t)t0 * 3 + e];
+        for (int e = tid; e < cnt * Nq; e += blockDim.x) {
+            const int tt = e / Nq, q = e % Nq;
+            const size_t src = (size_t)(t0 + tt) * Nq + q;
+            s_w[tt * FF_MAXQ + q] = ta.jw[src];
+            for (int x = 0; x < 3; x++) s_u[(tt * FF_MAXQ + q) * 3 + x] = ta.u[src * 3 + x];
+        }
+        for (int e = tid; e < cnt * 4; e += blockDim.x) {
+            const int tt = e / 4, k = e % 4;  // k: J0 M0 J1 M1
+            const double2* src = (k & 1) ? a.cM : a.cJ;
+            const int col = k < 2 ? c0 : c1;
+            double2 al = make_double2(0, 0), ga[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+            if (k < 2 || has1) {
+                for (int j = 0; j < 3; j++) {
+                    const int hn = ta.tri_half[(size_t)(t0 + tt) * 3 + j];
+                    if (hn < 0) break;
+                    const double2 cc = src[(int64_t)col * a.cs + hn % N];
+                    const double sg = coef[hn];
+                    al.x += cc.x * sg, al.y += cc.y * sg;
+                    for (int x = 0; x < 3; x++) {
+                        const double sp = sg * ta.pi[(size_t)hn * 3 + x];
+                        ga[x].x -= cc.x * sp, ga[x].y -= cc.y * sp;
+                    }
+                }
+            }
+            s_al[tt * 4 + k] = al;
+            for (int x = 0; x < 3; x++) s_ga[(tt * 4 + k) * 3 + x] = ga[x];
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int tt = lane; tt < cnt; tt += FF_LANES) {
+            const double rdc = r[0] * s_c[tt * 3] + r[1] * s_c[tt * 3 + 1] + r[2] * s_c[tt * 3 + 2];
+            double E0r = 0, E0i = 0, Eu[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int q = 0; q < Nq; q++) {
+                const double* u = &s_u[(tt * FF_MAXQ + q) * 3];
+                const double rd = rdc + (r[0] * u[0] + r[1] * u[1] + r[2] * u[2]);
+                double sn, cs;
+                sincos(a.kr * rd, &sn, &cs);
+                const double ea = a.ki != 0.0 ? exp(a.ki * rd) : 1.0;
+                const double w = s_w[tt * FF_MAXQ + q];
+                const double pr = cs * ea * w, pim = -sn * ea * w;  // exp(-i k rhat.r) w
+                E0r += pr, E0i += pim;
+#pragma unroll
+                for (int x = 0; x < 3; x++) Eu[x][0] += pr * u[x], Eu[x][1] += pim * u[x];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const double2 al = s_al[tt * 4 + k];
+#pragma unroll
+                for (int x = 0; x < 3; x++) {
+                    const double2 ga = s_ga[(tt * 4 + k) * 3 + x];
+                    acc[3 * k + x][0] += al.x * Eu[x][0] - al.y * Eu[x][1] + ga.x * E0r - ga.y * E0i;
+                    acc[3 * k + x][1] += al.x * Eu[x][1] + al.y * Eu[x][0] + ga.x * E0i + ga.y * E0r;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    double* red = sm;  // blockDim.x * 24
+    for (int i = 0; i < 12; i++) {
+        red[tid * 24 + 2 * i] = acc[i][0];
+        red[tid * 24 + 2 * i + 1] = acc[i][1];
+    }
+    __syncthreads();
+    if (!active || lane != 0) return;
+    for (int l = 1; l < FF_LANES; l++)
+        for (int i = 0; i < 24; i++) (&acc[0][0])[i] += red[(tid + l) * 24 + i];
+    ff_epilogue(a, o, d, r, acc);
+}
+
 // M_avg[i*ndir + d] = sum over o in order of Mo[o][i][d]
 __global__ void mueller_sum_kernel(const double* __restrict__ Mo, int n_orient, int nel,
                                    double* __restrict__ out) {
@@ -334,16 +455,25 @@ __global__ void mueller_sum_kernel(const double* __restrict__ Mo, int n_orient, 
     out[i] = s;
 }
 
-static int launch_ff(bem_ctx* ctx, FFArgs& a) {
+static int launch_ff(bem_ctx* ctx, const bem_geom* g, FFArgs& a) {
     int nchunk = (a.ndir + 63) / 64;
     int dpb = (a.ndir + nchunk - 1) / nchunk;
     int threads = dpb * FF_LANES;
-    size_t smem = std::max((size_t)FF_CHUNK * (6 * 8 + 4 * 16), (size_t)threads * 24 * 8);
-    BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(farfield_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
     dim3 grid(nchunk, a.n_orient);
     cudaEvent_t ev = ctx->prof_begin(PROF_FARFIELD);
-    farfield_kernel<<<grid, threads, smem, ctx->stream>>>(a, dpb);
+    if (ctx->ff_kernel == 0) {
+        if (g->Nq > FF_MAXQ) return fail(ctx, BEM_ERR_INVALID, "quadrature of %d points (at most %d)", g->Nq, FF_MAXQ);
+        size_t smem = std::max((size_t)FT_CHUNK * (3 + FF_MAXQ * 4) * 8 + (size_t)FT_CHUNK * 16 * 16,
+                               (size_t)threads * 24 * 8);
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(farfield_tri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem));
+        farfield_tri_kernel<<<grid, threads, smem, ctx->stream>>>(a, g->tri, g->nt, g->sing_coef, dpb);
+    } else {
+        size_t smem = std::max((size_t)FF_CHUNK * (6 * 8 + 4 * 16), (size_t)threads * 24 * 8);
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(farfield_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem));
+        farfield_kernel<<<grid, threads, smem, ctx->stream>>>(a, dpb);
+    }
     BEM_LAUNCHED(ctx);
     // algorithmic unit: one (orientation, direction, point) term, ~110 flop
     if (ev)
@@ -385,7 +515,7 @@ int farfield_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, in
     a.cs = N;
     a.rhat = (const double*)(ws + oR);
     a.Fv = (double2*)(ws + oF);
-    BEM_TRY(launch_ff(ctx, a));
+    BEM_TRY(launch_ff(ctx, g, a));
     BEM_TRY_CUDA(ctx, cudaMemcpyAsync(Fv_host, ws + oF, fb, cudaMemcpyDeviceToHost, ctx->stream));
     BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return BEM_OK;
@@ -427,7 +557,7 @@ int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, con
     a.Mo = M_orient_dev ? M_orient_dev : (double*)(ws + oMo);
     a.gamma_mirror = gamma_mirror;
     a.Fv = Fv_host ? (double2*)(ws + oFv) : nullptr;
-    BEM_TRY(launch_ff(ctx, a));
+    BEM_TRY(launch_ff(ctx, g, a));
     int nel = 16 * ntheta;
     mueller_sum_kernel<<<(nel + 255) / 256, 256, 0, ctx->stream>>>(a.Mo, n_orient, nel, (double*)(ws + oMa));
     BEM_LAUNCHED(ctx);
@@ -497,7 +627,7 @@ int mueller_noalloc(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx,
     a.w = d_w;
     a.Mo = d_Mo;  // every (o, i, d) entry is written: nothing to clear
     a.gamma_mirror = gamma_mirror;
-    BEM_TRY(launch_ff(ctx, a));
+    BEM_TRY(launch_ff(ctx, g, a));
     int nel = 16 * ntheta;
     mueller_sum_kernel<<<(nel + 255) / 256, 256, 0, ctx->stream>>>(d_Mo, n_orient, nel, M_out_dev);
     BEM_LAUNCHED(ctx);

@@ -104,3 +104,22 @@ def test_gamma_mirror_and_range(ctx):
     Mm, _ = bb.dense_run(ctx, v, t, 2.0, 1.31, orient=(3, 2, 2), ntheta=19, gamma_mirror=True)
     odd = [2, 3, 6, 7, 8, 9, 12, 13]
     assert np.all(Mm.reshape(16, -1)[odd] == 0.0)
+
+
+@pytest.mark.parametrize("m,q", [(1.3116, 7), (complex(1.5, 0.02), 4), (1.6, 13)])
+def test_farfield_by_triangles_matches_per_point_kernel(ctx, m, q):
+    # the default far field (phases shared by the RWG halves of a triangle)
+    # against the per-RWG-half-point kernel: Mueller matrices, per-orientation
+    # terms and far-field vectors
+    import bem_b200 as bb
+    v, t = bb.icosphere(1.0, 2)
+    out = {}
+    for kern in (1, 0):
+        bb.set_option(ctx, "farfield_kernel", kern)
+        try:
+            M, info = bb.dense_run(ctx, v, t, 2.0, m, quad_order=q, orient=(3, 4, 2), ntheta=37, per_orient=True)
+        finally:
+            bb.set_option(ctx, "farfield_kernel", 0)
+        out[kern] = (M, info["per_orient_mueller"])
+    assert rel(out[0][0], out[1][0]) < 1e-12
+    assert rel(out[0][1], out[1][1]) < 1e-12
