@@ -28,16 +28,27 @@ namespace bem {
 // ------------------------------------------------------------ geometry upload
 bool host_mesh_from(const double* verts, int nv, const int* tris, int nt, HostMesh* m);
 
-int geom_upload(bem_ctx* ctx, bem_geom* g) {
+// Position-dependent geometry arrays (everything the vertex coordinates
+// enter): per-half quadrature points, basis values, weights, divergences,
+// free vertices; triangle vertices; per-triangle centroid-relative data.
+struct PosArrays {
+    std::vector<double> px, py, pz, fx, fy, fz, cx, cy, cz, jw, div, coef, frx, fry, frz, tv, tc, tu, tjw, hpi;
+    std::vector<int> tri;
+};
+
+static void position_arrays(const bem_geom* g, PosArrays& A) {
     const HostMesh& m = g->mesh;
     const HostRWG& r = g->rwg;
     const Quad& q = g->quad;
     const int N = r.N, Nq = q.n, nt = m.nt();
     const size_t P = (size_t)2 * N * Nq;
-    // host staging
-    std::vector<double> px(P), py(P), pz(P), fx(P), fy(P), fz(P), cx(P), cy(P), cz(P), jw(P);
-    std::vector<double> div(2 * N), coef(2 * N), frx(2 * N), fry(2 * N), frz(2 * N);
-    std::vector<int> tri(2 * N);
+    auto& px = A.px; auto& py = A.py; auto& pz = A.pz; auto& fx = A.fx; auto& fy = A.fy; auto& fz = A.fz;
+    auto& cx = A.cx; auto& cy = A.cy; auto& cz = A.cz; auto& jw = A.jw;
+    for (auto* v : {&px, &py, &pz, &fx, &fy, &fz, &cx, &cy, &cz, &jw}) v->assign(P, 0.0);
+    auto& div = A.div; auto& coef = A.coef; auto& frx = A.frx; auto& fry = A.fry; auto& frz = A.frz;
+    for (auto* v : {&div, &coef, &frx, &fry, &frz}) v->assign(2 * N, 0.0);
+    auto& tri = A.tri;
+    tri.assign(2 * N, 0);
     for (int h = 0; h < 2; h++) {
         int sign = h == 0 ? 1 : -1;
         for (int n = 0; n < N; n++) {
@@ -69,41 +80,21 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
             }
         }
     }
-    // singular pairs: halves per triangle, ordered (test, source) items per
-    // unordered RWG pair
-    std::vector<std::vector<int>> on_tri(nt);
-    for (int h = 0; h < 2; h++)
-        for (int n = 0; n < N; n++) on_tri[h == 0 ? r.tri_p[n] : r.tri_m[n]].push_back(h * N + n);
-    std::map<std::pair<int, int>, std::vector<int>> slot;  // (m<=n) -> items (t, a, b)
-    for (int t = 0; t < nt; t++)
-        for (int a : on_tri[t])
-            for (int b : on_tri[t]) {
-                int mm = a % N, nn = b % N;
-                auto& v = slot[{std::min(mm, nn), std::max(mm, nn)}];
-                v.push_back(t);
-                v.push_back(a);
-                v.push_back(b);
-            }
-    std::vector<int> pair_mn, item_ptr{0}, item;
-    for (auto& kv : slot) {
-        pair_mn.push_back(kv.first.first);
-        pair_mn.push_back(kv.first.second);
-        item.insert(item.end(), kv.second.begin(), kv.second.end());
-        item_ptr.push_back((int)item.size() / 3);
-    }
-    std::vector<double> tv(9 * (size_t)nt);
+    auto& tv = A.tv;
+    tv.assign(9 * (size_t)nt, 0.0);
     for (int t = 0; t < nt; t++)
         for (int j = 0; j < 3; j++) {
             V3 v = m.verts[m.tris[3 * t + j]];
             tv[9 * t + 3 * j] = v.x, tv[9 * t + 3 * j + 1] = v.y, tv[9 * t + 3 * j + 2] = v.z;
         }
-    g->sing.npairs = (int)pair_mn.size() / 2;
-    g->sing.nitems = (int)item.size() / 3;
-
     // triangle-pair assembly data: per triangle the centroid, the quadrature
     // points relative to it (the same points as the halves') and area x
     // weight; per half the free vertex relative to its triangle's centroid
-    std::vector<double> tc(3 * (size_t)nt), tu(3 * (size_t)nt * Nq), tjw((size_t)nt * Nq), hpi(3 * (size_t)2 * N);
+    auto& tc = A.tc; auto& tu = A.tu; auto& tjw = A.tjw; auto& hpi = A.hpi;
+    tc.assign(3 * (size_t)nt, 0.0);
+    tu.assign(3 * (size_t)nt * Nq, 0.0);
+    tjw.assign((size_t)nt * Nq, 0.0);
+    hpi.assign(3 * (size_t)2 * N, 0.0);
     std::vector<double> tarea(nt, -1.0);
     for (int h = 0; h < 2; h++)
         for (int n = 0; n < N; n++) {
@@ -132,6 +123,45 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
             size_t i = ((size_t)h * N + n) * 3;
             hpi[i] = fr.x - tc[3 * t], hpi[i + 1] = fr.y - tc[3 * t + 1], hpi[i + 2] = fr.z - tc[3 * t + 2];
         }
+}
+
+int geom_upload(bem_ctx* ctx, bem_geom* g) {
+    const HostMesh& m = g->mesh;
+    const HostRWG& r = g->rwg;
+    const Quad& q = g->quad;
+    const int N = r.N, Nq = q.n, nt = m.nt();
+    const size_t P = (size_t)2 * N * Nq;
+    PosArrays A;
+    position_arrays(g, A);
+    auto& px = A.px; auto& py = A.py; auto& pz = A.pz; auto& fx = A.fx; auto& fy = A.fy; auto& fz = A.fz;
+    auto& cx = A.cx; auto& cy = A.cy; auto& cz = A.cz; auto& jw = A.jw;
+    auto& div = A.div; auto& coef = A.coef; auto& frx = A.frx; auto& fry = A.fry; auto& frz = A.frz;
+    auto& tri = A.tri; auto& tv = A.tv; auto& tc = A.tc; auto& tu = A.tu; auto& tjw = A.tjw; auto& hpi = A.hpi;
+    // singular pairs: halves per triangle, ordered (test, source) items per
+    // unordered RWG pair
+    std::vector<std::vector<int>> on_tri(nt);
+    for (int h = 0; h < 2; h++)
+        for (int n = 0; n < N; n++) on_tri[h == 0 ? r.tri_p[n] : r.tri_m[n]].push_back(h * N + n);
+    std::map<std::pair<int, int>, std::vector<int>> slot;  // (m<=n) -> items (t, a, b)
+    for (int t = 0; t < nt; t++)
+        for (int a : on_tri[t])
+            for (int b : on_tri[t]) {
+                int mm = a % N, nn = b % N;
+                auto& v = slot[{std::min(mm, nn), std::max(mm, nn)}];
+                v.push_back(t);
+                v.push_back(a);
+                v.push_back(b);
+            }
+    std::vector<int> pair_mn, item_ptr{0}, item;
+    for (auto& kv : slot) {
+        pair_mn.push_back(kv.first.first);
+        pair_mn.push_back(kv.first.second);
+        item.insert(item.end(), kv.second.begin(), kv.second.end());
+        item_ptr.push_back((int)item.size() / 3);
+    }
+    g->sing.npairs = (int)pair_mn.size() / 2;
+    g->sing.nitems = (int)item.size() / 3;
+
     // RWGs in the Morton order of their triangles' centroids: each triangle
     // in turn appends its RWGs not placed yet, so a tile of 16 consecutive
     // RWGs touches ~17 distinct triangles instead of ~21-32
@@ -272,6 +302,36 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     (void)d_fr;
     g->sing_coef = d_coef;
     g->sing_free = d_fr;
+    return BEM_OK;
+}
+
+int geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts) {
+    HostRWG& r = g->rwg;
+    HostMesh& m = g->mesh;
+    if (!verts || r.edge_lo.size() != (size_t)r.N || r.vfree_p.size() != (size_t)r.N)
+        return fail(ctx, BEM_ERR_INVALID, "vertex update needs a geometry built from its mesh");
+    for (int i = 0; i < m.nv(); i++) m.verts[i] = {verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]};
+    rwg_refresh(m, r);
+    PosArrays A;
+    position_arrays(g, A);
+    const int N = r.N;
+    const size_t P = A.px.size();
+    cudaStream_t st = ctx->stream;
+    double* dst[10] = {g->half.px, g->half.py, g->half.pz, g->half.fx, g->half.fy,
+                       g->half.fz, g->half.cx, g->half.cy, g->half.cz, g->half.jw};
+    const std::vector<double>* src[10] = {&A.px, &A.py, &A.pz, &A.fx, &A.fy, &A.fz, &A.cx, &A.cy, &A.cz, &A.jw};
+    for (int i = 0; i < 10; i++)
+        BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dst[i], src[i]->data(), P * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->half.div, A.div.data(), 2 * (size_t)N * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->sing_coef, A.coef.data(), 2 * (size_t)N * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->sing_free, A.frx.data(), 2 * (size_t)N * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->sing_free + 2 * N, A.fry.data(), 2 * (size_t)N * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->sing_free + 4 * N, A.frz.data(), 2 * (size_t)N * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->sing.tv, A.tv.data(), A.tv.size() * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->tri.c, A.tc.data(), A.tc.size() * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->tri.u, A.tu.data(), A.tu.size() * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->tri.jw, A.tjw.data(), A.tjw.size() * 8, cudaMemcpyHostToDevice, st));
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(g->tri.pi, A.hpi.data(), A.hpi.size() * 8, cudaMemcpyHostToDevice, st));
     return BEM_OK;
 }
 

@@ -65,6 +65,7 @@ struct HostRWG {
     std::vector<int> vfree_p, vfree_m;  // vertex index of the free vertices
     std::vector<V3> free_p, free_m;
     std::vector<double> length, area_p, area_m;
+    std::vector<int> edge_lo, edge_hi;  // vertex indices of the edge (empty: basis given by the caller)
 };
 
 struct Quad {
@@ -76,6 +77,9 @@ HostMesh make_icosphere(double radius, int refinements);
 HostMesh make_hex_prism(double aspect_ratio, int refinements);
 HostMesh subdivide_flat(const HostMesh& m);
 HostRWG build_rwg(const HostMesh& m);
+// Free vertices, edge lengths and areas of a mesh-built basis after the
+// vertices moved (same formulas as build_rwg).
+void rwg_refresh(const HostMesh& m, HostRWG& r);
 bool quadrature(int order, Quad* q);  // false: unsupported order
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
 void orientations(int na, int nb, int ng, int bsym, int gsym, bool mirror, bool sort,
@@ -227,6 +231,11 @@ int assemble_dev(bem_ctx* ctx, const bem_geom* g, double ke_re, double ke_im, do
                  void* Z, int64_t ldz, void* L, void* K, const unsigned char* rwg_mask = nullptr);
 constexpr int ASM_TILE = 16;  // RWGs per assembly band
 int geom_upload(bem_ctx* ctx, bem_geom* g);
+// Moves the vertices of a geometry made by bem_geom_create (nv x 3 doubles)
+// and refreshes every position-dependent device array in place, in the
+// context's stream order: same topology, RWG order, tiles and allocation,
+// and the values a geometry created from the moved mesh would have.
+int geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts);
 // rhs / farfield
 int rhs_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im, double eta,
             const double* RT_host, const double* E0_host, const double* khat_host, int n_orient,

@@ -125,9 +125,21 @@ HostRWG build_rwg(const HostMesh& m) {
         r.length.push_back(norm(sub(m.verts[kv.first.second], m.verts[kv.first.first])));
         r.area_p.push_back(tri_area(m, tp));
         r.area_m.push_back(tri_area(m, tm));
+        r.edge_lo.push_back(kv.first.first);
+        r.edge_hi.push_back(kv.first.second);
     }
     r.N = (int)r.tri_p.size();
     return r;
+}
+
+void rwg_refresh(const HostMesh& m, HostRWG& r) {
+    for (int n = 0; n < r.N; n++) {
+        r.free_p[n] = m.verts[r.vfree_p[n]];
+        r.free_m[n] = m.verts[r.vfree_m[n]];
+        r.length[n] = norm(sub(m.verts[r.edge_hi[n]], m.verts[r.edge_lo[n]]));
+        r.area_p[n] = tri_area(m, r.tri_p[n]);
+        r.area_m[n] = tri_area(m, r.tri_m[n]);
+    }
 }
 
 // Dunavant rules -- quadrature.h:14-70.  Barycentric (l1, l2), weights sum to 1.

@@ -355,6 +355,19 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
             return fail(ctx, BEM_ERR_OOM, "gradient buffers");
         }
         std::vector<unsigned char> mask(N);
+        // one working geometry, moved in place per evaluation (same topology,
+        // tiles and device arrays as a geometry created from the moved mesh)
+        struct GeomGuard {
+            bem_geom* g = nullptr;
+            ~GeomGuard() {
+                if (g) bem_geom_free(g);
+            }
+        } gw;
+        {
+            int Nw = 0;
+            BEM_TRY(bem_geom_create(ctx, vp.data(), p->nv, p->tris, p->nt, p->quad_order, &gw.g, &Nw));
+            if (Nw != N) return fail(ctx, BEM_ERR_INVALID, "working geometry has %d RWGs, not %d", Nw, N);
+        }
         for (int iv = 0; iv < p->nv; iv++) {
             std::fill(mask.begin(), mask.end(), 0);
             for (int mm : vrwg[iv]) mask[mm] = 1;
@@ -367,10 +380,8 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
                 double* Ms[2] = {Mp.data(), Mm.data()};
                 for (int sgn = 0; sgn < 2; sgn++) {
                     vp[3 * iv + comp] = v0 + (sgn == 0 ? h : -h);
-                    bem_geom* gs = nullptr;
-                    int Ns = 0;
-                    int st = bem_geom_create(ctx, vp.data(), p->nv, p->tris, p->nt, p->quad_order, &gs, &Ns);
-                    if (st == BEM_OK && Ns != N) st = fail(ctx, BEM_ERR_INVALID, "moved mesh changed its RWG count");
+                    bem_geom* gs = gw.g;
+                    int st = geom_set_vertices(ctx, gs, vp.data());
                     if (st == BEM_OK && cudaMemcpyAsync(Zs[sgn], dZbase.p, zb, cudaMemcpyDeviceToDevice,
                                                         ctx->stream) != cudaSuccess)
                         st = fail(ctx, BEM_ERR_CUDA, "operator copy");
@@ -384,7 +395,6 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
                     if (st == BEM_OK)
                         st = mueller_dev(ctx, gs, dX.p, n, RT.data(), w.data(), no, kext.real(), kext.imag(), eta_e,
                                          nt, p->gamma_mirror, Ms[sgn], nullptr);
-                    bem_geom_free(gs);
                     if (st != BEM_OK) {
                         vp[3 * iv + comp] = v0;
                         return st;
