@@ -728,6 +728,55 @@ def adjoint_grad_vertices(ctx: Context, verts, tris, ka, m, target, wt=None, **k
     return loss.value, grad, M
 
 
+def _misfit_function():
+    import torch
+
+    class MuellerMisfit(torch.autograd.Function):
+        """loss = sum_t wt_t (M11(theta_t) - target_t)^2 of the orientation-
+        averaged Mueller matrix; the gradients come from the adjoint entry
+        points (bem_adjoint_grad_vertices for the vertices, only when they
+        require a gradient, and bem_adjoint_grad for m), computed together
+        with the loss in the forward pass."""
+
+        @staticmethod
+        def forward(fctx, verts, m_re, m_im, bctx, tris, ka, target, wt, kw):
+            v = verts.detach().cpu().numpy().astype(np.float64)
+            m = complex(float(m_re), float(m_im))
+            gv = None
+            if verts.requires_grad:
+                loss, gv, _ = adjoint_grad_vertices(bctx, v, tris, ka, m, target, wt, **kw)
+            loss_m, gm, _ = adjoint_grad(bctx, v, tris, ka, m, target, wt, **kw)
+            if gv is None:
+                loss = loss_m
+            fctx.gv = None if gv is None else torch.from_numpy(gv).to(verts.dtype)
+            fctx.gm = torch.from_numpy(gm)
+            return torch.tensor(loss, dtype=torch.float64)
+
+        @staticmethod
+        def backward(fctx, gout):
+            gv = None if fctx.gv is None else gout * fctx.gv
+            return gv, gout * fctx.gm[0], gout * fctx.gm[1], None, None, None, None, None, None
+
+    return MuellerMisfit
+
+
+_MISFIT = None
+
+
+def mueller_misfit(ctx: Context, verts, tris, ka, m_re, m_im, target, wt=None, **kw):
+    """Differentiable M11 misfit for torch: verts (nv, 3) and m_re, m_im are
+    float64 torch tensors (CPU), the loss a 0-d tensor whose backward() fills
+    verts.grad (when verts requires it) and m_re.grad, m_im.grad from one
+    forward and one adjoint solve each (bem_adjoint_grad_vertices,
+    bem_adjoint_grad).  target: one value per scattering angle; **kw as
+    dense_run (orient, ...)."""
+    global _MISFIT
+    if _MISFIT is None:
+        _MISFIT = _misfit_function()
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    return _MISFIT.apply(verts, m_re, m_im, ctx, tris, ka, target, wt, kw)
+
+
 def c5_mesh(seed, refinements=3, rms=0.05, lmax=6, slope=2.0):
     """The seeded shape-gradient workload: an icosphere with a radial
     displacement r -> r (1 + g(rhat)), g a Gaussian random field of real
