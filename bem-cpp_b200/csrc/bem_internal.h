@@ -121,6 +121,7 @@ struct DevSingular {
 void* devmem_alloc(int device, size_t bytes);  // nullptr when out of memory
 void devmem_free(int device, void* p, size_t bytes);
 void devmem_cache_enable(int device, bool on);
+bool devmem_cache_enabled(int device);
 
 // Triangle-pair assembly: per-triangle quadrature data relative to the
 // centroid, and the RWGs in tiles of ASM_TILE ordered along a Morton curve of
@@ -217,7 +218,8 @@ struct bem_geom {
     double* sing_coef = nullptr;  // (2N) sign*l/(2A) per half
     double* sing_free = nullptr;  // (3*2N) free vertex per half, x | y | z blocks
     bem::DevTriAsm tri{};         // triangle-pair assembly data (Morton-ordered tiles)
-    void* dmem = nullptr;  // one allocation backing every device array
+    void* dmem = nullptr;  // one allocation backing every device array (devmem_alloc)
+    size_t dmem_bytes = 0;
 };
 
 namespace bem {

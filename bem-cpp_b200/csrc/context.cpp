@@ -135,6 +135,12 @@ void devmem_free(int device, void* p, size_t bytes) {
     cudaFree(p);
 }
 
+bool devmem_cache_enabled(int device) {
+    if (device < 0 || device >= 64) return false;
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    return g_cache[device].on;
+}
+
 void devmem_cache_enable(int device, bool on) {
     if (device < 0 || device >= 64) return;
     std::lock_guard<std::mutex> g(g_cache_mu);

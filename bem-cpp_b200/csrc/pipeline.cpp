@@ -16,10 +16,20 @@ using namespace bem;
 
 namespace {
 
+// Device buffer from the device-memory cache (devmem_alloc): a batch of
+// particles of one size allocates its buffers once.
 struct DevBuf {
     void* p = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+    bool alloc(int dev, size_t b) {
+        p = devmem_alloc(dev, b);
+        bytes = b;
+        device = dev;
+        return p != nullptr;
+    }
     void release() {
-        if (p) cudaFree(p);
+        if (p) devmem_free(device, p, bytes);
         p = nullptr;
     }
     ~DevBuf() { release(); }
@@ -43,7 +53,7 @@ int bem_assemble_L_K(bem_ctx* ctx, const double* verts, int nv, const int* tris,
     size_t bytes = (size_t)N * N * 16;
     DevBuf dL, dK;
     int s = BEM_OK;
-    if (cudaMalloc(&dL.p, bytes) != cudaSuccess || cudaMalloc(&dK.p, bytes) != cudaSuccess) {
+    if (!dL.alloc(ctx->device, bytes) || !dK.alloc(ctx->device, bytes)) {
         cudaGetLastError();
         s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
     }
@@ -66,7 +76,7 @@ int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tr
     size_t zb = (size_t)4 * N * N * 16;
     DevBuf dZ;
     int s = BEM_OK;
-    if (cudaMalloc(&dZ.p, zb) != cudaSuccess) {
+    if (!dZ.alloc(ctx->device, zb)) {
         cudaGetLastError();
         s = fail(ctx, BEM_ERR_OOM, "Z device buffer (%zu bytes)", zb);
     }
@@ -78,7 +88,7 @@ int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tr
     if (s == BEM_OK && (L_ext || K_ext)) {
         size_t b = (size_t)N * N * 16;
         DevBuf dL, dK;
-        if (cudaMalloc(&dL.p, b) != cudaSuccess || cudaMalloc(&dK.p, b) != cudaSuccess) {
+        if (!dL.alloc(ctx->device, b) || !dK.alloc(ctx->device, b)) {
             cudaGetLastError();
             s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
         }
@@ -134,11 +144,10 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
     }
     DevBuf dZ, dB, dX, dMo, dA;
     int s = BEM_OK;
-    if (cudaMalloc(&dZ.p, (size_t)n * n * 16) != cudaSuccess ||
-        cudaMalloc(&dB.p, (size_t)n * nrhs_max * 16) != cudaSuccess ||
-        cudaMalloc(&dX.p, (size_t)n * nrhs_max * 16) != cudaSuccess ||
-        cudaMalloc(&dMo.p, (size_t)std::min(batch, no) * 16 * nt * 8) != cudaSuccess ||
-        (gm && cudaMalloc(&dA.p, (size_t)n * n * 16) != cudaSuccess)) {
+    const int dev = ctx->device;
+    if (!dZ.alloc(dev, (size_t)n * n * 16) || !dB.alloc(dev, (size_t)n * nrhs_max * 16) ||
+        !dX.alloc(dev, (size_t)n * nrhs_max * 16) || !dMo.alloc(dev, (size_t)std::min(batch, no) * 16 * nt * 8) ||
+        (gm && !dA.alloc(dev, (size_t)n * n * 16))) {
         cudaGetLastError();
         bem_geom_free(g);
         return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs_max);
@@ -305,6 +314,12 @@ int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_resu
     if (!ctx || count < 0 || (count > 0 && (!problems || !results))) return BEM_ERR_INVALID;
     int first = BEM_OK;
     std::string first_msg;
+    // particles of one topology reuse their device buffers (operator,
+    // right-hand sides, factors, digit planes, geometry) through the device-
+    // memory cache for the duration of the batch; it is released at the end
+    // unless the caller keeps it on (cache_factor_memory)
+    const bool had_cache = devmem_cache_enabled(ctx->device);
+    if (!had_cache) devmem_cache_enable(ctx->device, true);
     for (int i = 0; i < count; i++) {
         int s = bem_dense_run(ctx, &problems[i], &results[i]);
         if (statuses) statuses[i] = s;
@@ -313,6 +328,7 @@ int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_resu
             first_msg = "particle " + std::to_string(i) + ": " + ctx->last_error;
         }
     }
+    if (!had_cache) devmem_cache_enable(ctx->device, false);
     if (first != BEM_OK) ctx->last_error = first_msg;
     return first;
 }
