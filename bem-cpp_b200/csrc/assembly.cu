@@ -244,7 +244,7 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
            o_hpi = take(hpi.size() * 8), o_trwg = take(tile_rwg.size() * 4), o_pos = take((size_t)N * 4),
            o_ttri = take(tile_tri.size() * 4), o_tntri = take((size_t)ntile * 4), o_tent = take(tile_ent.size()),
            o_tflag = take((size_t)ntile), o_rrec = take((size_t)N), o_thalf = take(tri_half.size() * 4);
-    g->dmem = devmem_alloc(ctx->device, off);
+    g->dmem = devmem_alloc(ctx->device, off, ctx);
     if (!g->dmem) return fail(ctx, BEM_ERR_OOM, "geometry arrays (%zu bytes)", off);
     g->dmem_bytes = off;
     char* base = (char*)g->dmem;
@@ -1156,7 +1156,7 @@ int bem_geom_create(bem_ctx* ctx, const double* verts, int nv, const int* tris, 
     }
     int s = cudaSetDevice(ctx->device) == cudaSuccess ? geom_upload(ctx, g) : BEM_ERR_CUDA;
     if (s != BEM_OK) {
-        if (g->dmem) devmem_free(ctx->device, g->dmem, g->dmem_bytes);
+        if (g->dmem) devmem_free(ctx->device, g->dmem, g->dmem_bytes, ctx);
         delete g;
         return s;
     }
@@ -1203,7 +1203,7 @@ int bem_geom_create_rwg(bem_ctx* ctx, const double* verts, int nv, const int* tr
     g->nt = nt;
     int s = cudaSetDevice(ctx->device) == cudaSuccess ? geom_upload(ctx, g) : BEM_ERR_CUDA;
     if (s != BEM_OK) {
-        if (g->dmem) devmem_free(ctx->device, g->dmem, g->dmem_bytes);
+        if (g->dmem) devmem_free(ctx->device, g->dmem, g->dmem_bytes, ctx);
         delete g;
         return s;
     }
@@ -1215,7 +1215,8 @@ int bem_geom_free(bem_geom* g) {
     if (!g) return BEM_OK;
     if (g->dmem) {
         cudaSetDevice(g->device);
-        devmem_free(g->device, g->dmem, g->dmem_bytes);  // waits for work using it
+        // last used on the creating context's stream (or the device waits)
+        devmem_free(g->device, g->dmem, g->dmem_bytes, g->ctx);
     }
     delete g;
     return BEM_OK;

@@ -118,8 +118,12 @@ struct DevSingular {
 // one size allocates once.  Per device and process-wide, so a factorisation
 // may outlive the context that made it.  Disabling frees the kept blocks; an
 // allocation that fails frees them and retries once.
-void* devmem_alloc(int device, size_t bytes);  // nullptr when out of memory
-void devmem_free(int device, void* p, size_t bytes);
+// owner: the context whose stream uses the block (cached blocks are handed
+// back only to their owner, in its stream order; null: any, after a device
+// synchronisation).  Contexts register as owners while they live.
+void* devmem_alloc(int device, size_t bytes, const void* owner);  // nullptr when out of memory
+void devmem_free(int device, void* p, size_t bytes, const void* owner);
+void devmem_owner(const void* owner, bool alive);
 void devmem_cache_enable(int device, bool on);
 bool devmem_cache_enabled(int device);
 

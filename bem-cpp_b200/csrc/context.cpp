@@ -2,6 +2,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <mutex>
+#include <set>
 
 #include "bem_internal.h"
 #include "ozaki.h"
@@ -72,32 +73,54 @@ int bem_ctx::prof_collect() {
 
 namespace bem {
 namespace {
+struct CachedBlock {
+    void* p;
+    size_t bytes;
+    const void* owner;  // context whose stream last used the block (null: synchronised)
+};
 struct DevCache {
     bool on = false;
-    std::vector<std::pair<void*, size_t>> blocks;
+    std::vector<CachedBlock> blocks;
 };
 std::mutex g_cache_mu;
 DevCache g_cache[64];
+std::set<const void*> g_owners;  // live contexts
 
-void trim_locked(int device) {
+void free_blocks_locked(int device, const void* owner, bool all) {
     DevCache& c = g_cache[device];
-    if (c.blocks.empty()) return;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
-    for (auto& b : c.blocks) cudaFree(b.first);
-    c.blocks.clear();
+    for (size_t i = 0; i < c.blocks.size();) {
+        if (all || c.blocks[i].owner == owner) {
+            cudaFree(c.blocks[i].p);
+            c.blocks.erase(c.blocks.begin() + i);
+        } else {
+            i++;
+        }
+    }
     cudaSetDevice(prev);
 }
 }  // namespace
 
-void* devmem_alloc(int device, size_t bytes) {
+void devmem_owner(const void* owner, bool alive) {
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    if (alive) {
+        g_owners.insert(owner);
+        return;
+    }
+    g_owners.erase(owner);
+    for (int d = 0; d < 64; d++)
+        if (!g_cache[d].blocks.empty()) free_blocks_locked(d, owner, false);
+}
+
+void* devmem_alloc(int device, size_t bytes, const void* owner) {
     if (device >= 0 && device < 64) {
         std::lock_guard<std::mutex> g(g_cache_mu);
         auto& bl = g_cache[device].blocks;
         for (size_t i = 0; i < bl.size(); i++)
-            if (bl[i].second == bytes) {
-                void* p = bl[i].first;
+            if (bl[i].bytes == bytes && (bl[i].owner == owner || bl[i].owner == nullptr)) {
+                void* p = bl[i].p;
                 bl.erase(bl.begin() + i);
                 return p;
             }
@@ -109,26 +132,30 @@ void* devmem_alloc(int device, size_t bytes) {
     {
         std::lock_guard<std::mutex> g(g_cache_mu);
         if (g_cache[device].blocks.empty()) return nullptr;
-        trim_locked(device);
+        free_blocks_locked(device, nullptr, true);
     }
     if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
     cudaGetLastError();
     return nullptr;
 }
 
-void devmem_free(int device, void* p, size_t bytes) {
+void devmem_free(int device, void* p, size_t bytes, const void* owner) {
     if (!p) return;
     if (device >= 0 && device < 64) {
         std::lock_guard<std::mutex> g(g_cache_mu);
         if (g_cache[device].on) {
-            // work queued on any stream of this device that still reads the
-            // block must finish before another factorisation reuses it
-            int prev = 0;
-            cudaGetDevice(&prev);
-            cudaSetDevice(device);
-            cudaDeviceSynchronize();
-            cudaSetDevice(prev);
-            g_cache[device].blocks.push_back({p, bytes});
+            // a block goes back to the live context that used it: its next
+            // user is that context's stream, ordered after the work still
+            // reading it.  Without a live owner, wait for the device first.
+            if (!owner || !g_owners.count(owner)) {
+                int prev = 0;
+                cudaGetDevice(&prev);
+                cudaSetDevice(device);
+                cudaDeviceSynchronize();
+                cudaSetDevice(prev);
+                owner = nullptr;
+            }
+            g_cache[device].blocks.push_back({p, bytes, owner});
             return;
         }
     }
@@ -145,7 +172,7 @@ void devmem_cache_enable(int device, bool on) {
     if (device < 0 || device >= 64) return;
     std::lock_guard<std::mutex> g(g_cache_mu);
     g_cache[device].on = on;
-    if (!on) trim_locked(device);
+    if (!on && !g_cache[device].blocks.empty()) free_blocks_locked(device, nullptr, true);
 }
 
 }  // namespace bem
@@ -194,6 +221,7 @@ int bem_ctx_create(int device, bem_ctx** out) {
         return BEM_ERR_CUDA;
     }
     c->stream = c->own_stream;
+    bem::devmem_owner(c, true);
     *out = c;
     return BEM_OK;
 }
@@ -202,6 +230,7 @@ int bem_ctx_destroy(bem_ctx* ctx) {
     if (!ctx) return BEM_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    bem::devmem_owner(ctx, false);  // frees the cached blocks it owns
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->tc_buf) cudaFree(ctx->tc_buf);
     if (ctx->oz_buf) cudaFree(ctx->oz_buf);
@@ -215,7 +244,10 @@ int bem_ctx_destroy(bem_ctx* ctx) {
 
 int bem_ctx_set_stream(bem_ctx* ctx, void* stream) {
     if (!ctx) return BEM_ERR_INVALID;
-    // NULL selects the legacy default stream (what torch's default stream is)
+    // NULL selects the legacy default stream (what torch's default stream is).
+    // Cached blocks of this context are reused in stream order: finish the
+    // old stream's work first.
+    cudaStreamSynchronize(ctx->stream);
     ctx->stream = (cudaStream_t)stream;
     return BEM_OK;
 }

@@ -754,8 +754,9 @@ int ozaki_prepare_z(bem_ctx* ctx, OzakiZ* oz_, const double2* Z, int64_t ldz, in
     oz_->plane = (int64_t)n * oz_->ldk;
     size_t bytes = (size_t)S * oz_->plane;
     oz_->device = ctx->device;
-    oz_->A = (int8_t*)devmem_alloc(ctx->device, bytes);
-    oz_->e = oz_->A ? (int*)devmem_alloc(ctx->device, (size_t)n * sizeof(int)) : nullptr;
+    oz_->owner = ctx;
+    oz_->A = (int8_t*)devmem_alloc(ctx->device, bytes, ctx);
+    oz_->e = oz_->A ? (int*)devmem_alloc(ctx->device, (size_t)n * sizeof(int), ctx) : nullptr;
     if (!oz_->A || !oz_->e) {
         ozaki_free(oz_);
         return fail(ctx, BEM_ERR_OOM, "ozaki digit planes (%zu bytes)", bytes);
@@ -770,8 +771,8 @@ int ozaki_prepare_z(bem_ctx* ctx, OzakiZ* oz_, const double2* Z, int64_t ldz, in
 }
 
 void ozaki_free(OzakiZ* oz_) {
-    devmem_free(oz_->device, oz_->A, (size_t)oz_->S * oz_->plane);
-    devmem_free(oz_->device, oz_->e, (size_t)oz_->n * sizeof(int));
+    devmem_free(oz_->device, oz_->A, (size_t)oz_->S * oz_->plane, oz_->owner);
+    devmem_free(oz_->device, oz_->e, (size_t)oz_->n * sizeof(int), oz_->owner);
     oz_->A = nullptr;
     oz_->e = nullptr;
 }

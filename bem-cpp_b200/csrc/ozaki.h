@@ -19,6 +19,7 @@ struct OzakiZ {
     int8_t* A = nullptr;
     int* e = nullptr;   // per-row power-of-two exponents
     int device = -1;    // where A and e live
+    const void* owner = nullptr;  // context whose stream uses them
 };
 
 size_t ozaki_z_bytes(int n, int S);

@@ -22,14 +22,16 @@ struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
     int device = -1;
-    bool alloc(int dev, size_t b) {
-        p = devmem_alloc(dev, b);
+    const void* owner = nullptr;
+    bool alloc(const bem_ctx* ctx, size_t b) {
+        p = devmem_alloc(ctx->device, b, ctx);
         bytes = b;
-        device = dev;
+        device = ctx->device;
+        owner = ctx;
         return p != nullptr;
     }
     void release() {
-        if (p) devmem_free(device, p, bytes);
+        if (p) devmem_free(device, p, bytes, owner);
         p = nullptr;
     }
     ~DevBuf() { release(); }
@@ -53,7 +55,7 @@ int bem_assemble_L_K(bem_ctx* ctx, const double* verts, int nv, const int* tris,
     size_t bytes = (size_t)N * N * 16;
     DevBuf dL, dK;
     int s = BEM_OK;
-    if (!dL.alloc(ctx->device, bytes) || !dK.alloc(ctx->device, bytes)) {
+    if (!dL.alloc(ctx, bytes) || !dK.alloc(ctx, bytes)) {
         cudaGetLastError();
         s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
     }
@@ -76,7 +78,7 @@ int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tr
     size_t zb = (size_t)4 * N * N * 16;
     DevBuf dZ;
     int s = BEM_OK;
-    if (!dZ.alloc(ctx->device, zb)) {
+    if (!dZ.alloc(ctx, zb)) {
         cudaGetLastError();
         s = fail(ctx, BEM_ERR_OOM, "Z device buffer (%zu bytes)", zb);
     }
@@ -88,7 +90,7 @@ int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tr
     if (s == BEM_OK && (L_ext || K_ext)) {
         size_t b = (size_t)N * N * 16;
         DevBuf dL, dK;
-        if (!dL.alloc(ctx->device, b) || !dK.alloc(ctx->device, b)) {
+        if (!dL.alloc(ctx, b) || !dK.alloc(ctx, b)) {
             cudaGetLastError();
             s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
         }
@@ -144,10 +146,9 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
     }
     DevBuf dZ, dB, dX, dMo, dA;
     int s = BEM_OK;
-    const int dev = ctx->device;
-    if (!dZ.alloc(dev, (size_t)n * n * 16) || !dB.alloc(dev, (size_t)n * nrhs_max * 16) ||
-        !dX.alloc(dev, (size_t)n * nrhs_max * 16) || !dMo.alloc(dev, (size_t)std::min(batch, no) * 16 * nt * 8) ||
-        (gm && !dA.alloc(dev, (size_t)n * n * 16))) {
+    if (!dZ.alloc(ctx, (size_t)n * n * 16) || !dB.alloc(ctx, (size_t)n * nrhs_max * 16) ||
+        !dX.alloc(ctx, (size_t)n * nrhs_max * 16) || !dMo.alloc(ctx, (size_t)std::min(batch, no) * 16 * nt * 8) ||
+        (gm && !dA.alloc(ctx, (size_t)n * n * 16))) {
         cudaGetLastError();
         bem_geom_free(g);
         return fail(ctx, BEM_ERR_OOM, "pipeline buffers for n=%d, nrhs=%d", n, nrhs_max);
@@ -307,19 +308,20 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
 }
 
 // Batched particles: every problem through the dense pipeline in turn on the
-// context's stream (device buffers are sized per particle and released before
-// the next).  statuses[i] (optional) receives each problem's status; a failing
-// particle does not stop the batch.  Returns BEM_OK, or the first failure.
+// context's stream.  statuses[i] (optional) receives each problem's status;
+// a failing particle does not stop the batch.  Returns BEM_OK, or the first
+// failure.  (Worker contexts on several streams were measured slower: the
+// persistent tensor-core kernels take one CTA per SM and do not overlap.)
 int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_result* results, int* statuses) {
     if (!ctx || count < 0 || (count > 0 && (!problems || !results))) return BEM_ERR_INVALID;
-    int first = BEM_OK;
-    std::string first_msg;
     // particles of one topology reuse their device buffers (operator,
     // right-hand sides, factors, digit planes, geometry) through the device-
     // memory cache for the duration of the batch; it is released at the end
     // unless the caller keeps it on (cache_factor_memory)
     const bool had_cache = devmem_cache_enabled(ctx->device);
     if (!had_cache) devmem_cache_enable(ctx->device, true);
+    int first = BEM_OK;
+    std::string first_msg;
     for (int i = 0; i < count; i++) {
         int s = bem_dense_run(ctx, &problems[i], &results[i]);
         if (statuses) statuses[i] = s;

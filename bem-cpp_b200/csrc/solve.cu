@@ -161,7 +161,7 @@ static int factor_lu32(bem_ctx* ctx, bem_lu* lu, int* d_info, double* fro, int* 
 static void lu_release(bem_lu* lu) {
     if (!lu) return;
     cudaSetDevice(lu->device);
-    if (lu->A32) bem::devmem_free(lu->device, lu->A32, (size_t)lu->n * lu->n * sizeof(float2));
+    if (lu->A32) bem::devmem_free(lu->device, lu->A32, (size_t)lu->n * lu->n * sizeof(float2), lu->ctx);
     if (lu->d_ipiv) cudaFree(lu->d_ipiv);
     if (lu->d_perm) cudaFree(lu->d_perm);
     bem::ozaki_free(&lu->oz);
@@ -205,7 +205,7 @@ int lu_factor_ex(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bool 
             break;
         }
         if (precision == BEM_PREC_FP32_REFINE) {
-            lu->A32 = (float2*)devmem_alloc(ctx->device, (size_t)n * n * sizeof(float2));
+            lu->A32 = (float2*)devmem_alloc(ctx->device, (size_t)n * n * sizeof(float2), ctx);
             if (!lu->A32) {
                 s = fail(ctx, BEM_ERR_OOM, "FP32 factor storage (%zu bytes)", (size_t)n * n * sizeof(float2));
                 break;
