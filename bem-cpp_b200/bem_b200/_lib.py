@@ -123,6 +123,7 @@ SIGNATURES = {
                                  C.POINTER(_P)]),
     "bem_geom_free": (_I, [_P]),
     "bem_geom_size": (_I, [_P]),
+    "bem_geom_set_vertices": (_I, [_P, _P, _P]),
     "bem_assemble_pmchwt_dev": (_I, [_P, _P, _D, _D, _D, _D, _D, _D, C.c_uint, _P, _L]),
     "bem_assemble_LK_dev": (_I, [_P, _P, _D, _D, C.c_uint, _P, _P, _L]),
     "bem_assemble_aext_dev": (_I, [_P, _P, _D, _D, _D, C.c_uint, _P, _L]),

@@ -252,6 +252,13 @@ class Geometry:
         self.quad_order = quad_order
         return self
 
+    def set_vertices(self, verts):
+        """Moves the mesh vertices in place (same topology; bem_geom_set_vertices)."""
+        v = _f64(verts)
+        assert v.shape == self.verts.shape
+        self.ctx.check(lib().bem_geom_set_vertices(self.ctx.h, self.h, _ptr(v)))
+        self.verts = v
+
     def close(self):
         if self.h:
             lib().bem_geom_free(self.h)

@@ -1224,6 +1224,12 @@ int bem_geom_free(bem_geom* g) {
 
 int bem_geom_size(const bem_geom* g) { return g ? g->N : 0; }
 
+int bem_geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts) {
+    if (!ctx || !g || !verts) return BEM_ERR_INVALID;
+    BEM_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    return geom_set_vertices(ctx, g, verts);
+}
+
 int bem_assemble_pmchwt_dev(bem_ctx* ctx, const bem_geom* g, double kext_re, double kext_im,
                             double kint_re, double kint_im, double eta_ext, double eta_int,
                             unsigned flags, void* Z_dev, int64_t ldz) {

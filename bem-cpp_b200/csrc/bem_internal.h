@@ -239,8 +239,9 @@ constexpr int ASM_TILE = 16;  // RWGs per assembly band
 int geom_upload(bem_ctx* ctx, bem_geom* g);
 // Moves the vertices of a geometry made by bem_geom_create (nv x 3 doubles)
 // and refreshes every position-dependent device array in place, in the
-// context's stream order: same topology, RWG order, tiles and allocation,
-// and the values a geometry created from the moved mesh would have.
+// context's stream order: same topology, RWG order, tiles and allocation.
+// Right-hand sides and far field equal a new geometry's; the operator does to
+// rounding (the kept tiles fix which orientation of a symmetric pair is computed).
 int geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts);
 // rhs / farfield
 int rhs_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im, double eta,

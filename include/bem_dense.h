@@ -160,6 +160,16 @@ int bem_geom_create_rwg(bem_ctx* ctx, const double* verts, int nv, const int* tr
                         int quad_order, bem_geom** out);
 int bem_geom_free(bem_geom* g);
 int bem_geom_size(const bem_geom* g);
+/* Moves the vertices of a geometry made by bem_geom_create (verts: nv x 3
+ * doubles, same mesh topology) in place: the position-dependent device data
+ * is recomputed and copied into the same allocation in the stream order of
+ * ctx, keeping the RWG order and the assembly tiles; right-hand sides and far
+ * field equal those of a geometry created from the moved mesh, the operator
+ * to rounding (each symmetric pair is computed in the orientation of the kept
+ * tiles).  For loops over shapes of one mesh (shape gradients,
+ * optimisation); no reference counterpart.
+ * BEM_ERR_INVALID for a geometry made by bem_geom_create_rwg. */
+int bem_geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts);
 
 /* --------------------------------------------------------------- assembly */
 
