@@ -765,8 +765,10 @@ __global__ void __launch_bounds__(256, 2) assemble_tri_kernel(AsmArgs a, DevTriA
                 const double* vp = &su[(ib * MAXQ + qb) * 3];
                 const double vx = vp[0], vy = vp[1], vz = vp[2], w = wa * sjw[ib * MAXQ + qb];
                 const double dx = Dx + (ux - vx), dy = Dy + (uy - vy), dz = Dz + (uz - vz);
-                const double R = sqrt(dx * dx + dy * dy + dz * dz);
-                const double Rs = fmax(R, 1e-15), invR = 1.0 / Rs;
+                // 1/R from one reciprocal square root (R clamped at 1e-15 as
+                // R^2 at 1e-30); R = R^2 / R
+                const double R2 = fmax(dx * dx + dy * dy + dz * dz, 1e-30);
+                const double invR = rsqrt(R2), Rs = R2 * invR, R = Rs;
                 const double i4R = __dmul_rn(INV4PI_D, invR);  // rounded alone, as in assemble_kernel
                 double sn, cs;
                 sincos(k.kr * Rs, &sn, &cs);
