@@ -100,8 +100,14 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * reused by the next factorisation of the same order, so a loop of solves of
  * one size allocates them once; the kept memory counts against the device
  * until the option is set back to 0, which frees it, or until an allocation
- * of this library fails, which frees it and retries).  Unknown names give
- * BEM_ERR_INVALID. */
+ * of this library fails, which frees it and retries; the dense pipeline's
+ * operator, right-hand-side and geometry buffers are cached the same way, and
+ * bem_batch_run turns the cache on for its duration), "gemm_group_m" (16,
+ * default: row tiles per raster group of the persistent tensor-core GEMM),
+ * "assembly_kernel" (0, default: triangle-pair moments over Morton-ordered
+ * tiles; 1: one thread per RWG pair, the reference's organisation),
+ * "farfield_kernel" (0, default: phases shared by the RWG halves of a
+ * triangle; 1: per RWG-half point).  Unknown names give BEM_ERR_INVALID. */
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
