@@ -6,7 +6,10 @@ orientation x polarisation right-hand sides are split into contiguous slices,
 each rank solves its slice and forms its part of the weighted Mueller sum,
 and one all-reduce (sum) of the 16 x ntheta partial Mueller matrices gives
 the orientation average -- the device-side counterpart of the reference's
---orient-range split with a JSON sum (cluster_bem.py:76-127).
+--orient-range split with a JSON sum (cluster_bem.py:76-127).  Batches of
+particles split the same way: each rank runs its contiguous slice of the
+particles and the results are gathered on every rank (cluster_bem.py farms
+one process per particle).
 """
 from __future__ import annotations
 
@@ -61,3 +64,32 @@ def orientation_average_distributed(ctx, geom, Z, RT, w, k_ext, eta_ext, ntheta=
         lu.close()
         part = api.mueller_from_solutions_dev(geom, X, RT[o0:o1], w[o0:o1], k_ext, eta_ext, ntheta)
     return allreduce_sum(part, device).reshape(4, 4, ntheta), stats
+
+
+def particle_slice(count: int, rank: int, world: int):
+    """Contiguous [p0, p1) of a batch of `count` particles for `rank`."""
+    return orientation_slice(count, rank, world)
+
+
+def batch_run_distributed(ctx, particles, rank=0, world=1, run=None):
+    """Particles split across ranks: rank r runs particle_slice(len, r, world)
+    with `run` (default: api.batch_run on this rank's context, no raising),
+    then every rank receives all results in particle order through one
+    all_gather_object of the default process group.  Returns the list of
+    (mueller, info) for every particle."""
+    import torch.distributed as dist
+    if run is None:
+        from . import api
+
+        def run(ps):
+            return api.batch_run(ctx, ps, raise_on_error=False)
+    p0, p1 = particle_slice(len(particles), rank, world)
+    mine = list(run(particles[p0:p1])) if p1 > p0 else []
+    if world <= 1 or not (dist.is_available() and dist.is_initialized()):
+        return mine
+    parts = [None] * world
+    dist.all_gather_object(parts, (p0, mine))
+    out = []
+    for q0, res in sorted(parts, key=lambda x: x[0]):
+        out.extend(res)
+    return out

@@ -65,3 +65,47 @@ def test_orientation_slice_covers_all():
             assert seen == list(range(n))
     with pytest.raises(ValueError):
         orientation_slice(5, 2, 2)
+
+
+def _worker_particles(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import sys
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                        "bem-cpp_b200"))
+        from bem_b200.parallel import batch_run_distributed
+        particles = [{"id": i} for i in range(11)]
+        seen = []
+
+        def run(ps):   # stands in for the device pipeline: one result per particle
+            seen.extend(p["id"] for p in ps)
+            return [(np.full((4, 4, 3), float(p["id"])), {"status": 0, "rank": rank}) for p in ps]
+        out = batch_run_distributed(None, particles, rank, world, run=run)
+        q.put((rank, seen, [float(m[0, 0, 0]) for m, _ in out], [i["rank"] for _, i in out]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_particle_split_and_gather():
+    import torch.multiprocessing as mp
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker_particles, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, seen0, ids0, who0), (r1, seen1, ids1, who1) = res
+    assert seen0 == list(range(0, 5)) and seen1 == list(range(5, 11))    # each particle once
+    assert ids0 == ids1 == [float(i) for i in range(11)]                  # gathered in order
+    assert who0 == who1 == [0] * 5 + [1] * 6
