@@ -20,6 +20,12 @@ call bem_dense_run (host mesh in, host Mueller matrix out).
 --impl reference: the reference's CPU path for the solve (LAPACK zgetrf /
 zgetrs through SciPy, bem_core.py:1637, 1713) on a bounded sample, scaled to
 the workload.
+
+--impl cusolver: the reference's GPU call for the solve, cuSOLVER getrf +
+getrs in FP64 (solver.cu:87-142; 64-bit API, baseline/cusolver_lu.cpp), on
+the same device-assembled Z and right-hand sides, with this library's FP64
+LU and FP32 + refinement solves timed beside it under the same clocks and
+the solutions compared.
 """
 from __future__ import annotations
 
@@ -57,7 +63,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="bem", choices=["bem", "reference"])
+    ap.add_argument("--impl", default="bem", choices=["bem", "reference", "cusolver"])
     ap.add_argument("--ref", type=int, default=5, help="icosphere refinement (5: 2N=61440)")
     ap.add_argument("--ka", type=float, default=15.0)
     ap.add_argument("--m", type=complex, default=complex(1.3116, 1e-4))
@@ -197,6 +203,107 @@ def run_reference(a):
             "e2e": {"value": val, "unit": "s/solve", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- cuSOLVER arm
+def run_cusolver(a):
+    import ctypes as C
+
+    import torch
+
+    import bem_b200 as bb
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    lib = C.CDLL(os.path.join(REPO, "baseline", "lib", "libcs_lu.so"))
+    lib.cs_lu_solve.restype = C.c_int
+    lib.cs_lu_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64]
+    torch.cuda.set_device(0)
+    ctx = bb.Context(0)
+    stream = torch.cuda.current_stream(0)
+
+    def cs_solve(Z, X):
+        # X: (nrhs, n) row-major = column-major n x nrhs, ldb = n
+        rc = lib.cs_lu_solve(C.c_void_p(stream.cuda_stream), C.c_void_p(Z.data_ptr()), Z.shape[0],
+                             C.c_void_p(X.data_ptr()), X.shape[1], X.shape[0])
+        if rc != 0:
+            raise RuntimeError(f"cs_lu_solve returned {rc}")
+
+    verts, tris = bb.icosphere(1.0, a.ref)
+    kx, ki, ee, ei = bb.physics(a.ka, a.m)
+    g = bb.Geometry(ctx, verts, tris, 7)
+    n = g.n
+    RT, _ = bb.generate_orientations(*a.orient, sort_nearest=True)
+    B = bb.rhs_planewave_dev(g, kx, ee, RT)
+    nrhs = B.shape[0]
+    # warm-up: library load and handles on a small well-conditioned system
+    gen = torch.Generator(device="cuda:0").manual_seed(0)
+    Zs = None
+    for _ in range(a.warmup):
+        Zs = torch.randn((2048, 2048), dtype=torch.complex128, device="cuda:0", generator=gen)
+        Zs += 2048 * torch.eye(2048, dtype=torch.complex128, device="cuda:0")
+        cs_solve(Zs, torch.randn((8, 2048), dtype=torch.complex128, device="cuda:0", generator=gen))
+    del Zs
+    Z = torch.empty((n, n), dtype=torch.complex128, device="cuda:0")
+    X = torch.empty_like(B)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize(0)
+        ev0.record(stream)
+        out = fn()
+        ev1.record(stream)
+        torch.cuda.synchronize(0)
+        return ev0.elapsed_time(ev1) / 1e3, out
+
+    sampler = ClockSampler(0)
+    t_cs = []
+    for _ in range(a.steps):
+        bb.assemble_pmchwt_dev(g, kx, ki, ee, ei, Z=Z)          # getrf overwrites Z
+        X.copy_(B)
+        t_cs.append(timed(lambda: cs_solve(Z, X))[0])
+    # this library on the same Z and right-hand sides, under the same clocks
+    bb.assemble_pmchwt_dev(g, kx, ki, ee, ei, Z=Z)
+    bb.set_residual_digits(ctx, a.residual_digits)
+    X32 = torch.empty_like(B)
+
+    def fp32_step():
+        lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+        lu.solve(B, X=X32, tol=a.tol, max_iter=12, raise_noconv=False)
+        lu.close()
+
+    fp32_step()
+    t32, _ = timed(fp32_step)
+
+    def fp64_step():
+        lu = bb.LU(ctx, Z, bb.PREC_FP64)                          # factors Z in place
+        X64, _ = lu.solve(B)
+        lu.close()
+        return X64
+
+    t64, X64 = timed(fp64_step)
+    clocks = sampler.stop()
+
+    def rel(U, V):
+        return float(((U - V).abs().pow(2).sum(dim=1).sqrt() / V.abs().pow(2).sum(dim=1).sqrt()).max().item())
+
+    val = statistics.median(t_cs)
+    flops = 8.0 * n ** 3 / 3.0 + 8.0 * n * n * nrhs
+    line = {"impl": "cusolver", "metric": METRIC, "value": val, "unit": "s/solve", "n_gpus": 1,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": val * 1e3, "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic (generated icosphere mesh and plane waves)", "config": workload(a, n),
+            "library": "cuSOLVER (CUDA toolkit) cusolverDnXgetrf + cusolverDnXgetrs(OP_T), FP64",
+            "step_times_s": t_cs,
+            "fp64_tflops": flops / val / 1e12, "fp64_frac_of_37tfs": flops / val / 1e12 / FP64_PEAK_TFS,
+            "bem_fp64_s_per_solve": t64, "bem_fp32_refine_s_per_solve": t32,
+            "speedup_fp32_refine_vs_cusolver": val / t32, "speedup_bem_fp64_vs_cusolver": val / t64,
+            "max_rel_err_cusolver_vs_bem_fp64": rel(X, X64),
+            "max_rel_err_fp32_refine_vs_cusolver": rel(X32, X), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    del Z, X, X32, X64, B
+    g.close()
+    ctx.close()
 
 
 def _n_rwg_ico(ref):
@@ -429,6 +536,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.impl == "cusolver":
+        run_cusolver(a)
     else:
         run_bem(a)
 
