@@ -10,6 +10,13 @@
 // complex row) and B' rows (Re b, -Im b) / (Im b, Re b) interleaved over k.
 // Every operand is split x = hi + lo with hi, lo rounded to TF32 and the
 // product taken as hi*hi + hi*lo + lo*hi, accumulated in FP32 in TMEM.
+// With the context option tensor_split = 1 the parts are FP16 instead (the
+// same 11 significant bits as TF32, at twice the tensor rate): each row of A'
+// and each complex column of B is first scaled by a power of two that brings
+// its largest part into [2^14, 2^15), so no part overflows FP16 and the parts
+// of small entries that fall below FP16's normal range lose at most 2^-38 of
+// the row's largest entry; the epilogue multiplies the accumulator by the
+// inverse scales of its row and column (exact: powers of two).
 //
 // Pack kernels write the hi / lo operands K-major; the GEMM kernel streams
 // 128 x 32 (A) and 256 x 32 (B) float tiles with TMA (128-byte swizzle, no
@@ -19,6 +26,7 @@
 // bounded (~1 s of clock cycles): on expiry the kernel records
 // BEM_ERR_TIMEOUT in the status word, frees its TMEM and returns.
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
@@ -113,6 +121,21 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// kind::f16 with FP16 A and B (both the same type), FP32 accumulate, K-major,
+// M = 128, N = 256; one MMA covers K = 16 halves = 32 bytes of a swizzle row,
+// the same byte step as K = 8 of kind::tf32.
+constexpr uint32_t IDESC_F16 = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC_F16), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -318,11 +341,17 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// F16: operand parts are FP16 (kind::f16, 64 halves per 128-byte stage row)
+// and sa / sb hold the (scale, inverse) pairs of the rows of A' and the
+// complex columns of B; else TF32 parts (kind::tf32, 32 floats per row).
+template <bool F16>
 __global__ void __launch_bounds__(192, 1)
 gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                        const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
                        float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int lower,
-                       int store, int group_m, int* status) {
+                       int store, int group_m, int* status, const float2* __restrict__ sa,
+                       const float2* __restrict__ sb) {
+    constexpr int BKE = F16 ? 2 * BK : BK;  // elements of K per stage (one 128-byte row)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
@@ -335,7 +364,7 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     __shared__ int issued_total, consumed_total;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nk = (K2 + BK - 1) / BK;
+    const int nk = (K2 + BKE - 1) / BKE;
     TileMap tm;
     tm.num_m = (M + BM - 1) / BM;
     tm.num_n = (2 * Nc + BN - 1) / BN;
@@ -379,10 +408,10 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                     unsigned char* st = smem + s * STAGE_BYTES;
                     const uint32_t fb = smem_u32(&full[s]);
                     mbar_expect_tx(fb, STAGE_BYTES);
-                    tma_load_2d(smem_u32(st), &tA_hi, kt * BK, mt * BM, fb);
-                    tma_load_2d(smem_u32(st + A_BYTES), &tA_lo, kt * BK, mt * BM, fb);
-                    tma_load_2d(smem_u32(st + 2 * A_BYTES), &tB_hi, kt * BK, ntl * BN, fb);
-                    tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tB_lo, kt * BK, ntl * BN, fb);
+                    tma_load_2d(smem_u32(st), &tA_hi, kt * BKE, mt * BM, fb);
+                    tma_load_2d(smem_u32(st + A_BYTES), &tA_lo, kt * BKE, mt * BM, fb);
+                    tma_load_2d(smem_u32(st + 2 * A_BYTES), &tB_hi, kt * BKE, ntl * BN, fb);
+                    tma_load_2d(smem_u32(st + 2 * A_BYTES + B_BYTES), &tB_lo, kt * BKE, ntl * BN, fb);
                     issued_total = it + 1;
                 }
             }
@@ -417,9 +446,15 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                         const uint32_t off = ks * 32;
                         const uint64_t dah = smem_desc(a_hi + off), dal = smem_desc(a_lo + off);
                         const uint64_t dbh = smem_desc(b_hi + off), dbl = smem_desc(b_lo + off);
-                        mma_tf32(acc, dah, dbh, (kt > 0 || ks > 0) ? 1u : 0u);
-                        mma_tf32(acc, dah, dbl, 1u);
-                        mma_tf32(acc, dal, dbh, 1u);
+                        if (F16) {
+                            mma_f16(acc, dah, dbh, (kt > 0 || ks > 0) ? 1u : 0u);
+                            mma_f16(acc, dah, dbl, 1u);
+                            mma_f16(acc, dal, dbh, 1u);
+                        } else {
+                            mma_tf32(acc, dah, dbh, (kt > 0 || ks > 0) ? 1u : 0u);
+                            mma_tf32(acc, dah, dbl, 1u);
+                            mma_tf32(acc, dal, dbh, 1u);
+                        }
                     }
                     mma_commit(smem_u32(&empty[s]));
                     consumed_total = it + 1;
@@ -480,6 +515,16 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
                 tmem_ld32(base + ch * 32, v);
                 const int c0 = ntl * (BN / 2) + ch * 16;
                 if (row < M && c0 < Nc) {
+                    if (F16) {
+                        // undo the row and column scales (powers of two: exact)
+                        const float ra = sa[row].y;
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const float f = c0 + j < Nc ? ra * sb[c0 + j].y : 0.f;
+                            v[2 * j] *= f;
+                            v[2 * j + 1] *= f;
+                        }
+                    }
                     if (!c_colmajor) {
                         float2* p = &C[(int64_t)row * ldc + c0];
                         const bool vec = ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (c0 + 16 <= Nc);
@@ -636,6 +681,146 @@ __global__ void pack_b_row_kernel(const float2* __restrict__ B, int64_t ldb, int
     }
 }
 
+// ---------------------------------------------------------------- FP16 split
+// Scale of one operand row (A') or complex column (B): the power of two s
+// with s * max(|Re|, |Im|) in [2^14, 2^15), stored with its inverse as
+// sc[t] = (s, 1/s).  Element k of item t is X[t * si + k * sk], times
+// dsc[k * dstride] when dsc is given (the D of an L D L^T update, applied as
+// the pack kernel applies it).  per_warp: one warp per item, lanes over k
+// (k contiguous); else one thread per item (items contiguous).
+__global__ void f16_scale_kernel(const float2* __restrict__ X, int64_t si, int64_t sk, int n, int K,
+                                 const float2* __restrict__ dsc, int64_t dstride, int per_warp,
+                                 float2* __restrict__ sc) {
+    float m = 0.f;
+    int t;
+    int k0 = 0, kstep = 1;
+    if (per_warp) {
+        t = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+        k0 = threadIdx.x & 31;
+        kstep = 32;
+    } else {
+        t = (int)((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+    }
+    if (t < n) {
+        for (int k = k0; k < K; k += kstep) {
+            float2 x = X[(int64_t)t * si + (int64_t)k * sk];
+            if (dsc) {
+                const float2 d = dsc[(int64_t)k * dstride];
+                x = make_float2(x.x * d.x - x.y * d.y, x.x * d.y + x.y * d.x);
+            }
+            m = fmaxf(m, fmaxf(fabsf(x.x), fabsf(x.y)));
+        }
+    }
+    if (per_warp) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) != 0) return;
+    }
+    if (t >= n) return;
+    float sv = 1.f, inv = 1.f;
+    if (m > 0.f && m <= 3.0e38f) {
+        int e;
+        frexpf(m, &e);  // m = f 2^e, f in [0.5, 1)
+        e = max(e, -100);
+        sv = ldexpf(1.f, 15 - e);
+        inv = ldexpf(1.f, e - 15);
+    }
+    sc[t] = make_float2(sv, inv);
+}
+
+__device__ __forceinline__ void split_h(float x, __half& h, __half& l) {
+    h = __float2half_rn(x);
+    l = __float2half_rn(x - __half2float(h));
+}
+
+// The FP16 counterparts of the four pack kernels above: same layouts, each
+// value multiplied by its row's (A) or column's (B) scale first.
+__global__ void pack_a_h_kernel(const float2* __restrict__ A, int64_t lda, int M, int K, __half* __restrict__ hi,
+                                __half* __restrict__ lo, int ld, const float2* __restrict__ sc) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t tot = (int64_t)M * (ld / 2);
+    if (t >= tot) return;
+    int i = (int)(t / (ld / 2)), k = (int)(t % (ld / 2));
+    float2 a = k < K ? A[(int64_t)i * lda + k] : make_float2(0.f, 0.f);
+    const float s = sc[i].x;
+    __half h0, h1, l0, l1;
+    split_h(a.x * s, h0, l0);
+    split_h(a.y * s, h1, l1);
+    reinterpret_cast<__half2*>(hi + (int64_t)i * ld)[k] = __halves2half2(h0, h1);
+    reinterpret_cast<__half2*>(lo + (int64_t)i * ld)[k] = __halves2half2(l0, l1);
+}
+
+__global__ void pack_a_trans_h_kernel(const float2* __restrict__ At, int64_t lda, int M, int K,
+                                      __half* __restrict__ hi, __half* __restrict__ lo, int ld,
+                                      const float2* __restrict__ sc) {
+    __shared__ float2 tile[32][33];
+    const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        int k = k0 + r, i = i0 + tx;
+        tile[r][tx] = (k < K && i < M) ? At[(int64_t)k * lda + i] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        int i = i0 + r, k = k0 + tx;
+        if (i >= M || k >= ld / 2) continue;
+        float2 a = tile[tx][r];
+        const float s = sc[i].x;
+        __half h0, h1, l0, l1;
+        split_h(a.x * s, h0, l0);
+        split_h(a.y * s, h1, l1);
+        reinterpret_cast<__half2*>(hi + (int64_t)i * ld)[k] = __halves2half2(h0, h1);
+        reinterpret_cast<__half2*>(lo + (int64_t)i * ld)[k] = __halves2half2(l0, l1);
+    }
+}
+
+__global__ void pack_b_col_h_kernel(const float2* __restrict__ B, int64_t ldb, int N, int K, __half* __restrict__ hi,
+                                    __half* __restrict__ lo, int ld, const float2* __restrict__ dsc,
+                                    int64_t dstride, const float2* __restrict__ sc) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t tot = (int64_t)N * (ld / 2);
+    if (t >= tot) return;
+    int j = (int)(t / (ld / 2)), k = (int)(t % (ld / 2));
+    float2 b = k < K ? B[(int64_t)j * ldb + k] : make_float2(0.f, 0.f);
+    if (dsc && k < K) {
+        const float2 d = dsc[(int64_t)k * dstride];
+        b = make_float2(b.x * d.x - b.y * d.y, b.x * d.y + b.y * d.x);
+    }
+    const float s = sc[j].x;
+    __half hr, hm, lr, lm;
+    split_h(b.x * s, hr, lr);
+    split_h(b.y * s, hm, lm);
+    reinterpret_cast<__half2*>(hi + (int64_t)(2 * j) * ld)[k] = __halves2half2(hr, __hneg(hm));
+    reinterpret_cast<__half2*>(hi + (int64_t)(2 * j + 1) * ld)[k] = __halves2half2(hm, hr);
+    reinterpret_cast<__half2*>(lo + (int64_t)(2 * j) * ld)[k] = __halves2half2(lr, __hneg(lm));
+    reinterpret_cast<__half2*>(lo + (int64_t)(2 * j + 1) * ld)[k] = __halves2half2(lm, lr);
+}
+
+__global__ void pack_b_row_h_kernel(const float2* __restrict__ B, int64_t ldb, int N, int K, __half* __restrict__ hi,
+                                    __half* __restrict__ lo, int ld, const float2* __restrict__ sc) {
+    __shared__ float2 tile[32][33];
+    const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8) {
+        int k = k0 + r, j = j0 + tx;
+        tile[r][tx] = (k < K && j < N) ? B[(int64_t)k * ldb + j] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        int j = j0 + r, k = k0 + tx;
+        if (j >= N || k >= ld / 2) continue;
+        float2 b = tile[tx][r];
+        const float s = sc[j].x;
+        __half hr, hm, lr, lm;
+        split_h(b.x * s, hr, lr);
+        split_h(b.y * s, hm, lm);
+        reinterpret_cast<__half2*>(hi + (int64_t)(2 * j) * ld)[k] = __halves2half2(hr, __hneg(hm));
+        reinterpret_cast<__half2*>(hi + (int64_t)(2 * j + 1) * ld)[k] = __halves2half2(hm, hr);
+        reinterpret_cast<__half2*>(lo + (int64_t)(2 * j) * ld)[k] = __halves2half2(lr, __hneg(lm));
+        reinterpret_cast<__half2*>(lo + (int64_t)(2 * j + 1) * ld)[k] = __halves2half2(lm, lr);
+    }
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------- host side
@@ -652,12 +837,16 @@ static int tc_encode_init(bem_ctx* ctx) {
     return BEM_OK;
 }
 
-static int make_map(bem_ctx* ctx, CUtensorMap* map, float* base, int rows, int ld, int box_rows) {
+// One operand plane: rows x ld elements (FP32, or FP16 when f16), rows of
+// 128 bytes per box (32 floats or 64 halves), 128-byte swizzle.
+static int make_map(bem_ctx* ctx, CUtensorMap* map, void* base, int rows, int ld, int box_rows, bool f16 = false) {
+    const int esz = f16 ? 2 : 4;
     cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
-    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * esz};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / esz), (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
-    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, es,
+    CUresult r = g_encode(map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base,
+                           dims, strides, box, es,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(ctx, BEM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -674,10 +863,16 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
     if (o.lower && (M != N || c_colmajor)) return fail(ctx, BEM_ERR_INVALID, "tc gemm: lower needs square row-major C");
     if (o.bscale && b_rowmajor) return fail(ctx, BEM_ERR_INVALID, "tc gemm: B scaling needs column-major B");
     BEM_TRY(tc_encode_init(ctx));
-    // K-major operand rows padded to a multiple of 32 floats (128 B)
-    const int ld = ((2 * K + tc::BK - 1) / tc::BK) * tc::BK;
+    // FP16 parts need the persistent kernel; the one-CTA-per-tile kernel keeps TF32
+    const bool f16 = ctx->tc_split == 1 && ctx->tc_persistent;
+    const size_t esz = f16 ? 2 : 4;
+    const int bke = f16 ? 2 * tc::BK : tc::BK;  // elements per 128-byte row
+    // K-major operand rows padded to a multiple of 128 bytes
+    const int ld = ((2 * K + bke - 1) / bke) * bke;
     size_t a_elems = (size_t)M * ld, b_elems = (size_t)2 * N * ld;
-    size_t need = 2 * (a_elems + b_elems) * sizeof(float) + 1024;
+    const size_t planes = 2 * (a_elems + b_elems) * esz;
+    const size_t sc_off = (planes + 255) & ~(size_t)255;
+    size_t need = (f16 ? sc_off + (size_t)(M + N) * sizeof(float2) : planes) + 1024;
     if (need > ctx->tc_bytes) {
         if (ctx->tc_buf) {
             BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -688,38 +883,79 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
         BEM_TRY_CUDA(ctx, cudaMalloc(&ctx->tc_buf, need));
         ctx->tc_bytes = need;
     }
-    float* a_hi = ctx->tc_buf;
-    float* a_lo = a_hi + a_elems;
-    float* b_hi = a_lo + a_elems;
-    float* b_lo = b_hi + b_elems;
+    char* base = reinterpret_cast<char*>(ctx->tc_buf);
+    void* a_hi = base;
+    void* a_lo = base + a_elems * esz;
+    void* b_hi = base + 2 * a_elems * esz;
+    void* b_lo = base + (2 * a_elems + b_elems) * esz;
+    float2* sc_a = f16 ? reinterpret_cast<float2*>(base + sc_off) : nullptr;
+    float2* sc_b = f16 ? sc_a + M : nullptr;
     cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
-    if (o.a_trans) {
-        dim3 g((M + 31) / 32, (ld / 2 + 31) / 32);
-        tc::pack_a_trans_kernel<<<g, 256, 0, ctx->stream>>>(A, lda, M, K, a_hi, a_lo, ld);
+    if (f16) {
+        // scales: rows of A (k contiguous unless A comes transposed), complex columns of B
+        if (o.a_trans)
+            tc::f16_scale_kernel<<<(M + 255) / 256, 256, 0, ctx->stream>>>(A, 1, lda, M, K, nullptr, 0, 0, sc_a);
+        else
+            tc::f16_scale_kernel<<<(unsigned)(((int64_t)M * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                A, lda, 1, M, K, nullptr, 0, 1, sc_a);
+        BEM_LAUNCHED(ctx);
+        if (b_rowmajor)
+            tc::f16_scale_kernel<<<(N + 255) / 256, 256, 0, ctx->stream>>>(B, 1, ldb, N, K, nullptr, 0, 0, sc_b);
+        else
+            tc::f16_scale_kernel<<<(unsigned)(((int64_t)N * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                B, ldb, 1, N, K, o.bscale, o.bscale_stride, 1, sc_b);
+        BEM_LAUNCHED(ctx);
+        __half *ah = (__half*)a_hi, *al = (__half*)a_lo, *bh = (__half*)b_hi, *bl = (__half*)b_lo;
+        if (o.a_trans) {
+            dim3 g((M + 31) / 32, (ld / 2 + 31) / 32);
+            tc::pack_a_trans_h_kernel<<<g, 256, 0, ctx->stream>>>(A, lda, M, K, ah, al, ld, sc_a);
+        } else {
+            int64_t tot = (int64_t)M * (ld / 2);
+            tc::pack_a_h_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, M, K, ah, al, ld,
+                                                                                       sc_a);
+        }
+        BEM_LAUNCHED(ctx);
+        if (b_rowmajor) {
+            dim3 g((N + 31) / 32, (ld / 2 + 31) / 32);
+            tc::pack_b_row_h_kernel<<<g, 256, 0, ctx->stream>>>(B, ldb, N, K, bh, bl, ld, sc_b);
+        } else {
+            int64_t tot = (int64_t)N * (ld / 2);
+            tc::pack_b_col_h_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
+                B, ldb, N, K, bh, bl, ld, o.bscale, o.bscale_stride, sc_b);
+        }
         BEM_LAUNCHED(ctx);
     } else {
-        int64_t tot = (int64_t)M * (ld / 2);
-        tc::pack_a_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, M, K, a_hi, a_lo, ld);
+        float *ah = (float*)a_hi, *al = (float*)a_lo, *bh = (float*)b_hi, *bl = (float*)b_lo;
+        if (o.a_trans) {
+            dim3 g((M + 31) / 32, (ld / 2 + 31) / 32);
+            tc::pack_a_trans_kernel<<<g, 256, 0, ctx->stream>>>(A, lda, M, K, ah, al, ld);
+            BEM_LAUNCHED(ctx);
+        } else {
+            int64_t tot = (int64_t)M * (ld / 2);
+            tc::pack_a_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(A, lda, M, K, ah, al, ld);
+            BEM_LAUNCHED(ctx);
+        }
+        if (b_rowmajor) {
+            dim3 g((N + 31) / 32, (ld / 2 + 31) / 32);
+            tc::pack_b_row_kernel<<<g, 256, 0, ctx->stream>>>(B, ldb, N, K, bh, bl, ld);
+        } else {
+            int64_t tot = (int64_t)N * (ld / 2);
+            tc::pack_b_col_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, N, K, bh, bl, ld,
+                                                                                         o.bscale, o.bscale_stride);
+        }
         BEM_LAUNCHED(ctx);
     }
-    if (b_rowmajor) {
-        dim3 g((N + 31) / 32, (ld / 2 + 31) / 32);
-        tc::pack_b_row_kernel<<<g, 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld);
-    } else {
-        int64_t tot = (int64_t)N * (ld / 2);
-        tc::pack_b_col_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(B, ldb, N, K, b_hi, b_lo, ld,
-                                                                                     o.bscale, o.bscale_stride);
-    }
-    BEM_LAUNCHED(ctx);
     CUtensorMap mah, mal, mbh, mbl;
-    BEM_TRY(make_map(ctx, &mah, a_hi, M, ld, tc::BM));
-    BEM_TRY(make_map(ctx, &mal, a_lo, M, ld, tc::BM));
-    BEM_TRY(make_map(ctx, &mbh, b_hi, 2 * N, ld, tc::BN));
-    BEM_TRY(make_map(ctx, &mbl, b_lo, 2 * N, ld, tc::BN));
+    BEM_TRY(make_map(ctx, &mah, a_hi, M, ld, tc::BM, f16));
+    BEM_TRY(make_map(ctx, &mal, a_lo, M, ld, tc::BM, f16));
+    BEM_TRY(make_map(ctx, &mbh, b_hi, 2 * N, ld, tc::BN, f16));
+    BEM_TRY(make_map(ctx, &mbl, b_lo, 2 * N, ld, tc::BN, f16));
     if (!ctx->tc_attr) {
         BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                tc::SMEM_BYTES));
-        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_persistent_kernel,
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_persistent_kernel<false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_persistent_kernel<true>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
         ctx->tc_attr = true;
     }
@@ -727,10 +963,10 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
         const int nm = (M + tc::BM - 1) / tc::BM;
         const int ntiles = o.lower ? nm * (nm + 1) / 2 : nm * ((2 * N + tc::BN - 1) / tc::BN);
         const int grid = std::min(ntiles, ctx->sm_count);
-        tc::gemm_persistent_kernel<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc,
-                                                                                c_colmajor ? 1 : 0, M, N, ld,
-                                                                                o.lower ? 1 : 0, o.store ? 1 : 0,
-                                                                                ctx->tc_group_m, ctx->d_status);
+        auto kern = f16 ? tc::gemm_persistent_kernel<true> : tc::gemm_persistent_kernel<false>;
+        kern<<<grid, 192, tc::SMEM_BYTES, ctx->stream>>>(mah, mal, mbh, mbl, C, ldc, c_colmajor ? 1 : 0, M, N, ld,
+                                                         o.lower ? 1 : 0, o.store ? 1 : 0, ctx->tc_group_m,
+                                                         ctx->d_status, sc_a, sc_b);
     } else {
         dim3 grid((2 * N + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
         if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "tc gemm: M too large");

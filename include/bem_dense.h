@@ -107,7 +107,14 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * "assembly_kernel" (0, default: triangle-pair moments over Morton-ordered
  * tiles; 1: one thread per RWG pair, the reference's organisation),
  * "farfield_kernel" (0, default: phases shared by the RWG halves of a
- * triangle; 1: per RWG-half point).  Unknown names give BEM_ERR_INVALID. */
+ * triangle; 1: per RWG-half point), "tensor_split" (1, default: FP32
+ * operands of the tensor-core GEMM split into two FP16 parts after a
+ * power-of-two scale per operand row / column that brings its largest part
+ * into [2^14, 2^15), kind::f16 at twice the TF32 rate, the persistent GEMM
+ * only; 0: into two TF32 parts, kind::tf32.  Both give FP32-class products;
+ * with FP16 parts an entry below about 2^-18 of its row's (column's) largest
+ * keeps fewer than 22 significant bits).  Unknown names give
+ * BEM_ERR_INVALID. */
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
@@ -370,7 +377,9 @@ int bem_amplitude_to_mueller(const double* S1, const double* S2, const double* S
  * use and testing: C -= A B with complex64 device buffers.  A: M x K with K
  * contiguous (A[i*lda + k]); B: K x N, b_rowmajor ? B[k*ldb + j] :
  * B[j*ldb + k]; C: M x N, c_colmajor ? C[j*ldc + i] : C[i*ldc + j].
- * Products are 3xTF32 (hi*hi + hi*lo + lo*hi), FP32 accumulation. */
+ * Products are hi*hi + hi*lo + lo*hi with FP32 accumulation; the parts are
+ * FP16 after power-of-two row / column scaling, or TF32 with the context
+ * option tensor_split = 0 (the name keeps the original TF32 form). */
 int bem_cgemm_tf32x3(bem_ctx* ctx, int M, int N, int K, const void* A, int64_t lda, const void* B,
                      int64_t ldb, int b_rowmajor, void* C, int64_t ldc, int c_colmajor);
 

@@ -15,8 +15,10 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def ctx():
+    # the TF32 split (tensor_split 0); the FP16 split has its own tests
     import bem_b200 as bb
     c = bb.Context(0)
+    bb.set_option(c, "tensor_split", 0)
     yield c
     c.close()
 
