@@ -824,7 +824,9 @@ def c4_particles(seed, count=64, orient=(4, 4, 1), ntheta=181, precision=PREC_FP
 
 
 def cgemm_tf32x3(ctx: Context, A, B, C, b_rowmajor=True, c_colmajor=False):
-    """C -= A B on the tensor cores (3xTF32), torch complex64 device tensors.
+    """C -= A B on the tensor cores, torch complex64 device tensors: three
+    products of two-part operands, FP16 parts after power-of-two row / column
+    scaling (default) or TF32 parts (set_option(ctx, "tensor_split", 0)).
     A: (M, K) row-major; B: (K, N) row-major if b_rowmajor else given as its
     transpose (N, K) row-major; C: (M, N) row-major, or (N, M) if c_colmajor."""
     M, K = A.shape
