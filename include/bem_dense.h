@@ -350,8 +350,7 @@ int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev,
                              int gamma_mirror, double* M_avg, double* M_orient_dev);
 
 /* Allocation-free variant of bem_farfield_mueller_dev, with no counterpart in
- * the reference.  For callers that cannot allocate device memory: code
- * running inside CUDA stream capture, where cudaMalloc is not allowed, and
+ * the reference.  For callers that cannot allocate device memory, such as
  * hosts whose device memory belongs to their own allocator (a serving stack
  * with a fixed pool).  Its only scratch (staged orientations, per-orientation
  * Mueller terms) is a file-scope device array of BEM_NOALLOC_SCRATCH_BYTES,
@@ -361,8 +360,7 @@ int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev,
  * partial results (the average is a weighted sum).  RT, w: host arrays as in
  * bem_farfield_mueller_dev.  M_avg_dev: caller's device buffer of 16*ntheta
  * doubles, written on the context's stream.  The first call on a device looks
- * up the scratch address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls share the one array: calls that overlap on
+ * up the scratch address (cudaGetSymbolAddress).  All calls share the one array: calls that overlap on
  * the GPU (different streams or contexts on one device) race on it. */
 #define BEM_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 int bem_farfield_mueller_noalloc(bem_ctx* ctx, const bem_geom* g, const void* X_dev, int64_t ldx,

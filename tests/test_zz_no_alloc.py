@@ -1,8 +1,7 @@
 """The allocation-free Mueller entry point (bem_farfield_mueller_noalloc).
 
-It exists for callers that cannot allocate device memory: code running
-inside CUDA stream capture, where cudaMalloc is not allowed, and hosts whose
-device memory is owned by their own allocator.  Its scratch is a static device
+It exists for callers that cannot allocate device memory, such as hosts
+whose device memory is owned by their own allocator.  Its scratch is a static device
 array shared by all calls, so this file checks it against the allocating
 entry point (bem_farfield_mueller_dev) over the C ABI on two calls in a row
 with different orientation sets: a stale second call would show there.  The
