@@ -39,6 +39,20 @@ def make_mesh(kind: str, param: float, ref: int):
     return _fetch(nv.value, nt.value, nr.value)
 
 
+def load_obj(path):
+    """The reference's load_obj on an existing file -> (verts, tris).  Its
+    counts of removed degenerate triangles and of non-manifold edges go to
+    stderr (mesh.cpp:220-245)."""
+    L = lib()
+    nv, nt = C.c_int(), C.c_int()
+    L.ref_load_obj.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.ref_load_obj(str(path).encode(), C.byref(nv), C.byref(nt))
+    verts = np.zeros((nv.value, 3))
+    tris = np.zeros((nt.value, 3), dtype=np.int32)
+    L.ref_get_mesh(_p(verts), _p(tris))
+    return verts, tris
+
+
 def _fetch(nv, nt, nr):
     L = lib()
     verts = np.zeros((nv, 3))

@@ -28,6 +28,17 @@ int ref_make_mesh(int kind, double param, int ref, int* nv, int* nt, int* nrwg) 
     return 0;
 }
 
+// load_obj (mesh.cpp:156-250) into the current mesh.  No RWG is built (the
+// file may hold a non-manifold mesh); the reference reports the removed
+// degenerate triangles and the non-manifold edges on stderr only.  The file
+// must exist: the reference exits on a missing one.
+int ref_load_obj(const char* path, int* nv, int* nt) {
+    g_mesh = load_obj(path);
+    *nv = g_mesh.nv();
+    *nt = g_mesh.nt();
+    return 0;
+}
+
 int ref_subdivide_flat(void) {
     g_mesh = subdivide_flat(g_mesh);
     g_rwg = build_rwg(g_mesh);

@@ -97,6 +97,47 @@ def test_load_obj_removes_degenerates(tmp_path):
     assert np.abs(v2 - v).max() < 1e-15
 
 
+def test_load_obj_matches_the_reference(tmp_path, capfd):
+    # quads (fan-triangulated), a repeated-vertex face, a zero-area face of
+    # three collinear vertices and a fin: a third triangle on an existing edge
+    import re
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("reference host library not built")
+    v, t = bb.hex_prism(1.0, 0)
+    extra = np.array([[0.0, 0.0, 5.0], [1.0, 1.0, 5.0], [2.0, 2.0, 5.0], [0.3, 0.2, 3.0]])
+    nv0 = len(v)
+    p = tmp_path / "m.obj"
+    with open(p, "w") as f:
+        f.write("# test mesh\n")
+        for x in np.vstack([v, extra]):
+            f.write(f"v {x[0]:.17g} {x[1]:.17g} {x[2]:.17g}\n")
+        tl = [list(x) for x in t]
+        # the first two triangles written as one quad when they share an edge
+        a, b = tl[0], tl[1]
+        shared = [x for x in a if x in b]
+        if len(shared) == 2:
+            (oa,), (ob,) = [x for x in a if x not in shared], [x for x in b if x not in shared]
+            i = a.index(oa)
+            quad = [a[i], a[(i + 1) % 3], ob, a[(i + 2) % 3]]
+            f.write("f " + " ".join(f"{q + 1}/{q + 1}" for q in quad) + "\n")
+            tl = tl[2:]
+        for tri in tl:
+            f.write("f " + " ".join(str(q + 1) for q in tri) + "\n")
+        f.write(f"f {nv0 + 1} {nv0 + 1} {nv0 + 2}\n")            # repeated vertex
+        f.write(f"f {nv0 + 1} {nv0 + 2} {nv0 + 3}\n")            # collinear: zero area
+        e0, e1 = t[2][0], t[2][1]
+        f.write(f"f {e0 + 1} {e1 + 1} {nv0 + 4}\n")              # fin on an existing edge
+    capfd.readouterr()
+    vr, tr = ref_host.load_obj(p)
+    err = capfd.readouterr().err
+    nd_ref = int(re.search(r"removed (\d+) degenerate", err).group(1))
+    nm_ref = int(re.search(r"(\d+) non-manifold edges", err).group(1))
+    v2, t2, nd, nm = bb.load_obj(p)
+    assert np.array_equal(v2, vr) and np.array_equal(t2, tr)
+    assert (nd, nm) == (nd_ref, nm_ref) == (2, 1)
+
+
 @pytest.mark.parametrize("order", [4, 7, 13])
 def test_quadrature(order):
     import bem_b200 as bb
