@@ -434,7 +434,8 @@ int bem_mesh_normalize(double* verts, int nv, const int* tris, int nt, double* a
     if (a_eq < 1e-30) {
         double c[3] = {0, 0, 0}, r2 = 0;
         for (int i = 0; i < nv; i++)
-            for (int d = 0; d < 3; d++) c[d] += verts[3 * i + d] / nv;
+            for (int d = 0; d < 3; d++) c[d] += verts[3 * i + d];
+        for (int d = 0; d < 3; d++) c[d] /= nv;
         for (int i = 0; i < nv; i++) {
             double s = 0;
             for (int d = 0; d < 3; d++) s += (verts[3 * i + d] - c[d]) * (verts[3 * i + d] - c[d]);

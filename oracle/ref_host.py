@@ -53,6 +53,23 @@ def load_obj(path):
     return verts, tris
 
 
+def mesh_utils(verts, tris):
+    """The reference's mesh_volume, mesh_dmax and normalize_mesh on (verts,
+    tris) -> (volume, dmax, a_eq, normalised verts)."""
+    L = lib()
+    v = np.ascontiguousarray(verts, dtype=np.float64)
+    t = np.ascontiguousarray(tris, dtype=np.int32)
+    L.ref_set_mesh(_p(v), len(v), _p(t), len(t))
+    for f in (L.ref_mesh_volume, L.ref_mesh_dmax, L.ref_normalize_mesh):
+        f.restype = C.c_double
+    vol, dmax = L.ref_mesh_volume(), L.ref_mesh_dmax()
+    a_eq = L.ref_normalize_mesh()
+    vn = np.zeros_like(v)
+    tn = np.zeros_like(t)
+    L.ref_get_mesh(_p(vn), _p(tn))
+    return vol, dmax, a_eq, vn
+
+
 def _fetch(nv, nt, nr):
     L = lib()
     verts = np.zeros((nv, 3))

@@ -39,6 +39,19 @@ int ref_load_obj(const char* path, int* nv, int* nt) {
     return 0;
 }
 
+// Make (verts, tris) the current mesh (no RWG built).
+void ref_set_mesh(const double* verts, int nv, const int* tris, int nt) {
+    g_mesh = Mesh();
+    for (int i = 0; i < nv; i++) g_mesh.verts.push_back(Vec3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]));
+    g_mesh.tris.assign(tris, tris + 3 * nt);
+}
+
+// mesh_volume, mesh_dmax, normalize_mesh (mesh.cpp:252-294) of the current
+// mesh; normalize_mesh rescales it in place (fetch it with ref_get_mesh).
+double ref_mesh_volume(void) { return mesh_volume(g_mesh); }
+double ref_mesh_dmax(void) { return mesh_dmax(g_mesh); }
+double ref_normalize_mesh(void) { return normalize_mesh(g_mesh); }
+
 int ref_subdivide_flat(void) {
     g_mesh = subdivide_flat(g_mesh);
     g_rwg = build_rwg(g_mesh);

@@ -138,6 +138,28 @@ def test_load_obj_matches_the_reference(tmp_path, capfd):
     assert (nd, nm) == (nd_ref, nm_ref) == (2, 1)
 
 
+@pytest.mark.parametrize("case", ["bumpy", "hex", "flat"])
+def test_mesh_utilities_match_the_reference(case):
+    # mesh_volume, mesh_dmax and normalize_mesh (with its bounding-sphere
+    # fallback for a zero-volume mesh) against the reference's own C++
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("reference host library not built")
+    if case == "bumpy":
+        v, t = bb.c5_mesh(3, refinements=2, rms=0.1)
+    elif case == "hex":
+        v, t = bb.hex_prism(0.6, 2)
+        v = 3.7 * v + np.array([0.3, -1.1, 2.0])
+    else:
+        v = np.array([[0.0, 0.0, 0.0], [2.0, 0.0, 0.0], [0.0, 1.5, 0.0], [1.0, 1.0, 0.0]])
+        t = np.array([[0, 1, 2], [1, 3, 2]])
+    vol, dmax, a_eq, vn = ref_host.mesh_utils(v, t)
+    assert bb.mesh_volume(v, t) == vol
+    assert bb.mesh_dmax(v) == dmax
+    v2, a2 = bb.normalize_mesh(v, t)
+    assert a2 == a_eq and np.array_equal(v2, vn)
+
+
 @pytest.mark.parametrize("order", [4, 7, 13])
 def test_quadrature(order):
     import bem_b200 as bb
