@@ -70,6 +70,22 @@ def mesh_utils(verts, tris):
     return vol, dmax, a_eq, vn
 
 
+def tri_quadrature(order):
+    """The reference's tri_quadrature(order) -> (pts (n, 2), wts (n,))."""
+    pts, wts = np.zeros(50), np.zeros(25)
+    n = lib().ref_tri_quadrature(int(order), _p(pts), _p(wts))
+    return pts[:2 * n].reshape(n, 2), wts[:n]
+
+
+def write_json(path, M, theta, ka, n_re, n_im, refinements, orient, times):
+    """The reference's write_json; M (4, 4, ntheta), theta in radians."""
+    Mf = np.ascontiguousarray(M, dtype=np.float64).reshape(-1)
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    d = C.c_double
+    lib().ref_write_json(str(path).encode(), _p(Mf), _p(th), len(th), d(ka), d(n_re), d(n_im), int(refinements),
+                         int(orient[0]), int(orient[1]), int(orient[2]), *[d(x) for x in times])
+
+
 def _fetch(nv, nt, nr):
     L = lib()
     verts = np.zeros((nv, 3))

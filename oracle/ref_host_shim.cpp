@@ -9,6 +9,8 @@
 #include "rhs.h"
 #include "orient.h"
 #include "graglia.h"
+#include "output.h"
+#include "quadrature.h"
 #include <cstring>
 #include <vector>
 
@@ -51,6 +53,25 @@ void ref_set_mesh(const double* verts, int nv, const int* tris, int nt) {
 double ref_mesh_volume(void) { return mesh_volume(g_mesh); }
 double ref_mesh_dmax(void) { return mesh_dmax(g_mesh); }
 double ref_normalize_mesh(void) { return normalize_mesh(g_mesh); }
+
+// tri_quadrature (quadrature.h:14-70), unknown orders included.
+int ref_tri_quadrature(int order, double* pts, double* wts) {
+    TriQuad q = tri_quadrature(order);
+    for (int i = 0; i < q.npts; i++) {
+        pts[2 * i] = q.pts[i][0];
+        pts[2 * i + 1] = q.pts[i][1];
+        wts[i] = q.wts[i];
+    }
+    return q.npts;
+}
+
+// write_json (output.cpp:5-64).
+void ref_write_json(const char* filename, const double* M, const double* theta, int ntheta, double ka,
+                    double n_re, double n_im, int refinements, int na, int nb, int ng, double t_asm,
+                    double t_solve, double t_ff, double t_total) {
+    write_json(filename, M, theta, ntheta, ka, n_re, n_im, refinements, na, nb, ng, t_asm, t_solve, t_ff,
+               t_total);
+}
 
 int ref_subdivide_flat(void) {
     g_mesh = subdivide_flat(g_mesh);

@@ -169,6 +169,47 @@ def test_quadrature(order):
     assert abs(w.sum() - 1.0) < 1e-12
 
 
+@pytest.mark.parametrize("order", [4, 7, 13, 5])
+def test_quadrature_matches_the_reference_cpp(order):
+    # the C ABI rejects an unknown order; the drop-in C++ header falls back to
+    # the 7-point rule as the reference does
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("reference host library not built")
+    pr, wr = ref_host.tri_quadrature(order)
+    p, w = bb.tri_quadrature(order if order in (4, 7, 13) else 7)
+    assert np.array_equal(p, pr) and np.array_equal(w, wr)
+
+
+def test_write_json_matches_the_reference_bytewise(tmp_path):
+    # the JSON of the drop-in write_json (libbem_compat.so) against the
+    # reference's output.cpp for the same inputs: cluster_bem.py parses it
+    import ctypes as C
+    import os
+    if not ref_host.available():
+        pytest.skip("reference host library not built")
+    so = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "bem-cpp_b200", "lib",
+                      "libbem_compat.so")
+    if not os.path.exists(so):
+        pytest.skip("libbem_compat.so not built")
+    rng = np.random.default_rng(4)
+    nt = 19
+    M = rng.standard_normal((4, 4, nt)) * 10.0 ** rng.uniform(-12, 3, (4, 4, nt))
+    M[0, 0, 3] = 0.0
+    M[1, 2, 5] = -0.0
+    theta = np.linspace(0.0, np.pi, nt)
+    args = dict(ka=5.123456789, n_re=1.3116, n_im=1e-4, refinements=3, orient=(8, 7, 2),
+                times=(1.234, 20.5, 0.999, 23.456))
+    ref_host.write_json(tmp_path / "ref.json", M, theta, **args)
+    lib = C.CDLL(so)
+    f = lib["_Z10write_jsonPKcPKdS2_idddiiiidddd"]      # write_json(const char*, const double*, ...)
+    d = C.c_double
+    Mf = np.ascontiguousarray(M.reshape(-1))
+    f(str(tmp_path / "ours.json").encode(), Mf.ctypes.data_as(C.c_void_p), theta.ctypes.data_as(C.c_void_p), nt,
+      d(args["ka"]), d(args["n_re"]), d(args["n_im"]), 3, 8, 7, 2, *[d(x) for x in args["times"]])
+    assert (tmp_path / "ours.json").read_bytes() == (tmp_path / "ref.json").read_bytes()
+
+
 def test_quadrature_rejects_unknown_order():
     import bem_b200 as bb
     with pytest.raises(bb.BemError):
