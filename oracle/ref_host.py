@@ -86,6 +86,27 @@ def write_json(path, M, theta, ka, n_re, n_im, refinements, orient, times):
                          int(orient[0]), int(orient[1]), int(orient[2]), *[d(x) for x in times])
 
 
+def farfield_cpu(cJ, cM, k_ext, eta_ext, r_hats, quad_order=7):
+    """compute_far_field_vec_batch_cpu on the mesh of the last make_mesh call:
+    cJ, cM (N,) complex, r_hats (ndir, 3) -> Fv (ndir, 3) complex."""
+    cJ = np.ascontiguousarray(cJ, dtype=np.complex128)
+    cM = np.ascontiguousarray(cM, dtype=np.complex128)
+    rh = np.ascontiguousarray(r_hats, dtype=np.float64)
+    Fv = np.zeros((len(rh), 3), dtype=np.complex128)
+    k = complex(k_ext)
+    lib().ref_farfield_cpu(int(quad_order), _p(cJ), _p(cM), C.c_double(k.real), C.c_double(k.imag),
+                           C.c_double(eta_ext), _p(rh), len(rh), _p(Fv))
+    return Fv
+
+
+def amplitude_to_mueller(S1, S2, S3, S4):
+    """The reference's amplitude_to_mueller -> M (4, 4, ntheta)."""
+    S = [np.ascontiguousarray(x, dtype=np.complex128) for x in (S1, S2, S3, S4)]
+    M = np.zeros(16 * len(S[0]))
+    lib().ref_amplitude_to_mueller(*[_p(x) for x in S], len(S[0]), _p(M))
+    return M.reshape(4, 4, -1)
+
+
 def _fetch(nv, nt, nr):
     L = lib()
     verts = np.zeros((nv, 3))

@@ -11,6 +11,7 @@
 #include "graglia.h"
 #include "output.h"
 #include "quadrature.h"
+#include "farfield.h"
 #include <cstring>
 #include <vector>
 
@@ -71,6 +72,29 @@ void ref_write_json(const char* filename, const double* M, const double* theta, 
                     double t_solve, double t_ff, double t_total) {
     write_json(filename, M, theta, ntheta, ka, n_re, n_im, refinements, na, nb, ng, t_asm, t_solve, t_ff,
                t_total);
+}
+
+// compute_far_field_vec_batch_cpu (farfield.cu:351-431) on the current mesh
+// and RWG: coefficients (N complex each), r_hats (ndir x 3) -> Fv (ndir x 3 complex).
+void ref_farfield_cpu(int quad_order, const double* cJ, const double* cM, double k_re, double k_im,
+                      double eta_ext, const double* r_hats, int ndir, double* Fv) {
+    FFCache cache;
+    cache.init(g_rwg, g_mesh, quad_order);
+    std::vector<Vec3> rh(ndir);
+    for (int d = 0; d < ndir; d++) rh[d] = Vec3(r_hats[3 * d], r_hats[3 * d + 1], r_hats[3 * d + 2]);
+    compute_far_field_vec_batch_cpu(cache, reinterpret_cast<const std::complex<double>*>(cJ),
+                                    reinterpret_cast<const std::complex<double>*>(cM),
+                                    std::complex<double>(k_re, k_im), eta_ext, rh.data(), ndir,
+                                    reinterpret_cast<std::complex<double>*>(Fv));
+}
+
+// amplitude_to_mueller (farfield.cu:464-508).
+void ref_amplitude_to_mueller(const double* S1, const double* S2, const double* S3, const double* S4,
+                              int ntheta, double* M) {
+    amplitude_to_mueller(reinterpret_cast<const std::complex<double>*>(S1),
+                         reinterpret_cast<const std::complex<double>*>(S2),
+                         reinterpret_cast<const std::complex<double>*>(S3),
+                         reinterpret_cast<const std::complex<double>*>(S4), ntheta, M);
 }
 
 int ref_subdivide_flat(void) {

@@ -49,3 +49,29 @@ def test_oracle_graglia_matches_reference_cpp():
     # 1e-6 in both, which amplifies rounding differences (3.5e-12 measured)
     assert worst_p < 1e-12, worst_p
     assert worst_v < 1e-10, worst_v
+
+
+@pytest.mark.parametrize("k,eta", [(4.0, 1.0), (complex(2.5, 0.03), 1.0)])
+def test_oracle_farfield_matches_reference_cpu_farfield(k, eta):
+    # the reference's own CPU far field (farfield.cu:351-431) on a hex prism in
+    # its RWG order, random coefficients, directions over the sphere
+    v, t, rwg = ref_host.make_mesh("hex", 0.8, 1)
+    N = rwg["N"]
+    rng = np.random.default_rng(9)
+    cJ = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    cM = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    rh = rng.standard_normal((25, 3))
+    rh /= np.linalg.norm(rh, axis=1, keepdims=True)
+    Fr = ref_host.farfield_cpu(cJ, cM, k, eta, rh, 7)
+    cache = bo.FarFieldCache(rwg, v, t, 7)
+    Fo = bo.far_field_vec(cache, cJ, cM, k, eta, rh)
+    assert np.abs(Fo - Fr).max() <= 1e-13 * np.abs(Fr).max()
+
+
+def test_amplitude_to_mueller_matches_reference_cpp():
+    import bem_b200 as bb
+    rng = np.random.default_rng(10)
+    S = [rng.standard_normal(37) + 1j * rng.standard_normal(37) for _ in range(4)]
+    Mr = ref_host.amplitude_to_mueller(*S)
+    assert np.array_equal(bb.amplitude_to_mueller(*S), Mr)
+    assert np.abs(bo.amplitude_to_mueller(*S) - Mr).max() <= 1e-15 * np.abs(Mr).max()
