@@ -1,0 +1,69 @@
+"""Host logic of bench.py on CPU: the clock record taken with nvidia-smi
+during the timed steps (here a stand-in nvidia-smi on PATH that prints the
+queried CSV columns), the peak fallback, the workload description and the
+command-line defaults the driver relies on."""
+import os
+import stat
+import sys
+import time
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+
+def _fake_smi(tmp_path, rows):
+    """A stand-in nvidia-smi that prints `rows` (CSV, the bench's query order)
+    then idles until it is terminated, as `-lms 200` would."""
+    script = tmp_path / "nvidia-smi"
+    body = "\n".join(f"echo '{r}'" for r in rows)
+    script.write_text(f"#!/bin/bash\n{body}\nexec sleep 30\n")
+    script.chmod(script.stat().st_mode | stat.S_IEXEC)
+    return str(tmp_path)
+
+
+@pytest.mark.parametrize("rows,expect", [
+    # idle samples before the load are left out of the median
+    (["0, 345, 1965, 120.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+      "0, 1500, 1965, 990.1, 0x4, Not Active, Not Active, Not Active, Active",
+      "0, 1492, 1965, 998.0, 0x4, Not Active, Not Active, Not Active, Active",
+      "0, 1485, 1965, 1001.2, 0x4, Not Active, Not Active, Not Active, Active"],
+     (1492.0, 1965.0, ["sw_power_cap"], 4)),
+    (["0, 1965, 1965, 700.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+      "0, 1800, 1965, 900.0, 0x40, Not Active, Active, Not Active, Not Active"],
+     (1882.5, 1965.0, ["hw_thermal_slowdown"], 2)),
+])
+def test_clock_sampler_reads_clocks_and_reasons(tmp_path, monkeypatch, rows, expect):
+    import bench
+    monkeypatch.setenv("PATH", _fake_smi(tmp_path, rows) + os.pathsep + os.environ["PATH"])
+    s = bench.ClockSampler(0)
+    time.sleep(0.5)
+    c = s.stop()
+    assert (c["sm_mhz"], c["sm_max_mhz"], c["reasons"], c["samples"]) == expect
+
+
+def test_clock_sampler_without_nvidia_smi(tmp_path, monkeypatch):
+    import bench
+    monkeypatch.setenv("PATH", str(tmp_path))
+    c = bench.ClockSampler(0).stop()
+    assert c["sm_mhz"] is None and c["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_peaks_fall_back_when_the_measured_file_is_absent(tmp_path, monkeypatch):
+    import bench
+    monkeypatch.setattr(bench, "REPO", str(tmp_path))
+    pk, basis = bench.peaks()
+    assert basis == "fallback" and pk["hbm_gbs"] == 6650.0 and pk["bf16_tflops"] == 1590.0
+
+
+def test_defaults_and_workload(monkeypatch):
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()
+    assert (a.gpus, a.warmup, a.impl, a.ref, tuple(a.orient), a.tensor_split) == (1, 3, "bem", 5, (45, 31, 1), 1)
+    assert a.warmup >= 3 and a.steps >= 1
+    w = bench.workload(a, 61440)
+    assert w["unknowns"] == 61440 and w["rhs"] == 2790 and "L2" in w["l2_policy"]
+    assert bench._n_rwg_ico(5) == 30720
