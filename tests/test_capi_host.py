@@ -242,3 +242,37 @@ def test_amplitude_to_mueller_host():
     rng = np.random.default_rng(3)
     S = [rng.standard_normal(17) + 1j * rng.standard_normal(17) for _ in range(4)]
     assert rel(bb.amplitude_to_mueller(*S), bo.amplitude_to_mueller(*S)) < 1e-15
+
+
+def _cli():
+    import os
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "bem-cpp_b200", "bin", "bem_cuda")
+    if not os.path.exists(p):
+        pytest.skip("bem_cuda not built")
+    return p
+
+
+def test_cli_accepts_every_reference_flag(tmp_path):
+    # every option of the reference's main.cpp:94-181 with its arguments; the
+    # missing OBJ file stops the run after parsing, before any device work
+    import subprocess
+    flags = ["--ka", "2", "--ri", "1.31", "0.001", "--ref", "2", "--orient", "4", "4", "1", "--ntheta", "19",
+             "--quad", "7", "--out", str(tmp_path / "r.json"), "--solver", "dense", "--prec", "none",
+             "--prec-r", "1.5", "--prec-bs", "64", "--prec-overlap", "1", "--digits", "3", "--gmres-tol", "1e-6",
+             "--gmres-restart", "50", "--max-leaf", "64", "--shape", "hex", "--ar", "1.2", "--orient-tol", "1e-4",
+             "--orient-sym", "1", "1", "--subdiv", "1", "--orient-range", "0", "4", "--single", "--gamma-mirror",
+             "--orient-auto", "3", "--goi", "--obj", str(tmp_path / "missing.obj")]
+    r = subprocess.run([_cli()] + flags, capture_output=True, text=True, timeout=60)
+    assert "Unknown option" not in r.stderr, r.stderr
+    assert r.returncode == 1 and "cannot open OBJ file" in r.stderr
+
+
+def test_cli_help_and_argument_errors():
+    import subprocess
+    for h in ("--help", "-h"):
+        r = subprocess.run([_cli(), h], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 0 and "--ka" in r.stdout and "--orient-range" in r.stdout
+    r = subprocess.run([_cli(), "--ka", "1", "--no-such-flag"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Unknown option: --no-such-flag" in r.stderr
+    r = subprocess.run([_cli(), "--ref", "2"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "--ka must be positive" in r.stderr
