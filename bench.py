@@ -451,7 +451,7 @@ def run_bem(a):
                   f"(B200 dense int8 rate = 2 x bf16)")
     else:
         peak = FP64_PEAK_TFS
-        pbasis = ("FP64: 37.0 TF/s measured on this pool (cuBLAS ZGEMM 8192^3; DFMA and m8n8k4 DMMA "
+        pbasis = ("FP64: 37.0 TF/s measured on B200 (cuBLAS ZGEMM 8192^3; DFMA and m8n8k4 DMMA "
                   "throughput probes 36-37 TF/s); MEASURED_PEAKS.json has no FP64 figure")
     traffic, tbasis = None, None
     if name in TRAFFIC_MODEL and (name != "residual" or a.residual_digits > 0):
