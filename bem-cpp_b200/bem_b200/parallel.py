@@ -45,6 +45,23 @@ def allreduce_max(x: float, device=None) -> float:
     return float(t.item())
 
 
+def raise_if_any_rank_failed(err, what):
+    """Every rank calls this after its local work, failed or not, so the
+    ranks take the same collective: one all_gather_object of the local error
+    (None or a message); if any rank failed, every rank raises RuntimeError
+    naming the first failed rank, instead of the others waiting in their next
+    collective until the process group's timeout."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        errs = [None] * dist.get_world_size()
+        dist.all_gather_object(errs, err)
+    else:
+        errs = [err]
+    for r, e in enumerate(errs):
+        if e is not None:
+            raise RuntimeError(f"{what}: rank {r} failed: {e}")
+
+
 def orientation_average_distributed(ctx, geom, Z, RT, w, k_ext, eta_ext, ntheta=181,
                                     precision=None, tol=0.0, rank=0, world=1, device=None):
     """Orientation-averaged Mueller matrix with the orientations split across
@@ -56,13 +73,17 @@ def orientation_average_distributed(ctx, geom, Z, RT, w, k_ext, eta_ext, ntheta=
         precision = PREC_FP32_REFINE
     o0, o1 = orientation_slice(len(w), rank, world)
     part = np.zeros((4, 4, ntheta))
-    stats = None
+    stats, err = None, None
     if o1 > o0:
-        B = api.rhs_planewave_dev(geom, k_ext, eta_ext, RT[o0:o1])
-        lu = api.LU(ctx, Z, precision)
-        X, stats = lu.solve(B, tol=tol)
-        lu.close()
-        part = api.mueller_from_solutions_dev(geom, X, RT[o0:o1], w[o0:o1], k_ext, eta_ext, ntheta)
+        try:
+            B = api.rhs_planewave_dev(geom, k_ext, eta_ext, RT[o0:o1])
+            lu = api.LU(ctx, Z, precision)
+            X, stats = lu.solve(B, tol=tol)
+            lu.close()
+            part = api.mueller_from_solutions_dev(geom, X, RT[o0:o1], w[o0:o1], k_ext, eta_ext, ntheta)
+        except Exception as ex:  # the collectives below are taken either way
+            err = f"{type(ex).__name__}: {ex}"
+    raise_if_any_rank_failed(err, "orientation_average_distributed")
     return allreduce_sum(part, device).reshape(4, 4, ntheta), stats
 
 
@@ -84,7 +105,12 @@ def batch_run_distributed(ctx, particles, rank=0, world=1, run=None):
         def run(ps):
             return api.batch_run(ctx, ps, raise_on_error=False)
     p0, p1 = particle_slice(len(particles), rank, world)
-    mine = list(run(particles[p0:p1])) if p1 > p0 else []
+    mine, err = [], None
+    try:
+        mine = list(run(particles[p0:p1])) if p1 > p0 else []
+    except Exception as ex:  # the collectives below are taken either way
+        err = f"{type(ex).__name__}: {ex}"
+    raise_if_any_rank_failed(err, "batch_run_distributed")
     if world <= 1 or not (dist.is_available() and dist.is_initialized()):
         return mine
     parts = [None] * world

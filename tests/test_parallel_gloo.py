@@ -109,3 +109,64 @@ def test_particle_split_and_gather():
     assert seen0 == list(range(0, 5)) and seen1 == list(range(5, 11))    # each particle once
     assert ids0 == ids1 == [float(i) for i in range(11)]                  # gathered in order
     assert who0 == who1 == [0] * 5 + [1] * 6
+
+
+def _worker_failure(rank, world, port, q):
+    # rank 1 fails inside its local work (an exception on the host, before
+    # any collective); every rank must still take the same collectives and
+    # raise naming rank 1, rather than wait for the process group's timeout
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=30))
+    try:
+        import sys
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                        "bem-cpp_b200"))
+        from bem_b200.parallel import batch_run_distributed, orientation_average_distributed
+        msgs = []
+
+        def run(ps):
+            if rank == 1:
+                raise MemoryError("injected on rank 1")
+            return [(np.zeros((4, 4, 3)), {"status": 0}) for _ in ps]
+        try:
+            batch_run_distributed(None, list(range(6)), rank, world, run=run)
+        except RuntimeError as ex:
+            msgs.append(str(ex))
+        # one orientation: rank 0 has none, rank 1 has it and fails (no device
+        # objects here, so its first device call raises)
+        try:
+            orientation_average_distributed(None, None, None, np.eye(3)[None], np.ones(1), 1.0, 1.0,
+                                            ntheta=3, rank=rank, world=world)
+        except RuntimeError as ex:
+            msgs.append(str(ex))
+        # the group is still usable afterwards
+        from bem_b200.parallel import allreduce_max
+        q.put((rank, msgs, allreduce_max(float(rank))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failing_rank_is_reported_on_every_rank():
+    import torch.multiprocessing as mp
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker_failure, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, msgs, mx in res:
+        assert len(msgs) == 2, (rank, msgs)
+        assert "batch_run_distributed: rank 1 failed: MemoryError: injected on rank 1" in msgs[0]
+        assert msgs[1].startswith("orientation_average_distributed: rank 1 failed")
+        assert mx == 1.0
