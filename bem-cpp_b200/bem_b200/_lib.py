@@ -98,6 +98,7 @@ SIGNATURES = {
     "bem_last_error": (C.c_char_p, [_P]),
     "bem_ctx_launch_count": (_L, [_P]),
     "bem_version": (C.c_char_p, []),
+    "bem_selftest_bounded_wait": (_I, [_P, C.c_int64, _I]),
     "bem_ctx_profile": (_I, [_P, _I]),
     "bem_ctx_set_tensor_cores": (_I, [_P, _I]),
     "bem_ctx_set_residual_digits": (_I, [_P, _I]),

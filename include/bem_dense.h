@@ -119,6 +119,12 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value);
 int bem_ctx_profile_read(bem_ctx* ctx, int cls, int64_t* launches, double* ms, double* flops,
                          double* bytes);
 const char* bem_version(void);
+/* The failure path of a bounded device-side wait, without a fault: one
+ * thread waits on a device flag for at most `cycles` SM clock cycles
+ * (0..4e9).  set_flag = 0: nothing sets the flag, the wait runs out and the
+ * call returns BEM_ERR_TIMEOUT with the context still usable; set_flag = 1:
+ * BEM_OK.  No counterpart in the reference (its CUDA errors exit). */
+int bem_selftest_bounded_wait(bem_ctx* ctx, int64_t cycles, int set_flag);
 
 /* ----------------------------------------------------- geometry (host) */
 /* Meshes are returned through caller buffers.  Pass NULL buffers to query
