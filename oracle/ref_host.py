@@ -70,6 +70,16 @@ def mesh_utils(verts, tris):
     return vol, dmax, a_eq, vn
 
 
+def rwg_of(verts, tris):
+    """The reference's build_rwg on (verts, tris) -> the rwg dict of make_mesh."""
+    L = lib()
+    v = np.ascontiguousarray(verts, dtype=np.float64)
+    t = np.ascontiguousarray(tris, dtype=np.int32)
+    L.ref_set_mesh(_p(v), len(v), _p(t), len(t))
+    nr = L.ref_build_rwg()
+    return _fetch(len(v), len(t), nr)[2]
+
+
 def tri_quadrature(order):
     """The reference's tri_quadrature(order) -> (pts (n, 2), wts (n,))."""
     pts, wts = np.zeros(50), np.zeros(25)

@@ -49,6 +49,12 @@ void ref_set_mesh(const double* verts, int nv, const int* tris, int nt) {
     g_mesh.tris.assign(tris, tris + 3 * nt);
 }
 
+// build_rwg (rwg.cpp:5-43) on the current mesh; fetch with ref_get_rwg.
+int ref_build_rwg(void) {
+    g_rwg = build_rwg(g_mesh);
+    return g_rwg.N;
+}
+
 // mesh_volume, mesh_dmax, normalize_mesh (mesh.cpp:252-294) of the current
 // mesh; normalize_mesh rescales it in place (fetch it with ref_get_mesh).
 double ref_mesh_volume(void) { return mesh_volume(g_mesh); }

@@ -160,6 +160,36 @@ def test_mesh_utilities_match_the_reference(case):
     assert a2 == a_eq and np.array_equal(v2, vn)
 
 
+@pytest.mark.parametrize("case", ["open_square", "open_cap", "fin", "unused_vertex", "single"])
+def test_rwg_edge_cases_match_the_reference(case):
+    # only edges shared by exactly two triangles carry a basis function
+    # (rwg.cpp:22): boundary edges of open surfaces and edges of three
+    # triangles get none; unused vertices change nothing
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("reference host library not built")
+    if case == "open_square":
+        v = np.array([[0.0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]])
+        t = np.array([[0, 1, 2], [0, 2, 3]])
+    elif case == "single":
+        v = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0]])
+        t = np.array([[0, 1, 2]])
+    else:
+        v, t = bb.icosphere(1.0, 1)
+        if case == "open_cap":
+            t = t[v[t].mean(axis=1)[:, 2] > -0.2]                 # the lower cap removed
+        elif case == "fin":
+            v = np.vstack([v, [[2.0, 2.0, 2.0]]])
+            t = np.vstack([t, [[t[0][0], t[0][1], len(v) - 1]]])  # a third triangle on one edge
+        else:
+            v = np.vstack([v, [[5.0, 5.0, 5.0]]])
+    r = ref_host.rwg_of(v, t)
+    o = bb.build_rwg(v, t)
+    assert o["N"] == r["N"]
+    for k in ("tri_p", "tri_m", "free_p", "free_m", "length", "area_p", "area_m"):
+        assert np.array_equal(o[k], r[k]), k
+
+
 @pytest.mark.parametrize("order", [4, 7, 13])
 def test_quadrature(order):
     import bem_b200 as bb
