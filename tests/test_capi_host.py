@@ -247,7 +247,9 @@ def test_quadrature_rejects_unknown_order():
 
 
 @pytest.mark.parametrize("args", [(8, 8, 1, 1, 1, False), (45, 31, 1, 1, 1, False),
-                                  (4, 3, 2, 2, 6, True), (5, 4, 3, 1, 1, True)])
+                                  (4, 3, 2, 2, 6, True), (5, 4, 3, 1, 1, True),
+                                  (1, 1, 1, 1, 1, False), (1, 7, 1, 1, 1, False), (6, 1, 5, 1, 1, False),
+                                  (3, 5, 4, 2, 1, False), (2, 2, 6, 1, 3, True), (12, 9, 2, 2, 2, True)])
 def test_orientations_match_reference_cpp(args):
     import bem_b200 as bb
     RT, w = bb.generate_orientations(*args)
