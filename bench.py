@@ -127,8 +127,20 @@ def cpu_sample(n_full, nrhs_full, n_s=8192, reps=1, seed=0):
     cores = os.cpu_count() or 1
     desc = (f"scipy LAPACK zgetrf+zgetrs on n={n_s}, nrhs={nr} (median of {reps}: factor "
             f"{tfm:.2f} s, solve {tsm:.2f} s), scaled by n^3 / n^2 nrhs to n={n_full}, "
-            f"nrhs={nrhs_full}")
+            f"nrhs={nrhs_full}; {_cpu_model()}, {cores} logical cores, OPENBLAS_NUM_THREADS="
+            f"{os.environ.get('OPENBLAS_NUM_THREADS', 'unset')}")
     return scaled, cores, desc, tfm + tsm
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "CPU model unknown"
 
 
 # ---------------------------------------------------------------- clocks
@@ -507,7 +519,7 @@ def run_bem(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        v, cores, desc, wall = cpu_sample(n, 2 * no_all, n_s=8192, reps=2)
+        v, cores, desc, wall = cpu_sample(n, 2 * no_all, n_s=8192, reps=3)
         cpu = {"value": v, "unit": "s/solve", "cores": cores, "kind": "port", "sample": desc}
 
     if rank == 0:

@@ -67,3 +67,11 @@ def test_defaults_and_workload(monkeypatch):
     w = bench.workload(a, 61440)
     assert w["unknowns"] == 61440 and w["rhs"] == 2790 and "L2" in w["l2_policy"]
     assert bench._n_rwg_ico(5) == 30720
+
+
+def test_cpu_sample_is_scaled_and_described():
+    import bench
+    v, cores, desc, wall = bench.cpu_sample(4096, 256, n_s=512, reps=3, seed=1)
+    assert v > wall > 0 and cores >= 1
+    assert "median of 3" in desc and "logical cores" in desc and "OPENBLAS_NUM_THREADS" in desc
+    assert "n=4096" in desc and "nrhs=256" in desc
