@@ -80,6 +80,15 @@ def rwg_of(verts, tris):
     return _fetch(len(v), len(t), nr)[2]
 
 
+def singular_corrections(k, quad_order, N):
+    """The reference's apply_singular_corrections (assembly.cu:208-321) on the
+    mesh and RWG of the last make_mesh / rwg_of call, into a zero N x N L."""
+    L = np.zeros((N, N), dtype=np.complex128)
+    k = complex(k)
+    lib().ref_singular_corrections(int(quad_order), C.c_double(k.real), C.c_double(k.imag), _p(L))
+    return L
+
+
 def tri_quadrature(order):
     """The reference's tri_quadrature(order) -> (pts (n, 2), wts (n,))."""
     pts, wts = np.zeros(50), np.zeros(25)

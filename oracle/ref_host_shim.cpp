@@ -19,6 +19,11 @@ static Mesh g_mesh;
 static RWG g_rwg;
 static std::vector<Orientation> g_or;
 
+// The current mesh and RWG, for the other translation unit of this library
+// (ref_asm_shim.cu).
+const Mesh& ref_current_mesh() { return g_mesh; }
+const RWG& ref_current_rwg() { return g_rwg; }
+
 extern "C" {
 
 // kind 0 = icosphere(radius=param, ref), 1 = hex_prism(aspect=param, ref)
