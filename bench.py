@@ -298,7 +298,11 @@ def run_cusolver(a):
         lu.close()
         return X64
 
+    ctx.profile(True)
     t64, X64 = timed(fp64_step)
+    fp64_classes = {k: {"launches": v[0], "s": v[1] / 1e3, "tflops": v[2] / max(v[1], 1e-9) / 1e9}
+                    for k, v in ctx.profile_read().items() if v[0] > 0}
+    ctx.profile(False)
     clocks = sampler.stop()
 
     def rel(U, V):
@@ -313,7 +317,7 @@ def run_cusolver(a):
             "library": "cuSOLVER (CUDA toolkit) cusolverDnXgetrf + cusolverDnXgetrs(OP_T), FP64",
             "step_times_s": t_cs,
             "fp64_tflops": flops / val / 1e12, "fp64_frac_of_37tfs": flops / val / 1e12 / FP64_PEAK_TFS,
-            "bem_fp64_s_per_solve": t64, "bem_fp32_refine_s_per_solve": t32,
+            "bem_fp64_s_per_solve": t64, "bem_fp64_classes": fp64_classes, "bem_fp32_refine_s_per_solve": t32,
             "speedup_fp32_refine_vs_cusolver": val / t32, "speedup_bem_fp64_vs_cusolver": val / t64,
             "max_rel_err_cusolver_vs_bem_fp64": rel(X, X64),
             "max_rel_err_fp32_refine_vs_cusolver": rel(X32, X), "clocks": clocks}
