@@ -22,7 +22,7 @@ struct PanelWS {
 // Optional replacement of the CUDA-core GEMM for the big updates
 // C -= A * B (A: M x K, K contiguous; B: K x N).  fn: B row-major (the U12
 // block of the factor), C row-major.  fn_solve: B and C column-major.
-// Options of the 3xTF32 tensor-core GEMM C -= op(A) op(B) (complex64).
+// Options of the three-product tensor-core GEMM C -= op(A) op(B) (complex64).
 struct TcOpts {
     bool b_rowmajor = false;  // B is K x N row-major (else given as N x K row-major, "column-major")
     bool c_colmajor = false;  // C column-major
@@ -62,7 +62,7 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
 
 void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm);
 // Complex-symmetric S = L D L^T without pivoting (complex64, lower triangle,
-// 3xTF32 tensor-core updates) and its multi-RHS solve.
+// tensor-core updates) and its multi-RHS solve.
 int sym_structure(bem_ctx* ctx, const double2* Z, int64_t ldz, int n, bool* sym, bool* sym_half);
 int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info);
 int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2* B, int64_t ldb, float2* X,
@@ -76,7 +76,7 @@ int lu_factor_ex(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bool 
 int lu_order(const bem_lu* lu);
 int lu_apply(bem_ctx* ctx, bem_lu* lu, const double2* B, int64_t ldb, double2* X, int64_t ldx, int nrhs);
 
-// 3xTF32 tensor-core updates (gemm_tc.cu); nullptr hooks when unavailable.
+// Tensor-core updates (gemm_tc.cu: FP16 or TF32 operand parts); nullptr hooks when unavailable.
 TrailingUpdate<float> tc_update_fp32(bem_ctx* ctx);
 
 }  // namespace bem

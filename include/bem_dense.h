@@ -37,7 +37,7 @@ typedef enum bem_status {
 
 typedef enum bem_precision {
     BEM_PREC_FP64 = 0,         /* complex128 LU and solves */
-    BEM_PREC_FP32_REFINE = 1   /* complex64 LU (3xTF32 tensor-core updates) + FP64 refinement */
+    BEM_PREC_FP32_REFINE = 1   /* complex64 LU (tensor-core updates, FP16 or TF32 operand parts) + FP64 refinement */
 } bem_precision;
 
 /* Assembly flags */
@@ -69,8 +69,8 @@ int64_t bem_ctx_launch_count(const bem_ctx* ctx);
  * 4 assembly, 5 far field / Mueller.  flops / bytes are the algorithmic
  * counts of the recorded launches (complex GEMM: 8 M N K flop). */
 int bem_ctx_profile(bem_ctx* ctx, int enable);
-/* FP32 factorisation / solve updates on the tensor cores (3xTF32 tcgen05,
- * default 1) or on the CUDA cores (0). */
+/* FP32 factorisation / solve updates on the tensor cores (three tcgen05
+ * products of two-part operands, default 1) or on the CUDA cores (0). */
 int bem_ctx_set_tensor_cores(bem_ctx* ctx, int enable);
 /* FP64 refinement residual of BEM_PREC_FP32_REFINE factorisations made after
  * this call: digits = 0 computes B - Z X with the FP64 (DMMA) complex GEMM;
