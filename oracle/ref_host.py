@@ -89,6 +89,20 @@ def singular_corrections(k, quad_order, N):
     return L
 
 
+def subdivide_flat(verts, tris):
+    """The reference's subdivide_flat (mesh.cpp:70-100) on (verts, tris) ->
+    (verts, tris, rwg dict of the subdivided mesh)."""
+    L = lib()
+    v = np.ascontiguousarray(verts, dtype=np.float64)
+    t = np.ascontiguousarray(tris, dtype=np.int32)
+    L.ref_set_mesh(_p(v), len(v), _p(t), len(t))
+    nr = L.ref_subdivide_flat()
+    nv, nt = C.c_int(), C.c_int()
+    L.ref_mesh_counts.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.ref_mesh_counts(C.byref(nv), C.byref(nt))
+    return _fetch(nv.value, nt.value, nr)
+
+
 def tri_quadrature(order):
     """The reference's tri_quadrature(order) -> (pts (n, 2), wts (n,))."""
     pts, wts = np.zeros(50), np.zeros(25)

@@ -54,6 +54,12 @@ void ref_set_mesh(const double* verts, int nv, const int* tris, int nt) {
     g_mesh.tris.assign(tris, tris + 3 * nt);
 }
 
+// Vertex and triangle counts of the current mesh.
+void ref_mesh_counts(int* nv, int* nt) {
+    *nv = g_mesh.nv();
+    *nt = g_mesh.nt();
+}
+
 // build_rwg (rwg.cpp:5-43) on the current mesh; fetch with ref_get_rwg.
 int ref_build_rwg(void) {
     g_rwg = build_rwg(g_mesh);

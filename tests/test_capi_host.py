@@ -308,3 +308,19 @@ def test_cli_help_and_argument_errors():
     assert r.returncode == 1 and "Unknown option: --no-such-flag" in r.stderr
     r = subprocess.run([_cli(), "--ref", "2"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "--ka must be positive" in r.stderr
+
+
+@pytest.mark.parametrize("mesh", ["hex", "bumpy"])
+def test_subdivide_flat_matches_the_reference(mesh):
+    # midpoint subdivision without projection (mesh.cpp:70-100), then the RWG
+    # of the refined mesh, against the reference's own C++
+    import bem_b200 as bb
+    if not ref_host.available():
+        pytest.skip("reference host library not built")
+    v, t = bb.hex_prism(0.9, 1) if mesh == "hex" else bb.c5_mesh(5, refinements=1, rms=0.1)
+    vr, tr, rr = ref_host.subdivide_flat(v, t)
+    v2, t2 = bb.subdivide_flat(v, t)
+    assert np.array_equal(v2, vr) and np.array_equal(t2, tr)
+    o = bb.build_rwg(v2, t2)
+    for k in ("tri_p", "tri_m", "free_p", "free_m", "length", "area_p", "area_m"):
+        assert np.array_equal(o[k], rr[k]), k
