@@ -62,7 +62,7 @@ class Context:
     def launches(self) -> int:
         return int(lib().bem_ctx_launch_count(self.h))
 
-    PROF_CLASSES = ("lu_update", "solve_update", "residual", "panel", "assembly", "farfield")
+    PROF_CLASSES = ("lu_update", "solve_update", "residual", "panel", "assembly", "farfield", "verify")
 
     def profile(self, enable=True):
         self.check(lib().bem_ctx_profile(self.h, int(bool(enable))))
@@ -588,12 +588,37 @@ def compute_farfield_batch(geom: Geometry, coeffs_J, coeffs_M, r_hats, k_ext, et
     return Fv
 
 
+def _check_solutions(geom: Geometry, X, RT, w):
+    """Checks the solution tensor and orientation arrays handed to the far-field
+    entry points as raw pointers: X complex128 on the geometry's device with
+    unit stride along a solution and one (par, perp) pair of rows per
+    orientation; one weight per orientation.  Returns (RT as (n, 9), w)."""
+    import torch
+    RT = _f64(RT).reshape(-1, 9)
+    w = _f64(w).reshape(-1)
+    if not (isinstance(X, torch.Tensor) and X.dtype == torch.complex128 and X.is_cuda
+            and X.device.index == geom.ctx.device and X.dim() == 2):
+        raise ValueError("X must be a 2-D complex128 tensor on the geometry's device")
+    if X.stride(1) != 1 or X.shape[1] < geom.n or X.stride(0) < geom.n:
+        raise ValueError(f"X rows must be contiguous solutions of length {geom.n}")
+    if X.shape[0] < 2 * RT.shape[0]:
+        raise ValueError(f"X has {X.shape[0]} rows, {2 * RT.shape[0]} needed for {RT.shape[0]} orientations")
+    if w.size != RT.shape[0]:
+        raise ValueError(f"{w.size} weights for {RT.shape[0]} orientations")
+    return RT, w
+
+
 def mueller_from_solutions_dev(geom: Geometry, X, RT, w, k_ext, eta_ext, ntheta=181,
                                gamma_mirror=False, M_orient=None):
     """Orientation-weighted Mueller sum (4,4,ntheta) from device solutions X
     (torch (2 n_orient, 2N), rows (par, perp) per orientation)."""
-    RT = _f64(RT).reshape(-1, 9)
-    w = _f64(w)
+    import torch
+    RT, w = _check_solutions(geom, X, RT, w)
+    if M_orient is not None and not (
+            isinstance(M_orient, torch.Tensor) and M_orient.dtype == torch.float64 and M_orient.is_cuda
+            and M_orient.device.index == geom.ctx.device and M_orient.is_contiguous()
+            and M_orient.numel() >= RT.shape[0] * 16 * int(ntheta)):
+        raise ValueError("M_orient must be a contiguous float64 device tensor of n_orient*16*ntheta elements")
     M = np.zeros((4, 4, ntheta))
     k = complex(k_ext)
     geom.ctx.check(lib().bem_farfield_mueller_dev(
@@ -851,7 +876,7 @@ def set_symmetric(ctx: Context, mode: int):
 
 
 def set_option(ctx: Context, name: str, value: int):
-    """Kernel-shape switches: "residual_pairs", "persistent_gemm"."""
+    """Named switches of bem_ctx_set_option (include/bem_dense.h lists them)."""
     ctx.check(lib().bem_ctx_set_option(ctx.h, name.encode(), int(value)))
 
 
@@ -865,8 +890,12 @@ def mueller_noalloc_dev(geom: Geometry, X, RT, w, k_ext, eta_ext, M_out, ntheta=
     """bem_farfield_mueller_noalloc: same sum as mueller_from_solutions_dev into
     the caller's device buffer M_out (torch float64, 16*ntheta), with no device
     allocation by the library (scratch is a static device array)."""
-    RT = _f64(RT).reshape(-1, 9)
-    w = _f64(w)
+    import torch
+    RT, w = _check_solutions(geom, X, RT, w)
+    if not (isinstance(M_out, torch.Tensor) and M_out.dtype == torch.float64 and M_out.is_cuda
+            and M_out.device.index == geom.ctx.device and M_out.is_contiguous()
+            and M_out.numel() >= 16 * int(ntheta)):
+        raise ValueError("M_out must be a contiguous float64 device tensor of at least 16*ntheta elements")
     k = complex(k_ext)
     geom.ctx.check(lib().bem_farfield_mueller_noalloc(
         geom.ctx.h, geom.h, _dptr(X), X.stride(0), _ptr(RT), _ptr(w), RT.shape[0], k.real, k.imag,

@@ -158,7 +158,8 @@ enum ProfClass {
     PROF_PANEL = 3,        // panel factorisation kernels
     PROF_ASSEMBLY = 4,     // PMCHWT assembly kernel
     PROF_FARFIELD = 5,     // far-field / Mueller kernel
-    PROF_NCLASS = 6
+    PROF_VERIFY = 6,       // FP64 residual of the columns checked after the refinement
+    PROF_NCLASS = 7
 };
 
 struct ProfPending {
@@ -184,6 +185,8 @@ struct bem_ctx {
     size_t oz_bytes = 0;
     bool oz_attr = false;
     int gmres_digits = 0;        // GMRES products with Z: 0 FP64 DMMA GEMM, 2..8 int8 Ozaki digits
+    int verify_cols = 64;        // refinement: columns whose error is measured with an FP64 residual
+                                 // at convergence (0: none, -1: all)
     int factor_sb = 2;           // L D L^T: 256-column blocks per trailing update (1 or 2)
     int solve_sb = 2;            // L D L^T solves: 256-row blocks per update (1 or 2)
     int oz_pace_epoch = 32;      // int8 residual: K slabs per pacing epoch (0: no pacing)

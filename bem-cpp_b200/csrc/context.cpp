@@ -292,6 +292,9 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
         ctx->tc_group_m = value;
     } else if (!std::strcmp(name, "persistent_gemm")) {
         ctx->tc_persistent = value != 0;
+    } else if (!std::strcmp(name, "verify_columns")) {
+        if (value < -1) return bem::fail(ctx, BEM_ERR_INVALID, "verify_columns must be -1, 0 or a column count");
+        ctx->verify_cols = value;
     } else if (!std::strcmp(name, "tensor_split")) {
         if (value != 0 && value != 1) return bem::fail(ctx, BEM_ERR_INVALID, "tensor_split must be 0 or 1");
         ctx->tc_split = value;

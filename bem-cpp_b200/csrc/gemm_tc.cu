@@ -1,5 +1,5 @@
-// 3xTF32 complex GEMM on the fifth-generation tensor cores (tcgen05 + TMA +
-// TMEM), used for the big updates of the FP32 factorisation and solves:
+// Three-product complex GEMM on the fifth-generation tensor cores (tcgen05 +
+// TMA + TMEM), used for the big updates of the FP32 factorisation and solves:
 //
 //   C -= A * B      A: M x K complex (K contiguous), B: K x N complex,
 //                   C: M x N complex64, row-major (LU) or column-major (solves)
@@ -8,23 +8,32 @@
 //   C'[i, 2j+{0,1}] -= sum_k' A'[i, k'] B'[2j+{0,1}, k']
 // with A'[i, 2k] = Re a_ik, A'[i, 2k+1] = Im a_ik (the raw float layout of a
 // complex row) and B' rows (Re b, -Im b) / (Im b, Re b) interleaved over k.
-// Every operand is split x = hi + lo with hi, lo rounded to TF32 and the
-// product taken as hi*hi + hi*lo + lo*hi, accumulated in FP32 in TMEM.
-// With the context option tensor_split = 1 the parts are FP16 instead (the
-// same 11 significant bits as TF32, at twice the tensor rate): each row of A'
-// and each complex column of B is first scaled by a power of two that brings
-// its largest part into [2^14, 2^15), so no part overflows FP16 and the parts
-// of small entries that fall below FP16's normal range lose at most 2^-38 of
-// the row's largest entry; the epilogue multiplies the accumulator by the
-// inverse scales of its row and column (exact: powers of two).
+// Every operand is split x = hi + lo and the product taken as
+// hi*hi + hi*lo + lo*hi, accumulated in FP32 in TMEM.  Two splits:
+//  * FP16 parts (context option tensor_split = 1, the default; kind::f16 at
+//    twice the TF32 rate): each row of A' and each complex column of B is
+//    first scaled by a power of two that brings its largest part into
+//    [2^14, 2^15), so no part overflows FP16, and the parts of small entries
+//    that fall below FP16's normal range lose at most 2^-38 of the row's
+//    largest entry; the epilogue multiplies the accumulator by the inverse
+//    scales of its row and column (exact: powers of two).
+//  * TF32 parts (tensor_split = 0; kind::tf32): hi, lo rounded to TF32.
 //
-// Pack kernels write the hi / lo operands K-major; the GEMM kernel streams
-// 128 x 32 (A) and 256 x 32 (B) float tiles with TMA (128-byte swizzle, no
-// multicast) through a 2-stage mbarrier pipeline; one thread issues
-// tcgen05.mma (M=128, N=256, K=8) into a 128 x 256 FP32 TMEM accumulator; four
-// warps read it back with tcgen05.ld and apply C -= acc.  Every wait is
-// bounded (~1 s of clock cycles): on expiry the kernel records
-// BEM_ERR_TIMEOUT in the status word, frees its TMEM and returns.
+// Pack kernels write the hi / lo operands K-major.  Both GEMM kernels stream
+// 128-row A and 256-row B tiles of one 128-byte swizzle row of K per stage
+// (32 floats or 64 halves) with TMA (no multicast) through a 2-stage mbarrier
+// pipeline: a stage holds hi and lo of both tiles, 96 KB, so two fill the
+// shared memory.  One thread issues tcgen05.mma (M = 128, N = 256; K = 8 for
+// TF32, 16 for FP16) into a 128 x 256 FP32 TMEM accumulator.
+//  * gemm_kernel: one CTA per output tile; four warps read the accumulator
+//    back with tcgen05.ld and apply C -= acc.
+//  * gemm_persistent_kernel (default): one CTA per SM walking the tiles in
+//    grouped raster order, warp-specialised (warp 0 TMA producer, warp 1 MMA
+//    issuer, warps 2-5 epilogue) with two TMEM accumulators (512 columns) so
+//    the epilogue of one tile overlaps the MMAs of the next.
+// Every wait is bounded (~1 s of clock cycles): on expiry the kernel records
+// BEM_ERR_TIMEOUT in the status word, drains the copies it issued, frees its
+// TMEM and returns.
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>

@@ -236,6 +236,9 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         r->stats.t_solve_ms += st.t_solve_ms;
         r->stats.t_refine_ms += st.t_refine_ms;
         r->stats.factorization = st.factorization;
+        r->stats.verified_columns += st.verified_columns;
+        r->stats.verified_rel_error = std::max(r->stats.verified_rel_error, st.verified_rel_error);
+        r->stats.exact_residual_sweeps = std::max(r->stats.exact_residual_sweeps, st.exact_residual_sweeps);
         for (int i = 0; i < 12; i++) r->stats.update_hist[i] = std::max(r->stats.update_hist[i], st.update_hist[i]);
         r->t_solve_s += secs(ts);
         auto tf = std::chrono::steady_clock::now();

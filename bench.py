@@ -444,6 +444,20 @@ def run_bem(a):
             dist.all_reduce(e, op=dist.ReduceOp.MAX)
             err = float(e.item())
 
+    # the metric's second bar: the orientation-averaged Mueller matrix of the
+    # FP32 + refinement solution against that of the FP64 solution
+    merr = None
+    if X64 is not None:
+        from bem_b200.parallel import allreduce_sum
+        M32 = bb.mueller_from_solutions_dev(g, X, RTr, wr, kx, ee, ntheta=181)
+        M64 = bb.mueller_from_solutions_dev(g, X64, RTr, wr, kx, ee, ntheta=181)
+        if world > 1:
+            M32 = allreduce_sum(M32, device=f"cuda:{local}").reshape(M32.shape)
+            M64 = allreduce_sum(M64, device=f"cuda:{local}").reshape(M64.shape)
+        merr = {"rel_fro": float(np.linalg.norm(M32 - M64) / np.linalg.norm(M64)),
+                "max_abs_over_max_M11": float(np.abs(M32 - M64).max() / np.abs(M64[0, 0]).max()),
+                "M11_max_rel": float((np.abs(M32[0, 0] - M64[0, 0]) / np.abs(M64[0, 0])).max())}
+
     # dominant kernel of the timed steps -> roofline
     pk, basis = peaks()
     dom = max(prof.items(), key=lambda kv: kv[1][1])
@@ -548,6 +562,10 @@ def run_bem(a):
                 "max_rel_err_vs_fp64": err, "refine_iterations": its,
                 "refine_update_hist": stats[-1].get("update_hist"),
                 "est_rel_err": stats[-1].get("est_rel_error"),
+                "verified_rel_err": stats[-1].get("verified_rel_error"),
+                "verified_columns": stats[-1].get("verified_columns"),
+                "exact_residual_sweeps": stats[-1].get("exact_residual_sweeps"),
+                "mueller_err_vs_fp64": merr,
                 "t_factor_s": stats[-1]["t_factor_ms"] / 1e3, "t_first_solve_s": stats[-1]["t_solve_ms"] / 1e3,
                 "t_refine_s": stats[-1]["t_refine_ms"] / 1e3,
                 "converged": all(s["converged"] for s in stats),

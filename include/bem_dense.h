@@ -66,7 +66,8 @@ int64_t bem_ctx_launch_count(const bem_ctx* ctx);
  * every launch of a class.  bem_ctx_profile(ctx, 1) clears the counters and
  * starts recording, 0 stops.  Classes: 0 LU trailing update, 1 triangular
  * solve block updates, 2 FP64 refinement residual, 3 panel factorisation,
- * 4 assembly, 5 far field / Mueller.  flops / bytes are the algorithmic
+ * 4 assembly, 5 far field / Mueller, 6 the FP64 residual of the columns
+ * checked after the refinement.  flops / bytes are the algorithmic
  * counts of the recorded launches (complex GEMM: 8 M N K flop). */
 int bem_ctx_profile(bem_ctx* ctx, int enable);
 /* FP32 factorisation / solve updates on the tensor cores (three tcgen05
@@ -107,7 +108,9 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * "assembly_kernel" (0, default: triangle-pair moments over Morton-ordered
  * tiles; 1: one thread per RWG pair, the reference's organisation),
  * "farfield_kernel" (0, default: phases shared by the RWG halves of a
- * triangle; 1: per RWG-half point), "tensor_split" (1, default: FP32
+ * triangle; 1: per RWG-half point), "verify_columns" (64, default: after the refinement converges, the error of
+ * 64 columns is measured with an FP64 residual, see bem_lu_solve_dev; -1:
+ * every column; 0: no check), "tensor_split" (1, default: FP32
  * operands of the tensor-core GEMM split into two FP16 parts after a
  * power-of-two scale per operand row / column that brings its largest part
  * into [2^14, 2^15), kind::f16 at twice the TF32 rate, the persistent GEMM
@@ -244,6 +247,11 @@ typedef struct bem_solve_stats {
     double update_hist[12];  /* max relative update of sweeps 1..12 */
     int factorization;       /* FP32 factors used: 0 LU with partial pivoting, 1 L D L^T of Z,
                                 2 L D L^T of Z diag(I, -I); -1 FP64 */
+    int verified_columns;    /* columns whose error was measured at convergence (option verify_columns) */
+    double verified_rel_error; /* max over those columns of max|e| / max|x|, e = (factors)^-1 (B - Z X)
+                                  with B - Z X in the FP64 GEMM */
+    int exact_residual_sweeps; /* sweeps that fell back to the FP64 GEMM residual, after a check showed
+                                  the int8 residual's floor above the tolerance (or without its memory) */
 } bem_solve_stats;
 
 /* Factorises the row-major n x n complex128 matrix Z_dev (leading dimension
@@ -256,9 +264,18 @@ int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precisi
 /* X = Z^-1 B for nrhs columns (column-major, leading dimensions ldb / ldx; X may
  * alias B).  FP32_REFINE refines in FP64 (residual B - Z X with the FP64 Z,
  * correction through the FP32 factors) until the estimated relative error of
- * every column, rho/(1-rho) times its last relative update with rho the
- * observed contraction, is below `tol` (default 1e-11 when tol <= 0), or
- * max_iter sweeps (default 10) were run (BEM_ERR_NOCONV). */
+ * every column is below `tol` (default 1e-11 when tol <= 0), or max_iter
+ * sweeps (default 10) were run (BEM_ERR_NOCONV).  The estimate is the larger
+ * of two: rho/(1-rho) times the last relative update, rho the observed
+ * contraction (how far the sweeps are from their limit), and the error
+ * measured directly at that point on the columns of the option
+ * verify_columns (default 64, -1 all, 0 none; a sample takes half its
+ * columns evenly spaced and half where the last sweep's relative update was
+ * largest): the FP64-GEMM residual of each, solved through the factors, with
+ * the sampled maximum tripled for the columns not checked.  The second term sees the
+ * floor that the int8 residual's digit truncation leaves, which the updates
+ * cannot; when it is above tol the remaining sweeps compute the residual in
+ * the FP64 GEMM (stats->exact_residual_sweeps) and the check is repeated. */
 int bem_lu_solve_dev(bem_ctx* ctx, bem_lu* lu, const void* B_dev, int64_t ldb,
                      void* X_dev, int64_t ldx, int nrhs, double tol, int max_iter,
                      bem_solve_stats* stats);
@@ -361,11 +378,17 @@ int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev,
  * with a fixed pool).  Its only scratch (staged orientations, per-orientation
  * Mueller terms) is a file-scope device array of BEM_NOALLOC_SCRATCH_BYTES,
  * held by every GPU that loads the library until exit; the call itself
- * allocates nothing.  Calls whose n_orient * (16 ntheta + 10) doubles do not
- * fit are rejected with BEM_ERR_INVALID: split the orientations and add the
- * partial results (the average is a weighted sum).  RT, w: host arrays as in
- * bem_farfield_mueller_dev.  M_avg_dev: caller's device buffer of 16*ntheta
- * doubles, written on the context's stream.  The first call on a device looks
+ * allocates nothing.  The scratch holds three segments, each rounded up to a
+ * multiple of 256 bytes: 72 n_orient bytes (orientations), 8 n_orient bytes
+ * (weights) and 128 ntheta n_orient bytes (per-orientation terms); a call
+ * whose rounded sum exceeds BEM_NOALLOC_SCRATCH_BYTES is rejected with
+ * BEM_ERR_INVALID: split the orientations and add the partial results (the
+ * average is a weighted sum).  RT, w: host arrays as in
+ * bem_farfield_mueller_dev, copied to the scratch in the context's stream
+ * order: pageable memory is read before the call returns, but pinned memory
+ * may still be read afterwards, so keep pinned RT and w unchanged until that
+ * stream has passed the call.  M_avg_dev: caller's device buffer of
+ * 16*ntheta doubles, written on the context's stream.  The first call on a device looks
  * up the scratch address (cudaGetSymbolAddress).  All calls share the one array: calls that overlap on
  * the GPU (different streams or contexts on one device) race on it. */
 #define BEM_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)

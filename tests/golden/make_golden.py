@@ -15,8 +15,8 @@ on small seeded cases, and stores inputs and outputs as ``.npz`` files:
                   (column 0); solutions and the inner iteration counts it prints
 
 "Z probes" are Z @ v for a seeded complex vector v, diag(Z), ||Z||_F and
-Z[::s, ::s].  Usage:  python tests/golden/make_golden.py --ref /root/reference
-[--only gmres]
+Z[::s, ::s].  Usage:  python tests/golden/make_golden.py --ref <reference checkout>
+[--only gmres]  (--ref defaults to the environment variable BEM_REFERENCE_DIR).
 """
 from __future__ import annotations
 
@@ -46,10 +46,15 @@ def rwg_arrays(rwg):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("BEM_REFERENCE_DIR"))
     ap.add_argument("--only", choices=["gmres"], default=None)
     a = ap.parse_args()
-    os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(REPO, "_work", "numba_cache"))
+    if not a.ref or not os.path.isdir(os.path.join(a.ref, "python")):
+        ap.error("give the reference checkout with --ref or BEM_REFERENCE_DIR")
+    # bem_core's numba functions cache next to their source unless told
+    # otherwise; the reference tree is read-only
+    import tempfile
+    os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="bem_golden_numba_"))
     sys.path.insert(0, os.path.join(a.ref, "python"))
     sys.path.insert(0, REPO)
     import bem_core as bc  # noqa: E402  (the reference, read-only)

@@ -1,0 +1,157 @@
+"""FP32 factors + FP64 refinement on systems harder than the metric's sphere.
+
+The refinement (bem_lu_solve_dev) reports convergence only when its error
+estimate is below the tolerance; the estimate includes an a-posteriori check
+of the refined solution with an FP64-GEMM residual (option verify_columns),
+because the update sizes alone cannot see the error floor that the int8
+residual's digit truncation leaves.  Here every column of a converged solve is
+compared with the FP64 LU solution of the same device-assembled Z (the
+reference's lu_solve_full semantics, solver.cu:87-142) at the metric's bar,
+1e-9 relative, and the orientation-averaged Mueller matrices at 1e-6, on:
+
+* the C2 hex prism (aspect 1.4286, refinement 3, 2N = 4608) at ka = 5 with a
+  higher, absorbing index m = 1.6 + 0.01i, 8 x 8 x 1 orientations;
+* a high-contrast icosphere (refinement 3, 2N = 3840, m = 3) at ka = 2.287,
+  on the sharp Mie resonance of the sphere near x = 2.28 (width 0.01 in x):
+  in a scan of ka = 2.20..2.36 in steps of 0.003 on this 1280-triangle
+  polyhedron the first refinement correction peaks there (2.9e-4, against
+  about 4e-5 away from resonances) and the forward M11 with it;
+* a faceted crystal read from an OBJ file (the convex hull of 40 seeded
+  points on an ellipsoid, flat-subdivided twice), ka = 4, m = 1.5 + 0.005i.
+
+A last case makes the int8 floor large on purpose (3 digits instead of 7):
+without the check the sweeps report convergence far above the tolerance;
+with it the library finds the floor, switches to FP64 residuals and meets
+the bar."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 5e-10
+KA_RESONANCE = 2.287
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import bem_b200 as bb
+    c = bb.Context(0)
+    yield c
+    c.close()
+
+
+def _crystal_obj(path, seed=7, npts=40):
+    """Writes the convex hull of seeded points on an ellipsoid as an OBJ file
+    with outward-facing triangles."""
+    from scipy.spatial import ConvexHull
+    rng = np.random.default_rng(seed)
+    p = rng.standard_normal((npts, 3))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    p *= np.array([1.3, 1.0, 0.7])
+    hull = ConvexHull(p)
+    c = p.mean(axis=0)
+    with open(path, "w") as f:
+        for x in p:
+            f.write(f"v {x[0]:.17g} {x[1]:.17g} {x[2]:.17g}\n")
+        for s in hull.simplices:
+            a, b, d = (int(i) for i in s)
+            nrm = np.cross(p[b] - p[a], p[d] - p[a])
+            if np.dot(nrm, p[[a, b, d]].mean(axis=0) - c) < 0:
+                b, d = d, b
+            f.write(f"f {a + 1} {b + 1} {d + 1}\n")
+
+
+def _mesh(bb, case, tmp_path):
+    if case == "hex_m1.6":
+        v, t = bb.hex_prism(1.4286, 3)
+        return v, t, 5.0, complex(1.6, 0.01), (8, 8, 1)
+    if case == "sphere_resonance":
+        v, t = bb.icosphere(1.0, 3)
+        return v, t, KA_RESONANCE, complex(3.0, 0.0), (4, 4, 1)
+    path = tmp_path / "crystal.obj"
+    _crystal_obj(path)
+    v, t, ndeg, nman = bb.load_obj(path)
+    assert ndeg == 0 and nman == 0
+    v, _ = bb.normalize_mesh(v, t)
+    for _ in range(2):
+        v, t = bb.subdivide_flat(v, t)
+    return v, t, 4.0, complex(1.5, 0.005), (4, 4, 1)
+
+
+def _column_errors(X, Xref):
+    e = (X - Xref).abs()
+    two = (e.pow(2).sum(dim=1).sqrt() / Xref.abs().pow(2).sum(dim=1).sqrt()).cpu().numpy()
+    mx = (e.amax(dim=1) / Xref.abs().amax(dim=1)).cpu().numpy()
+    return two, mx
+
+
+@pytest.mark.parametrize("case", ["hex_m1.6", "sphere_resonance", "faceted_obj"])
+def test_converged_columns_meet_the_bar(ctx, case, tmp_path):
+    import bem_b200 as bb
+    v, t, ka, m, orient = _mesh(bb, case, tmp_path)
+    g = bb.Geometry(ctx, v, t, 7)
+    kx, ki, ee, ei = bb.physics(ka, m)
+    Z = bb.assemble_pmchwt_dev(g, kx, ki, ee, ei)
+    RT, w = bb.generate_orientations(*orient)
+    B = bb.rhs_planewave_dev(g, kx, ee, RT)
+    lu64 = bb.LU(ctx, Z.clone(), bb.PREC_FP64)
+    X64, _ = lu64.solve(B)
+    lu64.close()
+    lu32 = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+    X32, st = lu32.solve(B, tol=TOL, max_iter=15)
+    lu32.close()
+    two, mx = _column_errors(X32, X64)
+    print(f"{case}: 2N={g.n} nrhs={B.shape[0]} sweeps={st['iterations']} hist={st['update_hist']} "
+          f"est={st['est_rel_error']:.2e} verified={st['verified_rel_error']:.2e} "
+          f"exact_sweeps={st['exact_residual_sweeps']} true max={mx.max():.2e} 2-norm={two.max():.2e}")
+    assert st["converged"] == 1
+    assert st["verified_columns"] == min(64, B.shape[0])
+    assert two.max() < 1e-9 and mx.max() < 1e-9, (two.max(), mx.max(), st)
+    # the library's own estimate covers the true error of every column
+    assert mx.max() <= st["est_rel_error"], (mx.max(), st)
+    M64 = bb.mueller_from_solutions_dev(g, X64, RT, w, kx, ee, ntheta=181)
+    M32 = bb.mueller_from_solutions_dev(g, X32, RT, w, kx, ee, ntheta=181)
+    assert rel(M32, M64) < 1e-6
+    g.close()
+
+
+def test_check_finds_the_int8_floor(ctx):
+    import bem_b200 as bb
+    v, t = bb.hex_prism(1.4286, 3)
+    g = bb.Geometry(ctx, v, t, 7)
+    kx, ki, ee, ei = bb.physics(5.0, 1.3116)
+    Z = bb.assemble_pmchwt_dev(g, kx, ki, ee, ei)
+    RT, w = bb.generate_orientations(8, 8, 1)
+    B = bb.rhs_planewave_dev(g, kx, ee, RT)
+    lu64 = bb.LU(ctx, Z.clone(), bb.PREC_FP64)
+    X64, _ = lu64.solve(B)
+    lu64.close()
+    bb.set_residual_digits(ctx, 3)
+    try:
+        # without the check: the updates contract and the sweeps stop,
+        # blind to the residual's floor
+        bb.set_option(ctx, "verify_columns", 0)
+        lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+        Xa, sta = lu.solve(B, tol=TOL, max_iter=15, raise_noconv=False)
+        lu.close()
+        _, mxa = _column_errors(Xa, X64)
+        assert sta["exact_residual_sweeps"] == 0
+        assert mxa.max() > 10 * TOL, (mxa.max(), sta)
+        # with the check (default): the floor is measured, the sweeps switch
+        # to FP64 residuals, and the bar is met
+        bb.set_option(ctx, "verify_columns", 64)
+        lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+        Xb, stb = lu.solve(B, tol=TOL, max_iter=15)
+        lu.close()
+        twob, mxb = _column_errors(Xb, X64)
+        print(f"3 digits: unchecked err {mxa.max():.2e} (est {sta['est_rel_error']:.2e}); checked err "
+              f"{mxb.max():.2e} est {stb['est_rel_error']:.2e} exact sweeps {stb['exact_residual_sweeps']}")
+        assert stb["converged"] == 1 and stb["exact_residual_sweeps"] >= 1
+        assert twob.max() < 1e-9 and mxb.max() < 1e-9
+        assert mxb.max() <= stb["est_rel_error"]
+    finally:
+        bb.set_residual_digits(ctx, 7)
+        bb.set_option(ctx, "verify_columns", 64)
+        g.close()
