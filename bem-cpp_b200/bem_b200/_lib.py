@@ -38,7 +38,8 @@ class SolveStats(C.Structure):
                 ("t_factor_ms", C.c_double), ("t_solve_ms", C.c_double),
                 ("t_refine_ms", C.c_double), ("update_hist", C.c_double * 12),
                 ("factorization", C.c_int), ("verified_columns", C.c_int),
-                ("verified_rel_error", C.c_double), ("exact_residual_sweeps", C.c_int)]
+                ("verified_rel_error", C.c_double), ("exact_residual_sweeps", C.c_int),
+                ("info", C.c_int)]
 
     def as_dict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_}

@@ -271,8 +271,9 @@ int lu_solve_full(std::complex<double>* Z, int n, std::complex<double>* B, int n
     bem_solve_stats st;
     int s = bem_lu_solve_full(ctx(), reinterpret_cast<double*>(Z), n, reinterpret_cast<double*>(B), nrhs, prec, &st);
     if (s == BEM_ERR_SINGULAR) {
-        std::fprintf(stderr, "  LU factorization failed: %s\n", bem_last_error(g_ctx));
-        return 1;
+        // the reference returns cuSOLVER's info (solver.cu:115-121)
+        std::fprintf(stderr, "  LU factorization failed: info=%d\n", st.info);
+        return st.info > 0 ? st.info : 1;
     }
     check(s, "lu_solve_full");
     std::printf("  LU solve full (%dx%d, %d RHS): %.2fs\n", n, n, nrhs, t.elapsed_s());

@@ -253,28 +253,28 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     std::vector<double>* src[10] = {&px, &py, &pz, &fx, &fy, &fz, &cx, &cy, &cz, &jw};
     for (int i = 0; i < 10; i++) {
         *pts[i] = (double*)(base + o_pt[i]);
-        BEM_TRY_CUDA(ctx, cudaMemcpy(*pts[i], src[i]->data(), P * 8, cudaMemcpyHostToDevice));
+        BEM_TRY(h2d(ctx, *pts[i], src[i]->data(), P * 8));
     }
     g->half.div = (double*)(base + o_div);
     g->half.tri = (int*)(base + o_tri);
     double* d_coef = (double*)(base + o_coef);
     double* d_fr = (double*)(base + o_fr);
-    BEM_TRY_CUDA(ctx, cudaMemcpy(g->half.div, div.data(), 2 * N * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(d_coef, coef.data(), 2 * N * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(d_fr, frx.data(), 2 * N * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(d_fr + 2 * N, fry.data(), 2 * N * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(d_fr + 4 * N, frz.data(), 2 * N * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(g->half.tri, tri.data(), 2 * N * 4, cudaMemcpyHostToDevice));
+    BEM_TRY(h2d(ctx, g->half.div, div.data(), 2 * N * 8));
+    BEM_TRY(h2d(ctx, d_coef, coef.data(), 2 * N * 8));
+    BEM_TRY(h2d(ctx, d_fr, frx.data(), 2 * N * 8));
+    BEM_TRY(h2d(ctx, d_fr + 2 * N, fry.data(), 2 * N * 8));
+    BEM_TRY(h2d(ctx, d_fr + 4 * N, frz.data(), 2 * N * 8));
+    BEM_TRY(h2d(ctx, g->half.tri, tri.data(), 2 * N * 4));
     g->sing.pair_mn = (int*)(base + o_pmn);
     g->sing.item_ptr = (int*)(base + o_iptr);
     g->sing.item = (int*)(base + o_item);
     g->sing.P = (double*)(base + o_P);
     g->sing.V = (double*)(base + o_V);
     g->sing.tv = (double*)(base + o_tv);
-    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.pair_mn, pair_mn.data(), pair_mn.size() * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.item_ptr, item_ptr.data(), item_ptr.size() * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.item, item.data(), item.size() * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(g->sing.tv, tv.data(), tv.size() * 8, cudaMemcpyHostToDevice));
+    BEM_TRY(h2d(ctx, g->sing.pair_mn, pair_mn.data(), pair_mn.size() * 4));
+    BEM_TRY(h2d(ctx, g->sing.item_ptr, item_ptr.data(), item_ptr.size() * 4));
+    BEM_TRY(h2d(ctx, g->sing.item, item.data(), item.size() * 4));
+    BEM_TRY(h2d(ctx, g->sing.tv, tv.data(), tv.size() * 8));
     DevTriAsm& ta = g->tri;
     ta.c = (double*)(base + o_tc);
     ta.u = (double*)(base + o_tu);
@@ -289,16 +289,16 @@ int geom_upload(bem_ctx* ctx, bem_geom* g) {
     ta.rwg_rec = (unsigned char*)(base + o_rrec);
     ta.ntile = ntile;
     ta.tri_half = (int*)(base + o_thalf);
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tri_half, tri_half.data(), tri_half.size() * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.c, tc.data(), tc.size() * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.u, tu.data(), tu.size() * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.jw, tjw.data(), tjw.size() * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.pi, hpi.data(), hpi.size() * 8, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_rwg, tile_rwg.data(), tile_rwg.size() * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.pos, pos.data(), (size_t)N * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_tri, tile_tri.data(), tile_tri.size() * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_ntri, tile_ntri.data(), (size_t)ntile * 4, cudaMemcpyHostToDevice));
-    BEM_TRY_CUDA(ctx, cudaMemcpy(ta.tile_ent, tile_ent.data(), tile_ent.size(), cudaMemcpyHostToDevice));
+    BEM_TRY(h2d(ctx, ta.tri_half, tri_half.data(), tri_half.size() * 4));
+    BEM_TRY(h2d(ctx, ta.c, tc.data(), tc.size() * 8));
+    BEM_TRY(h2d(ctx, ta.u, tu.data(), tu.size() * 8));
+    BEM_TRY(h2d(ctx, ta.jw, tjw.data(), tjw.size() * 8));
+    BEM_TRY(h2d(ctx, ta.pi, hpi.data(), hpi.size() * 8));
+    BEM_TRY(h2d(ctx, ta.tile_rwg, tile_rwg.data(), tile_rwg.size() * 4));
+    BEM_TRY(h2d(ctx, ta.pos, pos.data(), (size_t)N * 4));
+    BEM_TRY(h2d(ctx, ta.tile_tri, tile_tri.data(), tile_tri.size() * 4));
+    BEM_TRY(h2d(ctx, ta.tile_ntri, tile_ntri.data(), (size_t)ntile * 4));
+    BEM_TRY(h2d(ctx, ta.tile_ent, tile_ent.data(), tile_ent.size()));
     // half coefficient and free vertex live right after div (see fixup kernel)
     (void)d_coef;
     (void)d_fr;

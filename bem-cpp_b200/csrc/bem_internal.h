@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -19,6 +20,14 @@ struct Error {
 
 // Records a failure on the context and returns its status.
 int fail(bem_ctx* ctx, int status, const char* fmt, ...);
+
+// Host <-> device copies in the context's stream order (its stream may be a
+// non-blocking one, which the legacy default stream of cudaMemcpy does not
+// wait for): h2d stages the host data before it returns and precedes the
+// kernels launched after it; d2h waits for the stream, so the data is on the
+// host when it returns.
+int h2d(bem_ctx* ctx, void* dst, const void* src, size_t bytes);
+int d2h(bem_ctx* ctx, void* dst, const void* src, size_t bytes);
 
 #define BEM_TRY_CUDA(ctx, call)                                                         \
     do {                                                                                \
@@ -185,6 +194,8 @@ struct bem_ctx {
     size_t oz_bytes = 0;
     bool oz_attr = false;
     int gmres_digits = 0;        // GMRES products with Z: 0 FP64 DMMA GEMM, 2..8 int8 Ozaki digits
+    int grad_method = 0;         // adjoint gradients: 0 contraction kernels (grad_geom.cu), 1 central
+                                 // differences of reassembled operators
     int verify_cols = 64;        // refinement: columns whose error is measured with an FP64 residual
                                  // at convergence (0: none, -1: all)
     int factor_sb = 2;           // L D L^T: 256-column blocks per trailing update (1 or 2)
@@ -247,6 +258,17 @@ int geom_upload(bem_ctx* ctx, bem_geom* g);
 // Right-hand sides and far field equal a new geometry's; the operator does to
 // rounding (the kept tiles fix which orientation of a symmetric pair is computed).
 int geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts);
+// grad_geom.cu: the adjoint contractions of the shape gradient.  X, Lam:
+// forward and adjoint solutions (column-major 2N x ncols); RT_dev, hp_dev,
+// rh_dev: the orientations and the far-field adjoint weights h and rhat x h
+// per (column, angle, component) on the device.  grad_v (host, 3 nv, may be
+// null) receives dloss/dv; dpsi_dk (host, 4 doubles) the complex
+// contractions sum S . d(Z D)/dRe k_int and sum S . d(Z D)/dIm k_int,
+// dpsi_deta (2 doubles) sum S . d(Z D)/deta_int.
+int adjoint_geometry(bem_ctx* ctx, const bem_geom* g, std::complex<double> kext, std::complex<double> kint,
+                     double eta_e, double eta_i, unsigned flags, const void* X, const void* Lam, int ncols,
+                     const double* RT_dev, int n_orient, const void* hp_dev, const void* rh_dev, int ntheta,
+                     double* grad_v, double* dpsi_dk, double* dpsi_deta);
 // rhs / farfield
 int rhs_dev(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im, double eta,
             const double* RT_host, const double* E0_host, const double* khat_host, int n_orient,

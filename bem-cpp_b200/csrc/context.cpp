@@ -21,6 +21,19 @@ int fail(bem_ctx* ctx, int status, const char* fmt, ...) {
     return status;
 }
 
+int h2d(bem_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return BEM_OK;
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return BEM_OK;
+}
+
+int d2h(bem_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return BEM_OK;
+    BEM_TRY_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return BEM_OK;
+}
+
 }  // namespace bem
 
 cudaEvent_t bem_ctx::prof_begin(int cls) {
@@ -292,6 +305,9 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
         ctx->tc_group_m = value;
     } else if (!std::strcmp(name, "persistent_gemm")) {
         ctx->tc_persistent = value != 0;
+    } else if (!std::strcmp(name, "gradient_method")) {
+        if (value != 0 && value != 1) return bem::fail(ctx, BEM_ERR_INVALID, "gradient_method must be 0 or 1");
+        ctx->grad_method = value;
     } else if (!std::strcmp(name, "verify_columns")) {
         if (value < -1) return bem::fail(ctx, BEM_ERR_INVALID, "verify_columns must be -1, 0 or a column count");
         ctx->verify_cols = value;

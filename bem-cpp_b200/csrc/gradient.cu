@@ -182,8 +182,9 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
     }
     const int no = (int)w.size(), nc = 2 * no, nt = p->ntheta;
     const size_t zb = (size_t)n * n * 16, xb = (size_t)n * nc * 16;
+    const bool fd = ctx->grad_method == 1;  // derivatives of reassembled operators (else the contraction kernels)
     DevMem dZ, dZp, dX, dB, dL, dY;
-    if (cudaMalloc(&dZ.p, zb) != cudaSuccess || cudaMalloc(&dZp.p, zb) != cudaSuccess ||
+    if (cudaMalloc(&dZ.p, zb) != cudaSuccess || (fd && cudaMalloc(&dZp.p, zb) != cudaSuccess) ||
         cudaMalloc(&dX.p, xb) != cudaSuccess || cudaMalloc(&dB.p, xb) != cudaSuccess ||
         cudaMalloc(&dL.p, xb) != cudaSuccess || cudaMalloc(&dY.p, xb) != cudaSuccess) {
         cudaGetLastError();
@@ -200,7 +201,7 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
     // the vertex derivatives reassemble only the tiles around a moved vertex
     // into a copy of the unperturbed operator
     DevMem dZbase;
-    if (grad_v) {
+    if (grad_v && fd) {
         if (cudaMalloc(&dZbase.p, zb) != cudaSuccess) {
             cudaGetLastError();
             return fail(ctx, BEM_ERR_OOM, "gradient buffers for n=%d", n);
@@ -311,6 +312,23 @@ static int adjoint_core(bem_ctx* ctx, const bem_problem* p, const double* target
         *re = tr;
         return (int)BEM_OK;
     };
+    if (!fd) {
+        // the contraction kernels (grad_geom.cu): vertex gradient, and the
+        // interior wavenumber / impedance contractions for m
+        const double am = std::abs(m), am3 = am * am * am;
+        double dk[4] = {0, 0, 0, 0}, deta[2] = {0, 0};
+        BEM_TRY(adjoint_geometry(ctx, g, kext, kext * m, eta_e, 1.0 / am, p->asm_flags, dX.p, dL.p, nc,
+                                 (const double*)dRT.p, no, dH.p, dRh.p, nt, grad_v, dk, deta));
+        if (grad_out) {
+            // k_i = k_e m with k_e real: d/dRe m = k_e d/dRe k_i, d/dIm m = k_e d/dIm k_i;
+            // eta_i = 1/|m|
+            grad_out[0] = -(kext.real() * dk[0] + (-m.real() / am3) * deta[0]);
+            grad_out[1] = -(kext.real() * dk[2] + (-m.imag() / am3) * deta[0]);
+        }
+        *loss_out = loss;
+        if (mueller_out) std::memcpy(mueller_out, M.data(), M.size() * 8);
+        return BEM_OK;
+    }
     // dZ/dp by central differences in m, contracted with lambda and x
     const double delta = 1e-5;
     for (int comp = 0; grad_out && comp < 2; comp++) {

@@ -60,9 +60,8 @@ int bem_assemble_L_K(bem_ctx* ctx, const double* verts, int nv, const int* tris,
         s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
     }
     if (s == BEM_OK) s = assemble_dev(ctx, g, k_re, k_im, 0, 0, 1, 1, 0, 1, nullptr, N, dL.p, dK.p);
-    if (s == BEM_OK && (cudaMemcpy(L, dL.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                        cudaMemcpy(K, dK.p, bytes, cudaMemcpyDeviceToHost) != cudaSuccess))
-        s = fail(ctx, BEM_ERR_CUDA, "download L/K");
+    if (s == BEM_OK) s = d2h(ctx, L, dL.p, bytes);
+    if (s == BEM_OK) s = d2h(ctx, K, dK.p, bytes);
     bem_geom_free(g);
     return s;
 }
@@ -85,8 +84,7 @@ int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tr
     if (s == BEM_OK)
         s = assemble_dev(ctx, g, kext_re, kext_im, kint_re, kint_im, eta_ext, eta_int, 0, 2, dZ.p, 2 * N,
                          nullptr, nullptr);
-    if (s == BEM_OK && cudaMemcpy(Z, dZ.p, zb, cudaMemcpyDeviceToHost) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "download Z");
+    if (s == BEM_OK) s = d2h(ctx, Z, dZ.p, zb);
     if (s == BEM_OK && (L_ext || K_ext)) {
         size_t b = (size_t)N * N * 16;
         DevBuf dL, dK;
@@ -95,10 +93,8 @@ int bem_assemble_pmchwt(bem_ctx* ctx, const double* verts, int nv, const int* tr
             s = fail(ctx, BEM_ERR_OOM, "L/K device buffers");
         }
         if (s == BEM_OK) s = assemble_dev(ctx, g, kext_re, kext_im, 0, 0, 1, 1, 0, 1, nullptr, N, dL.p, dK.p);
-        if (s == BEM_OK && L_ext && cudaMemcpy(L_ext, dL.p, b, cudaMemcpyDeviceToHost) != cudaSuccess)
-            s = fail(ctx, BEM_ERR_CUDA, "download L_ext");
-        if (s == BEM_OK && K_ext && cudaMemcpy(K_ext, dK.p, b, cudaMemcpyDeviceToHost) != cudaSuccess)
-            s = fail(ctx, BEM_ERR_CUDA, "download K_ext");
+        if (s == BEM_OK && L_ext) s = d2h(ctx, L_ext, dL.p, b);
+        if (s == BEM_OK && K_ext) s = d2h(ctx, K_ext, dK.p, b);
     }
     bem_geom_free(g);
     return s;
@@ -248,10 +244,8 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
         for (size_t i = 0; i < Mb.size(); i++) Mavg[i] += Mb[i];
         if (r->per_orient_mueller || r->per_orient_weight) {
             Mo.resize((size_t)nb * 16 * nt);
-            if (cudaMemcpy(Mo.data(), dMo.p, Mo.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
-                s = fail(ctx, BEM_ERR_CUDA, "per-orientation Mueller download");
-                break;
-            }
+            s = d2h(ctx, Mo.data(), dMo.p, Mo.size() * 8);
+            if (s != BEM_OK) break;
             for (int o = 0; o < nb; o++) {
                 const double wo = w[o0 + o];
                 if (r->per_orient_weight) r->per_orient_weight[o0 + o] = wo;

@@ -664,8 +664,7 @@ int bem_rhs_planewave(bem_ctx* ctx, const bem_geom* g, double k_re, double k_im,
     size_t bytes = (size_t)2 * g->N * 16;
     BEM_TRY_CUDA(ctx, cudaMalloc(&d, bytes));
     int s = rhs_dev(ctx, g, k_re, k_im, eta_ext, nullptr, E0, k_hat, 1, d, 2 * g->N);
-    if (s == BEM_OK && cudaMemcpy(b, d, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "download b");
+    if (s == BEM_OK) s = d2h(ctx, b, d, bytes);
     cudaFree(d);
     return s;
 }

@@ -133,10 +133,10 @@ static int finish_factor(bem_ctx* ctx, bem_lu* lu, int* d_info, int* info) {
     BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (h[1] != 0) return fail(ctx, h[1], "device-side wait in the panel factorisation gave up");
     lu->ipiv.resize(lu->n);
-    BEM_TRY_CUDA(ctx, cudaMemcpy(lu->ipiv.data(), lu->d_ipiv, lu->n * sizeof(int), cudaMemcpyDeviceToHost));
+    BEM_TRY(d2h(ctx, lu->ipiv.data(), lu->d_ipiv, lu->n * sizeof(int)));
     std::vector<int> perm;
     pivots_to_perm(lu->ipiv, perm);
-    BEM_TRY_CUDA(ctx, cudaMemcpy(lu->d_perm, perm.data(), lu->n * sizeof(int), cudaMemcpyHostToDevice));
+    BEM_TRY(h2d(ctx, lu->d_perm, perm.data(), lu->n * sizeof(int)));
     if (info) *info = h[0];
     return BEM_OK;
 }
@@ -565,7 +565,9 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
                 BEM_TRY(verify_columns(ctx, lu, B, ldb, X, ldx, verify_set(nrhs, nv, col_upd), vws, &tc, &ver));
                 stats.verified_rel_error = ver;
                 stats.verified_columns = nv;
-                est = std::max(est, ver * (nv < nrhs ? 3.0 : 1.0));
+                // checked columns: the factors invert Z only to about the
+                // sweep's contraction, so allow 10 % on the measured error
+                est = std::max(est, ver * (nv < nrhs ? 3.0 : 1.1));
                 stats.est_rel_error = est;
                 fresh = true;
             }
@@ -676,11 +678,9 @@ int bem_lu_factorize(bem_ctx* ctx, double* Z, int n, int* ipiv, int* info) {
     BEM_TRY_CUDA(ctx, cudaMalloc(&d, bytes));
     bem_lu* lu = nullptr;
     int s = BEM_OK, inf = 0;
-    if (cudaMemcpy(d, Z, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "copy Z to device");
+    s = h2d(ctx, d, Z, bytes);
     if (s == BEM_OK) s = lu_factor(ctx, d, n, n, BEM_PREC_FP64, &lu, &inf);
-    if (s == BEM_OK && cudaMemcpy(Z, d, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "copy factors to host");
+    if (s == BEM_OK) s = d2h(ctx, Z, d, bytes);
     if (s == BEM_OK)
         for (int i = 0; i < n; i++) ipiv[i] = lu->ipiv[i] + 1;
     if (lu) lu_release(lu);
@@ -708,14 +708,12 @@ int bem_lu_solve(bem_ctx* ctx, const double* Z_lu, const int* ipiv, int n, doubl
         cudaGetLastError();
         s = fail(ctx, BEM_ERR_OOM, "lu_solve buffers");
     }
-    if (s == BEM_OK && (cudaMemcpy(dz, Z_lu, zb, cudaMemcpyHostToDevice) != cudaSuccess ||
-                        cudaMemcpy(db, B, bb, cudaMemcpyHostToDevice) != cudaSuccess ||
-                        cudaMemcpy(dp, perm.data(), n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess))
-        s = fail(ctx, BEM_ERR_CUDA, "upload");
+    if (s == BEM_OK) s = h2d(ctx, dz, Z_lu, zb);
+    if (s == BEM_OK) s = h2d(ctx, db, B, bb);
+    if (s == BEM_OK) s = h2d(ctx, dp, perm.data(), n * sizeof(int));
     if (s == BEM_OK)
         s = getrs<double>(ctx, (const double2*)dz, n, n, dp, (const double2*)db, n, (double2*)dx, n, nrhs, nullptr);
-    if (s == BEM_OK && cudaMemcpy(B, dx, bb, cudaMemcpyDeviceToHost) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "download");
+    if (s == BEM_OK) s = d2h(ctx, B, dx, bb);
     cudaFree(dz);
     cudaFree(db);
     cudaFree(dx);
@@ -738,16 +736,19 @@ int bem_lu_solve_full(bem_ctx* ctx, double* Z, int n, double* B, int nrhs, int p
         cudaGetLastError();
         s = fail(ctx, BEM_ERR_OOM, "lu_solve_full buffers");
     }
-    if (s == BEM_OK && (cudaMemcpy(dz, Z, zb, cudaMemcpyHostToDevice) != cudaSuccess ||
-                        cudaMemcpy(db, B, bb, cudaMemcpyHostToDevice) != cudaSuccess))
-        s = fail(ctx, BEM_ERR_CUDA, "upload");
+    if (s == BEM_OK) s = h2d(ctx, dz, Z, zb);
+    if (s == BEM_OK) s = h2d(ctx, db, B, bb);
     if (s == BEM_OK) s = lu_factor(ctx, dz, n, n, precision, &lu, &info);
-    if (s == BEM_OK && info > 0) s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+    if (s == BEM_OK && info > 0) {
+        s = fail(ctx, BEM_ERR_SINGULAR, "zero pivot at %d", info);
+        if (stats) {
+            std::memset(stats, 0, sizeof *stats);
+            stats->info = info;
+        }
+    }
     if (s == BEM_OK) s = lu_solve(ctx, lu, db, n, db, n, nrhs, 0.0, 0, stats);
-    if (s == BEM_OK && cudaMemcpy(B, db, bb, cudaMemcpyDeviceToHost) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "download X");
-    if (s == BEM_OK && precision == BEM_PREC_FP64 && cudaMemcpy(Z, dz, zb, cudaMemcpyDeviceToHost) != cudaSuccess)
-        s = fail(ctx, BEM_ERR_CUDA, "download factors");
+    if (s == BEM_OK) s = d2h(ctx, B, db, bb);
+    if (s == BEM_OK && precision == BEM_PREC_FP64) s = d2h(ctx, Z, dz, zb);
     if (lu) lu_release(lu);
     cudaFree(dz);
     cudaFree(db);

@@ -252,6 +252,8 @@ typedef struct bem_solve_stats {
                                   with B - Z X in the FP64 GEMM */
     int exact_residual_sweeps; /* sweeps that fell back to the FP64 GEMM residual, after a check showed
                                   the int8 residual's floor above the tolerance (or without its memory) */
+    int info;                /* bem_lu_solve_full: the LU's info (0, or the 1-based index of the first
+                                zero pivot, with BEM_ERR_SINGULAR) */
 } bem_solve_stats;
 
 /* Factorises the row-major n x n complex128 matrix Z_dev (leading dimension
@@ -272,7 +274,8 @@ int bem_lu_factor_dev(bem_ctx* ctx, void* Z_dev, int n, int64_t ldz, int precisi
  * verify_columns (default 64, -1 all, 0 none; a sample takes half its
  * columns evenly spaced and half where the last sweep's relative update was
  * largest): the FP64-GEMM residual of each, solved through the factors, with
- * the sampled maximum tripled for the columns not checked.  The second term sees the
+ * the sampled maximum tripled for the columns not checked (and the checked
+ * ones taken 10 % above their measured error).  The second term sees the
  * floor that the int8 residual's digit truncation leaves, which the updates
  * cannot; when it is above tol the remaining sweeps compute the residual in
  * the FP64 GEMM (stats->exact_residual_sweeps) and the check is repeated. */
