@@ -82,6 +82,7 @@ struct Quad {
     double l1[25], l2[25], w[25];
 };
 
+bool host_mesh_from(const double* verts, int nv, const int* tris, int nt, HostMesh* m);
 HostMesh make_icosphere(double radius, int refinements);
 HostMesh make_hex_prism(double aspect_ratio, int refinements);
 HostMesh subdivide_flat(const HostMesh& m);
@@ -194,6 +195,8 @@ struct bem_ctx {
     size_t oz_bytes = 0;
     bool oz_attr = false;
     int gmres_digits = 0;        // GMRES products with Z: 0 FP64 DMMA GEMM, 2..8 int8 Ozaki digits
+    bool batch_buckets = true;   // bem_batch_run: FP64 particles of one size batched (else one at a time)
+    bool lu_autotune = true;     // batched LU shape from the autotuner (else NB 256, W 16)
     int grad_method = 0;         // adjoint gradients: 0 contraction kernels (grad_geom.cu), 1 central
                                  // differences of reassembled operators
     int verify_cols = 64;        // refinement: columns whose error is measured with an FP64 residual
@@ -258,6 +261,25 @@ int geom_upload(bem_ctx* ctx, bem_geom* g);
 // Right-hand sides and far field equal a new geometry's; the operator does to
 // rounding (the kept tiles fix which orientation of a symmetric pair is computed).
 int geom_set_vertices(bem_ctx* ctx, bem_geom* g, const double* verts);
+// Batched FP64 LU of `batch` equally sized row-major matrices A + i sA
+// (pivots d_ipiv + i n, info d_info + i): every step of the blocked
+// factorisation is one launch for the whole batch (the panel kernel's CTAs
+// of all matrices meet at one grid barrier).  NB: block columns per trailing
+// update, W: panel width (<= 32); the shapes the autotuner chooses from.
+struct LuShape {
+    int NB = 256, W = 16;
+};
+int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int batch, int* d_ipiv, int* d_info,
+                  LuShape shape);
+// The batched LU's shape for (n, batch), chosen by timing the candidates
+// once on test matrices of order n and kept for the process.
+int tune_lu_shape(bem_ctx* ctx, int n, int batch, LuShape* out);
+// X_i = (P_i^T L_i U_i)^-1 B_i for the batch (perm d_perm + i n).
+int getrs_batched(bem_ctx* ctx, const double2* LU, int64_t lda, int64_t sA, int n, int batch, const int* d_perm,
+                  const double2* B, int64_t ldb, int64_t sB, double2* X, int64_t ldx, int64_t sX, int nrhs,
+                  int NB = 256);
+
+void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm);
 // grad_geom.cu: the adjoint contractions of the shape gradient.  X, Lam:
 // forward and adjoint solutions (column-major 2N x ncols); RT_dev, hp_dev,
 // rh_dev: the orientations and the far-field adjoint weights h and rhat x h

@@ -305,6 +305,10 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
         ctx->tc_group_m = value;
     } else if (!std::strcmp(name, "persistent_gemm")) {
         ctx->tc_persistent = value != 0;
+    } else if (!std::strcmp(name, "batch_buckets")) {
+        ctx->batch_buckets = value != 0;
+    } else if (!std::strcmp(name, "lu_autotune")) {
+        ctx->lu_autotune = value != 0;
     } else if (!std::strcmp(name, "gradient_method")) {
         if (value != 0 && value != 1) return bem::fail(ctx, BEM_ERR_INVALID, "gradient_method must be 0 or 1");
         ctx->grad_method = value;

@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "bem_internal.h"
@@ -38,13 +39,15 @@ template <typename R>
 int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int64_t lda,
           const typename C2T<R>::type* B, int64_t ldb, bool b_kmajor,
           typename C2T<R>::type* C, int64_t ldc, bool c_colmajor,
-          typename C2T<R>::type alpha, typename C2T<R>::type beta, int prof_cls) {
-    if (M <= 0 || N <= 0) return BEM_OK;
+          typename C2T<R>::type alpha, typename C2T<R>::type beta, int prof_cls, int batch, int64_t sA,
+          int64_t sB, int64_t sC) {
+    if (M <= 0 || N <= 0 || batch <= 0) return BEM_OK;
     if (K <= 0) {
         // C = beta*C only; our callers never need it with beta != 1
         return BEM_OK;
     }
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    if (batch > 1 && sizeof(R) != 8) return fail(ctx, BEM_ERR_INVALID, "batched GEMM is FP64 only");
+    dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
     if (grid.y > 65535) return fail(ctx, BEM_ERR_INVALID, "gemm M too large");
     cudaEvent_t ev = prof_cls >= 0 ? ctx->prof_begin(prof_cls) : nullptr;
     if (sizeof(R) == 8) {
@@ -62,7 +65,8 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
                                                        dmma::SMEM_BYTES));
                 attr[slot].fetch_or(bit);
             }
-            kern<<<grid, 128, dmma::SMEM_BYTES, ctx->stream>>>(M, N, K, Ad, lda, Bd, ldb, Cd, ldc, al, be);
+            kern<<<grid, 128, dmma::SMEM_BYTES, ctx->stream>>>(M, N, K, Ad, lda, Bd, ldb, Cd, ldc, al, be, sA, sB,
+                                                               sC);
             return BEM_OK;
         };
         int s;
@@ -84,8 +88,8 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
     }
     BEM_LAUNCHED(ctx);
     if (ev)
-        ctx->prof_end(prof_cls, ev, 8.0 * M * N * K,
-                      (double)sizeof(typename C2T<R>::type) * ((double)M * K + (double)K * N + 2.0 * M * N));
+        ctx->prof_end(prof_cls, ev, 8.0 * M * N * K * batch,
+                      (double)sizeof(typename C2T<R>::type) * ((double)M * K + (double)K * N + 2.0 * M * N) * batch);
     return BEM_OK;
 }
 
@@ -134,10 +138,12 @@ template <typename R> __device__ __forceinline__ R cabs1(typename C2T<R>::type v
 // Factors the sub-panel rows [r0, n), columns [r0, r0+w) of the row-major
 // matrix A.  CTA b owns panel rows [b*Rp, min((b+1)*Rp, nrows)) (relative
 // to r0) in shared memory; Rp >= w so the w pivot rows live in CTA 0.
+// Batched: CTAs [i Gm, (i+1) Gm) factor matrix i (A + i sA, pivots ipiv +
+// i sPiv, info + i); every CTA of the grid meets at the one barrier.
 template <typename R>
 __global__ void __launch_bounds__(256)
 panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nrows, int w, int Rp,
-             int* __restrict__ ipiv, int* __restrict__ info, PanelWS ws) {
+             int* __restrict__ ipiv, int* __restrict__ info, PanelWS ws, int Gm, int64_t sA, int sPiv) {
     using C2 = typename C2T<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C2* tile = (C2*)smem_raw;                   // Rp * w
@@ -149,13 +155,18 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
     __shared__ R s_best;
     __shared__ int s_brow, s_bown;
 
-    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int G = Gm, mi = blockIdx.x / Gm, b = blockIdx.x % Gm, tid = threadIdx.x;
+    const unsigned Gall = gridDim.x;
+    A += mi * sA;
+    ipiv += mi * sPiv;
+    info += mi;
     const int lane = tid & 31, warp = tid >> 5;
     const int lo = b * Rp;
     const int nloc = max(0, min(Rp, nrows - lo));
-    R* cval = (R*)ws.cval;
-    C2* cdata = (C2*)ws.cdata;
-    C2* disp = (C2*)ws.disp;
+    R* cval = (R*)ws.cval + (size_t)mi * 2 * Gm;
+    int* crow = ws.crow + (size_t)mi * 2 * Gm;
+    C2* cdata = (C2*)ws.cdata + (size_t)mi * 2 * Gm * w;
+    C2* disp = (C2*)ws.disp + (size_t)mi * 2 * w;
 
     for (int e = tid; e < nloc * w; e += blockDim.x) {
         int i = e / w, c = e % w;
@@ -187,7 +198,7 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
             s_best = bv;
             s_brow = br;
             __stcg(&cval[par * G + b], bv);
-            __stcg(&ws.crow[par * G + b], br);
+            __stcg(&crow[par * G + b], br);
         }
         __syncthreads();
         br = s_brow;
@@ -196,14 +207,14 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
         if (b == 0)
             for (int c = tid; c < w; c += blockDim.x) __stcg(&disp[par * w + c], tile[jj * w + c]);
         // 2. all candidates published
-        if (!grid_barrier(ws.bar, (unsigned)(jj + 1) * G, ws.status, &s_flag)) return;
+        if (!grid_barrier(ws.bar, (unsigned)(jj + 1) * Gall, ws.status, &s_flag)) return;
         // 3. global argmax (|re|+|im| max, smallest row on ties)
         bv = (R)-1;
         br = 0x7fffffff;
         int bo = -1;
         for (int k = tid; k < G; k += blockDim.x) {
             R v = __ldcg(&cval[par * G + k]);
-            int r = __ldcg(&ws.crow[par * G + k]);
+            int r = __ldcg(&crow[par * G + k]);
             if (r == 0x7fffffff) continue;
             if (v > bv || (v == bv && r < br)) bv = v, br = r, bo = k;
         }
@@ -285,8 +296,10 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
 // two ranges [c0a, c1a) and [c0b, c1b); one thread per column.
 template <typename R>
 __global__ void laswp_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, const int* __restrict__ ipiv,
-                             int k0, int k1, int c0a, int c1a, int c0b, int c1b) {
+                             int k0, int k1, int c0a, int c1a, int c0b, int c1b, int64_t sA = 0, int sPiv = 0) {
     using C2 = typename C2T<R>::type;
+    A += blockIdx.y * sA;  // batched: blockIdx.y selects the matrix
+    ipiv += blockIdx.y * sPiv;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int na = c1a - c0a;
     int c;
@@ -306,7 +319,10 @@ __global__ void laswp_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda,
 template <typename R>
 __global__ void permute_rows_kernel(const typename C2T<R>::type* __restrict__ B, int64_t ldb,
                                     typename C2T<R>::type* __restrict__ X, int64_t ldx, const int* __restrict__ perm,
-                                    int n, int nrhs) {
+                                    int n, int nrhs, int64_t sB = 0, int64_t sX = 0, int sPerm = 0) {
+    B += blockIdx.y * sB;  // batched: blockIdx.y selects the system
+    X += blockIdx.y * sX;
+    if (perm) perm += blockIdx.y * sPerm;
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)n * nrhs) return;
     int r = (int)(i % n), c = (int)(i / n);
@@ -410,7 +426,10 @@ template <typename C2> __device__ __forceinline__ C2 cdiv(C2 a, C2 d) {
 template <typename R, bool UPPER, bool B_ROWMAJOR, int RB, int MODE = 0>
 __global__ void __launch_bounds__(TRSM_KB)
 trsm_block_kernel(const typename C2T<R>::type* __restrict__ T, int64_t ldt, int r0, int kb,
-                  typename C2T<R>::type* __restrict__ B, int64_t ldb, int br0, int c0, int c1) {
+                  typename C2T<R>::type* __restrict__ B, int64_t ldb, int br0, int c0, int c1, int64_t strideT = 0,
+                  int64_t strideB = 0) {
+    T += blockIdx.y * strideT;  // batched: blockIdx.y selects the system
+    B += blockIdx.y * strideB;
     constexpr bool TRANS = (MODE & TRSM_TRANS) != 0, UNIT = (MODE & TRSM_UNIT) != 0,
                    DIVDIAG = (MODE & TRSM_DIVDIAG) != 0;
     auto tel = [&](int i, int j) {  // element (i, j) of the triangle, block-relative
@@ -533,7 +552,8 @@ template <typename R> struct TrsmRB {
 // B's rows of the block start at br0 (at r0, the block's own rows, when br0 < 0).
 template <typename R, bool UPPER, bool B_ROWMAJOR, int MODE = 0>
 int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0, int kb,
-               typename C2T<R>::type* B, int64_t ldb, int c0, int c1, int br0 = -1) {
+               typename C2T<R>::type* B, int64_t ldb, int c0, int c1, int br0 = -1, int batch = 1, int64_t sT = 0,
+               int64_t sB = 0) {
     if (br0 < 0) br0 = r0;
     using C2 = typename C2T<R>::type;
     constexpr int RB = B_ROWMAJOR ? TrsmRB<R>::rows_major : TrsmRB<R>::col_major;
@@ -549,9 +569,9 @@ int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set.fetch_or(bit);
     }
-    const int grid = (c1 - c0 + RB - 1) / RB;
+    const dim3 grid((c1 - c0 + RB - 1) / RB, batch);
     trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB, MODE><<<grid, TRSM_KB, smem, ctx->stream>>>(T, ldt, r0, kb, B, ldb,
-                                                                                           br0, c0, c1);
+                                                                                           br0, c0, c1, sT, sB);
     BEM_LAUNCHED(ctx);
     return BEM_OK;
 }
@@ -560,8 +580,8 @@ int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0
 // columns [c0, c1): the U12 step of the factorisation.
 template <typename R>
 int trsm_rows_lower_unit(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int r0, int kb,
-                         int c0, int c1) {
-    return trsm_block<R, false, true>(ctx, A, lda, r0, kb, A, lda, c0, c1);
+                         int c0, int c1, int batch = 1, int64_t sA = 0) {
+    return trsm_block<R, false, true>(ctx, A, lda, r0, kb, A, lda, c0, c1, -1, batch, sA, sA);
 }
 
 // ------------------------------------------------------------------ getrf
@@ -618,8 +638,10 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
             size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
             if (smem > smem0) return fail(ctx, BEM_ERR_INVALID, "panel smem bound violated");
             BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
+            int64_t s0 = 0;
+            int p0 = 0;
             void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
-                            &d_ipiv, &d_info, &pw};
+                            &d_ipiv, &d_info, &pw, &G, &s0, &p0};
             cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
             BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G), dim3(256),
                                                           args, smem, ctx->stream));
@@ -708,6 +730,219 @@ int getrs(bem_ctx* ctx, const typename C2T<R>::type* LU, int64_t lda, int n, con
     return BEM_OK;
 }
 
+// ------------------------------------------------------------- batched FP64
+// The blocked LU of getrf for a batch of equally sized matrices, one launch
+// per step for the whole batch.  The panel's CTAs per matrix (Gm) are as many
+// as fit co-resident next to the other matrices' (one cooperative grid);
+// batches larger than that are factored in chunks.
+int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int batch, int* d_ipiv, int* d_info,
+                  LuShape shape) {
+    using R = double;
+    using C2 = double2;
+    const int NB = shape.NB, W = shape.W;
+    if (n < 1 || batch < 1) return fail(ctx, BEM_ERR_INVALID, "batched LU: n=%d batch=%d", n, batch);
+    if (W < 1 || W > 32 || NB < W || NB > TRSM_KB || NB % W != 0)
+        return fail(ctx, BEM_ERR_INVALID, "batched LU shape NB=%d W=%d", NB, W);
+    const size_t smem_max = 220 * 1024;
+    const int Rp_max = (int)std::min<int64_t>(n, ((int64_t)smem_max / (int64_t)sizeof(C2) - W) / W);
+    if (Rp_max < 2 * W) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel does not fit");
+    const int Gm_min = (n + Rp_max - 1) / Rp_max;
+    // CTAs per matrix for the first panel, and the batch chunk that fits
+    int Gm = std::max(Gm_min, std::min(std::max(1, n / W), ctx->sm_count));
+    int Rp0 = 0, occ = 0;
+    size_t smem0 = 0;
+    int chunk = 0;
+    BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem_max));
+    for (;;) {
+        Rp0 = std::max((n + Gm - 1) / Gm, 2 * W);
+        smem0 = ((size_t)Rp0 * W + W) * sizeof(C2);
+        BEM_TRY_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<R>, 256, smem0));
+        if (occ < 1) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel kernel does not fit on an SM");
+        chunk = std::min(batch, occ * ctx->sm_count / Gm);
+        if (chunk >= batch || Gm == Gm_min) break;
+        Gm = std::max(Gm_min, std::min(Gm - 1, occ * ctx->sm_count / batch));
+    }
+    if (chunk < 1) return fail(ctx, BEM_ERR_INVALID, "batched LU: no co-resident panel grid");
+    if (chunk < batch) {
+        for (int b0 = 0; b0 < batch; b0 += chunk) {
+            const int nb = std::min(chunk, batch - b0);
+            BEM_TRY(getrf_batched(ctx, A + (int64_t)b0 * sA, lda, sA, n, nb, d_ipiv + (int64_t)b0 * n, d_info + b0,
+                                  shape));
+        }
+        return BEM_OK;
+    }
+    size_t ws_bytes = 0;
+    auto take = [&](size_t b) { size_t o = ws_bytes; ws_bytes += (b + 255) & ~(size_t)255; return o; };
+    const size_t per = (size_t)batch * 2 * Gm;
+    size_t o_cval = take(per * sizeof(R)), o_crow = take(per * 4), o_cdata = take(per * W * sizeof(C2)),
+           o_disp = take((size_t)batch * 2 * W * sizeof(C2)), o_bar = take(256);
+    BEM_TRY(ctx->ensure_ws(ws_bytes));
+    char* ws = (char*)ctx->ws;
+    PanelWS pw;
+    pw.cval = ws + o_cval;
+    pw.crow = (int*)(ws + o_crow);
+    pw.cdata = ws + o_cdata;
+    pw.disp = ws + o_disp;
+    pw.bar = (unsigned*)(ws + o_bar);
+    pw.status = ctx->d_status;
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, batch * sizeof(int), ctx->stream));
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+    const C2 m1 = mk<C2>(-1, 0), p1 = mk<C2>(1, 0);
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = std::min(NB, n - j0);
+        for (int i0 = j0; i0 < j0 + jb; i0 += W) {
+            const int iw = std::min(W, j0 + jb - i0);
+            const int nrows = n - i0;
+            int G = std::min(Gm, std::max(1, nrows / iw));
+            const int Rp = (nrows + G - 1) / G;
+            G = (nrows + Rp - 1) / Rp;
+            const size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
+            if (smem > smem0 || Rp < iw) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel bound violated");
+            BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
+            int spiv = n;
+            void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
+                            &d_ipiv, &d_info, &pw, &G, &sA, &spiv};
+            cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
+            BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G * batch), dim3(256), args,
+                                                          smem, ctx->stream));
+            BEM_LAUNCHED(ctx);
+            if (ev)
+                ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2 * batch,
+                              (double)nrows * iw * 2 * sizeof(C2) * batch);
+            const int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
+            const int ncol = (ca1 - ca0) + (cb1 - cb0);
+            if (ncol > 0) {
+                laswp_kernel<R><<<dim3((ncol + 255) / 256, batch), 256, 0, ctx->stream>>>(
+                    A, lda, d_ipiv, i0, i0 + iw, ca0, ca1, cb0, cb1, sA, n);
+                BEM_LAUNCHED(ctx);
+            }
+            if (cb1 > cb0) {
+                BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, i0, iw, cb0, cb1, batch, sA));
+                BEM_TRY(cgemm<R>(ctx, n - i0 - iw, cb1 - cb0, iw, A + (int64_t)(i0 + iw) * lda + i0, lda,
+                                 A + (int64_t)i0 * lda + cb0, lda, false, A + (int64_t)(i0 + iw) * lda + cb0, lda,
+                                 false, m1, p1, -1, batch, sA, sA, sA));
+            }
+        }
+        const int ncol = j0 + (n - j0 - jb);
+        if (ncol > 0) {
+            laswp_kernel<R><<<dim3((ncol + 255) / 256, batch), 256, 0, ctx->stream>>>(A, lda, d_ipiv, j0, j0 + jb, 0,
+                                                                                      j0, j0 + jb, n, sA, n);
+            BEM_LAUNCHED(ctx);
+        }
+        const int c0 = j0 + jb;
+        if (c0 < n) {
+            BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0, jb, c0, n, batch, sA));
+            const int Mt = n - c0;
+            BEM_TRY(cgemm<R>(ctx, Mt, Mt, jb, A + (int64_t)c0 * lda + j0, lda, A + (int64_t)j0 * lda + c0, lda, false,
+                             A + (int64_t)c0 * lda + c0, lda, false, m1, p1, PROF_LU_UPDATE, batch, sA, sA, sA));
+        }
+    }
+    return BEM_OK;
+}
+
+int getrs_batched(bem_ctx* ctx, const double2* LU, int64_t lda, int64_t sA, int n, int batch, const int* d_perm,
+                  const double2* B, int64_t ldb, int64_t sB, double2* X, int64_t ldx, int64_t sX, int nrhs, int NB) {
+    using R = double;
+    using C2 = double2;
+    if (nrhs <= 0 || batch <= 0) return BEM_OK;
+    if (NB < 1 || NB > TRSM_KB) return fail(ctx, BEM_ERR_INVALID, "batched solve block %d", NB);
+    const int64_t tot = (int64_t)n * nrhs;
+    permute_rows_kernel<R><<<dim3((unsigned)((tot + 255) / 256), batch), 256, 0, ctx->stream>>>(
+        B, ldb, X, ldx, d_perm, n, nrhs, sB, sX, n);
+    BEM_LAUNCHED(ctx);
+    const C2 m1 = mk<C2>(-1, 0), p1 = mk<C2>(1, 0);
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int jb = std::min(NB, n - j0);
+        BEM_TRY((trsm_block<R, false, false>(ctx, LU, lda, j0, jb, X, ldx, 0, nrhs, -1, batch, sA, sX)));
+        const int below = n - j0 - jb;
+        if (below > 0)
+            BEM_TRY(cgemm<R>(ctx, below, nrhs, jb, LU + (int64_t)(j0 + jb) * lda + j0, lda, X + j0, ldx, true,
+                             X + j0 + jb, ldx, true, m1, p1, PROF_SOLVE_UPDATE, batch, sA, sX, sX));
+    }
+    const int nblk = (n + NB - 1) / NB;
+    for (int bi = nblk - 1; bi >= 0; bi--) {
+        const int j0 = bi * NB, jb = std::min(NB, n - j0);
+        BEM_TRY((trsm_block<R, true, false>(ctx, LU, lda, j0, jb, X, ldx, 0, nrhs, -1, batch, sA, sX)));
+        if (j0 > 0)
+            BEM_TRY(cgemm<R>(ctx, j0, nrhs, jb, LU + j0, lda, X + j0, ldx, true, X, ldx, true, m1, p1,
+                             PROF_SOLVE_UPDATE, batch, sA, sX, sX));
+    }
+    return BEM_OK;
+}
+
+// Deterministic fill of a batch of test matrices for the autotuner: entries
+// in [-1, 1) from an integer hash, plus n on the diagonal.
+static __global__ void tune_fill_kernel(double2* A, int n, int64_t total) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const double re = (double)(h & 0xFFFFFF) / 8388608.0 - 1.0, im = (double)((h >> 24) & 0xFFFFFF) / 8388608.0 - 1.0;
+    const int64_t e = i % ((int64_t)n * n);
+    const bool diag = e / n == e % n;
+    A[i] = make_double2(re + (diag ? n : 0.0), im);
+}
+
+// Shape of the batched FP64 LU for (n, batch): every candidate block / panel
+// width is timed once (after one warm-up) on min(batch, 8) test matrices of
+// order n, and the fastest kept for the context's later batches of that
+// shape.
+int tune_lu_shape(bem_ctx* ctx, int n, int batch, LuShape* out) {
+    static std::map<std::pair<int, int>, LuShape> cache;  // per process: (n, batch) -> shape
+    const int tb = std::min(batch, 8);
+    const auto key = std::make_pair(n, tb);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        *out = it->second;
+        return BEM_OK;
+    }
+    const LuShape cands[] = {{256, 16}, {128, 16}, {256, 32}, {128, 32}, {256, 8}, {64, 16}};
+    const size_t nn = (size_t)n * n;
+    void* A = devmem_alloc(ctx->device, nn * tb * sizeof(double2), ctx);
+    void* ip = devmem_alloc(ctx->device, (size_t)n * tb * sizeof(int) + (size_t)tb * sizeof(int), ctx);
+    if (!A || !ip) {
+        if (A) devmem_free(ctx->device, A, nn * tb * sizeof(double2), ctx);
+        if (ip) devmem_free(ctx->device, ip, (size_t)n * tb * sizeof(int) + (size_t)tb * sizeof(int), ctx);
+        *out = LuShape{};
+        return BEM_OK;  // no room to tune: the default shape
+    }
+    int* d_ipiv = (int*)ip;
+    int* d_info = d_ipiv + (size_t)n * tb;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    LuShape pick{};
+    int s = BEM_OK;
+    for (const LuShape& c : cands) {
+        if (c.NB > n && c.NB != 256) continue;
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && s == BEM_OK; rep++) {
+            const int64_t tot = (int64_t)nn * tb;
+            tune_fill_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>((double2*)A, n, tot);
+            ctx->launches++;
+            cudaEventRecord(e0, ctx->stream);
+            s = getrf_batched(ctx, (double2*)A, n, (int64_t)nn, n, tb, d_ipiv, d_info, c);
+            cudaEventRecord(e1, ctx->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) s = fail(ctx, BEM_ERR_CUDA, "LU autotuner");
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (s != BEM_OK) break;
+        if (ms < best) best = ms, pick = c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    devmem_free(ctx->device, A, nn * tb * sizeof(double2), ctx);
+    devmem_free(ctx->device, ip, (size_t)n * tb * sizeof(int) + (size_t)tb * sizeof(int), ctx);
+    if (s != BEM_OK) return s;
+    cache[key] = pick;
+    *out = pick;
+    return BEM_OK;
+}
+
 template int getrf<double>(bem_ctx*, double2*, int64_t, int, int*, int*, const TrailingUpdate<double>*);
 template int getrf<float>(bem_ctx*, float2*, int64_t, int, int*, int*, const TrailingUpdate<float>*);
 template int getrs<double>(bem_ctx*, const double2*, int64_t, int, const int*, const double2*, int64_t,
@@ -715,9 +950,9 @@ template int getrs<double>(bem_ctx*, const double2*, int64_t, int, const int*, c
 template int getrs<float>(bem_ctx*, const float2*, int64_t, int, const int*, const float2*, int64_t,
                           float2*, int64_t, int, const TrailingUpdate<float>*);
 template int cgemm<double>(bem_ctx*, int, int, int, const double2*, int64_t, const double2*, int64_t, bool,
-                           double2*, int64_t, bool, double2, double2, int);
+                           double2*, int64_t, bool, double2, double2, int, int, int64_t, int64_t, int64_t);
 template int cgemm<float>(bem_ctx*, int, int, int, const float2*, int64_t, const float2*, int64_t, bool,
-                          float2*, int64_t, bool, float2, float2, int);
+                          float2*, int64_t, bool, float2, float2, int, int, int64_t, int64_t, int64_t);
 
 // ============================================================ L D L^T
 // Complex-symmetric factorisation without pivoting, S = L D L^T, for the

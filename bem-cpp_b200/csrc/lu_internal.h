@@ -45,11 +45,14 @@ template <typename R> struct TrailingUpdate {
     void* state = nullptr;
 };
 
+// batch > 1 (FP64 only): `batch` products with the operands offset by sA,
+// sB, sC elements per product.
 template <typename R>
 int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int64_t lda,
           const typename C2T<R>::type* B, int64_t ldb, bool b_kmajor,
           typename C2T<R>::type* C, int64_t ldc, bool c_colmajor,
-          typename C2T<R>::type alpha, typename C2T<R>::type beta, int prof_cls = -1);
+          typename C2T<R>::type alpha, typename C2T<R>::type beta, int prof_cls = -1, int batch = 1,
+          int64_t sA = 0, int64_t sB = 0, int64_t sC = 0);
 
 template <typename R>
 int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipiv, int* d_info,

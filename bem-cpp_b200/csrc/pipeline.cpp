@@ -7,6 +7,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -304,11 +305,140 @@ int bem_dense_run(bem_ctx* ctx, const bem_problem* p, bem_result* r) {
     return s;
 }
 
-// Batched particles: every problem through the dense pipeline in turn on the
-// context's stream.  statuses[i] (optional) receives each problem's status;
-// a failing particle does not stop the batch.  Returns BEM_OK, or the first
-// failure.  (Worker contexts on several streams were measured slower: the
-// persistent tensor-core kernels take one CTA per SM and do not overlap.)
+}  // extern "C"
+
+namespace {
+
+// A bucket of FP64 particles with the same system size: every particle's
+// operator assembled into one batch, one batched LU and one batched solve of
+// all their right-hand sides (each launch covers the whole bucket), then the
+// far field / Mueller matrix of each.  The batched LU is the blocked LU of the
+// single path step for step (bitwise the same factors with the default shape).
+int run_fp64_bucket(bem_ctx* ctx, const bem_problem* problems, const std::vector<int>& idx, bem_result* results,
+                    int* statuses) {
+    auto t_all = std::chrono::steady_clock::now();
+    const int cnt = (int)idx.size();
+    std::vector<bem_geom*> gs(cnt, nullptr);
+    std::vector<std::vector<double>> RTs(cnt), ws(cnt);
+    int n = 0, nrhs = 0, s = BEM_OK;
+    for (int i = 0; i < cnt && s == BEM_OK; i++) {
+        const bem_problem* p = &problems[idx[i]];
+        int N = 0;
+        s = bem_geom_create(ctx, p->verts, p->nv, p->tris, p->nt, p->quad_order, &gs[i], &N);
+        if (s != BEM_OK) break;
+        n = 2 * N;
+        if (p->single) {
+            RTs[i] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+            ws[i] = {1.0};
+        } else {
+            orientations(p->n_alpha, p->n_beta, p->n_gamma, p->beta_sym < 1 ? 1 : p->beta_sym,
+                         p->gamma_sym < 1 ? 1 : p->gamma_sym, p->gamma_mirror != 0, true, RTs[i], ws[i]);
+        }
+        nrhs = std::max(nrhs, 2 * (int)ws[i].size());
+    }
+    const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs;
+    DevBuf dZ, dB, dX, dP;
+    if (s == BEM_OK && (!dZ.alloc(ctx, nn * cnt * 16) || !dB.alloc(ctx, nb * cnt * 16) ||
+                        !dX.alloc(ctx, nb * cnt * 16) || !dP.alloc(ctx, ((size_t)2 * n * cnt + cnt) * sizeof(int)))) {
+        cudaGetLastError();
+        s = fail(ctx, BEM_ERR_OOM, "bucket of %d particles of order %d", cnt, n);
+    }
+    double t_asm = 0, t_solve = 0, t_ff = 0;
+    LuShape shape;
+    if (s == BEM_OK && ctx->lu_autotune) s = tune_lu_shape(ctx, n, cnt, &shape);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < cnt && s == BEM_OK; i++) {
+        const bem_problem* p = &problems[idx[i]];
+        const std::complex<double> m(p->m_re, p->m_im), kext(p->ka, 0.0), kint = kext * m;
+        s = assemble_dev(ctx, gs[i], kext.real(), kext.imag(), kint.real(), kint.imag(), 1.0, 1.0 / std::abs(m),
+                         p->asm_flags, 2, (double2*)dZ.p + nn * i, n, nullptr, nullptr);
+    }
+    if (s == BEM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "bucket assembly: %s", cudaGetErrorString(cudaGetLastError()));
+    t_asm = secs(t0);
+    auto t1 = std::chrono::steady_clock::now();
+    int* d_ipiv = (int*)dP.p;
+    int* d_perm = d_ipiv + (size_t)n * cnt;
+    int* d_info = d_perm + (size_t)n * cnt;
+    std::vector<int> info(cnt, 0), piv((size_t)n * cnt), perm;
+    if (s == BEM_OK) s = getrf_batched(ctx, (double2*)dZ.p, n, (int64_t)nn, n, cnt, d_ipiv, d_info, shape);
+    if (s == BEM_OK) s = d2h(ctx, info.data(), d_info, cnt * sizeof(int));
+    if (s == BEM_OK) {
+        int h_st = 0;
+        s = d2h(ctx, &h_st, ctx->d_status, sizeof(int));
+        if (s == BEM_OK && h_st != 0) s = fail(ctx, h_st, "device-side wait in the batched panel factorisation");
+    }
+    if (s == BEM_OK) s = d2h(ctx, piv.data(), d_ipiv, piv.size() * sizeof(int));
+    if (s == BEM_OK) {
+        std::vector<int> all((size_t)n * cnt);
+        for (int i = 0; i < cnt; i++) {
+            std::vector<int> pv(piv.begin() + (size_t)n * i, piv.begin() + (size_t)n * (i + 1));
+            pivots_to_perm(pv, perm);
+            std::copy(perm.begin(), perm.end(), all.begin() + (size_t)n * i);
+        }
+        s = h2d(ctx, d_perm, all.data(), all.size() * sizeof(int));
+    }
+    if (s == BEM_OK) {
+        BEM_TRY_CUDA(ctx, cudaMemsetAsync(dB.p, 0, nb * cnt * 16, ctx->stream));
+        for (int i = 0; i < cnt && s == BEM_OK; i++) {
+            const bem_problem* p = &problems[idx[i]];
+            s = rhs_dev(ctx, gs[i], p->ka, 0.0, 1.0, RTs[i].data(), nullptr, nullptr, (int)ws[i].size(),
+                        (double2*)dB.p + nb * i, n);
+        }
+    }
+    if (s == BEM_OK)
+        s = getrs_batched(ctx, (const double2*)dZ.p, n, (int64_t)nn, n, cnt, d_perm, (const double2*)dB.p, n,
+                          (int64_t)nb, (double2*)dX.p, n, (int64_t)nb, nrhs, shape.NB);
+    if (s == BEM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        s = fail(ctx, BEM_ERR_CUDA, "bucket solve: %s", cudaGetErrorString(cudaGetLastError()));
+    t_solve = secs(t1);
+    auto t2 = std::chrono::steady_clock::now();
+    for (int i = 0; i < cnt; i++) {
+        const bem_problem* p = &problems[idx[i]];
+        bem_result* r = &results[idx[i]];
+        int si = s;
+        if (si == BEM_OK && info[i] > 0) si = fail(ctx, BEM_ERR_SINGULAR, "particle %d: zero pivot at %d", idx[i], info[i]);
+        if (si == BEM_OK) {
+            const int no = (int)ws[i].size(), nt = p->ntheta;
+            std::vector<double> M((size_t)16 * nt);
+            si = mueller_dev(ctx, gs[i], (double2*)dX.p + nb * i, n, RTs[i].data(), ws[i].data(), no, p->ka, 0.0, 1.0,
+                             nt, p->gamma_mirror, M.data(), nullptr);
+            if (si == BEM_OK) std::memcpy(r->mueller, M.data(), M.size() * 8);
+            r->N = n / 2;
+            r->n_orient = no;
+            r->n_computed = no;
+            std::memset(&r->stats, 0, sizeof r->stats);
+            r->stats.converged = 1;
+            r->stats.factorization = -1;
+        }
+        if (statuses) statuses[idx[i]] = si;
+    }
+    t_ff = secs(t2);
+    for (int i = 0; i < cnt; i++) {
+        bem_result* r = &results[idx[i]];
+        // the bucket's phase times, shared equally by its particles
+        r->t_assembly_s = t_asm / cnt;
+        r->t_solve_s = t_solve / cnt;
+        r->t_farfield_s = t_ff / cnt;
+        r->t_total_s = secs(t_all) / cnt;
+        if (gs[i]) bem_geom_free(gs[i]);
+    }
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Batched particles.  FP64 particles of one system size (without adaptive
+// orientation stopping, GMRES or per-orientation output) go through
+// run_fp64_bucket: one batched assembly pass, batched LU and batched solve per
+// size, with the LU's block / panel shape chosen by the autotuner; the others
+// through the dense pipeline in turn.  statuses[i] (optional) receives each
+// problem's status; a failing particle does not stop the batch.  Returns
+// BEM_OK, or the first failure.  (Worker contexts on several streams were
+// measured slower: the persistent tensor-core kernels take one CTA per SM and
+// do not overlap.)
 int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_result* results, int* statuses) {
     if (!ctx || count < 0 || (count > 0 && (!problems || !results))) return BEM_ERR_INVALID;
     // particles of one topology reuse their device buffers (operator,
@@ -319,11 +449,33 @@ int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_resu
     if (!had_cache) devmem_cache_enable(ctx->device, true);
     int first = BEM_OK;
     std::string first_msg;
+    std::vector<int> st(count, BEM_OK);
+    std::vector<char> done(count, 0);
+    if (ctx->batch_buckets) {
+        // FP64 particles grouped by system size (2N from the mesh's RWG count)
+        std::map<int, std::vector<int>> buckets;
+        for (int i = 0; i < count; i++) {
+            const bem_problem& p = problems[i];
+            if (p.precision != BEM_PREC_FP64 || p.solver != BEM_SOLVER_LU || p.orient_tol > 0 ||
+                results[i].per_orient_mueller || results[i].per_orient_weight || !results[i].mueller ||
+                !(p.ka > 0) || p.ntheta < 2 || (!p.single && p.orient_i0 >= 0))
+                continue;
+            HostMesh hm;
+            if (!host_mesh_from(p.verts, p.nv, p.tris, p.nt, &hm)) continue;
+            buckets[build_rwg(hm).N].push_back(i);
+        }
+        for (auto& kv : buckets) {
+            if (kv.second.size() < 2) continue;
+            std::vector<int> sts(count, BEM_OK);
+            run_fp64_bucket(ctx, problems, kv.second, results, sts.data());
+            for (int i : kv.second) st[i] = sts[i], done[i] = 1;
+        }
+    }
     for (int i = 0; i < count; i++) {
-        int s = bem_dense_run(ctx, &problems[i], &results[i]);
-        if (statuses) statuses[i] = s;
-        if (s != BEM_OK && first == BEM_OK) {
-            first = s;
+        if (!done[i]) st[i] = bem_dense_run(ctx, &problems[i], &results[i]);
+        if (statuses) statuses[i] = st[i];
+        if (st[i] != BEM_OK && first == BEM_OK) {
+            first = st[i];
             first_msg = "particle " + std::to_string(i) + ": " + ctx->last_error;
         }
     }

@@ -55,7 +55,12 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 template <bool B_KMAJOR, bool C_COLMAJOR>
 __global__ void __launch_bounds__(128, 3)
 zgemm_kernel(int M, int N, int K, const double2* __restrict__ A, int64_t lda, const double2* __restrict__ B,
-             int64_t ldb, double2* __restrict__ C, int64_t ldc, double2 alpha, double2 beta) {
+             int64_t ldb, double2* __restrict__ C, int64_t ldc, double2 alpha, double2 beta, int64_t sA = 0,
+             int64_t sB = 0, int64_t sC = 0) {
+    // a batch of equally shaped products: blockIdx.z selects the matrices
+    A += blockIdx.z * sA;
+    B += blockIdx.z * sB;
+    C += blockIdx.z * sC;
     extern __shared__ __align__(16) double sm[];
     double* As = sm;                          // STAGES x A_STAGE
     double* Bs = sm + STAGES * A_STAGE;       // STAGES x B_STAGE

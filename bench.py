@@ -19,9 +19,13 @@ plain FP64 LU + solve of the same Z is timed once beside it and is the
 oracle of the 1e-9 error check.  e2e = the whole pipeline through the C ABI
 call bem_dense_run (host mesh in, host Mueller matrix out).
 
---impl reference: the reference's CPU path for the solve (LAPACK zgetrf /
-zgetrs through SciPy, bem_core.py:1637, 1713) on a bounded sample, scaled to
-the workload.
+--impl reference: the reference's CPU dense path (python/bem_core.py,
+restated by the oracle: assembly, LAPACK zgetrf / zgetrs as bem_core.py:1637,
+1713 call them, far field) on bounded samples scaled to the workload; value
+is the solve, e2e the whole path.
+
+--config c1 | c2 | c4 | c5: the other workloads of the path (run_config);
+the default, c3, is the metric's.
 
 --impl cusolver: the reference's GPU call for the solve, cuSOLVER getrf +
 getrs in FP64 (solver.cu:87-142; 64-bit API, baseline/cusolver_lu.cpp), on
@@ -90,6 +94,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c3: the metric's workload; c1, c2, c4, c5: the other configurations")
     return ap.parse_args()
 
 
@@ -101,46 +107,28 @@ def workload(a, n):
 
 
 # ---------------------------------------------------------------- CPU baseline
-def cpu_sample(n_full, nrhs_full, n_s=8192, reps=1, seed=0):
-    """Oracle LAPACK solve (zgetrf + zgetrs, complex128) of an n_s x n_s
-    seeded matrix with nrhs_s = nrhs_full * n_s / n_full right-hand sides;
-    scaled by (n/n_s)^3 for the factorisation and (n/n_s)^2 (nrhs/nrhs_s) for
-    the solves.  Returns (s/solve scaled, cores, description)."""
-    import numpy as np
-    from oracle import bem_oracle  # noqa: F401  (the oracle's LU is scipy's LAPACK)
-    from scipy.linalg import lu_factor, lu_solve
-    rng = np.random.default_rng(seed)
-    A = rng.standard_normal((n_s, n_s)) + 1j * rng.standard_normal((n_s, n_s))
-    nr = max(1, round(nrhs_full * n_s / n_full))
-    B = rng.standard_normal((n_s, nr)) + 1j * rng.standard_normal((n_s, nr))
-    tf, ts = [], []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        f = lu_factor(A)
-        t1 = time.perf_counter()
-        lu_solve(f, B)
-        t2 = time.perf_counter()
-        tf.append(t1 - t0)
-        ts.append(t2 - t1)
-    tfm, tsm = statistics.median(tf), statistics.median(ts)
-    scaled = tfm * (n_full / n_s) ** 3 + tsm * (n_full / n_s) ** 2 * (nrhs_full / nr)
-    cores = os.cpu_count() or 1
-    desc = (f"scipy LAPACK zgetrf+zgetrs on n={n_s}, nrhs={nr} (median of {reps}: factor "
-            f"{tfm:.2f} s, solve {tsm:.2f} s), scaled by n^3 / n^2 nrhs to n={n_full}, "
-            f"nrhs={nrhs_full}; {_cpu_model()}, {cores} logical cores, OPENBLAS_NUM_THREADS="
-            f"{os.environ.get('OPENBLAS_NUM_THREADS', 'unset')}")
-    return scaled, cores, desc, tfm + tsm
+# The reference's CPU dense path (python/bem_core.py: assemble_pmchwt :1032,
+# lu_factor / lu_solve :1637 / :1713, the far field of
+# orientation_average_mueller_batched :1606) restated by the oracle and timed
+# on samples scaled by operation counts (oracle/cpu_dense_path.py).  At
+# 2N = 61440 one sample is ~5 s of CPU work; the full path would take hours.
+def c3_sample_kw(ref):
+    import bem_b200 as bb
+    vs, ts = bb.icosphere(1.0, min(ref, 3))
+    return dict(rows=2, n_lu=4096, n_ff=1, ff_dirs=19, sing_mesh=(vs, ts))
 
 
-def _cpu_model():
-    try:
-        with open("/proc/cpuinfo") as f:
-            for line in f:
-                if line.startswith("model name"):
-                    return line.split(":", 1)[1].strip()
-    except OSError:
-        pass
-    return "CPU model unknown"
+def cpu_dense_path(verts, tris, ka, m, n_orient, ntheta=181, reps=1, **sample):
+    """Median over `reps` of the sampled CPU reference path; returns the dict of
+    oracle.cpu_dense_path.time_dense_path with the medians."""
+    from oracle.cpu_dense_path import time_dense_path
+    runs = [time_dense_path(verts, tris, ka, m, n_orient, ntheta, seed=i, **sample) for i in range(reps)]
+    out = dict(runs[-1])
+    for k in ("assembly", "lu", "solve", "farfield", "total", "solve_only"):
+        if k in out:
+            out[k] = statistics.median(r[k] for r in runs)
+    out["description"] += f" (median of {reps})" if reps > 1 else ""
+    return out
 
 
 # ---------------------------------------------------------------- clocks
@@ -198,27 +186,39 @@ def peaks():
 
 # ---------------------------------------------------------------- reference arm
 def run_reference(a):
+    """The reference's CPU dense path on this host's cores: each step one
+    bounded sample of the workload (oracle/cpu_dense_path.py), scaled to the
+    full size.  value: the solve (LU + the 2790-column solves), the metric's
+    scope; e2e: assembly + solve + far field, the scope of this library's e2e
+    line."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import numpy as np  # noqa: F401
-    nrhs = 2 * a.orient[0] * a.orient[1] * a.orient[2]
+    import bem_b200 as bb
+    verts, tris = bb.icosphere(1.0, a.ref)
+    no = a.orient[0] * a.orient[1] * a.orient[2]
     n = 2 * _n_rwg_ico(a.ref)
-    vals = []
+    kw = c3_sample_kw(a.ref)
+    vals, tots, last = [], [], None
     for i in range(a.warmup + a.steps):
-        v, cores, desc, wall = cpu_sample(n, nrhs, n_s=6144, reps=1, seed=i)
+        from oracle.cpu_dense_path import time_dense_path
+        r = time_dense_path(verts, tris, a.ka, a.m, no, 181, seed=i, **kw)
         if i >= a.warmup:
-            vals.append(v)
-    val = statistics.median(vals)
+            vals.append(r["solve_only"])
+            tots.append(r["total"])
+            last = r
+    val, tot = statistics.median(vals), statistics.median(tots)
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "s/solve",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": val * 1e3,
             "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
-            "dtype": "complex128", "data": "synthetic (seeded matrix of the workload's kind)",
+            "dtype": "complex128", "data": "synthetic (generated icosphere mesh and plane waves)",
             "config": workload(a, n),
-            "cpu_baseline": {"value": val, "unit": "s/solve", "cores": cores, "kind": "port",
-                             "sample": desc},
-            "e2e": {"value": val, "unit": "s/solve", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "extrapolated": "each step times a sample of every phase and scales it by operation counts",
+            "phases_s": {k: last[k] for k in ("assembly", "lu", "solve", "farfield")},
+            "cpu_baseline": {"value": val, "unit": "s/solve", "cores": last["cores"], "kind": "port",
+                             "sample": last["description"]},
+            "e2e": {"value": tot, "unit": "s/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "scope": "assembly + LU + solves + far field / Mueller (sampled, scaled)"}}
     print(json.dumps(line), flush=True)
 
 
@@ -537,8 +537,10 @@ def run_bem(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        v, cores, desc, wall = cpu_sample(n, 2 * no_all, n_s=8192, reps=3)
-        cpu = {"value": v, "unit": "s/solve", "cores": cores, "kind": "port", "sample": desc}
+        r = cpu_dense_path(verts, tris, a.ka, a.m, no_all, 181, reps=3, **c3_sample_kw(a.ref))
+        cpu = {"value": r["solve_only"], "unit": "s/solve", "cores": r["cores"], "kind": "port",
+               "sample": r["description"], "e2e_value": r["total"],
+               "phases_s": {k: r[k] for k in ("assembly", "lu", "solve", "farfield")}}
 
     if rank == 0:
         its = [s["iterations"] for s in stats]
@@ -579,9 +581,303 @@ def run_bem(a):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- other configurations
+CONFIGS = {
+    "c1": {"metric": "s per C1 run: icosphere r2 (2N=960), ka=1, m=1.3116, single orientation, 181 angles, FP64",
+           "workload": "icosphere ref 2 (2N=960), ka=1, m=1.3116, quad 7, --single (k=z, E=x/y), 181 angles"},
+    "c2": {"metric": "s/solve at C2: hex prism AR 1.4286 r3 (2N=4608), ka=5, 128 RHS, FP64 LU + solves",
+           "workload": "hex prism AR=1.4286 ref 3 (2N=4608), ka=5, m=1.3116, quad 7, 8x8x1 orientations x 2 pol"},
+    "c4": {"metric": "s per batch of 64 seeded hex prisms (2N 1152 / 4608): assembly + LU + solves + Mueller",
+           "workload": "64 hex prisms from seed 0: AR U[0.5,2], ref 2 or 3, ka U[1,5], Re m U[1.3,1.6], "
+                       "Im m logU[1e-6,1e-2], 4x4x1 orientations x 2 pol, 181 angles"},
+    "c5": {"metric": "s per adjoint gradient at C5: 1926 vertex coordinates + Re/Im m",
+           "workload": "icosphere ref 3 (642 vertices, 2N=3840) displaced by a seeded degree<=6 field (RMS 0.05), "
+                       "ka=5, m=1.5+0.01i, 8x8x1 orientations, loss sum (M11 - M11_sphere)^2 over 181 angles"},
+}
+
+
+def _ref_gpu_run(args):
+    """The reference's own GPU dense path (its sources built by
+    oracle/Makefile into oracle/_ref/ref_dense_branch, driven by the same
+    consumer program the tests build against this library), and the same
+    program built against this library's compat surface: wall times and the
+    phase times each reports through write_json."""
+    import shutil
+    import tempfile
+    exe_ref = os.path.join(REPO, "oracle", "_ref", "ref_dense_branch")
+    if not os.path.exists(exe_ref):
+        return {"unavailable": "oracle/_ref/ref_dense_branch not built (needs the reference sources)"}
+    tmp = tempfile.mkdtemp(prefix="bem_refgpu_")
+    lib = os.path.join(REPO, "bem-cpp_b200", "lib")
+    exe_ours = os.path.join(tmp, "dense_branch")
+    r = subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(REPO, "include", "bem"),
+                        "-I" + os.path.join(REPO, "include"), "-o", exe_ours,
+                        os.path.join(REPO, "tests", "compat", "dense_branch.cpp"), "-L" + lib,
+                        "-Wl,-rpath," + lib, "-lbem_compat", "-lbemdense"], capture_output=True, text=True)
+    if r.returncode != 0:
+        return {"unavailable": "compat consumer did not build: " + r.stderr[-200:]}
+    out = {}
+    for tag, exe in (("reference", exe_ref), ("bem", exe_ours)):
+        d = os.path.join(tmp, tag)
+        os.makedirs(d)
+        t0 = time.perf_counter()
+        p = subprocess.run([exe, d] + args, capture_output=True, text=True, timeout=1200)
+        wall = time.perf_counter() - t0
+        if p.returncode != 0:
+            out[tag] = {"rc": p.returncode, "stderr": p.stderr[-300:]}
+            continue
+        ph = [ln for ln in p.stdout.splitlines() if ln.startswith("phase seconds:")]
+        vals = [float(x) for x in ph[-1].split()[3::2]] if ph else [None] * 3
+        out[tag] = {"wall_s": wall, "assembly_s": vals[0], "rhs_lu_solve_full_s": vals[1],
+                    "farfield_mueller_s": vals[2]}
+    if all("wall_s" in out.get(k, {}) for k in ("reference", "bem")):
+        import numpy as np
+        with open(os.path.join(tmp, "reference", "orient.json")) as f:
+            mr = np.array(json.load(f)["mueller"])
+        with open(os.path.join(tmp, "bem", "orient.json")) as f:
+            mb = np.array(json.load(f)["mueller"])
+        out["mueller_rel_diff"] = float(np.linalg.norm(mb - mr) / np.linalg.norm(mr))
+    shutil.rmtree(tmp, ignore_errors=True)
+    out["program"] = ("tests/compat/dense_branch.cpp (the dense branch's calls: assemble_pmchwt, lu_factorize_cuda + "
+                      "lu_solve_cuda, lu_solve_full, far field, write_json) with arguments " + " ".join(args))
+    return out
+
+
+def _clocked(fn, steps, warmup, stream, local=0):
+    """Runs fn warmup + steps times; returns (per-step device seconds over the
+    timed steps, results of the timed steps, clocks)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(local)
+    e0.record(stream)
+    res = [fn() for _ in range(steps)]
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    clocks = sampler.stop()
+    return e0.elapsed_time(e1) / 1e3 / steps, res, clocks
+
+
+def _roofline_from_profile(prof, bf16):
+    """Dominant kernel class of a profiled region: achieved algorithmic rate
+    against its peak (FP64 classes 37 TF/s, tensor-core FP32 updates 3xFP16 of
+    the sustained bf16 figure, the int8 residual 2 x bf16, assembly / far field
+    in counted units per second with no peak)."""
+    if not prof:
+        return None
+    name, (nl, ms, fl, by) = max(prof.items(), key=lambda kv: kv[1][1])
+    if nl == 0 or ms <= 0:
+        return None
+    rate = fl / (ms / 1e3)
+    share = {k: v[1] / max(1e-9, sum(x[1] for x in prof.values())) for k, v in prof.items()}
+    if name in ("assembly", "farfield"):
+        unit = 64.0 if name == "assembly" else 110.0
+        return {"bound": "fp64-simt", "kernel": name, "achieved": rate / unit, "peak": None,
+                "unit": "quadrature-pair evaluations/s" if name == "assembly" else "far-field point terms/s",
+                "frac": None, "traffic": None, "launches": nl, "ms_per_launch": ms / nl, "share": share}
+    return {"bound": "tensor", "kernel": name, "achieved": rate / 1e12, "peak": None, "unit": "TFLOP/s",
+            "frac": None, "traffic": None, "launches": nl, "ms_per_launch": ms / nl, "share": share,
+            "peak_basis": f"FP64 37 TF/s; 3xFP16 {bf16 / 3:.0f} TF/s; int8 {2 * bf16:.0f} TOPS"}
+
+
+def run_config(a):
+    import numpy as np
+    import torch
+
+    import bem_b200 as bb
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    c = CONFIGS[a.config]
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(0)
+    pk, basis = peaks()
+    bf16 = pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
+    line = {"metric": c["metric"], "unit": "s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "data": "synthetic (generated meshes and plane waves)", "config": {"workload": c["workload"]}}
+    if a.impl == "reference":
+        line["impl"] = "reference"
+    ctx = None if a.impl == "reference" else bb.Context(0)
+
+    def cpu_leg(reps):
+        if a.config == "c1":
+            v, t = bb.icosphere(1.0, 2)
+            r = cpu_dense_path(v, t, 1.0, 1.3116, 1, 181, reps=reps)
+            return r, r["total"]
+        if a.config == "c2":
+            v, t = bb.hex_prism(1.4286, 3)
+            r = cpu_dense_path(v, t, 5.0, 1.3116, 64, 181, reps=reps, rows=32, n_ff=8)
+            return r, r["solve_only"]
+        if a.config == "c4":
+            parts = bb.c4_particles(0, 64)
+            tot, descs, cores = 0.0, [], 1
+            for ref in (2, 3):
+                sel = [p for p in parts if p["meta"]["refinements"] == ref]
+                p0 = sel[0]
+                r = cpu_dense_path(p0["verts"], p0["tris"], p0["ka"], p0["m"], 16, 181, reps=reps,
+                                   rows=None if ref == 2 else 48, n_ff=None if ref == 2 else 4)
+                tot += r["total"] * len(sel)
+                cores = r["cores"]
+                descs.append(f"{len(sel)} x (2N={r['n']}: {r['description']})")
+            return {"total": tot, "description": "; ".join(descs), "cores": cores}, tot
+        # c5: the reference has no gradient code; a CPU user would difference
+        # the forward path, two forward runs per coordinate and per Re/Im m
+        v, t = bb.c5_mesh(11, refinements=3, rms=0.05)
+        r = cpu_dense_path(v, t, 5.0, complex(1.5, 0.01), 64, 181, reps=reps, rows=24, n_ff=4)
+        ncoord = 3 * len(v) + 2
+        r = dict(r)
+        r["description"] = (f"central differences of the forward path: 2 x {ncoord} forward runs of "
+                            + r["description"])
+        return r, 2 * ncoord * r["total"]
+
+    if a.impl == "reference":
+        vals = []
+        for i in range(a.warmup + a.steps):
+            r, v = cpu_leg(1)
+            if i >= a.warmup:
+                vals.append(v)
+        val = statistics.median(vals)
+        line.update({"value": val, "ms_per_step": val * 1e3, "dtype": "complex128",
+                     "cpu_baseline": {"value": val, "unit": "s", "cores": r["cores"], "kind": "port",
+                                      "sample": r["description"]},
+                     "e2e": {"value": r.get("total", val), "unit": "s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        if a.config in ("c1", "c2"):
+            args = (["2", "1.0", "1.3116", "0", "1", "1", "1", "181"] if a.config == "c1" else
+                    ["3", "5.0", "1.3116", "0", "8", "8", "1", "181", "1.4286"])
+            line["reference_gpu"] = _ref_gpu_run(args)
+        print(json.dumps(line), flush=True)
+        return
+
+    launches0 = ctx.launches
+    if a.config in ("c1", "c2"):
+        if a.config == "c1":
+            v, t = bb.icosphere(1.0, 2)
+            ka, m, RT, w = 1.0, 1.3116, np.eye(3)[None], np.array([1.0])
+        else:
+            v, t = bb.hex_prism(1.4286, 3)
+            ka, m = 5.0, 1.3116
+            RT, w = bb.generate_orientations(8, 8, 1)
+        g = bb.Geometry(ctx, v, t, 7)
+        kx, ki, ee, ei = bb.physics(ka, m)
+        Z = torch.empty((g.n, g.n), dtype=torch.complex128, device="cuda:0")
+        B = bb.rhs_planewave_dev(g, kx, ee, RT)
+        X = torch.empty_like(B)
+
+        def step64():
+            bb.assemble_pmchwt_dev(g, kx, ki, ee, ei, Z=Z)
+            lu = bb.LU(ctx, Z, bb.PREC_FP64)
+            lu.solve(B, X=X)
+            lu.close()
+            return bb.mueller_from_solutions_dev(g, X, RT, w, kx, ee, ntheta=181)
+
+        ctx.profile(True)
+        t64, Ms, clocks = _clocked(step64, a.steps, a.warmup, stream)
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        bb.set_option(ctx, "cache_factor_memory", 1)
+
+        def step32():
+            bb.assemble_pmchwt_dev(g, kx, ki, ee, ei, Z=Z)
+            lu = bb.LU(ctx, Z, bb.PREC_FP32_REFINE)
+            _, st = lu.solve(B, X=X, tol=2e-10, max_iter=12, raise_noconv=False)
+            lu.close()
+            return bb.mueller_from_solutions_dev(g, X, RT, w, kx, ee, ntheta=181), st
+
+        t32, res32, _ = _clocked(step32, a.steps, a.warmup, stream)
+        bb.set_option(ctx, "cache_factor_memory", 0)
+        M64, (M32, st32) = Ms[-1], res32[-1]
+        # e2e through bem_dense_run (host mesh -> host Mueller)
+        walls = []
+        for i in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            Mp, info = bb.dense_run(ctx, v, t, ka, m, single=a.config == "c1",
+                                    orient=(8, 8, 1), ntheta=181, precision=bb.PREC_FP64)
+            if i >= a.warmup:
+                walls.append(time.perf_counter() - t0)
+        h2d = v.nbytes + t.astype(np.int32).nbytes
+        line.update({"value": t64, "ms_per_step": t64 * 1e3, "dtype": "complex128",
+                     "step": "assembly + FP64 LU + solves + far field / Mueller, device-resident",
+                     "fp32_refine_s": t32, "fp32_refine_vs_fp64": t64 / t32,
+                     "fp32_refine_mueller_rel_err": float(np.linalg.norm(M32 - M64) / np.linalg.norm(M64)),
+                     "fp32_refine_est_rel_err": st32["est_rel_error"],
+                     "e2e": {"value": statistics.median(walls), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                             "d2h_bytes_per_step": int(Mp.nbytes), "scope": "bem_dense_run FP64"},
+                     "e2e_mueller_rel_diff": float(np.linalg.norm(Mp - M64) / np.linalg.norm(M64)),
+                     "roofline": _roofline_from_profile(prof, bf16), "clocks": clocks})
+    elif a.config == "c4":
+        p32 = bb.c4_particles(0, 64, precision=bb.PREC_FP32_REFINE)
+        p64 = bb.c4_particles(0, 64, precision=bb.PREC_FP64)
+        bb.batch_run(ctx, p64[:2])  # library load and first allocations
+        walls, clocks = {}, None
+        res = {}
+        for tag, parts in (("fp64", p64), ("fp32", p32)):
+            ws = []
+            for i in range(a.warmup + a.steps):
+                sampler = ClockSampler(0) if (tag == "fp32" and i == a.warmup) else None
+                t0 = time.perf_counter()
+                out = bb.batch_run(ctx, parts)
+                if i >= a.warmup:
+                    ws.append(time.perf_counter() - t0)
+                if sampler is not None:
+                    clocks = sampler.stop()
+            walls[tag] = statistics.median(ws)
+            res[tag] = out
+        errs = [float(np.linalg.norm(r32[0] - r64[0]) / np.linalg.norm(r64[0]))
+                for r32, r64 in zip(res["fp32"], res["fp64"])]
+        sizes = sorted({r[1]["N"] * 2 for r in res["fp64"]})
+        line.update({"value": walls["fp32"], "ms_per_step": walls["fp32"] * 1e3,
+                     "dtype": "complex64 factors + complex128 refinement (FP64 batch beside it)",
+                     "fp64_s": walls["fp64"], "fp32_refine_vs_fp64": walls["fp64"] / walls["fp32"],
+                     "max_particle_mueller_rel_err_fp32_vs_fp64": max(errs), "sizes_2N": sizes,
+                     "counts": {str(n): sum(1 for r in res["fp64"] if 2 * r[1]["N"] == n) for n in sizes},
+                     "e2e": {"value": walls["fp32"], "unit": "s",
+                             "h2d_bytes_per_step": int(sum(p["verts"].nbytes + p["tris"].nbytes for p in p32)),
+                             "d2h_bytes_per_step": int(64 * 16 * 181 * 8),
+                             "scope": "bem_batch_run: host meshes -> host Mueller matrices"},
+                     "clocks": clocks})
+    else:  # c5
+        v, t = bb.c5_mesh(11, refinements=3, rms=0.05)
+        vs, ts = bb.icosphere(1.0, 3)
+        ka, m = 5.0, complex(1.5, 0.01)
+        Ms, _ = bb.dense_run(ctx, vs, ts, ka, m, orient=(8, 8, 1), ntheta=181)
+        target = Ms[0, 0].copy()
+        walls, clocks = [], None
+        for i in range(a.warmup + a.steps):
+            sampler = ClockSampler(0) if i == a.warmup else None
+            t0 = time.perf_counter()
+            lv, gv, _ = bb.adjoint_grad_vertices(ctx, v, t, ka, m, target, orient=(8, 8, 1))
+            lm, gm, _ = bb.adjoint_grad(ctx, v, t, ka, m, target, orient=(8, 8, 1))
+            if i >= a.warmup:
+                walls.append(time.perf_counter() - t0)
+            if sampler is not None:
+                clocks = sampler.stop()
+        val = statistics.median(walls)
+        line.update({"value": val, "ms_per_step": val * 1e3, "dtype": "complex128",
+                     "step": "bem_adjoint_grad_vertices + bem_adjoint_grad: each one FP64 forward solve, one "
+                             "adjoint solve and the contraction kernels",
+                     "loss": lv, "grad_m": gm.tolist(), "grad_v_max": float(np.abs(gv).max()),
+                     "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": int(v.nbytes + t.nbytes),
+                             "d2h_bytes_per_step": int(gv.nbytes + gm.nbytes),
+                             "scope": "host mesh -> host gradients"},
+                     "clocks": clocks})
+    line["gpu_launches"] = int(ctx.launches - launches0)
+    if not a.no_cpu:
+        r, v = cpu_leg(1 if a.config in ("c4", "c5") else 3)
+        line["cpu_baseline"] = {"value": v, "unit": "s", "cores": r["cores"], "kind": "port",
+                                "sample": r["description"]}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.config != "c3":
+        run_config(a)
+    elif a.impl == "reference":
         run_reference(a)
     elif a.impl == "cusolver":
         run_cusolver(a)

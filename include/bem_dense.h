@@ -108,7 +108,15 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * "assembly_kernel" (0, default: triangle-pair moments over Morton-ordered
  * tiles; 1: one thread per RWG pair, the reference's organisation),
  * "farfield_kernel" (0, default: phases shared by the RWG halves of a
- * triangle; 1: per RWG-half point), "verify_columns" (64, default: after the refinement converges, the error of
+ * triangle; 1: per RWG-half point), "batch_buckets" (1, default: bem_batch_run batches FP64 particles of one
+ * system size -- one assembly pass, one batched LU and one batched solve per
+ * size; 0: one particle at a time), "lu_autotune" (1, default: the batched
+ * LU's block and panel widths are chosen by timing the candidates once per
+ * (size, batch) in the process; 0: 256 / 16, the single LU's shape, whose
+ * factors are bitwise those of bem_lu_factor_dev), "gradient_method" (0,
+ * default: the adjoint gradients contract the operator's derivative in
+ * kernels; 1: central differences of reassembled operators, for checking),
+ * "verify_columns" (64, default: after the refinement converges, the error of
  * 64 columns is measured with an FP64 residual, see bem_lu_solve_dev; -1:
  * every column; 0: no check), "tensor_split" (1, default: FP32
  * operands of the tensor-core GEMM split into two FP16 parts after a
@@ -493,10 +501,17 @@ int bem_adjoint_grad_vertices(bem_ctx* ctx, const bem_problem* p, const double* 
                               double* loss, double* grad_verts, double* mueller);
 
 /* Batched particles (many small scatterers, e.g. the seeded hex-prism sets
- * that cluster_bem.py farms out one process per particle): bem_dense_run for
- * problems[0..count) on this context, results[i] for each; statuses[i]
- * (optional) gets each particle's status and a failure does not stop the
- * batch.  Returns BEM_OK or the first particle's failure. */
+ * that cluster_bem.py farms out one process per particle): the dense pipeline
+ * for problems[0..count) on this context, results[i] for each.  FP64
+ * particles of one system size (LU solver, no adaptive stopping, no
+ * per-orientation output, full orientation set) run as a bucket: their
+ * operators assembled into one batch, one batched LU and one batched solve
+ * (each launch covering every particle of the size; option batch_buckets),
+ * with the LU's block / panel widths from the autotuner (lu_autotune); the
+ * bucket's phase times are shared equally by its particles' results.  Other
+ * particles run one at a time as bem_dense_run.  statuses[i] (optional) gets
+ * each particle's status and a failure does not stop the batch.  Returns
+ * BEM_OK or the first particle's failure. */
 int bem_batch_run(bem_ctx* ctx, const bem_problem* problems, int count, bem_result* results,
                   int* statuses);
 

@@ -69,9 +69,19 @@ def test_defaults_and_workload(monkeypatch):
     assert bench._n_rwg_ico(5) == 30720
 
 
-def test_cpu_sample_is_scaled_and_described():
+def test_cpu_dense_path_sample_is_scaled_and_described():
+    # the reference's CPU dense path (oracle restatement) on samples of an
+    # icosphere of refinement 1: the row sample scales to about the full
+    # assembly, the LU sample by n^3, and the description names every sample
     import bench
-    v, cores, desc, wall = bench.cpu_sample(4096, 256, n_s=512, reps=3, seed=1)
-    assert v > wall > 0 and cores >= 1
-    assert "median of 3" in desc and "logical cores" in desc and "OPENBLAS_NUM_THREADS" in desc
-    assert "n=4096" in desc and "nrhs=256" in desc
+    from oracle import bem_oracle as bo
+    v, t = bo.icosphere(1.0, 1)
+    full = bench.cpu_dense_path(v, t, 1.0, 1.3116, 2, 19)
+    samp = bench.cpu_dense_path(v, t, 1.0, 1.3116, 2, 19, reps=3, rows=30, n_lu=96, n_ff=1, ff_dirs=7)
+    for r in (full, samp):
+        assert r["total"] >= r["solve_only"] > 0 and r["cores"] >= 1 and r["n"] == 240
+        assert "logical cores" in r["description"] and "OPENBLAS_NUM_THREADS" in r["description"]
+    assert "assembly full" in full["description"]
+    assert "30 of 120 test rows" in samp["description"] and "median of 3" in samp["description"]
+    assert "scaled by (n/96)^3" in samp["description"] and "1 of 2 orientations at 7 of 19" in samp["description"]
+    assert 0.2 < samp["assembly"] / full["assembly"] < 5.0

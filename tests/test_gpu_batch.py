@@ -1,6 +1,9 @@
-"""Batched particles (bem_batch_run): the seeded hex-prism workload, each
-particle identical to its own bem_dense_run, one against the oracle, and a
-failing particle that does not stop the batch."""
+"""Batched particles (bem_batch_run): the seeded hex-prism workload.  FP64
+particles of one system size run as a bucket (one assembly pass, one batched
+LU and one batched solve per size): with the single LU's block shape every
+particle is bitwise its own bem_dense_run, with the autotuned shape within
+rounding of it; one particle against the oracle; FP32 + refinement against
+FP64 per particle; and a failing particle that does not stop the batch."""
 import numpy as np
 import pytest
 
@@ -19,16 +22,46 @@ def ctx():
 
 def test_batch_equals_individual_runs(ctx):
     import bem_b200 as bb
-    parts = bb.c4_particles(seed=3, count=4, ntheta=37)
-    out = bb.batch_run(ctx, parts)
-    assert len(out) == 4
-    for p, (M, info) in zip(parts, out):
+    parts = bb.c4_particles(seed=5, count=6, ntheta=37)
+    sizes = [p["meta"]["refinements"] for p in parts]
+    assert min(sizes.count(2), sizes.count(3)) >= 2, "seed 5 draws three of each size: both buckets batched"
+    ref = []
+    for p in parts:
+        kw = {k: v for k, v in p.items() if k != "meta"}
+        ref.append(bb.dense_run(ctx, **kw)[0])
+    try:
+        bb.set_option(ctx, "lu_autotune", 0)  # the single LU's shape: bitwise the same factors
+        out = bb.batch_run(ctx, parts)
+    finally:
+        bb.set_option(ctx, "lu_autotune", 1)
+    assert len(out) == 6
+    for M1, (M, info) in zip(ref, out):
         assert info["status"] == 0
         assert info["N"] in (576, 2304) and info["n_orient"] == 16
-        kw = {k: v for k, v in p.items() if k != "meta"}
-        M1, _ = bb.dense_run(ctx, **kw)
         assert np.array_equal(M, M1)
         assert np.all(np.isfinite(M)) and np.all(M[0, 0] > 0)
+    # the autotuned block / panel widths: other rounding, same solution
+    out = bb.batch_run(ctx, parts)
+    for M1, (M, info) in zip(ref, out):
+        assert info["status"] == 0 and rel(M, M1) < 1e-12
+    # one at a time (batch_buckets 0) is the dense pipeline itself
+    try:
+        bb.set_option(ctx, "batch_buckets", 0)
+        out = bb.batch_run(ctx, parts[:2])
+    finally:
+        bb.set_option(ctx, "batch_buckets", 1)
+    assert all(np.array_equal(M, M1) for M1, (M, _) in zip(ref, out))
+
+
+def test_fp32_refine_particles_against_fp64(ctx):
+    import bem_b200 as bb
+    p64 = bb.c4_particles(seed=4, count=8, ntheta=37)
+    p32 = bb.c4_particles(seed=4, count=8, ntheta=37, precision=bb.PREC_FP32_REFINE)
+    o64, o32 = bb.batch_run(ctx, p64), bb.batch_run(ctx, p32)
+    for (M64, i64), (M32, i32) in zip(o64, o32):
+        assert i64["status"] == 0 and i32["status"] == 0
+        assert i32["stats"]["converged"] == 1
+        assert rel(M32, M64) < 1e-6
 
 
 def test_batch_particle_against_oracle(ctx):

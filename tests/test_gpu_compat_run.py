@@ -154,8 +154,11 @@ def test_far_field_and_json_through_the_surface(run):
     Fv = bo.far_field_vec(cache, X1[0, :N], X1[0, N:], 1.0, 1.0, rh)
     e_th = np.stack([np.cos(th), np.zeros_like(th), -np.sin(th)], axis=1)
     e_ph = np.tile([0.0, 1.0, 0.0], (NTHETA, 1))
-    assert rel(F[0], np.sum(Fv * e_th, axis=1)) < 1e-12
-    assert rel(F[1], np.sum(Fv * e_ph, axis=1)) < 1e-12
+    # (for this sphere and x polarisation F_phi vanishes in the phi = 0 plane
+    # up to rounding: compare on the scale of F_theta)
+    Ft, Fp = np.sum(Fv * e_th, axis=1), np.sum(Fv * e_ph, axis=1)
+    assert rel(F[0], Ft) < 1e-12
+    assert np.abs(F[1] - Fp).max() < 1e-12 * np.abs(Ft).max()
 
 
 def test_singular_matrix_reports_lapack_info(run):
