@@ -602,6 +602,318 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
     }
 }
 
+// ------------------------------------------------------- CTA pairs (cta_group::2)
+// FP16-part products on clusters of two CTAs (one TPC): a 256-row x 256-column
+// tile, each CTA loading its 128 rows of A (hi, lo) and 128 of the tile's 256
+// B' rows (hi, lo), the even CTA issuing tcgen05.mma.cta_group::2 (M = 256,
+// N = 256), which reads both CTAs' shared memory and accumulates each CTA's
+// 128 rows in its own TMEM.  A stage is 64 KB per CTA (96 KB for the one-CTA
+// tile, whose B is not shared), so three stages fit: per SM, 64 KB of operands
+// per 384 MMA cycles against 96 KB.  Barriers as in the int8 pair kernel
+// (ozaki.cu): full[s] on the even CTA expects both CTAs' bytes; empty[s] and
+// tfull[b] receive the MMA commits multicast to the pair; tempty[b] on the
+// even CTA counts the eight epilogue warps of both.  No load is multicast.
+constexpr int P_ROWS = 128;                               // A rows per CTA
+constexpr int P_BROWS = 128;                              // B' rows per CTA
+constexpr int P_STAGES = 3;
+constexpr int P_A_BYTES = P_ROWS * 128;                   // 16 KB per part
+constexpr int P_B_BYTES = P_BROWS * 128;                  // 16 KB per part
+constexpr int P_STAGE_BYTES = 2 * P_A_BYTES + 2 * P_B_BYTES;  // 64 KB
+constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256;
+constexpr uint32_t P_IDESC_F16 = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                                 ((uint32_t)(256 >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cl_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_idx() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_count() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_map(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cl_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// TMA load into this CTA's shared memory, its bytes counted on the even CTA's barrier
+__device__ __forceinline__ void tma_load_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void mma_f16_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+            tmem_d),
+        "l"(a), "l"(b), "r"(P_IDESC_F16), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z),
+        "r"(z));
+}
+// arrive on the barrier at this shared offset in both CTAs of the pair
+__device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+        "h"((uint16_t)3)
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar_cluster) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+
+// Tiles of 256 rows x 128 complex columns in groups of gm row tiles, column
+// by column.  Lower (square row-major C): a group's columns stop at its last
+// row's diagonal, and tiles wholly above the diagonal (nt >= 2 mt + 2) are
+// skipped by every role alike.
+struct PairTiles {
+    int num_m, num_n, gm, lower;
+    __device__ __forceinline__ int gwidth(int g) const {
+        const int first = g * gm, gs = min(gm, num_m - first);
+        return lower ? min(num_n, 2 * (first + gs)) : num_n;
+    }
+    __device__ __forceinline__ int count() const {
+        int c = 0;
+        for (int g = 0; g * gm < num_m; g++) c += min(gm, num_m - g * gm) * gwidth(g);
+        return c;
+    }
+    __device__ __forceinline__ bool tile(int t, int& mt, int& nt) const {
+        int g = 0;
+        for (;; g++) {
+            const int c = min(gm, num_m - g * gm) * gwidth(g);
+            if (t < c) break;
+            t -= c;
+        }
+        const int first = g * gm, gs = min(gm, num_m - first);
+        mt = first + t % gs;
+        nt = t / gs;
+        return !(lower && nt >= 2 * mt + 2);
+    }
+};
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+                 const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
+                 float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int lower, int store,
+                 int group_m, int* status, const float2* __restrict__ sa, const float2* __restrict__ sb) {
+    constexpr int BKE = 2 * BK;  // halves of K per stage (one 128-byte row)
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(smem + P_STAGES * P_STAGE_BYTES);
+    uint64_t* full = bars;                    // [P_STAGES], used in the even CTA
+    uint64_t* empty = bars + P_STAGES;        // [P_STAGES]
+    uint64_t* tfull = bars + 2 * P_STAGES;    // [2]
+    uint64_t* tempty = bars + 2 * P_STAGES + 2;  // [2], used in the even CTA
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * P_STAGES + 4);
+    __shared__ volatile int abort_flag;
+    __shared__ int issued_total, consumed_total;
+
+    const uint32_t rank = cl_rank();
+    const bool even = rank == 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nk = (K2 + BKE - 1) / BKE;
+    PairTiles tm;
+    tm.num_m = (M + 2 * P_ROWS - 1) / (2 * P_ROWS);
+    tm.num_n = (2 * Nc + 2 * P_BROWS - 1) / (2 * P_BROWS);
+    tm.gm = group_m > 0 ? group_m : 8;
+    tm.lower = lower;
+    const int ntiles = tm.count();
+    const int cid = (int)cl_idx(), ncl = (int)cl_count();
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        issued_total = consumed_total = 0;
+        for (int s = 0; s < P_STAGES; s++) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), 8);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS2));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    cl_sync();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;
+            for (int t = cid; t < ntiles && !abort_flag; t += ncl) {
+                int mt, nt;
+                if (!tm.tile(t, mt, nt)) continue;
+                const int ya = mt * 2 * P_ROWS + (int)rank * P_ROWS;
+                const int yb = nt * 2 * P_BROWS + (int)rank * P_BROWS;
+                for (int kt = 0; kt < nk; kt++, it++) {
+                    const int s = it % P_STAGES;
+                    if (!mbar_wait(smem_u32(&empty[s]), ((it / P_STAGES) & 1) ^ 1, status, &abort_flag)) break;
+                    unsigned char* st = smem + s * P_STAGE_BYTES;
+                    const uint32_t fb = cl_map(smem_u32(&full[s]), 0);
+                    if (even) mbar_expect_tx(smem_u32(&full[s]), 2 * P_STAGE_BYTES);
+                    tma_load_pair(smem_u32(st), &tA_hi, kt * BKE, ya, fb);
+                    tma_load_pair(smem_u32(st + P_A_BYTES), &tA_lo, kt * BKE, ya, fb);
+                    tma_load_pair(smem_u32(st + 2 * P_A_BYTES), &tB_hi, kt * BKE, yb, fb);
+                    tma_load_pair(smem_u32(st + 2 * P_A_BYTES + P_B_BYTES), &tB_lo, kt * BKE, yb, fb);
+                    issued_total = it + 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && even) {
+            int it = 0, lt = 0;
+            for (int t = cid; t < ntiles && !abort_flag; t += ncl) {
+                int mt, nt;
+                if (!tm.tile(t, mt, nt)) continue;
+                const int b = lt & 1;
+                lt++;
+                if (!mbar_wait(smem_u32(&tempty[b]), (((lt - 1) >> 1) & 1) ^ 1, status, &abort_flag)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * 256);
+                bool ok = true;
+                for (int kt = 0; kt < nk; kt++, it++) {
+                    const int s = it % P_STAGES;
+                    if (!mbar_wait(smem_u32(&full[s]), (it / P_STAGES) & 1, status, &abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    unsigned char* st = smem + s * P_STAGE_BYTES;
+                    const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + P_A_BYTES);
+                    const uint32_t b_hi = smem_u32(st + 2 * P_A_BYTES), b_lo = smem_u32(st + 2 * P_A_BYTES + P_B_BYTES);
+#pragma unroll
+                    for (int ks = 0; ks < BK / 8; ks++) {
+                        const uint32_t off = ks * 32;
+                        const uint64_t dah = smem_desc(a_hi + off), dal = smem_desc(a_lo + off);
+                        const uint64_t dbh = smem_desc(b_hi + off), dbl = smem_desc(b_lo + off);
+                        mma_f16_pair(acc, dah, dbh, (kt > 0 || ks > 0) ? 1u : 0u);
+                        mma_f16_pair(acc, dah, dbl, 1u);
+                        mma_f16_pair(acc, dal, dbh, 1u);
+                    }
+                    mma_commit_pair(smem_u32(&empty[s]));
+                    consumed_total = it + 1;
+                }
+                mma_commit_pair(smem_u32(&tfull[b]));
+                if (!ok) break;
+            }
+        }
+    } else {
+        // epilogue warps 2..5 of both CTAs: TMEM lane quarter = warp % 4
+        const int q = warp & 3;
+        const uint32_t te0 = cl_map(smem_u32(&tempty[0]), 0), te1 = cl_map(smem_u32(&tempty[1]), 0);
+        int lt = 0;
+        for (int t = cid; t < ntiles; t += ncl) {
+            int mt, nt;
+            if (!tm.tile(t, mt, nt)) continue;
+            const int b = lt & 1;
+            const int ph = (lt >> 1) & 1;
+            lt++;
+            bool ok = mbar_wait(smem_u32(&tfull[b]), ph, status, &abort_flag);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // lower: this CTA's 128 rows wholly above the diagonal are not written
+            const bool write = !(lower && nt >= 2 * mt + (int)rank + 1);
+            const int row = mt * 2 * P_ROWS + (int)rank * P_ROWS + q * 32 + lane;
+            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
+#pragma unroll 1
+            for (int ch = 0; ch < 256 / 32 && write; ch++) {
+                float v[32];
+                tmem_ld32(base + ch * 32, v);
+                const int c0 = nt * P_BROWS + ch * 16;
+                if (row < M && c0 < Nc) {
+                    const float ra = sa[row].y;
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const float f = c0 + j < Nc ? ra * sb[c0 + j].y : 0.f;
+                        v[2 * j] *= f;
+                        v[2 * j + 1] *= f;
+                    }
+                    if (!c_colmajor) {
+                        float2* p = &C[(int64_t)row * ldc + c0];
+                        const bool vec = ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (c0 + 16 <= Nc);
+                        if (vec) {
+                            float4* p4 = reinterpret_cast<float4*>(p);
+                            float4 c[8];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) c[j] = store ? make_float4(0.f, 0.f, 0.f, 0.f) : p4[j];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) {
+                                c[j].x -= v[4 * j];
+                                c[j].y -= v[4 * j + 1];
+                                c[j].z -= v[4 * j + 2];
+                                c[j].w -= v[4 * j + 3];
+                                p4[j] = c[j];
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; j++)
+                                if (c0 + j < Nc) {
+                                    float2 c = store ? make_float2(0.f, 0.f) : p[j];
+                                    c.x -= v[2 * j];
+                                    c.y -= v[2 * j + 1];
+                                    p[j] = c;
+                                }
+                        }
+                    } else {
+                        const int nj = min(16, Nc - c0);
+                        float2 c[16];
+#pragma unroll
+                        for (int j = 0; j < 16; j++)
+                            if (j < nj) c[j] = store ? make_float2(0.f, 0.f) : C[(int64_t)(c0 + j) * ldc + row];
+#pragma unroll
+                        for (int j = 0; j < 16; j++)
+                            if (j < nj) {
+                                c[j].x -= v[2 * j];
+                                c[j].y -= v[2 * j + 1];
+                                C[(int64_t)(c0 + j) * ldc + row] = c[j];
+                            }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_remote(b ? te1 : te0);
+        }
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // an aborted run: let the copies counted on the even CTA's barriers land
+    if (threadIdx.x == 0 && abort_flag && even) {
+        for (int it = consumed_total; it < issued_total; it++) {
+            long long t0 = clock64();
+            while (!mbar_try(smem_u32(&full[it % P_STAGES]), (it / P_STAGES) & 1) && clock64() - t0 < WAIT_CYCLES) {
+            }
+        }
+    }
+    cl_sync();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS2));
+    }
+    cl_sync();
+}
+
 // ---------------------------------------------------------------- packing
 // A (complex, K contiguous): hi/lo[i*ld + 2k + {0,1}] = split(Re/Im a_ik), zero padded
 __global__ void pack_a_kernel(const float2* __restrict__ A, int64_t lda, int M, int K, float* __restrict__ hi,
@@ -968,7 +1280,23 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
         ctx->tc_attr = true;
     }
-    if (ctx->tc_persistent) {
+    if (f16 && ctx->tc_pair) {
+        // 128-row B' boxes: each CTA of a pair loads half of the tile's 256 B' rows
+        CUtensorMap pbh, pbl;
+        BEM_TRY(make_map(ctx, &pbh, b_hi, 2 * N, ld, tc::P_BROWS, true));
+        BEM_TRY(make_map(ctx, &pbl, b_lo, 2 * N, ld, tc::P_BROWS, true));
+        if (!ctx->tc_pair_attr) {
+            BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(tc::gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   tc::P_SMEM_BYTES));
+            ctx->tc_pair_attr = true;
+        }
+        const int nm = (M + 2 * tc::P_ROWS - 1) / (2 * tc::P_ROWS), nn = (2 * N + 255) / 256;
+        const int ntiles = o.lower ? nm * std::min(nn, 2 * nm) : nm * nn;  // an upper bound for the lower raster
+        const int grid = 2 * std::max(1, std::min(ntiles, ctx->sm_count / 2));
+        tc::gemm_pair_kernel<<<grid, 192, tc::P_SMEM_BYTES, ctx->stream>>>(
+            mah, mal, pbh, pbl, C, ldc, c_colmajor ? 1 : 0, M, N, ld, o.lower ? 1 : 0, o.store ? 1 : 0,
+            std::max(1, ctx->tc_group_m / 2), ctx->d_status, sc_a, sc_b);
+    } else if (ctx->tc_persistent) {
         const int nm = (M + tc::BM - 1) / tc::BM;
         const int ntiles = o.lower ? nm * (nm + 1) / 2 : nm * ((2 * N + tc::BN - 1) / tc::BN);
         const int grid = std::min(ntiles, ctx->sm_count);

@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--tensor-split", type=int, default=1, choices=[0, 1],
                     help="FP32 operand split of the tensor-core GEMMs: 0 = 3xTF32, 1 = 3xFP16 with "
                          "power-of-two row / column scales")
+    ap.add_argument("--gemm-pairs", type=int, default=0, choices=[0, 1],
+                    help="FP16-part tensor-core GEMM on CTA pairs (cta_group::2, 256-row tiles)")
     ap.add_argument("--no-factor-cache", action="store_true",
                     help="free the FP32 factors and digit planes after every step instead of reusing them")
     ap.add_argument("--no-fp64", action="store_true")
@@ -398,6 +400,7 @@ def run_bem(a):
     bb.set_option(ctx, "solve_superblock", a.solve_superblock)
     bb.set_option(ctx, "gemm_group_m", a.gemm_group_m)
     bb.set_option(ctx, "tensor_split", a.tensor_split)
+    bb.set_option(ctx, "gemm_pairs", a.gemm_pairs)
     # a loop of solves of one size keeps its factor / digit-plane memory
     bb.set_option(ctx, "cache_factor_memory", 0 if a.no_factor_cache else 1)
     X = torch.empty_like(B)
@@ -555,6 +558,8 @@ def run_bem(a):
                 "config": {**workload(a, n), "parallelism": f"rhs-split x{world}" if world > 1 else "single",
                            "operand_split": ("3xFP16 with power-of-two row / column scales (tensor_split 1)"
                                              if a.tensor_split == 1 else "3xTF32"),
+                           "fp32_gemm_tiles": ("256-row CTA-pair tiles (cta_group::2)" if a.gemm_pairs else
+                                               "128-row one-CTA tiles"),
                            "factor_memory": ("allocated and freed by every step" if a.no_factor_cache else
                                              "FP32 factors and digit planes allocated once, reused by every step "
                                              "(cache_factor_memory)")},
