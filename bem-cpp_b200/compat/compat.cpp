@@ -72,21 +72,105 @@ Mesh unflatten(const std::vector<double>& v, const std::vector<int>& t) {
     return m;
 }
 
-// Device geometry for (rwg, mesh) with the caller's RWG order.
-bem_geom* make_geom(const RWG& rwg, const Mesh& mesh, int quad_order) {
+// Device geometries of the calls, keyed by their full content (mesh arrays,
+// RWG arrays, quadrature order).  The reference's surface passes host meshes
+// call by call -- compute_rhs_planewave once per polarisation and
+// orientation, FFCacheGPU::upload once per far-field batch -- so one mesh
+// reaches the library many times in a run; each distinct content is uploaded
+// once and shared.  Entries in use are counted; at most kGeomKept unused
+// ones stay resident (least recently used freed first).
+struct GeomEntry {
+    std::vector<char> key;
+    bem_geom* g;
+    int refs;
+    unsigned long long used;
+};
+std::vector<GeomEntry> g_geoms;
+unsigned long long g_geom_clock = 0;
+constexpr int kGeomKept = 4;
+
+template <typename T> void key_put(std::vector<char>& k, const T* p, size_t n) {
+    const char* b = reinterpret_cast<const char*>(p);
+    k.insert(k.end(), b, b + n * sizeof(T));
+}
+
+bem_geom* geom_acquire(const std::vector<char>& key, bem_geom* (*make)(const void*), const void* arg) {
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (auto& e : g_geoms)
+            if (e.key == key) {
+                e.refs++;
+                e.used = ++g_geom_clock;
+                return e.g;
+            }
+    }
+    bem_geom* g = make(arg);
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_geoms.push_back({key, g, 1, ++g_geom_clock});
+    return g;
+}
+
+void geom_release(bem_geom* g) {
+    std::vector<bem_geom*> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        int unused = 0;
+        for (auto& e : g_geoms) {
+            if (e.g == g && e.refs > 0) e.refs--;
+            unused += e.refs == 0;
+        }
+        while (unused > kGeomKept) {
+            size_t lru = g_geoms.size();
+            for (size_t i = 0; i < g_geoms.size(); i++)
+                if (g_geoms[i].refs == 0 && (lru == g_geoms.size() || g_geoms[i].used < g_geoms[lru].used)) lru = i;
+            drop.push_back(g_geoms[lru].g);
+            g_geoms.erase(g_geoms.begin() + (long)lru);
+            unused--;
+        }
+    }
+    for (bem_geom* d : drop) bem_geom_free(d);
+}
+
+struct RwgGeomArgs {
+    const RWG* rwg;
+    const Mesh* mesh;
+    int order;
+};
+
+bem_geom* make_rwg_geom(const void* p) {
+    const RwgGeomArgs& a = *static_cast<const RwgGeomArgs*>(p);
+    const RWG& rwg = *a.rwg;
     std::vector<double> v, fp(3 * rwg.N), fm(3 * rwg.N);
-    flatten(mesh, v);
+    flatten(*a.mesh, v);
     for (int n = 0; n < rwg.N; n++) {
         fp[3 * n] = rwg.free_p[n].x, fp[3 * n + 1] = rwg.free_p[n].y, fp[3 * n + 2] = rwg.free_p[n].z;
         fm[3 * n] = rwg.free_m[n].x, fm[3 * n + 1] = rwg.free_m[n].y, fm[3 * n + 2] = rwg.free_m[n].z;
     }
-    int order = (quad_order == 4 || quad_order == 13) ? quad_order : 7;
     bem_geom* g = nullptr;
-    check(bem_geom_create_rwg(ctx(), v.data(), mesh.nv(), mesh.tris.data(), mesh.nt(), rwg.N, rwg.tri_p.data(),
-                              rwg.tri_m.data(), fp.data(), fm.data(), rwg.length.data(), rwg.area_p.data(),
-                              rwg.area_m.data(), order, &g),
+    check(bem_geom_create_rwg(ctx(), v.data(), a.mesh->nv(), a.mesh->tris.data(), a.mesh->nt(), rwg.N,
+                              rwg.tri_p.data(), rwg.tri_m.data(), fp.data(), fm.data(), rwg.length.data(),
+                              rwg.area_p.data(), rwg.area_m.data(), a.order, &g),
           "geometry upload");
     return g;
+}
+
+// Device geometry for (rwg, mesh) with the caller's RWG order; give it back
+// with geom_release.
+bem_geom* make_geom(const RWG& rwg, const Mesh& mesh, int quad_order) {
+    RwgGeomArgs a{&rwg, &mesh, (quad_order == 4 || quad_order == 13) ? quad_order : 7};
+    std::vector<char> key;
+    const int head[5] = {1, a.order, mesh.nv(), mesh.nt(), rwg.N};
+    key_put(key, head, 5);
+    key_put(key, mesh.verts.data(), mesh.verts.size());
+    key_put(key, mesh.tris.data(), mesh.tris.size());
+    key_put(key, rwg.tri_p.data(), rwg.tri_p.size());
+    key_put(key, rwg.tri_m.data(), rwg.tri_m.size());
+    key_put(key, rwg.free_p.data(), rwg.free_p.size());
+    key_put(key, rwg.free_m.data(), rwg.free_m.size());
+    key_put(key, rwg.length.data(), rwg.length.size());
+    key_put(key, rwg.area_p.data(), rwg.area_p.size());
+    key_put(key, rwg.area_m.data(), rwg.area_m.size());
+    return geom_acquire(key, make_rwg_geom, &a);
 }
 
 Mesh mesh_call(int (*fn)(double, int, int*, int*, double*, int*), double p, int r) {
@@ -204,7 +288,7 @@ void assemble_L_K_cuda(const RWG& rwg, const Mesh& mesh, std::complex<double> k,
     cudaMemcpy(K, dK, bytes, cudaMemcpyDeviceToHost);
     cudaFree(dL);
     cudaFree(dK);
-    bem_geom_free(g);
+    geom_release(g);
 }
 
 // ---------------------------------------------------------------- pmchwt.h
@@ -241,7 +325,7 @@ void assemble_pmchwt(const RWG& rwg, const Mesh& mesh, std::complex<double> k_ex
         cudaFree(dL);
         cudaFree(dK);
     }
-    bem_geom_free(g);
+    geom_release(g);
     std::printf("  Total PMCHWT assembly: %.1fs\n", t.elapsed_s());
 }
 
@@ -287,7 +371,7 @@ void compute_rhs_planewave(const RWG& rwg, const Mesh& mesh, std::complex<double
     double e[3] = {E0.x, E0.y, E0.z}, kh[3] = {k_hat.x, k_hat.y, k_hat.z};
     check(bem_rhs_planewave(ctx(), g, k_ext.real(), k_ext.imag(), eta_ext, e, kh, reinterpret_cast<double*>(b)),
           "compute_rhs_planewave");
-    bem_geom_free(g);
+    geom_release(g);
 }
 
 // ---------------------------------------------------------------- orient.h
@@ -399,25 +483,38 @@ void FFCache::init(const RWG& rwg, const Mesh& mesh, int order) {
 
 // The device copy is the library's own geometry (same RWG order: the cache
 // was made from build_rwg of this mesh).
-void FFCacheGPU::upload(const FFCache& cache) {
-    N = cache.N;
-    Nq = cache.Nq;
+namespace {
+bem_geom* make_cache_geom(const void* p) {
+    const FFCache& cache = *static_cast<const FFCache*>(p);
     int nv = (int)cache.mesh_verts.size() / 3, nt = (int)cache.mesh_tris.size() / 3, Ng = 0;
     bem_geom* g = nullptr;
     check(bem_geom_create(ctx(), cache.mesh_verts.data(), nv, cache.mesh_tris.data(), nt, cache.quad_order, &g, &Ng),
           "FFCacheGPU::upload");
-    if (Ng != N) {
-        std::fprintf(stderr, "FFCacheGPU::upload: RWG count %d differs from the cache (%d)\n", Ng, N);
+    if (Ng != cache.N) {
+        std::fprintf(stderr, "FFCacheGPU::upload: RWG count %d differs from the cache (%d)\n", Ng, cache.N);
         std::exit(1);
     }
-    geom = g;
+    return g;
+}
+}  // namespace
+
+void FFCacheGPU::upload(const FFCache& cache) {
+    free();
+    N = cache.N;
+    Nq = cache.Nq;
+    std::vector<char> key;
+    const int head[4] = {2, cache.quad_order, (int)cache.mesh_verts.size(), (int)cache.mesh_tris.size()};
+    key_put(key, head, 4);
+    key_put(key, cache.mesh_verts.data(), cache.mesh_verts.size());
+    key_put(key, cache.mesh_tris.data(), cache.mesh_tris.size());
+    bem_geom* g = geom_acquire(key, make_cache_geom, &cache);
     initialized = true;
     std::printf("  FFCacheGPU: uploaded %d quad points (%.1f MB)\n", 2 * N * Nq,
                 (2.0 * N * Nq * 7.0 * sizeof(double)) / (1024.0 * 1024.0));
 }
 
 void FFCacheGPU::free() {
-    if (initialized && geom) bem_geom_free((bem_geom*)geom);
+    if (initialized && geom) geom_release((bem_geom*)geom);
     geom = nullptr;
     initialized = false;
 }

@@ -199,6 +199,8 @@ struct bem_ctx {
     int gmres_digits = 0;        // GMRES products with Z: 0 FP64 DMMA GEMM, 2..8 int8 Ozaki digits
     bool batch_buckets = true;   // bem_batch_run: FP64 particles of one size batched (else one at a time)
     bool lu_autotune = true;     // batched LU shape from the autotuner (else NB 256, W 16)
+    bool panel_clusters = true;  // LU sub-panels that fit one thread-block cluster run on it (cluster
+                                 // barrier per column) instead of the cooperative grid
     int grad_method = 0;         // adjoint gradients: 0 contraction kernels (grad_geom.cu), 1 central
                                  // differences of reassembled operators
     int verify_cols = 64;        // refinement: columns whose error is measured with an FP64 residual

@@ -285,6 +285,8 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
     } else if (!std::strcmp(name, "residual_pace_lead")) {
         if (value < 0) return bem::fail(ctx, BEM_ERR_INVALID, "residual_pace_lead must be >= 0");
         ctx->oz_pace_lead = value;
+    } else if (!std::strcmp(name, "panel_clusters")) {
+        ctx->panel_clusters = value != 0;
     } else if (!std::strcmp(name, "gmres_digits")) {
         if (value != 0 && (value < 2 || value > bem::oz::S_MAX))
             return bem::fail(ctx, BEM_ERR_INVALID, "gmres_digits must be 0 or 2..%d", bem::oz::S_MAX);

@@ -8,7 +8,10 @@
 //     for each sub-panel of width W inside it:
 //       panel_kernel  -- cooperative kernel, whole sub-panel held in shared
 //                        memory across all SMs, one grid barrier per column
-//                        (pivot search, swap, scale, rank-1 update)
+//                        (pivot search, swap, scale, rank-1 update); panels
+//                        that fit the shared memory of one cluster of at
+//                        most 8 CTAs run panel_cluster_kernel instead, with
+//                        a cluster barrier per column
 //       laswp + small TRSM + thin GEMM for the rest of the block column
 //     laswp of the block's pivots on the other columns
 //     U12 = L11^-1 A12  (blocked TRSM)
@@ -17,6 +20,7 @@
 //
 // The pivot rule is the one of LAPACK izamax: largest |re| + |im|, first
 // index on ties.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -289,6 +293,229 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
         int i = e / w, c = e % w;
         A[(int64_t)(r0 + lo + i) * lda + r0 + c] = tile[e];
     }
+}
+
+// ----------------------------------------------------- cluster panel kernel
+// The sub-panel of panel_kernel on one thread-block cluster per matrix.  The
+// C CTAs of a cluster hold the panel rows in shared memory (CTA b: rows
+// [b Rp, (b+1) Rp), Rp >= w, so the w pivot rows live in CTA 0), publish
+// their pivot candidate in their own shared memory and read the others'
+// through distributed shared memory.  A cluster barrier per column takes the
+// place of the grid barrier: no global workspace, no spin loop, and the
+// clusters of a batch are independent (no co-residency condition).  The
+// candidate buffers alternate between two parities, so a CTA that runs ahead
+// into column jj + 1 never overwrites what a slower one still reads for jj
+// (it cannot pass the barrier of jj before that one has arrived).  Same
+// pivot rule (largest |re| + |im|, smallest row on ties) and the same
+// arithmetic per element as panel_kernel.
+template <typename R>
+__global__ void __launch_bounds__(256)
+panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nrows, int w, int Rp,
+                     int* __restrict__ ipiv, int* __restrict__ info, int64_t sA, int sPiv) {
+    using C2 = typename C2T<R>::type;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C2* tile = (C2*)smem_raw;            // Rp * w
+    C2* s_piv = tile + (size_t)Rp * w;   // w: the pivot row
+    C2* s_cdata = s_piv + w;             // 2 * w: this CTA's candidate row, per parity
+    C2* s_disp = s_cdata + 2 * w;        // 2 * w: row jj (CTA 0), per parity
+    __shared__ R s_cval[2];
+    __shared__ int s_crow[2];
+    __shared__ R s_val[8];
+    __shared__ int s_row[8];
+    __shared__ R s_best;
+    __shared__ int s_brow, s_bown;
+
+    const int C = (int)cluster.num_blocks(), b = (int)cluster.block_rank(), tid = threadIdx.x;
+    const int mi = blockIdx.x / C;
+    A += mi * sA;
+    ipiv += mi * sPiv;
+    info += mi;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int lo = b * Rp;
+    const int nloc = max(0, min(Rp, nrows - lo));
+
+    for (int e = tid; e < nloc * w; e += blockDim.x) {
+        int i = e / w, c = e % w;
+        tile[e] = A[(int64_t)(r0 + lo + i) * lda + r0 + c];
+    }
+    __syncthreads();
+
+    for (int jj = 0; jj < w; jj++) {
+        const int par = jj & 1;
+        // 1. local pivot candidate among rows >= jj, published with its row
+        R bv = (R)-1;
+        int br = 0x7fffffff;
+        for (int i = tid; i < nloc; i += blockDim.x) {
+            int gr = lo + i;
+            if (gr < jj) continue;
+            R v = cabs1<R>(tile[i * w + jj]);
+            if (v > bv || (v == bv && gr < br)) bv = v, br = gr;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            R ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int orw = __shfl_down_sync(0xffffffffu, br, o);
+            if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw;
+        }
+        if (lane == 0) s_val[warp] = bv, s_row[warp] = br;
+        __syncthreads();
+        if (tid == 0) {
+            for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+                if (s_val[k] > bv || (s_val[k] == bv && s_row[k] < br)) bv = s_val[k], br = s_row[k];
+            s_cval[par] = bv;
+            s_crow[par] = br;
+            s_brow = br;
+        }
+        __syncthreads();
+        br = s_brow;
+        if (br != 0x7fffffff)
+            for (int c = tid; c < w; c += blockDim.x) s_cdata[par * w + c] = tile[(br - lo) * w + c];
+        if (b == 0)
+            for (int c = tid; c < w; c += blockDim.x) s_disp[par * w + c] = tile[jj * w + c];
+        // 2. every candidate published
+        cluster.sync();
+        // 3. cluster-wide argmax over the C candidates (warp 0; C <= 32)
+        if (warp == 0) {
+            bv = (R)-1;
+            br = 0x7fffffff;
+            int bo = -1;
+            if (lane < C) {
+                const R v = *cluster.map_shared_rank(&s_cval[par], lane);
+                const int r = *cluster.map_shared_rank(&s_crow[par], lane);
+                if (r != 0x7fffffff) bv = v, br = r, bo = lane;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                R ov = __shfl_down_sync(0xffffffffu, bv, o);
+                int orw = __shfl_down_sync(0xffffffffu, br, o);
+                int oo = __shfl_down_sync(0xffffffffu, bo, o);
+                if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bo = oo;
+            }
+            if (lane == 0) {
+                bool zero = !(bv > (R)0);
+                if (zero) {
+                    br = jj;  // no interchange; LAPACK records info and skips the scaling
+                    bo = -1;
+                    if (b == 0) atomicCAS(info, 0, r0 + jj + 1);
+                }
+                s_brow = br;
+                s_bown = bo;
+                s_best = bv;
+                if (b == 0) ipiv[r0 + jj] = r0 + br;
+            }
+        }
+        __syncthreads();
+        const int piv = s_brow, own = s_bown;
+        const bool zero = !(s_best > (R)0);
+        {
+            const C2* src = own >= 0 ? cluster.map_shared_rank(s_cdata, own) + par * w
+                                     : cluster.map_shared_rank(s_disp, 0) + par * w;
+            for (int c = tid; c < w; c += blockDim.x) s_piv[c] = src[c];
+        }
+        __syncthreads();
+        // 4. interchange rows jj and piv
+        if (piv != jj) {
+            if (b == 0)
+                for (int c = tid; c < w; c += blockDim.x) tile[jj * w + c] = s_piv[c];
+            if (piv >= lo && piv < lo + nloc) {
+                const C2* dsp = cluster.map_shared_rank(s_disp, 0) + par * w;
+                for (int c = tid; c < w; c += blockDim.x) tile[(piv - lo) * w + c] = dsp[c];
+            }
+        }
+        __syncthreads();
+        // 5. scale column jj below the diagonal, rank-1 update of the rest
+        if (!zero) {
+            C2 p = s_piv[jj];
+            R den = p.x * p.x + p.y * p.y;
+            C2 inv;
+            inv.x = p.x / den;
+            inv.y = -p.y / den;
+            for (int i = tid; i < nloc; i += blockDim.x) {
+                int gr = lo + i;
+                if (gr <= jj) continue;
+                C2 a = tile[i * w + jj];
+                C2 l;
+                l.x = a.x * inv.x - a.y * inv.y;
+                l.y = a.x * inv.y + a.y * inv.x;
+                tile[i * w + jj] = l;
+            }
+            __syncthreads();
+            const int wr = w - jj - 1;
+            if (wr > 0)
+                for (int e = tid; e < nloc * wr; e += blockDim.x) {
+                    int i = e / wr, c = jj + 1 + e % wr;
+                    int gr = lo + i;
+                    if (gr <= jj) continue;
+                    C2 l = tile[i * w + jj], u = s_piv[c], x = tile[i * w + c];
+                    x.x -= l.x * u.x - l.y * u.y;
+                    x.y -= l.x * u.y + l.y * u.x;
+                    tile[i * w + c] = x;
+                }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nloc * w; e += blockDim.x) {
+        int i = e / w, c = e % w;
+        A[(int64_t)(r0 + lo + i) * lda + r0 + c] = tile[e];
+    }
+    // no CTA leaves while another may still read its shared memory
+    cluster.sync();
+}
+
+constexpr int PANEL_CLUSTER_MAX = 8;                // portable cluster size
+constexpr size_t PANEL_CLUSTER_SMEM = 200 * 1024;   // shared memory per CTA
+
+// CTAs per cluster for a sub-panel of nrows x w (elements of `esz` bytes):
+// about 384 rows per CTA, every CTA holding at least w rows, at most 8 CTAs
+// whose rows fit their shared memory; 0 when the panel does not fit one
+// cluster (panel_kernel takes it).
+static int panel_cluster_size(int nrows, int w, size_t esz) {
+    int C = std::min(PANEL_CLUSTER_MAX, std::max(1, (nrows + 383) / 384));
+    C = std::max(1, std::min(C, nrows / std::max(w, 1)));
+    for (; C <= PANEL_CLUSTER_MAX; C++) {
+        const int Rp = (nrows + C - 1) / C;
+        if (Rp < w) return 0;
+        if (((size_t)Rp * w + 5 * (size_t)w) * esz <= PANEL_CLUSTER_SMEM) return C;
+    }
+    return 0;
+}
+
+// One launch of panel_cluster_kernel: `batch` matrices (A + i sA, pivots
+// ipiv + i sPiv, info + i), C CTAs per matrix.
+template <typename R>
+static int launch_panel_cluster(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int i0, int nrows, int iw,
+                                int* d_ipiv, int* d_info, int batch, int64_t sA, int sPiv, int C) {
+    using C2 = typename C2T<R>::type;
+    static std::atomic<unsigned long long> attr_set{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_set.load() & bit)) {
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_cluster_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)PANEL_CLUSTER_SMEM));
+        attr_set.fetch_or(bit);
+    }
+    const int Rp = (nrows + C - 1) / C;
+    const size_t smem = ((size_t)Rp * iw + 5 * (size_t)iw) * sizeof(C2);
+    if (smem > PANEL_CLUSTER_SMEM || Rp < iw) return fail(ctx, BEM_ERR_INVALID, "cluster panel bound violated");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(C * batch));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
+    BEM_TRY_CUDA(ctx, cudaLaunchKernelEx(&cfg, panel_cluster_kernel<R>, A, lda, i0, nrows, iw, Rp, d_ipiv, d_info,
+                                         sA, sPiv));
+    BEM_LAUNCHED(ctx);
+    if (ev)
+        ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2 * batch,
+                      (double)nrows * iw * 2 * sizeof(C2) * batch);
+    return BEM_OK;
 }
 
 // ------------------------------------------------------------------ laswp
@@ -631,22 +858,29 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
         for (int i0 = j0; i0 < j0 + jb; i0 += W) {
             const int iw = std::min(W, j0 + jb - i0);
             const int nrows = n - i0;
-            int G = std::min(Gcap, std::max(1, nrows / iw));
-            G = std::min(G, Gmax_sm);
-            int Rp = (nrows + G - 1) / G;
-            G = (nrows + Rp - 1) / Rp;
-            size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
-            if (smem > smem0) return fail(ctx, BEM_ERR_INVALID, "panel smem bound violated");
-            BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
-            int64_t s0 = 0;
-            int p0 = 0;
-            void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
-                            &d_ipiv, &d_info, &pw, &G, &s0, &p0};
-            cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
-            BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G), dim3(256),
-                                                          args, smem, ctx->stream));
-            BEM_LAUNCHED(ctx);
-            if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2, (double)nrows * iw * 2 * sizeof(C2));
+            const int Cl = ctx->panel_clusters ? panel_cluster_size(nrows, iw, sizeof(C2)) : 0;
+            if (Cl > 0) {
+                BEM_TRY(launch_panel_cluster<R>(ctx, A, lda, i0, nrows, iw, d_ipiv, d_info, 1, 0, 0, Cl));
+            } else {
+                int G = std::min(Gcap, std::max(1, nrows / iw));
+                G = std::min(G, Gmax_sm);
+                int Rp = (nrows + G - 1) / G;
+                G = (nrows + Rp - 1) / Rp;
+                size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
+                if (smem > smem0) return fail(ctx, BEM_ERR_INVALID, "panel smem bound violated");
+                BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
+                int64_t s0 = 0;
+                int p0 = 0;
+                void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
+                                &d_ipiv, &d_info, &pw, &G, &s0, &p0};
+                cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
+                BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G), dim3(256),
+                                                              args, smem, ctx->stream));
+                BEM_LAUNCHED(ctx);
+                if (ev)
+                    ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2,
+                                  (double)nrows * iw * 2 * sizeof(C2));
+            }
             // interchanges on the rest of this block column
             int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
             int ncol = (ca1 - ca0) + (cb1 - cb0);
@@ -744,6 +978,9 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
     if (W < 1 || W > 32 || NB < W || NB > TRSM_KB || NB % W != 0)
         return fail(ctx, BEM_ERR_INVALID, "batched LU shape NB=%d W=%d", NB, W);
     const size_t smem_max = 220 * 1024;
+    // every sub-panel fits one cluster (the first is the tallest): no
+    // cooperative grid, no chunking of the batch
+    const bool all_clusters = ctx->panel_clusters && panel_cluster_size(n, W, sizeof(C2)) > 0;
     const int Rp_max = (int)std::min<int64_t>(n, ((int64_t)smem_max / (int64_t)sizeof(C2) - W) / W);
     if (Rp_max < 2 * W) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel does not fit");
     const int Gm_min = (n + Rp_max - 1) / Rp_max;
@@ -763,6 +1000,7 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
         if (chunk >= batch || Gm == Gm_min) break;
         Gm = std::max(Gm_min, std::min(Gm - 1, occ * ctx->sm_count / batch));
     }
+    if (all_clusters) chunk = batch;
     if (chunk < 1) return fail(ctx, BEM_ERR_INVALID, "batched LU: no co-resident panel grid");
     if (chunk < batch) {
         for (int b0 = 0; b0 < batch; b0 += chunk) {
@@ -794,22 +1032,27 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
         for (int i0 = j0; i0 < j0 + jb; i0 += W) {
             const int iw = std::min(W, j0 + jb - i0);
             const int nrows = n - i0;
-            int G = std::min(Gm, std::max(1, nrows / iw));
-            const int Rp = (nrows + G - 1) / G;
-            G = (nrows + Rp - 1) / Rp;
-            const size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
-            if (smem > smem0 || Rp < iw) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel bound violated");
-            BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
-            int spiv = n;
-            void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
-                            &d_ipiv, &d_info, &pw, &G, &sA, &spiv};
-            cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
-            BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G * batch), dim3(256), args,
-                                                          smem, ctx->stream));
-            BEM_LAUNCHED(ctx);
-            if (ev)
-                ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2 * batch,
-                              (double)nrows * iw * 2 * sizeof(C2) * batch);
+            const int Cl = ctx->panel_clusters ? panel_cluster_size(nrows, iw, sizeof(C2)) : 0;
+            if (Cl > 0) {
+                BEM_TRY(launch_panel_cluster<R>(ctx, A, lda, i0, nrows, iw, d_ipiv, d_info, batch, sA, n, Cl));
+            } else {
+                int G = std::min(Gm, std::max(1, nrows / iw));
+                const int Rp = (nrows + G - 1) / G;
+                G = (nrows + Rp - 1) / Rp;
+                const size_t smem = ((size_t)Rp * iw + iw) * sizeof(C2);
+                if (smem > smem0 || Rp < iw) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel bound violated");
+                BEM_TRY_CUDA(ctx, cudaMemsetAsync(pw.bar, 0, sizeof(unsigned), ctx->stream));
+                int spiv = n;
+                void* args[] = {&A, (void*)&lda, (void*)&i0, (void*)&nrows, (void*)&iw, (void*)&Rp,
+                                &d_ipiv, &d_info, &pw, &G, &sA, &spiv};
+                cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
+                BEM_TRY_CUDA(ctx, cudaLaunchCooperativeKernel((void*)panel_kernel<R>, dim3(G * batch), dim3(256),
+                                                              args, smem, ctx->stream));
+                BEM_LAUNCHED(ctx);
+                if (ev)
+                    ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2 * batch,
+                                  (double)nrows * iw * 2 * sizeof(C2) * batch);
+            }
             const int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
             const int ncol = (ca1 - ca0) + (cb1 - cb0);
             if (ncol > 0) {

@@ -91,14 +91,29 @@ def parse():
                          "power-of-two row / column scales")
     ap.add_argument("--gemm-pairs", type=int, default=0, choices=[0, 1],
                     help="FP16-part tensor-core GEMM on CTA pairs (cta_group::2, 256-row tiles)")
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="any other bem_ctx_set_option switch (repeatable), e.g. residual_pace_epoch=16")
     ap.add_argument("--no-factor-cache", action="store_true",
                     help="free the FP32 factors and digit planes after every step instead of reusing them")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
-                    help="c3: the metric's workload; c1, c2, c4, c5: the other configurations")
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "gemm"],
+                    help="c3: the metric's workload; c1, c2, c4, c5: the other configurations; gemm: the FP32 "
+                         "tensor-core GEMM alone at the L D L^T trailing-update shape")
+    ap.add_argument("--gemm-n", type=int, default=12288, help="--config gemm: rows of C (complex)")
+    ap.add_argument("--gemm-shape", default="factor", choices=["factor", "solve"],
+                    help="--config gemm: factor: square row-major C -= A B (B row-major); solve: C (n x 2790, "
+                         "column-major) -= A B with B column-major, the multi-RHS solve's update")
     return ap.parse_args()
+
+
+def extra_options(a):
+    out = {}
+    for kv in a.option:
+        name, _, value = kv.partition("=")
+        out[name.strip()] = int(value)
+    return out
 
 
 def workload(a, n):
@@ -401,6 +416,8 @@ def run_bem(a):
     bb.set_option(ctx, "gemm_group_m", a.gemm_group_m)
     bb.set_option(ctx, "tensor_split", a.tensor_split)
     bb.set_option(ctx, "gemm_pairs", a.gemm_pairs)
+    for name, value in extra_options(a).items():
+        bb.set_option(ctx, name, value)
     # a loop of solves of one size keeps its factor / digit-plane memory
     bb.set_option(ctx, "cache_factor_memory", 0 if a.no_factor_cache else 1)
     X = torch.empty_like(B)
@@ -560,6 +577,7 @@ def run_bem(a):
                                              if a.tensor_split == 1 else "3xTF32"),
                            "fp32_gemm_tiles": ("256-row CTA-pair tiles (cta_group::2)" if a.gemm_pairs else
                                                "128-row one-CTA tiles"),
+                           **({"options": extra_options(a)} if a.option else {}),
                            "factor_memory": ("allocated and freed by every step" if a.no_factor_cache else
                                              "FP32 factors and digit planes allocated once, reused by every step "
                                              "(cache_factor_memory)")},
@@ -632,9 +650,9 @@ def _ref_gpu_run(args):
             out[tag] = {"rc": p.returncode, "stderr": p.stderr[-300:]}
             continue
         ph = [ln for ln in p.stdout.splitlines() if ln.startswith("phase seconds:")]
-        vals = [float(x) for x in ph[-1].split()[3::2]] if ph else [None] * 3
-        out[tag] = {"wall_s": wall, "assembly_s": vals[0], "rhs_lu_solve_full_s": vals[1],
-                    "farfield_mueller_s": vals[2]}
+        words = ph[-1].split()[2:] if ph else []
+        out[tag] = {"wall_s": wall}
+        out[tag].update({words[i].replace("+", "_") + "_s": float(words[i + 1]) for i in range(0, len(words) - 1, 2)})
     if all("wall_s" in out.get(k, {}) for k in ("reference", "bem")):
         import numpy as np
         with open(os.path.join(tmp, "reference", "orient.json")) as f:
@@ -687,12 +705,68 @@ def _roofline_from_profile(prof, bf16):
             "peak_basis": f"FP64 37 TF/s; 3xFP16 {bf16 / 3:.0f} TF/s; int8 {2 * bf16:.0f} TOPS"}
 
 
+def run_gemm(a):
+    """The FP32 tensor-core GEMM of the factorisation alone: C -= A B with
+    complex64 A (n x 512), B (512 x n) and a square row-major C (n x n), the
+    shape of an L D L^T super-block trailing update, timed with CUDA events
+    over the steps (C larger than L2 for n >= 4096)."""
+    import torch
+
+    import bem_b200 as bb
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream(0)
+    ctx = bb.Context(0)
+    bb.set_option(ctx, "tensor_split", a.tensor_split)
+    bb.set_option(ctx, "gemm_pairs", a.gemm_pairs)
+    bb.set_option(ctx, "gemm_group_m", a.gemm_group_m)
+    for name, value in extra_options(a).items():
+        bb.set_option(ctx, name, value)
+    n, K = a.gemm_n, 512
+    solve = a.gemm_shape == "solve"
+    ncol = 2790 if solve else n
+    g = torch.Generator(device="cuda:0").manual_seed(0)
+    A = torch.randn((n, K), dtype=torch.complex64, device="cuda:0", generator=g)
+    # solve: B given as its transpose (ncol x K row-major), C stored as (ncol x n) row-major
+    B = torch.randn((ncol, K) if solve else (K, ncol), dtype=torch.complex64, device="cuda:0", generator=g)
+    C = torch.zeros((ncol, n) if solve else (n, ncol), dtype=torch.complex64, device="cuda:0")
+    launches0 = ctx.launches
+    t, _, clocks = _clocked(lambda: bb.cgemm_tf32x3(ctx, A, B, C, b_rowmajor=not solve, c_colmajor=solve),
+                            a.steps, a.warmup, stream)
+    pk, basis = peaks()
+    bf16 = pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
+    flops = 8.0 * n * ncol * K
+    peak = bf16 / 3.0 if a.tensor_split == 1 else bf16 / 6.0
+    line = {"metric": f"TFLOP/s of the FP32 tensor-core GEMM, C -= A B, {n} x {ncol} x {K} complex64",
+            "value": flops / t / 1e12, "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "complex64 (3xFP16 parts)" if a.tensor_split == 1 else "complex64 (3xTF32 parts)",
+            "data": "synthetic (seeded normal operands)",
+            "config": {"workload": (f"C {n} x {ncol} column-major, A {n} x {K} row-major, B {K} x {ncol} column-major "
+                                    "(the multi-RHS solve's update)" if solve else
+                                    f"C {n} x {n} row-major, A {n} x {K}, B {K} x {n} row-major (the factorisation's "
+                                    "trailing update)"),
+                       "tiles": "256-row CTA pairs" if a.gemm_pairs else "128-row one-CTA tiles",
+                       "l2_policy": "C larger than L2" if 8 * n * ncol > 126e6 else "C within L2"},
+            "roofline": {"bound": "tensor", "achieved": flops / t / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": flops / t / 1e12 / peak, "traffic": None,
+                         "peak_basis": f"{basis} sustained bf16 {bf16} TF/s / 3 split terms"
+                                       + ("" if a.tensor_split == 1 else " / 2 (tf32)")},
+            "gpu_launches": int(ctx.launches - launches0), "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def run_config(a):
     import numpy as np
     import torch
 
     import bem_b200 as bb
 
+    if a.config == "gemm":
+        return run_gemm(a)
     if int(os.environ.get("RANK", "0")) != 0:
         return
     c = CONFIGS[a.config]

@@ -116,6 +116,14 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * factors are bitwise those of bem_lu_factor_dev), "gradient_method" (0,
  * default: the adjoint gradients contract the operator's derivative in
  * kernels; 1: central differences of reassembled operators, for checking),
+ * "panel_clusters" (1, default: the sub-panels of the pivoted LU that fit the
+ * shared memory of one cluster of at most 8 CTAs -- all of them up to order
+ * ~6000 -- are factored by one thread-block cluster per matrix, one cluster
+ * barrier per column; 0: every sub-panel on the cooperative grid, one grid
+ * barrier per column; both give the same pivots and factors),
+ * "gemm_pairs" (0, default: the FP16-part tensor-core GEMM on 128-row tiles,
+ * one CTA each; 1: 256-row tiles on CTA pairs, tcgen05.mma.cta_group::2, each
+ * CTA loading half of a tile's B operand),
  * "verify_columns" (64, default: after the refinement converges, the error of
  * 64 columns is measured with an FP64 residual, see bem_lu_solve_dev; -1:
  * every column; 0: no check), "tensor_split" (1, default: FP32

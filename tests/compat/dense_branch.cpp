@@ -172,6 +172,7 @@ int main(int argc, char** argv) {
         compute_rhs_planewave(rwg, mesh, k_ext, eta_ext, RT * Vec3(0, 1, 0), RT * Vec3(0, 0, 1), quad,
                               &Bo[(2 * o + 1) * N2]);
     }
+    const double t_rhs = solve_timer.elapsed_s();
     Zs = Z;
     if (lu_solve_full(Zs.data(), N2, Bo.data(), n_calls) != 0) return 5;
     const double t_solve = solve_timer.elapsed_s();
@@ -194,7 +195,7 @@ int main(int argc, char** argv) {
     std::fprintf(f, "%d %d\n", info, full);
     std::fclose(f);
     std::printf("single-orientation |F_theta(0)| = %.6e\n", std::abs(Fth[0]));
-    std::printf("phase seconds: assembly %.6f rhs+lu_solve_full %.6f farfield+mueller %.6f\n", t_asm, t_solve,
-                t_ff);
+    std::printf("phase seconds: assembly %.6f rhs %.6f lu_solve_full %.6f farfield+mueller %.6f\n", t_asm, t_rhs,
+                t_solve - t_rhs, t_ff);
     return 0;
 }

@@ -139,3 +139,41 @@ def test_factor_memory_cache_reuses_blocks_bitwise(ctx):
         bb.set_option(ctx, "cache_factor_memory", 0)
     assert torch.cuda.mem_get_info()[0] >= free0 - (2 << 20)
     assert np.array_equal(X0, X1) and np.array_equal(X1, X2)
+
+
+@pytest.mark.parametrize("n", [40, 700, 2000, 4608, 7000])
+def test_cluster_panels_match_grid_panels(ctx, n):
+    # the sub-panels on thread-block clusters (default: every sub-panel of
+    # up to ~6000 rows) against the cooperative grid kernel: the same pivot
+    # rule and per-element arithmetic, so the same pivots and factors; at
+    # n = 7000 the first sub-panels are too tall for a cluster and the two
+    # kernels alternate within one factorisation
+    import bem_b200 as bb
+    A = _rand(n, 10 + n)
+    A[:, 5] = 0.0  # a zero pivot on the way: info and the skipped scaling
+    out = {}
+    try:
+        for mode in (1, 0):
+            bb.set_option(ctx, "panel_clusters", mode)
+            out[mode] = bb.lu_factorize_cuda(ctx, A)
+    finally:
+        bb.set_option(ctx, "panel_clusters", 1)
+    (F1, p1, i1), (F0, p0, i0) = out[1], out[0]
+    assert i1 == i0 == 6
+    assert np.array_equal(p1, p0)
+    assert rel(F1, F0) < 1e-13
+
+
+def test_cluster_panels_batched(ctx):
+    # batched factorisation (one cluster per matrix in one launch) against
+    # the single LU of each matrix
+    import bem_b200 as bb
+    parts = bb.c4_particles(seed=5, count=3, ntheta=19)
+    single = [bb.dense_run(ctx, **{k: v for k, v in p.items() if k != "meta"})[0] for p in parts]
+    try:
+        bb.set_option(ctx, "lu_autotune", 0)
+        out = bb.batch_run(ctx, parts)
+    finally:
+        bb.set_option(ctx, "lu_autotune", 1)
+    for M1, (M, info) in zip(single, out):
+        assert info["status"] == 0 and np.array_equal(M, M1)

@@ -56,7 +56,7 @@ def test_pair_gemm_matches_fp64(ctx, M, N, K, b_rowmajor, c_colmajor):
     ref32 = c64(C0) - c64(A) @ c64(Bm)
     scale = float(K) ** 0.5 * 2.0
     err = (out - ref32).abs().max().item() / scale
-    assert err <= 1.5e-7 * K + 1e-6, err
+    assert err <= 1.5e-7 * K + 2e-6, err
     assert (out - (C0 - A @ Bm)).abs().max().item() / scale < 3e-5
 
 
