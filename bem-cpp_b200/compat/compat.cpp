@@ -507,7 +507,7 @@ void FFCacheGPU::upload(const FFCache& cache) {
     key_put(key, head, 4);
     key_put(key, cache.mesh_verts.data(), cache.mesh_verts.size());
     key_put(key, cache.mesh_tris.data(), cache.mesh_tris.size());
-    bem_geom* g = geom_acquire(key, make_cache_geom, &cache);
+    geom = geom_acquire(key, make_cache_geom, &cache);
     initialized = true;
     std::printf("  FFCacheGPU: uploaded %d quad points (%.1f MB)\n", 2 * N * Nq,
                 (2.0 * N * Nq * 7.0 * sizeof(double)) / (1024.0 * 1024.0));

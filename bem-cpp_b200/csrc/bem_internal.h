@@ -188,7 +188,7 @@ struct bem_ctx {
     int asm_kernel = 0;          // assembly: 0 triangle-pair moments (Morton tiles), 1 per RWG pair
     int tc_group_m = 16;         // row tiles per raster group of the persistent tensor-core GEMM
     bool tc_persistent = true;  // persistent tensor-core GEMM (else one CTA per tile)
-    bool tc_pair = false;       // FP16-part GEMM on CTA pairs (cta_group::2, 256-row tiles)
+    bool tc_pair = true;        // FP16-part GEMM on CTA pairs (cta_group::2, 256-row tiles)
     bool tc_pair_attr = false;
     int tc_split = 1;           // FP32 operand split: 1 = 3xFP16 with power-of-two row / column scales, 0 = 3xTF32
     int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)
@@ -209,8 +209,6 @@ struct bem_ctx {
     int solve_sb = 2;            // L D L^T solves: 256-row blocks per update (1 or 2)
     int oz_pace_epoch = 32;      // int8 residual: K slabs per pacing epoch (0: no pacing)
     int oz_pace_lead = 2;        // epochs of lead over the grid average before a CTA waits
-    bool oz_pair = false;        // int8 residual on CTA pairs (cta_group::2); off: the pairs draw
-                                 // more power and more DRAM traffic than they save under the 1 kW cap
     bool prof = false;
     std::vector<ProfPending> prof_pending;
     std::vector<cudaEvent_t> prof_pool;

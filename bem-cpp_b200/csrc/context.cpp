@@ -277,9 +277,7 @@ int64_t bem_ctx_launch_count(const bem_ctx* ctx) { return ctx ? ctx->launches : 
 
 int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
     if (!ctx || !name) return BEM_ERR_INVALID;
-    if (!std::strcmp(name, "residual_pairs")) {
-        ctx->oz_pair = value != 0;
-    } else if (!std::strcmp(name, "residual_pace_epoch")) {
+    if (!std::strcmp(name, "residual_pace_epoch")) {
         if (value < 0) return bem::fail(ctx, BEM_ERR_INVALID, "residual_pace_epoch must be >= 0");
         ctx->oz_pace_epoch = value;
     } else if (!std::strcmp(name, "residual_pace_lead")) {

@@ -43,7 +43,6 @@ constexpr long long WAIT_CYCLES = 2000000000LL;
 // single-CTA tiles then spans ~16 row tiles x ~9 column tiles, which balances
 // the re-reads of the (larger) Z digit rows against those of the X digit rows.
 constexpr int GROUP_M = 16;
-constexpr int GROUP_M_PAIR = 8;  // 256-row tiles of the CTA pairs
 constexpr int MAXP = 4;  // digit pairs per accumulator group
 
 // 2^k for a normal k, 0 below the normal range (those terms are far below
@@ -372,246 +371,6 @@ residual_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
     }
 }
 
-// ------------------------------------------------------- CTA pairs (cta_group::2)
-// A cluster of two CTAs (one TPC) computes a 256-row x 256-column tile: each
-// CTA loads its 128 rows of the Z digits and its 128 of the 256 X' digit rows,
-// the even CTA issues tcgen05.mma.cta_group::2 (M = 256, N = 256), which reads
-// both CTAs' shared memory and accumulates each CTA's 128 rows in its own
-// TMEM.  Per SM that is 32 KB of operands per 512 MMA cycles instead of 48 KB
-// for the single-CTA tile, and six pipeline stages instead of four.
-// Barriers:
-//   full[s]   even CTA only: one arrival (its producer, expecting both CTAs'
-//             bytes) plus the transactions of both CTAs' .cta_group::2 loads;
-//   empty[s]  both CTAs: the MMA commit, multicast to the pair;
-//   tfull[b]  both CTAs: the MMA commit after a tile, multicast to the pair;
-//   tempty[b] even CTA: 8 arrivals, the 4 epilogue warps of each CTA.
-// Every wait is bounded; all threads of both CTAs pass the same two cluster
-// barriers (after set-up, before and after the TMEM release).
-constexpr int P_ROWS = 128;                        // Z rows per CTA (256 per pair)
-constexpr int P_BROWS = 128;                       // X' rows per CTA (256 per pair)
-constexpr int P_STAGES = 6;
-constexpr int P_A_BYTES = P_ROWS * BKB;            // 16 KB
-constexpr int P_B_BYTES = P_BROWS * BKB;           // 16 KB
-constexpr int P_STAGE_BYTES = P_A_BYTES + P_B_BYTES;
-constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256;
-// kind::i8, signed A and B, int32 accumulate, M = 256 (the pair), N = 256.
-constexpr uint32_t P_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
-                             ((uint32_t)(256 >> 4) << 24);
-
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ uint32_t cluster_idx() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ uint32_t cluster_count() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
-    return r;
-}
-// shared::cluster address of the same shared variable in CTA `rank`
-__device__ __forceinline__ uint32_t map_rank(uint32_t addr, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
-    return r;
-}
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// TMA load into this CTA's shared memory whose transaction bytes count on the
-// barrier `bar` of the pair's even CTA (no multicast)
-__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
-        "%3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
-__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
-    uint32_t z = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(tmem_d),
-        "l"(a), "l"(b), "r"(P_IDESC), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-// arrive on the barrier at this shared offset in both CTAs of the pair
-__device__ __forceinline__ void mma_commit_pair(uint32_t bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
-        "h"((uint16_t)3)
-        : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar_cluster) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
-}
-
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
-residual_pair_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
-                     const __grid_constant__ Groups G, double2* __restrict__ R, int64_t ldr,
-                     const int* __restrict__ e_row, const int* __restrict__ f_col, int n, int nrhs, int K2p,
-                     int* status) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* bars = (uint64_t*)(smem + P_STAGES * P_STAGE_BYTES);
-    uint64_t* full = bars;
-    uint64_t* empty = bars + P_STAGES;
-    uint64_t* tfull = bars + 2 * P_STAGES;
-    uint64_t* tempty = bars + 2 * P_STAGES + 2;
-    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * P_STAGES + 4);
-    __shared__ volatile int abort_flag;
-    __shared__ int issued_total, consumed_total;
-
-    const uint32_t rank = cluster_rank();
-    const bool even = rank == 0;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nk = K2p / BKB;
-    const int num_m = (n + 2 * P_ROWS - 1) / (2 * P_ROWS), num_n = (2 * nrhs + BN - 1) / BN;
-    const int ntiles = num_m * num_n;
-    const int cid = (int)cluster_idx(), ncl = (int)cluster_count();
-    auto unit_tile = [&](int t, int& mt, int& ntl) {
-        const int per = GROUP_M_PAIR * num_n;
-        const int gi = t / per, first_m = gi * GROUP_M_PAIR;
-        const int gsz = min(GROUP_M_PAIR, num_m - first_m);
-        const int r = t % per;
-        mt = first_m + r % gsz;
-        ntl = r / gsz;
-    };
-
-    if (threadIdx.x == 0) {
-        abort_flag = 0;
-        issued_total = consumed_total = 0;
-        for (int s = 0; s < P_STAGES; s++) {
-            mbar_init(smem_u32(&full[s]), 1);
-            mbar_init(smem_u32(&empty[s]), 1);
-        }
-        for (int b = 0; b < 2; b++) {
-            mbar_init(smem_u32(&tfull[b]), 1);
-            mbar_init(smem_u32(&tempty[b]), 8);
-        }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    cluster_sync();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-
-    if (warp == 0) {
-        if (lane == 0) {
-            int it = 0;
-            for (int gr = 0; gr < G.ng && !abort_flag; gr++)
-            for (int u = cid; u < ntiles && !abort_flag; u += ncl) {
-                int mt, ntl;
-                unit_tile(u, mt, ntl);
-                const Group& g = G.g[gr];
-                for (int p = 0; p < g.np && !abort_flag; p++) {
-                    const int ya = g.s[p] * n + mt * 2 * P_ROWS + (int)rank * P_ROWS;
-                    const int yb = g.t[p] * 2 * nrhs + ntl * BN + (int)rank * P_BROWS;
-                    for (int kt = 0; kt < nk; kt++, it++) {
-                        const int s = it % P_STAGES;
-                        if (!mbar_wait(smem_u32(&empty[s]), ((it / P_STAGES) & 1) ^ 1, status, &abort_flag)) break;
-                        unsigned char* st = smem + s * P_STAGE_BYTES;
-                        const uint32_t fb = map_rank(smem_u32(&full[s]), 0);
-                        if (even) mbar_expect_tx(smem_u32(&full[s]), 2 * P_STAGE_BYTES);
-                        tma_load_2d_pair(smem_u32(st), &tA, kt * BKB, ya, fb);
-                        tma_load_2d_pair(smem_u32(st + P_A_BYTES), &tB, kt * BKB, yb, fb);
-                        issued_total = it + 1;
-                    }
-                }
-            }
-        }
-    } else if (warp == 1) {
-        if (lane == 0 && even) {
-            int it = 0, lt = 0;
-            bool stop = false;
-            for (int gr = 0; gr < G.ng && !stop; gr++)
-            for (int u = cid; u < ntiles && !stop; u += ncl, lt++) {
-                const Group& g = G.g[gr];
-                const int b = lt & 1;
-                if (!mbar_wait(smem_u32(&tempty[b]), ((lt >> 1) & 1) ^ 1, status, &abort_flag)) {
-                    stop = true;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t acc = tmem + (uint32_t)(b * 256);
-                bool ok = true;
-                for (int p = 0; p < g.np && ok; p++) {
-                    for (int kt = 0; kt < nk; kt++, it++) {
-                        const int s = it % P_STAGES;
-                        if (!mbar_wait(smem_u32(&full[s]), (it / P_STAGES) & 1, status, &abort_flag)) {
-                            ok = false;
-                            break;
-                        }
-                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                        unsigned char* st = smem + s * P_STAGE_BYTES;
-                        const uint32_t a0 = smem_u32(st), b0 = smem_u32(st + P_A_BYTES);
-#pragma unroll
-                        for (int ks = 0; ks < BKB / 32; ks++) {
-                            const uint32_t off = ks * 32;
-                            mma_i8_pair(acc, smem_desc(a0 + off), smem_desc(b0 + off),
-                                        (p > 0 || kt > 0 || ks > 0) ? 1u : 0u);
-                        }
-                        mma_commit_pair(smem_u32(&empty[s]));
-                        consumed_total = it + 1;
-                    }
-                }
-                mma_commit_pair(smem_u32(&tfull[b]));
-                if (!ok) stop = true;
-            }
-        }
-    } else {
-        const int q = warp & 3;
-        const uint32_t tempty0 = map_rank(smem_u32(&tempty[0]), 0), tempty1 = map_rank(smem_u32(&tempty[1]), 0);
-        int lt = 0;
-        bool stop = false;
-        for (int gr = 0; gr < G.ng && !stop; gr++)
-        for (int u = cid; u < ntiles; u += ncl, lt++) {
-            const int b = lt & 1;
-            bool ok = mbar_wait(smem_u32(&tfull[b]), (lt >> 1) & 1, status, &abort_flag);
-            ok = __all_sync(0xffffffffu, ok);
-            if (!ok) {
-                stop = true;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            int mt, ntl;
-            unit_tile(u, mt, ntl);
-            const int row = mt * 2 * P_ROWS + (int)rank * P_ROWS + q * 32 + lane;
-            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
-            drain_tile(base, R, ldr, row, n, e_row, f_col, ntl * (BN / 2), nrhs, G.g[gr].d);
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive_remote(b ? tempty1 : tempty0);
-        }
-    }
-    __syncwarp();
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    // an aborted run: let the copies counted on this CTA's barriers land
-    if (threadIdx.x == 0 && abort_flag && even) {
-        for (int it = consumed_total; it < issued_total; it++) {
-            long long t0 = clock64();
-            while (!mbar_try(smem_u32(&full[it % P_STAGES]), (it / P_STAGES) & 1) && clock64() - t0 < WAIT_CYCLES) {
-            }
-        }
-    }
-    cluster_sync();
-    if (warp == 1) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
-    }
-    cluster_sync();
-}
-
 // ---------------------------------------------------------------- slicing
 // e[i] = ilogb(max_k |Z'[i,k]|) + 2 (so |Z'[i,k] 2^-e| < 1/2); 0 for a zero row.
 __global__ void row_exp_kernel(const double2* __restrict__ Z, int64_t ldz, int n, int* __restrict__ e) {
@@ -833,38 +592,16 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
     if (!ctx->oz_attr) {
         BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(oz::residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                oz::SMEM_BYTES));
-        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(oz::residual_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               oz::P_SMEM_BYTES));
         ctx->oz_attr = true;
     }
-    bool done = false;
-    if (ctx->oz_pair) {
-        // CTA pairs: 256-row tiles, each CTA loads 128 of the 256 X' rows of a tile
-        CUtensorMap tB2;
-        BEM_TRY(encode_i8(ctx, &tB2, Bd, (int64_t)S * 2 * nrhs, ldk, oz::P_BROWS));
-        const int ntiles = ((n + 2 * oz::P_ROWS - 1) / (2 * oz::P_ROWS)) * ((2 * nrhs + oz::BN - 1) / oz::BN);
-        const int grid = 2 * std::min(ntiles, std::max(1, ctx->sm_count / 2));
-        oz::residual_pair_kernel<<<grid, 192, oz::P_SMEM_BYTES, ctx->stream>>>(tA, tB2, G, R, ldr, oz_->e, f, n, nrhs,
-                                                                              (int)ldk, ctx->d_status);
-        if (cudaPeekAtLastError() == cudaSuccess) {
-            ctx->launches++;
-            done = true;
-        } else {
-            // clusters of two 197 KB CTAs not schedulable here: single-CTA tiles from now on
-            cudaGetLastError();
-            ctx->oz_pair = false;
-        }
-    }
-    if (!done) {
-        const int ntiles = ((n + oz::BM - 1) / oz::BM) * ((2 * nrhs + oz::BN - 1) / oz::BN);
-        const int grid = std::min(ntiles, ctx->sm_count);
-        unsigned* pace = (unsigned*)(ctx->d_status + 32);  // a spare word of the context's status block
-        BEM_TRY_CUDA(ctx, cudaMemsetAsync(pace, 0, sizeof(unsigned), ctx->stream));
-        oz::residual_kernel<<<grid, 192, oz::SMEM_BYTES, ctx->stream>>>(tA, tB, G, R, ldr, oz_->e, f, n, nrhs,
-                                                                        (int)ldk, pace, ctx->oz_pace_epoch,
-                                                                        ctx->oz_pace_lead, ctx->d_status);
-        BEM_LAUNCHED(ctx);
-    }
+    const int ntiles = ((n + oz::BM - 1) / oz::BM) * ((2 * nrhs + oz::BN - 1) / oz::BN);
+    const int grid = std::min(ntiles, ctx->sm_count);
+    unsigned* pace = (unsigned*)(ctx->d_status + 32);  // a spare word of the context's status block
+    BEM_TRY_CUDA(ctx, cudaMemsetAsync(pace, 0, sizeof(unsigned), ctx->stream));
+    oz::residual_kernel<<<grid, 192, oz::SMEM_BYTES, ctx->stream>>>(tA, tB, G, R, ldr, oz_->e, f, n, nrhs,
+                                                                    (int)ldk, pace, ctx->oz_pace_epoch,
+                                                                    ctx->oz_pace_lead, ctx->d_status);
+    BEM_LAUNCHED(ctx);
     if (ev) {
         // int8 digit-pair products (2 M N K each, M = n, N = 2 nrhs, K = 2 n);
         // bytes: the digit planes of Z and X once, R read and written once

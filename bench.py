@@ -78,8 +78,6 @@ def parse():
                     help="refinement target: estimated max-column relative error")
     ap.add_argument("--residual-digits", type=int, default=7,
                     help="int8 digits of the refinement residual (0: FP64 DMMA GEMM)")
-    ap.add_argument("--residual-pairs", type=int, default=0,
-                    help="int8 residual on 2-CTA clusters (1) or one CTA per tile (0)")
     ap.add_argument("--factor-superblock", type=int, default=2, choices=[1, 2],
                     help="256-column blocks per L D L^T trailing update")
     ap.add_argument("--solve-superblock", type=int, default=2, choices=[1, 2],
@@ -89,8 +87,9 @@ def parse():
     ap.add_argument("--tensor-split", type=int, default=1, choices=[0, 1],
                     help="FP32 operand split of the tensor-core GEMMs: 0 = 3xTF32, 1 = 3xFP16 with "
                          "power-of-two row / column scales")
-    ap.add_argument("--gemm-pairs", type=int, default=0, choices=[0, 1],
-                    help="FP16-part tensor-core GEMM on CTA pairs (cta_group::2, 256-row tiles)")
+    ap.add_argument("--gemm-pairs", type=int, default=1, choices=[0, 1],
+                    help="FP16-part tensor-core GEMM on CTA pairs (1, cta_group::2, 256-row tiles) or one CTA "
+                         "per 128-row tile (0)")
     ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
                     help="any other bem_ctx_set_option switch (repeatable), e.g. residual_pace_epoch=16")
     ap.add_argument("--no-factor-cache", action="store_true",
@@ -410,7 +409,6 @@ def run_bem(a):
         torch.cuda.empty_cache()
 
     bb.set_residual_digits(ctx, a.residual_digits)
-    bb.set_option(ctx, "residual_pairs", a.residual_pairs)
     bb.set_option(ctx, "factor_superblock", a.factor_superblock)
     bb.set_option(ctx, "solve_superblock", a.solve_superblock)
     bb.set_option(ctx, "gemm_group_m", a.gemm_group_m)

@@ -86,9 +86,7 @@ int bem_ctx_set_residual_digits(bem_ctx* ctx, int digits);
  * pivoting on a zero pivot or when the refinement does not converge; mode 0
  * always uses LU with partial pivoting. */
 int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
-/* Kernel-shape switches, mainly for measurement: "residual_pairs" (0, default:
- * one CTA per tile; 1: the int8 residual on 2-CTA clusters, cta_group::2),
- * "persistent_gemm" (1, default: persistent tensor-core GEMM; 0: one CTA per
+/* Kernel-shape switches, mainly for measurement: "persistent_gemm" (1, default: persistent tensor-core GEMM; 0: one CTA per
  * tile), "residual_pace_epoch" / "residual_pace_lead" (32 / 2: the int8
  * residual's CTAs report every 32 K slabs and wait, softly, when more than 2
  * epochs ahead of the grid average, so a wave shares its digit rows in L2;
@@ -121,9 +119,9 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * ~6000 -- are factored by one thread-block cluster per matrix, one cluster
  * barrier per column; 0: every sub-panel on the cooperative grid, one grid
  * barrier per column; both give the same pivots and factors),
- * "gemm_pairs" (0, default: the FP16-part tensor-core GEMM on 128-row tiles,
- * one CTA each; 1: 256-row tiles on CTA pairs, tcgen05.mma.cta_group::2, each
- * CTA loading half of a tile's B operand),
+ * "gemm_pairs" (1, default: the FP16-part tensor-core GEMM on 256-row tiles
+ * of CTA pairs, tcgen05.mma.cta_group::2, each CTA loading half of a tile's
+ * B operand; 0: 128-row tiles, one CTA each),
  * "verify_columns" (64, default: after the refinement converges, the error of
  * 64 columns is measured with an FP64 residual, see bem_lu_solve_dev; -1:
  * every column; 0: no check), "tensor_split" (1, default: FP32

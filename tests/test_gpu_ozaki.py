@@ -169,9 +169,10 @@ def test_residual_method_needs_digit_planes(ctx):
 
 
 @pytest.mark.parametrize("n,nrhs", [(1, 1), (300, 129), (700, 300)])
-def test_cta_pair_kernel_matches_single_cta(ctx, n, nrhs):
-    # the 2-CTA (cta_group::2) residual computes the same integer sums and
-    # applies the groups in the same order: bitwise identical to one CTA per tile
+def test_pacing_does_not_change_the_residual(ctx, n, nrhs):
+    # the producers' pacing (residual_pace_epoch / residual_pace_lead) only
+    # delays TMA loads: every tile still sums the same integer products in
+    # the same group order, so the residual is bitwise the same
     import torch
     import bem_b200 as bb
     rng = np.random.default_rng(77 + n)
@@ -182,14 +183,16 @@ def test_cta_pair_kernel_matches_single_cta(ctx, n, nrhs):
     lu = bb.LU(ctx, Zt, bb.PREC_FP32_REFINE)
     Bt = torch.from_numpy(B.copy()).cuda()
     Xt = torch.from_numpy(X.copy()).cuda()
+    out = []
     try:
-        bb.set_option(ctx, "residual_pairs", 1)
-        R2 = lu.residual(Bt, Xt, method=1).cpu().numpy()
-        bb.set_option(ctx, "residual_pairs", 0)
-        R1 = lu.residual(Bt, Xt, method=1).cpu().numpy()
+        for epoch, lead in ((32, 2), (0, 2), (1, 0)):
+            bb.set_option(ctx, "residual_pace_epoch", epoch)
+            bb.set_option(ctx, "residual_pace_lead", lead)
+            out.append(lu.residual(Bt, Xt, method=1).cpu().numpy())
     finally:
-        bb.set_option(ctx, "residual_pairs", 0)
+        bb.set_option(ctx, "residual_pace_epoch", 32)
+        bb.set_option(ctx, "residual_pace_lead", 2)
         lu.close()
-    assert np.array_equal(R1, R2)
+    assert all(np.array_equal(out[0], R) for R in out[1:])
     with pytest.raises(bb.BemError):
         bb.set_option(ctx, "no_such_option", 1)
