@@ -609,17 +609,23 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
 // N = 256), which reads both CTAs' shared memory and accumulates each CTA's
 // 128 rows in its own TMEM.  A stage is 64 KB per CTA (96 KB for the one-CTA
 // tile, whose B is not shared), so three stages fit: per SM, 64 KB of operands
-// per 384 MMA cycles against 96 KB.  Barriers as in the int8 pair kernel
-// (ozaki.cu): full[s] on the even CTA expects both CTAs' bytes; empty[s] and
-// tfull[b] receive the MMA commits multicast to the pair; tempty[b] on the
-// even CTA counts the eight epilogue warps of both.  No load is multicast.
+// per 384 MMA cycles against 96 KB.  Barriers: full[s] lives on the even CTA
+// and expects both CTAs' bytes (one arrival, its producer's, plus the
+// transactions of both CTAs' .cta_group::2 loads); empty[s] and tfull[b]
+// receive the MMA commits multicast to the pair; tempty[b] on the even CTA
+// counts the eight epilogue warps of both.  No load is multicast.  A row-major
+// C is written through a per-warp staging buffer: a warp's 32 TMEM rows x 16
+// complex columns go to shared memory and come back as 2 rows x 16 columns
+// per instruction, so every global access of C covers whole 128-byte lines.
 constexpr int P_ROWS = 128;                               // A rows per CTA
 constexpr int P_BROWS = 128;                              // B' rows per CTA
 constexpr int P_STAGES = 3;
 constexpr int P_A_BYTES = P_ROWS * 128;                   // 16 KB per part
 constexpr int P_B_BYTES = P_BROWS * 128;                  // 16 KB per part
 constexpr int P_STAGE_BYTES = 2 * P_A_BYTES + 2 * P_B_BYTES;  // 64 KB
-constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256;
+constexpr int P_EPI_PITCH = 18;                           // complex per staged row (16 + 2: no bank conflicts)
+constexpr int P_EPI_BYTES = 4 * 32 * P_EPI_PITCH * 8;     // 4 epilogue warps x 32 rows
+constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256 + P_EPI_BYTES;
 constexpr uint32_t P_IDESC_F16 = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(256 >> 3) << 17) |
                                  ((uint32_t)(256 >> 4) << 24);
 
@@ -718,6 +724,7 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
     uint64_t* tfull = bars + 2 * P_STAGES;    // [2]
     uint64_t* tempty = bars + 2 * P_STAGES + 2;  // [2], used in the even CTA
     uint32_t* tmem_slot = (uint32_t*)(bars + 2 * P_STAGES + 4);
+    float2* epi = (float2*)(smem + P_STAGES * P_STAGE_BYTES + 256);  // [4 warps][32 rows][P_EPI_PITCH]
     __shared__ volatile int abort_flag;
     __shared__ int issued_total, consumed_total;
 
@@ -849,31 +856,11 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
                         v[2 * j + 1] *= f;
                     }
                     if (!c_colmajor) {
-                        float2* p = &C[(int64_t)row * ldc + c0];
-                        const bool vec = ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (c0 + 16 <= Nc);
-                        if (vec) {
-                            float4* p4 = reinterpret_cast<float4*>(p);
-                            float4 c[8];
+                        // staged: this thread's row into shared memory ...
+                        float4* st4 = reinterpret_cast<float4*>(epi + ((size_t)q * 32 + lane) * P_EPI_PITCH);
 #pragma unroll
-                            for (int j = 0; j < 8; j++) c[j] = store ? make_float4(0.f, 0.f, 0.f, 0.f) : p4[j];
-#pragma unroll
-                            for (int j = 0; j < 8; j++) {
-                                c[j].x -= v[4 * j];
-                                c[j].y -= v[4 * j + 1];
-                                c[j].z -= v[4 * j + 2];
-                                c[j].w -= v[4 * j + 3];
-                                p4[j] = c[j];
-                            }
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < 16; j++)
-                                if (c0 + j < Nc) {
-                                    float2 c = store ? make_float2(0.f, 0.f) : p[j];
-                                    c.x -= v[2 * j];
-                                    c.y -= v[2 * j + 1];
-                                    p[j] = c;
-                                }
-                        }
+                        for (int j = 0; j < 8; j++)
+                            st4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
                     } else {
                         const int nj = min(16, Nc - c0);
                         float2 c[16];
@@ -888,6 +875,31 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
                                 C[(int64_t)(c0 + j) * ldc + row] = c[j];
                             }
                     }
+                }
+                if (!c_colmajor) {
+                    // ... and back as 2 rows x 16 complex columns per instruction: whole
+                    // 128-byte lines of C per access
+                    __syncwarp();
+                    const int row0 = mt * 2 * P_ROWS + (int)rank * P_ROWS + q * 32;
+                    const int cj = lane & 15, col = c0 + cj;
+                    float2 c[16];
+#pragma unroll
+                    for (int it = 0; it < 16; it++) {  // the reads in flight together
+                        const int grow = row0 + 2 * it + (lane >> 4);
+                        c[it] = (store || grow >= M || col >= Nc) ? make_float2(0.f, 0.f)
+                                                                   : C[(int64_t)grow * ldc + col];
+                    }
+#pragma unroll
+                    for (int it = 0; it < 16; it++) {
+                        const int r = 2 * it + (lane >> 4), grow = row0 + r;
+                        if (grow < M && col < Nc) {
+                            const float2 a = epi[((size_t)q * 32 + r) * P_EPI_PITCH + cj];
+                            c[it].x -= a.x;
+                            c[it].y -= a.y;
+                            C[(int64_t)grow * ldc + col] = c[it];
+                        }
+                    }
+                    __syncwarp();
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -139,6 +139,60 @@ template <typename R> __device__ __forceinline__ R cabs1(typename C2T<R>::type v
 }
 
 // ------------------------------------------------------------ panel kernel
+// The two per-element operations of a panel column, with explicit fused
+// multiply-adds so that every panel kernel rounds them alike:
+// l = a inv and x - l u (complex).
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+template <typename C2> __device__ __forceinline__ C2 panel_mul(C2 a, C2 inv) {
+    C2 l;
+    l.x = fma_rn(a.x, inv.x, -(a.y * inv.y));
+    l.y = fma_rn(a.x, inv.y, a.y * inv.x);
+    return l;
+}
+template <typename C2> __device__ __forceinline__ C2 panel_msub(C2 x, C2 l, C2 u) {
+    x.x = fma_rn(-l.x, u.x, fma_rn(l.y, u.y, x.x));
+    x.y = fma_rn(-l.x, u.y, fma_rn(-l.y, u.x, x.y));
+    return x;
+}
+
+// Column jj of a panel tile after the interchange: rows below the pivot row
+// are scaled by 1/pivot (l = a inv) and the columns right of jj take the
+// rank-1 update x -= l u (u: the pivot row).  tpr = w rounded up to a power
+// of two threads per row, so a row's threads sit in one warp: they read
+// a[i][jj] before the thread of column jj overwrites it with l (__syncwarp),
+// with no integer division per element.  Every thread runs the same number
+// of passes.
+template <typename R>
+__device__ __forceinline__ void panel_eliminate(typename C2T<R>::type* tile, int w, int nloc, int lo, int jj,
+                                                const typename C2T<R>::type* s_piv, typename C2T<R>::type inv) {
+    using C2 = typename C2T<R>::type;
+    int tpr = 1;
+    while (tpr < w) tpr <<= 1;
+    const int rpp = (int)blockDim.x / tpr, cc = (int)threadIdx.x % tpr, i0 = (int)threadIdx.x / tpr;
+    const int passes = (nloc + rpp - 1) / rpp;
+    C2 u;
+    u.x = 0;
+    u.y = 0;
+    if (cc < w) u = s_piv[cc];
+    for (int ps = 0; ps < passes; ps++) {
+        const int i = i0 + ps * rpp;
+        const bool act = i < nloc && lo + i > jj && cc >= jj && cc < w;
+        C2 a;
+        a.x = 0;
+        a.y = 0;
+        if (act) a = tile[i * w + jj];
+        const C2 l = panel_mul(a, inv);
+        __syncwarp();
+        if (act) {
+            if (cc == jj)
+                tile[i * w + jj] = l;
+            else
+                tile[i * w + cc] = panel_msub(tile[i * w + cc], l, u);
+        }
+    }
+}
+
 // Factors the sub-panel rows [r0, n), columns [r0, r0+w) of the row-major
 // matrix A.  CTA b owns panel rows [b*Rp, min((b+1)*Rp, nrows)) (relative
 // to r0) in shared memory; Rp >= w so the w pivot rows live in CTA 0.
@@ -154,10 +208,9 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
     C2* s_piv = tile + (size_t)Rp * w;          // w
     __shared__ R s_val[8];
     __shared__ int s_row[8];
-    __shared__ int s_owner[8];
     __shared__ int s_flag;
     __shared__ R s_best;
-    __shared__ int s_brow, s_bown;
+    __shared__ int s_brow;
 
     const int G = Gm, mi = blockIdx.x / Gm, b = blockIdx.x % Gm, tid = threadIdx.x;
     const unsigned Gall = gridDim.x;
@@ -212,44 +265,44 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
             for (int c = tid; c < w; c += blockDim.x) __stcg(&disp[par * w + c], tile[jj * w + c]);
         // 2. all candidates published
         if (!grid_barrier(ws.bar, (unsigned)(jj + 1) * Gall, ws.status, &s_flag)) return;
-        // 3. global argmax (|re|+|im| max, smallest row on ties)
-        bv = (R)-1;
-        br = 0x7fffffff;
-        int bo = -1;
-        for (int k = tid; k < G; k += blockDim.x) {
-            R v = __ldcg(&cval[par * G + k]);
-            int r = __ldcg(&crow[par * G + k]);
-            if (r == 0x7fffffff) continue;
-            if (v > bv || (v == bv && r < br)) bv = v, br = r, bo = k;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            R ov = __shfl_down_sync(0xffffffffu, bv, o);
-            int orw = __shfl_down_sync(0xffffffffu, br, o);
-            int oo = __shfl_down_sync(0xffffffffu, bo, o);
-            if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bo = oo;
-        }
-        if (lane == 0) s_val[warp] = bv, s_row[warp] = br, s_owner[warp] = bo;
-        __syncthreads();
-        if (tid == 0) {
-            for (int k = 1; k < (int)(blockDim.x >> 5); k++)
-                if (s_val[k] > bv || (s_val[k] == bv && s_row[k] < br)) bv = s_val[k], br = s_row[k], bo = s_owner[k];
-            bool zero = !(bv > (R)0);
+        // 3. global argmax (|re|+|im| max, smallest row on ties); warp 0 also
+        // fetches the pivot row
+        if (warp == 0) {
+            bv = (R)-1;
+            br = 0x7fffffff;
+            int bo = -1;
+            for (int k = lane; k < G; k += 32) {
+                R v = __ldcg(&cval[par * G + k]);
+                int r = __ldcg(&crow[par * G + k]);
+                if (r == 0x7fffffff) continue;
+                if (v > bv || (v == bv && r < br)) bv = v, br = r, bo = k;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                R ov = __shfl_down_sync(0xffffffffu, bv, o);
+                int orw = __shfl_down_sync(0xffffffffu, br, o);
+                int oo = __shfl_down_sync(0xffffffffu, bo, o);
+                if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bo = oo;
+            }
+            bv = __shfl_sync(0xffffffffu, bv, 0);
+            br = __shfl_sync(0xffffffffu, br, 0);
+            bo = __shfl_sync(0xffffffffu, bo, 0);
+            const bool zero = !(bv > (R)0);
             if (zero) {
                 br = jj;  // no interchange; LAPACK records info and skips the scaling
                 bo = -1;
-                atomicCAS(info, 0, r0 + jj + 1);
             }
-            s_brow = br;
-            s_bown = bo;
-            s_best = bv;
-            if (b == 0) ipiv[r0 + jj] = r0 + br;
+            if (lane < w)
+                s_piv[lane] = bo >= 0 ? __ldcg(&cdata[((size_t)par * G + bo) * w + lane]) : __ldcg(&disp[par * w + lane]);
+            if (lane == 0) {
+                if (zero) atomicCAS(info, 0, r0 + jj + 1);
+                s_brow = br;
+                s_best = bv;
+                if (b == 0) ipiv[r0 + jj] = r0 + br;
+            }
         }
         __syncthreads();
-        const int piv = s_brow, own = s_bown;
+        const int piv = s_brow;
         const bool zero = !(s_best > (R)0);
-        for (int c = tid; c < w; c += blockDim.x)
-            s_piv[c] = own >= 0 ? __ldcg(&cdata[((size_t)par * G + own) * w + c]) : __ldcg(&disp[par * w + c]);
-        __syncthreads();
         // 4. interchange rows jj and piv
         if (piv != jj) {
             if (b == 0)
@@ -265,27 +318,7 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
             C2 inv;
             inv.x = p.x / den;
             inv.y = -p.y / den;
-            for (int i = tid; i < nloc; i += blockDim.x) {
-                int gr = lo + i;
-                if (gr <= jj) continue;
-                C2 a = tile[i * w + jj];
-                C2 l;
-                l.x = a.x * inv.x - a.y * inv.y;
-                l.y = a.x * inv.y + a.y * inv.x;
-                tile[i * w + jj] = l;
-            }
-            __syncthreads();
-            const int wr = w - jj - 1;
-            if (wr > 0)
-                for (int e = tid; e < nloc * wr; e += blockDim.x) {
-                    int i = e / wr, c = jj + 1 + e % wr;
-                    int gr = lo + i;
-                    if (gr <= jj) continue;
-                    C2 l = tile[i * w + jj], u = s_piv[c], x = tile[i * w + c];
-                    x.x -= l.x * u.x - l.y * u.y;
-                    x.y -= l.x * u.y + l.y * u.x;
-                    tile[i * w + c] = x;
-                }
+            panel_eliminate<R>(tile, w, nloc, lo, jj, s_piv, inv);
         }
         __syncthreads();
     }
@@ -298,165 +331,180 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
 // ----------------------------------------------------- cluster panel kernel
 // The sub-panel of panel_kernel on one thread-block cluster per matrix.  The
 // C CTAs of a cluster hold the panel rows in shared memory (CTA b: rows
-// [b Rp, (b+1) Rp), Rp >= w, so the w pivot rows live in CTA 0), publish
-// their pivot candidate in their own shared memory and read the others'
-// through distributed shared memory.  A cluster barrier per column takes the
-// place of the grid barrier: no global workspace, no spin loop, and the
-// clusters of a batch are independent (no co-residency condition).  The
-// candidate buffers alternate between two parities, so a CTA that runs ahead
-// into column jj + 1 never overwrites what a slower one still reads for jj
-// (it cannot pass the barrier of jj before that one has arrived).  Same
-// pivot rule (largest |re| + |im|, smallest row on ties) and the same
-// arithmetic per element as panel_kernel.
+// [b Rp, (b+1) Rp), Rp >= w, so the w pivot rows live in CTA 0); each
+// thread owns whole rows (row pitch WT + 1 complex: no bank conflicts) and is
+// the only one to update them.  Per column jj:
+//   A. every thread updates its rows for the pivot of column jj (row jj
+//      takes the pivot row u, the pivot row takes the former row jj, rows
+//      below jj are scaled by 1/u_jj in column jj and take the rank-1 update
+//      x -= l u right of it) and keeps the largest |re| + |im| of column
+//      jj + 1 among them (smallest row on ties);
+//   B. every warp publishes its candidate with that row's values in its
+//      CTA's shared memory, CTA 0's owner of row jj + 1 publishes that row;
+//   C. cluster barrier;
+//   D. warp 0 of every CTA reads the C x 8 candidates through distributed
+//      shared memory and reduces them alike: pivot row, its values u, row
+//      jj + 1's values, 1/u_jj+1 -- into its own shared memory;
+//   E. block barrier.
+// One cluster barrier and one block barrier per column, no spin loop.  The
+// candidate buffers alternate between two parities: a CTA in column jj + 2
+// cannot have passed barrier C of jj + 1 before every CTA has finished step
+// D of jj.  Same pivot rule and per-element arithmetic (panel_mul,
+// panel_msub) as panel_kernel, so the same pivots and factors.
+constexpr int PC_THREADS = 256, PC_WARPS = PC_THREADS / 32;
+
 template <typename R>
-__global__ void __launch_bounds__(256)
+__device__ __forceinline__ void warp_argmax(R& bv, int& br, int& bk) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const R ov = __shfl_down_sync(0xffffffffu, bv, o);
+        const int orw = __shfl_down_sync(0xffffffffu, br, o);
+        const int ok = __shfl_down_sync(0xffffffffu, bk, o);
+        if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bk = ok;
+    }
+}
+
+template <typename R, int WT>
+__global__ void __launch_bounds__(PC_THREADS)
 panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nrows, int w, int Rp,
                      int* __restrict__ ipiv, int* __restrict__ info, int64_t sA, int sPiv) {
     using C2 = typename C2T<R>::type;
     namespace cg = cooperative_groups;
+    constexpr int PITCH = WT + 1;
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C2* tile = (C2*)smem_raw;            // Rp * w
-    C2* s_piv = tile + (size_t)Rp * w;   // w: the pivot row
-    C2* s_cdata = s_piv + w;             // 2 * w: this CTA's candidate row, per parity
-    C2* s_disp = s_cdata + 2 * w;        // 2 * w: row jj (CTA 0), per parity
-    __shared__ R s_cval[2];
-    __shared__ int s_crow[2];
-    __shared__ R s_val[8];
-    __shared__ int s_row[8];
-    __shared__ R s_best;
-    __shared__ int s_brow, s_bown;
+    C2* tile = (C2*)smem_raw;                          // Rp * PITCH
+    C2* pub_data = tile + (size_t)Rp * PITCH;          // [2][PC_WARPS][32]: candidate rows
+    C2* disp = pub_data + 2 * PC_WARPS * 32;           // [2][32]: the next pivot row's former values (CTA 0)
+    __shared__ R pub_v[2][PC_WARPS];
+    __shared__ int pub_row[2][PC_WARPS];
+    __shared__ C2 s_u[32], s_dv[32];
+    __shared__ C2 s_inv;
+    __shared__ int s_piv, s_zero;
 
     const int C = (int)cluster.num_blocks(), b = (int)cluster.block_rank(), tid = threadIdx.x;
     const int mi = blockIdx.x / C;
     A += mi * sA;
     ipiv += mi * sPiv;
     info += mi;
-    const int lane = tid & 31, warp = tid >> 5;
+    const int lane = tid & 31, q = tid >> 5;
     const int lo = b * Rp;
     const int nloc = max(0, min(Rp, nrows - lo));
+    const int K = C * PC_WARPS;  // candidates per column
+    C2 zero;
+    zero.x = 0;
+    zero.y = 0;
 
     for (int e = tid; e < nloc * w; e += blockDim.x) {
-        int i = e / w, c = e % w;
-        tile[e] = A[(int64_t)(r0 + lo + i) * lda + r0 + c];
+        const int i = e / w, c = e % w;
+        tile[i * PITCH + c] = A[(int64_t)(r0 + lo + i) * lda + r0 + c];
     }
     __syncthreads();
 
-    for (int jj = 0; jj < w; jj++) {
-        const int par = jj & 1;
-        // 1. local pivot candidate among rows >= jj, published with its row
-        R bv = (R)-1;
-        int br = 0x7fffffff;
-        for (int i = tid; i < nloc; i += blockDim.x) {
-            int gr = lo + i;
-            if (gr < jj) continue;
-            R v = cabs1<R>(tile[i * w + jj]);
-            if (v > bv || (v == bv && gr < br)) bv = v, br = gr;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            R ov = __shfl_down_sync(0xffffffffu, bv, o);
-            int orw = __shfl_down_sync(0xffffffffu, br, o);
-            if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw;
-        }
-        if (lane == 0) s_val[warp] = bv, s_row[warp] = br;
-        __syncthreads();
-        if (tid == 0) {
-            for (int k = 1; k < (int)(blockDim.x >> 5); k++)
-                if (s_val[k] > bv || (s_val[k] == bv && s_row[k] < br)) bv = s_val[k], br = s_row[k];
-            s_cval[par] = bv;
-            s_crow[par] = br;
-            s_brow = br;
-        }
-        __syncthreads();
-        br = s_brow;
-        if (br != 0x7fffffff)
-            for (int c = tid; c < w; c += blockDim.x) s_cdata[par * w + c] = tile[(br - lo) * w + c];
-        if (b == 0)
-            for (int c = tid; c < w; c += blockDim.x) s_disp[par * w + c] = tile[jj * w + c];
-        // 2. every candidate published
-        cluster.sync();
-        // 3. cluster-wide argmax over the C candidates (warp 0; C <= 32)
-        if (warp == 0) {
+    // candidate for column 0: every row
+    R bv = (R)-1;
+    int br = 0x7fffffff, bk = 0;
+    for (int i = tid; i < nloc; i += PC_THREADS) {
+        const R v = cabs1<R>(tile[i * PITCH]);
+        if (v > bv || (v == bv && lo + i < br)) bv = v, br = lo + i;
+    }
+
+    for (int jn = 0; jn <= w; jn++) {
+        // jn >= 1: step A for column jj = jn - 1 (its pivot is in s_*), with
+        // the candidate for column jn
+        if (jn >= 1) {
+            const int jj = jn - 1, piv = s_piv;
+            const bool zp = s_zero != 0;
+            const C2 inv = s_inv;
             bv = (R)-1;
             br = 0x7fffffff;
-            int bo = -1;
-            if (lane < C) {
-                const R v = *cluster.map_shared_rank(&s_cval[par], lane);
-                const int r = *cluster.map_shared_rank(&s_crow[par], lane);
-                if (r != 0x7fffffff) bv = v, br = r, bo = lane;
+            for (int i = tid; i < nloc; i += PC_THREADS) {
+                const int gr = lo + i;
+                C2* row = tile + (size_t)i * PITCH;
+                if (gr == jj) {
+                    for (int c = 0; c < w; c++) row[c] = s_u[c];
+                } else if (gr > jj) {
+                    const bool isp = gr == piv && piv != jj;  // takes the former row jj
+                    if (isp)
+                        for (int c = 0; c < w; c++) row[c] = s_dv[c];
+                    if (!zp) {
+                        const C2 l = panel_mul(row[jj], inv);
+                        row[jj] = l;
+                        for (int c = jj + 1; c < w; c++) row[c] = panel_msub(row[c], l, s_u[c]);
+                    }
+                    if (jn < w) {
+                        const R v = cabs1<R>(row[jn]);
+                        if (v > bv || (v == bv && gr < br)) bv = v, br = gr;
+                    }
+                }
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                R ov = __shfl_down_sync(0xffffffffu, bv, o);
-                int orw = __shfl_down_sync(0xffffffffu, br, o);
-                int oo = __shfl_down_sync(0xffffffffu, bo, o);
-                if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bo = oo;
+        }
+        if (jn == w) break;
+        const int par = jn & 1;
+        // B. publish this warp's candidate for column jn with its row, and row jn
+        warp_argmax<R>(bv, br, bk);
+        br = __shfl_sync(0xffffffffu, br, 0);
+        __syncwarp();
+        if (lane == 0) {
+            pub_v[par][q] = bv;
+            pub_row[par][q] = br;
+        }
+        if (br != 0x7fffffff && lane < w) pub_data[(par * PC_WARPS + q) * 32 + lane] = tile[(br - lo) * PITCH + lane];
+        if (b == 0 && (jn % PC_THREADS) / 32 == q && lane < w) disp[par * 32 + lane] = tile[jn * PITCH + lane];
+        // C. every candidate of the cluster published
+        cluster.sync();
+        // D. the pivot of column jn, in warp 0 of every CTA
+        if (q == 0) {
+            R gv = (R)-1;
+            int grw = 0x7fffffff, gk = -1;
+            for (int k = lane; k < K; k += 32) {
+                const int rk = k / PC_WARPS, sk = k % PC_WARPS;
+                const int r = *cluster.map_shared_rank(&pub_row[par][sk], rk);
+                const R v = *cluster.map_shared_rank(&pub_v[par][sk], rk);
+                if (r != 0x7fffffff && (v > gv || (v == gv && r < grw))) gv = v, grw = r, gk = k;
             }
+            warp_argmax<R>(gv, grw, gk);
+            gv = __shfl_sync(0xffffffffu, gv, 0);
+            grw = __shfl_sync(0xffffffffu, grw, 0);
+            gk = __shfl_sync(0xffffffffu, gk, 0);
+            const bool zp = !(gv > (R)0);
+            if (zp) {
+                grw = jn;  // no interchange; LAPACK records info and skips the scaling
+                gk = -1;
+            }
+            C2 u = zero;
+            if (lane < w) {
+                const C2 dv = cluster.map_shared_rank(disp, 0)[par * 32 + lane];
+                u = gk >= 0 ? cluster.map_shared_rank(pub_data, gk / PC_WARPS)[(par * PC_WARPS + gk % PC_WARPS) * 32 + lane]
+                            : dv;
+                s_dv[lane] = dv;
+                s_u[lane] = u;
+            }
+            C2 p;
+            p.x = __shfl_sync(0xffffffffu, u.x, jn);
+            p.y = __shfl_sync(0xffffffffu, u.y, jn);
             if (lane == 0) {
-                bool zero = !(bv > (R)0);
-                if (zero) {
-                    br = jj;  // no interchange; LAPACK records info and skips the scaling
-                    bo = -1;
-                    if (b == 0) atomicCAS(info, 0, r0 + jj + 1);
+                C2 inv = zero;
+                if (!zp) {
+                    const R den = p.x * p.x + p.y * p.y;
+                    inv.x = p.x / den;
+                    inv.y = -p.y / den;
                 }
-                s_brow = br;
-                s_bown = bo;
-                s_best = bv;
-                if (b == 0) ipiv[r0 + jj] = r0 + br;
-            }
-        }
-        __syncthreads();
-        const int piv = s_brow, own = s_bown;
-        const bool zero = !(s_best > (R)0);
-        {
-            const C2* src = own >= 0 ? cluster.map_shared_rank(s_cdata, own) + par * w
-                                     : cluster.map_shared_rank(s_disp, 0) + par * w;
-            for (int c = tid; c < w; c += blockDim.x) s_piv[c] = src[c];
-        }
-        __syncthreads();
-        // 4. interchange rows jj and piv
-        if (piv != jj) {
-            if (b == 0)
-                for (int c = tid; c < w; c += blockDim.x) tile[jj * w + c] = s_piv[c];
-            if (piv >= lo && piv < lo + nloc) {
-                const C2* dsp = cluster.map_shared_rank(s_disp, 0) + par * w;
-                for (int c = tid; c < w; c += blockDim.x) tile[(piv - lo) * w + c] = dsp[c];
-            }
-        }
-        __syncthreads();
-        // 5. scale column jj below the diagonal, rank-1 update of the rest
-        if (!zero) {
-            C2 p = s_piv[jj];
-            R den = p.x * p.x + p.y * p.y;
-            C2 inv;
-            inv.x = p.x / den;
-            inv.y = -p.y / den;
-            for (int i = tid; i < nloc; i += blockDim.x) {
-                int gr = lo + i;
-                if (gr <= jj) continue;
-                C2 a = tile[i * w + jj];
-                C2 l;
-                l.x = a.x * inv.x - a.y * inv.y;
-                l.y = a.x * inv.y + a.y * inv.x;
-                tile[i * w + jj] = l;
-            }
-            __syncthreads();
-            const int wr = w - jj - 1;
-            if (wr > 0)
-                for (int e = tid; e < nloc * wr; e += blockDim.x) {
-                    int i = e / wr, c = jj + 1 + e % wr;
-                    int gr = lo + i;
-                    if (gr <= jj) continue;
-                    C2 l = tile[i * w + jj], u = s_piv[c], x = tile[i * w + c];
-                    x.x -= l.x * u.x - l.y * u.y;
-                    x.y -= l.x * u.y + l.y * u.x;
-                    tile[i * w + c] = x;
+                s_inv = inv;
+                s_piv = grw;
+                s_zero = zp ? 1 : 0;
+                if (b == 0) {
+                    if (zp) atomicCAS(info, 0, r0 + jn + 1);
+                    ipiv[r0 + jn] = r0 + grw;
                 }
+            }
         }
+        // E. the pivot known to every thread of this CTA
         __syncthreads();
     }
+    __syncthreads();
     for (int e = tid; e < nloc * w; e += blockDim.x) {
-        int i = e / w, c = e % w;
-        A[(int64_t)(r0 + lo + i) * lda + r0 + c] = tile[e];
+        const int i = e / w, c = e % w;
+        A[(int64_t)(r0 + lo + i) * lda + r0 + c] = tile[i * PITCH + c];
     }
     // no CTA leaves while another may still read its shared memory
     cluster.sync();
@@ -469,13 +517,18 @@ constexpr size_t PANEL_CLUSTER_SMEM = 200 * 1024;   // shared memory per CTA
 // about 384 rows per CTA, every CTA holding at least w rows, at most 8 CTAs
 // whose rows fit their shared memory; 0 when the panel does not fit one
 // cluster (panel_kernel takes it).
+static int panel_cluster_pitch(int w) { return (w <= 8 ? 8 : w <= 16 ? 16 : 32) + 1; }
+static size_t panel_cluster_smem(int Rp, int w, size_t esz) {
+    return ((size_t)Rp * panel_cluster_pitch(w) + 2 * PC_WARPS * 32 + 2 * 32) * esz;
+}
 static int panel_cluster_size(int nrows, int w, size_t esz) {
+    if (w < 1 || w > 32) return 0;
     int C = std::min(PANEL_CLUSTER_MAX, std::max(1, (nrows + 383) / 384));
-    C = std::max(1, std::min(C, nrows / std::max(w, 1)));
+    C = std::max(1, std::min(C, nrows / w));
     for (; C <= PANEL_CLUSTER_MAX; C++) {
         const int Rp = (nrows + C - 1) / C;
         if (Rp < w) return 0;
-        if (((size_t)Rp * w + 5 * (size_t)w) * esz <= PANEL_CLUSTER_SMEM) return C;
+        if (panel_cluster_smem(Rp, w, esz) <= PANEL_CLUSTER_SMEM) return C;
     }
     return 0;
 }
@@ -489,16 +542,21 @@ static int launch_panel_cluster(bem_ctx* ctx, typename C2T<R>::type* A, int64_t 
     static std::atomic<unsigned long long> attr_set{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);
     if (!(attr_set.load() & bit)) {
-        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_cluster_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_cluster_kernel<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)PANEL_CLUSTER_SMEM));
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_cluster_kernel<R, 16>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_CLUSTER_SMEM));
+        BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(panel_cluster_kernel<R, 32>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_CLUSTER_SMEM));
         attr_set.fetch_or(bit);
     }
+    auto kern = iw <= 8 ? panel_cluster_kernel<R, 8> : iw <= 16 ? panel_cluster_kernel<R, 16> : panel_cluster_kernel<R, 32>;
     const int Rp = (nrows + C - 1) / C;
-    const size_t smem = ((size_t)Rp * iw + 5 * (size_t)iw) * sizeof(C2);
-    if (smem > PANEL_CLUSTER_SMEM || Rp < iw) return fail(ctx, BEM_ERR_INVALID, "cluster panel bound violated");
+    const size_t smem = panel_cluster_smem(Rp, iw, sizeof(C2));
+    if (smem > PANEL_CLUSTER_SMEM || Rp < iw || iw > 32) return fail(ctx, BEM_ERR_INVALID, "cluster panel bound violated");
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(C * batch));
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(PC_THREADS);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = ctx->stream;
     cudaLaunchAttribute at[1];
@@ -509,8 +567,7 @@ static int launch_panel_cluster(bem_ctx* ctx, typename C2T<R>::type* A, int64_t 
     cfg.attrs = at;
     cfg.numAttrs = 1;
     cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
-    BEM_TRY_CUDA(ctx, cudaLaunchKernelEx(&cfg, panel_cluster_kernel<R>, A, lda, i0, nrows, iw, Rp, d_ipiv, d_info,
-                                         sA, sPiv));
+    BEM_TRY_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, A, lda, i0, nrows, iw, Rp, d_ipiv, d_info, sA, sPiv));
     BEM_LAUNCHED(ctx);
     if (ev)
         ctx->prof_end(PROF_PANEL, ev, 8.0 * (double)nrows * iw * iw / 2 * batch,
@@ -1248,8 +1305,15 @@ __global__ void sym_check_kernel(const double2* __restrict__ Z, int64_t ldz, int
 // triangle receives L, the diagonal D (the upper triangle is not touched).
 // One CTA of 1024 threads; 32-column sub-panels of the block's rows are
 // eliminated column by column in shared memory, then the rest of the block's
-// lower triangle is updated with them.  *info: first zero pivot (1-based).
-constexpr int LDLT_SP = 32, LDLT_PITCH = LDLT_SP + 1;
+// lower triangle is updated with them: T = D L^T of the sub-panel is formed
+// once in shared memory, and each thread accumulates a 4 x 4 set of outputs
+// of a 128 x 128 block (rows ty + 32 r, columns tx + 32 c), so that the 32
+// threads of a warp read one L entry by broadcast and 32 consecutive T
+// entries per k.  *info: first zero pivot (1-based).
+constexpr int LDLT_SP = 32, LDLT_PITCH = LDLT_SP + 1, LDLT_TP = 256;
+constexpr size_t ldlt_smem_bytes(size_t esz) {
+    return ((size_t)256 * LDLT_PITCH + (size_t)LDLT_SP * LDLT_TP) * esz;
+}
 
 template <typename R>
 __global__ void __launch_bounds__(1024)
@@ -1304,20 +1368,54 @@ ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int
         // the block's remaining lower triangle: A[i][c] -= sum_k L[i][k] d_k L[c][k]
         const int rest = rows - w;
         if (rest > 0) {
-            for (int e = tid; e < rest * rest; e += nth) {
-                const int ii = w + e / rest, cc = w + e % rest;
-                if (cc > ii) continue;
-                C2 acc = A[(int64_t)(j0 + c0 + ii) * lda + j0 + c0 + cc];
-                for (int k = 0; k < w; k++) {
-                    const C2 dk = P[k * LDLT_PITCH + k], li = P[ii * LDLT_PITCH + k], lc = P[cc * LDLT_PITCH + k];
-                    C2 t;  // d_k * l_c
-                    t.x = dk.x * lc.x - dk.y * lc.y;
-                    t.y = dk.x * lc.y + dk.y * lc.x;
-                    acc.x -= li.x * t.x - li.y * t.y;
-                    acc.y -= li.x * t.y + li.y * t.x;
-                }
-                A[(int64_t)(j0 + c0 + ii) * lda + j0 + c0 + cc] = acc;
+            C2* T = P + (size_t)256 * LDLT_PITCH;  // [k][c] = d_k L[w + c][k]
+            for (int e = tid; e < w * rest; e += nth) {
+                const int k = e / rest, c = e % rest;
+                const C2 dk = P[k * LDLT_PITCH + k], lc = P[(w + c) * LDLT_PITCH + k];
+                C2 t;
+                t.x = dk.x * lc.x - dk.y * lc.y;
+                t.y = dk.x * lc.y + dk.y * lc.x;
+                T[k * LDLT_TP + c] = t;
             }
+            __syncthreads();
+            const int ty = tid >> 5, tx = tid & 31, nbk = (rest + 127) / 128;
+            for (int bi = 0; bi < nbk; bi++)
+                for (int bc = 0; bc <= bi; bc++) {
+                    C2 acc[4][4];
+                    int ii[4], cc[4];
+#pragma unroll
+                    for (int r = 0; r < 4; r++) ii[r] = bi * 128 + ty + 32 * r;
+#pragma unroll
+                    for (int c = 0; c < 4; c++) cc[c] = bc * 128 + tx + 32 * c;
+#pragma unroll
+                    for (int r = 0; r < 4; r++)
+#pragma unroll
+                        for (int c = 0; c < 4; c++)
+                            acc[r][c] = (ii[r] < rest && cc[c] <= ii[r])
+                                            ? A[(int64_t)(j0 + c0 + w + ii[r]) * lda + j0 + c0 + w + cc[c]]
+                                            : zero;
+#pragma unroll 4
+                    for (int k = 0; k < w; k++) {
+                        C2 a[4], b[4];
+#pragma unroll
+                        for (int r = 0; r < 4; r++) a[r] = ii[r] < rest ? P[(w + ii[r]) * LDLT_PITCH + k] : zero;
+#pragma unroll
+                        for (int c = 0; c < 4; c++) b[c] = T[k * LDLT_TP + cc[c]];
+#pragma unroll
+                        for (int r = 0; r < 4; r++)
+#pragma unroll
+                            for (int c = 0; c < 4; c++) {
+                                acc[r][c].x -= a[r].x * b[c].x - a[r].y * b[c].y;
+                                acc[r][c].y -= a[r].x * b[c].y + a[r].y * b[c].x;
+                            }
+                    }
+#pragma unroll
+                    for (int r = 0; r < 4; r++)
+#pragma unroll
+                        for (int c = 0; c < 4; c++)
+                            if (ii[r] < rest && cc[c] <= ii[r])
+                                A[(int64_t)(j0 + c0 + w + ii[r]) * lda + j0 + c0 + w + cc[c]] = acc[r][c];
+                }
         }
         __syncthreads();
     }
@@ -1368,7 +1466,8 @@ __global__ void neg_eye_kernel(float2* __restrict__ W, int jb) {
 int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
     using C2 = float2;
     const int NB = TRSM_KB;
-    const size_t smem = (size_t)NB * LDLT_PITCH * sizeof(C2);
+    const size_t smem = ldlt_smem_bytes(sizeof(C2));
+    static_assert(ldlt_smem_bytes(sizeof(float2)) <= 227 * 1024, "L D L^T diagonal block shared memory");
     BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(ldlt_diag_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));

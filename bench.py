@@ -101,9 +101,10 @@ def parse():
                     help="c3: the metric's workload; c1, c2, c4, c5: the other configurations; gemm: the FP32 "
                          "tensor-core GEMM alone at the L D L^T trailing-update shape")
     ap.add_argument("--gemm-n", type=int, default=12288, help="--config gemm: rows of C (complex)")
+    ap.add_argument("--gemm-ncol", type=int, default=2790, help="--config gemm --gemm-shape solve: columns of C")
     ap.add_argument("--gemm-shape", default="factor", choices=["factor", "solve"],
                     help="--config gemm: factor: square row-major C -= A B (B row-major); solve: C (n x 2790, "
-                         "column-major) -= A B with B column-major, the multi-RHS solve's update")
+                         "column-major, --gemm-ncol) -= A B with B column-major, the multi-RHS solve's update")
     return ap.parse_args()
 
 
@@ -724,7 +725,7 @@ def run_gemm(a):
         bb.set_option(ctx, name, value)
     n, K = a.gemm_n, 512
     solve = a.gemm_shape == "solve"
-    ncol = 2790 if solve else n
+    ncol = a.gemm_ncol if solve else n
     g = torch.Generator(device="cuda:0").manual_seed(0)
     A = torch.randn((n, K), dtype=torch.complex64, device="cuda:0", generator=g)
     # solve: B given as its transpose (ncol x K row-major), C stored as (ncol x n) row-major
