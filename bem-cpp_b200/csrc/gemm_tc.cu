@@ -1020,7 +1020,9 @@ __global__ void pack_b_row_kernel(const float2* __restrict__ B, int64_t ldb, int
 // sc[t] = (s, 1/s).  Element k of item t is X[t * si + k * sk], times
 // dsc[k * dstride] when dsc is given (the D of an L D L^T update, applied as
 // the pack kernel applies it).  per_warp: one warp per item, lanes over k
-// (k contiguous); else one thread per item (items contiguous).
+// (k contiguous); else 32 items per block of 256 threads (items contiguous
+// across the lanes of a warp), the 8 warps over interleaved k, reduced in
+// shared memory.
 __global__ void f16_scale_kernel(const float2* __restrict__ X, int64_t si, int64_t sk, int n, int K,
                                  const float2* __restrict__ dsc, int64_t dstride, int per_warp,
                                  float2* __restrict__ sc) {
@@ -1032,7 +1034,9 @@ __global__ void f16_scale_kernel(const float2* __restrict__ X, int64_t si, int64
         k0 = threadIdx.x & 31;
         kstep = 32;
     } else {
-        t = (int)((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+        t = (int)blockIdx.x * 32 + (int)(threadIdx.x & 31);
+        k0 = (int)(threadIdx.x >> 5);
+        kstep = (int)(blockDim.x >> 5);
     }
     if (t < n) {
         for (int k = k0; k < K; k += kstep) {
@@ -1048,6 +1052,12 @@ __global__ void f16_scale_kernel(const float2* __restrict__ X, int64_t si, int64
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         if ((threadIdx.x & 31) != 0) return;
+    } else {
+        __shared__ float part[32][33];
+        part[threadIdx.x >> 5][threadIdx.x & 31] = m;
+        __syncthreads();
+        if (threadIdx.x >= 32) return;
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, part[w][threadIdx.x]);
     }
     if (t >= n) return;
     float sv = 1.f, inv = 1.f;
@@ -1227,13 +1237,13 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
     if (f16) {
         // scales: rows of A (k contiguous unless A comes transposed), complex columns of B
         if (o.a_trans)
-            tc::f16_scale_kernel<<<(M + 255) / 256, 256, 0, ctx->stream>>>(A, 1, lda, M, K, nullptr, 0, 0, sc_a);
+            tc::f16_scale_kernel<<<(M + 31) / 32, 256, 0, ctx->stream>>>(A, 1, lda, M, K, nullptr, 0, 0, sc_a);
         else
             tc::f16_scale_kernel<<<(unsigned)(((int64_t)M * 32 + 255) / 256), 256, 0, ctx->stream>>>(
                 A, lda, 1, M, K, nullptr, 0, 1, sc_a);
         BEM_LAUNCHED(ctx);
         if (b_rowmajor)
-            tc::f16_scale_kernel<<<(N + 255) / 256, 256, 0, ctx->stream>>>(B, 1, ldb, N, K, nullptr, 0, 0, sc_b);
+            tc::f16_scale_kernel<<<(N + 31) / 32, 256, 0, ctx->stream>>>(B, 1, ldb, N, K, nullptr, 0, 0, sc_b);
         else
             tc::f16_scale_kernel<<<(unsigned)(((int64_t)N * 32 + 255) / 256), 256, 0, ctx->stream>>>(
                 B, ldb, 1, N, K, o.bscale, o.bscale_stride, 1, sc_b);
