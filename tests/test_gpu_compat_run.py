@@ -168,3 +168,49 @@ def test_singular_matrix_reports_lapack_info(run):
     info, full = (int(x) for x in open(run / "singular.txt").read().split())
     assert info == N + 1      # the zeroed column N is the first zero pivot (1-based)
     assert full == N + 1      # lu_solve_full returns the same info, as the reference's does
+
+
+def test_geometry_cache_of_the_surface(tmp_path):
+    # compute_rhs_planewave and FFCacheGPU::upload take host meshes call by
+    # call and share device geometries kept by content: six distinct meshes
+    # (more than the four unused geometries kept), the first again, the
+    # first with one vertex moved, and far-field uploads of two meshes in
+    # turn must each give what a fresh geometry of that mesh gives
+    import bem_b200 as bb
+    cxx = shutil.which("g++")
+    exe = tmp_path / "geom_cache"
+    r = subprocess.run([cxx, "-O1", "-std=c++17", "-Wall", "-Werror",
+                        "-I" + os.path.join(REPO, "include", "bem"), "-I" + os.path.join(REPO, "include"),
+                        "-o", str(exe), os.path.join(REPO, "tests", "compat", "geom_cache.cpp"),
+                        "-L" + LIB, "-Wl,-rpath," + LIB, "-lbem_compat", "-lbemdense"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = tmp_path / "out"
+    out.mkdir()
+    r = subprocess.run([str(exe), str(out)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (r.stdout[-1500:], r.stderr[-1500:])
+    meshes = [bb.icosphere(1.0, 1), bb.hex_prism(1.3, 1), bb.icosphere(0.7, 1), bb.hex_prism(0.8, 1),
+              bb.icosphere(1.0, 2), bb.hex_prism(1.5, 2)]
+    ctx = bb.Context(0)
+    try:
+        def fresh(v, t):
+            g = bb.Geometry(ctx, v, t, 7)
+            B = bb.rhs_planewave_dev(g, 2.0, 1.0, np.eye(3)[None])[0].cpu().numpy()
+            g.close()
+            return B
+        got = [np.fromfile(out / f"rhs{i}.bin", dtype=np.complex128) for i in range(len(meshes))]
+        for (v, t), b in zip(meshes, got):
+            assert rel(b, fresh(v, t)) < 1e-14
+        again = np.fromfile(out / "rhs0_again.bin", dtype=np.complex128)
+        assert np.array_equal(again, got[0])
+        v0, t0 = meshes[0]
+        vm = np.array(v0, dtype=np.float64).copy()
+        vm[0] *= 1.05
+        moved = np.fromfile(out / "rhs0_moved.bin", dtype=np.complex128)
+        assert rel(moved, got[0]) > 1e-6
+        assert rel(moved, fresh(vm, t0)) < 1e-14
+    finally:
+        ctx.close()
+    ff0, ff1, ff0b = (np.fromfile(out / f, dtype=np.complex128) for f in ("ff0.bin", "ff1.bin", "ff0_again.bin"))
+    assert np.array_equal(ff0, ff0b) and np.all(np.isfinite(ff0))
+    assert rel(ff1, ff0) > 1e-3
