@@ -1346,13 +1346,14 @@ ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int
             }
             __syncthreads();
             // rank-1 update of the sub-panel's remaining columns (lower part):
-            // a[i][c] -= l_i (d l_c), d l_c being the unscaled a[c][jj]
-            const int wr = w - jj - 1;
-            if (!zp && wr > 0) {
-                for (int e = tid; e < (rows - jj - 1) * wr; e += nth) {
-                    const int i = jj + 1 + e / wr, c = jj + 1 + e % wr;
-                    if (c > i) continue;
-                    const C2 l = P[i * LDLT_PITCH + jj], wc = wcol[c];
+            // a[i][c] -= l_i (d l_c), d l_c being the unscaled a[c][jj]; a
+            // warp per row, lane = column (LDLT_SP = 32), no index division
+            if (!zp && jj + 1 < w) {
+                const int c = tid & 31;
+                const C2 wc = wcol[c < w ? c : 0];
+                for (int i = jj + 1 + (tid >> 5); i < rows; i += nth >> 5) {
+                    if (c <= jj || c >= w || c > i) continue;
+                    const C2 l = P[i * LDLT_PITCH + jj];
                     C2 x = P[i * LDLT_PITCH + c];
                     x.x -= l.x * wc.x - l.y * wc.y;
                     x.y -= l.x * wc.y + l.y * wc.x;
