@@ -353,14 +353,30 @@ panel_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0, int nro
 // panel_msub) as panel_kernel, so the same pivots and factors.
 constexpr int PC_THREADS = 256, PC_WARPS = PC_THREADS / 32;
 
-template <typename R>
-__device__ __forceinline__ void warp_argmax(R& bv, int& br, int& bk) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const R ov = __shfl_down_sync(0xffffffffu, bv, o);
-        const int orw = __shfl_down_sync(0xffffffffu, br, o);
-        const int ok = __shfl_down_sync(0xffffffffu, bk, o);
-        if (ov > bv || (ov == bv && orw < br)) bv = ov, br = orw, bk = ok;
-    }
+// The warp's largest bv, the smallest br among the lanes holding it and that
+// lane's bk, in every lane.  bv >= 0 (a lane without a candidate holds 0 with
+// br = INT_MAX): the bit patterns of non-negative floating-point numbers
+// order like unsigned integers, so integer warp reductions find it.
+__device__ __forceinline__ void warp_argmax_bits(unsigned hi, unsigned lo, int& br, int& bk, unsigned& mhi,
+                                                 unsigned& mlo) {
+    mhi = __reduce_max_sync(0xffffffffu, hi);
+    mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const bool top = hi == mhi && lo == mlo;
+    const unsigned mrow = __reduce_min_sync(0xffffffffu, top ? (unsigned)br : 0xffffffffu);
+    const unsigned win = __ballot_sync(0xffffffffu, top && (unsigned)br == mrow);
+    bk = __shfl_sync(0xffffffffu, bk, __ffs(win) - 1);
+    br = (int)mrow;
+}
+__device__ __forceinline__ void warp_argmax(double& bv, int& br, int& bk) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(bv);
+    unsigned mhi, mlo;
+    warp_argmax_bits((unsigned)(b >> 32), (unsigned)b, br, bk, mhi, mlo);
+    bv = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+}
+__device__ __forceinline__ void warp_argmax(float& bv, int& br, int& bk) {
+    unsigned mhi, mlo;
+    warp_argmax_bits(__float_as_uint(bv), 0u, br, bk, mhi, mlo);
+    bv = __uint_as_float(mhi);
 }
 
 template <typename R, int WT>
@@ -401,7 +417,7 @@ panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0,
     __syncthreads();
 
     // candidate for column 0: every row
-    R bv = (R)-1;
+    R bv = (R)0;
     int br = 0x7fffffff, bk = 0;
     for (int i = tid; i < nloc; i += PC_THREADS) {
         const R v = cabs1<R>(tile[i * PITCH]);
@@ -415,7 +431,7 @@ panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0,
             const int jj = jn - 1, piv = s_piv;
             const bool zp = s_zero != 0;
             const C2 inv = s_inv;
-            bv = (R)-1;
+            bv = (R)0;
             br = 0x7fffffff;
             for (int i = tid; i < nloc; i += PC_THREADS) {
                 const int gr = lo + i;
@@ -441,8 +457,7 @@ panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0,
         if (jn == w) break;
         const int par = jn & 1;
         // B. publish this warp's candidate for column jn with its row, and row jn
-        warp_argmax<R>(bv, br, bk);
-        br = __shfl_sync(0xffffffffu, br, 0);
+        warp_argmax(bv, br, bk);  // in every lane
         __syncwarp();
         if (lane == 0) {
             pub_v[par][q] = bv;
@@ -450,22 +465,23 @@ panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0,
         }
         if (br != 0x7fffffff && lane < w) pub_data[(par * PC_WARPS + q) * 32 + lane] = tile[(br - lo) * PITCH + lane];
         if (b == 0 && (jn % PC_THREADS) / 32 == q && lane < w) disp[par * 32 + lane] = tile[jn * PITCH + lane];
-        // C. every candidate of the cluster published
-        cluster.sync();
+        // C. every candidate of the cluster published (a one-CTA cluster:
+        // the block barrier)
+        if (C > 1)
+            cluster.sync();
+        else
+            __syncthreads();
         // D. the pivot of column jn, in warp 0 of every CTA
         if (q == 0) {
-            R gv = (R)-1;
+            R gv = (R)0;
             int grw = 0x7fffffff, gk = -1;
             for (int k = lane; k < K; k += 32) {
                 const int rk = k / PC_WARPS, sk = k % PC_WARPS;
-                const int r = *cluster.map_shared_rank(&pub_row[par][sk], rk);
-                const R v = *cluster.map_shared_rank(&pub_v[par][sk], rk);
+                const int r = C > 1 ? *cluster.map_shared_rank(&pub_row[par][sk], rk) : pub_row[par][sk];
+                const R v = C > 1 ? *cluster.map_shared_rank(&pub_v[par][sk], rk) : pub_v[par][sk];
                 if (r != 0x7fffffff && (v > gv || (v == gv && r < grw))) gv = v, grw = r, gk = k;
             }
-            warp_argmax<R>(gv, grw, gk);
-            gv = __shfl_sync(0xffffffffu, gv, 0);
-            grw = __shfl_sync(0xffffffffu, grw, 0);
-            gk = __shfl_sync(0xffffffffu, gk, 0);
+            warp_argmax(gv, grw, gk);  // in every lane
             const bool zp = !(gv > (R)0);
             if (zp) {
                 grw = jn;  // no interchange; LAPACK records info and skips the scaling
@@ -473,9 +489,10 @@ panel_cluster_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int r0,
             }
             C2 u = zero;
             if (lane < w) {
-                const C2 dv = cluster.map_shared_rank(disp, 0)[par * 32 + lane];
-                u = gk >= 0 ? cluster.map_shared_rank(pub_data, gk / PC_WARPS)[(par * PC_WARPS + gk % PC_WARPS) * 32 + lane]
-                            : dv;
+                const C2* dsrc = C > 1 ? cluster.map_shared_rank(disp, 0) : disp;
+                const C2* usrc = C > 1 ? cluster.map_shared_rank(pub_data, gk >= 0 ? gk / PC_WARPS : 0) : pub_data;
+                const C2 dv = dsrc[par * 32 + lane];
+                u = gk >= 0 ? usrc[(par * PC_WARPS + gk % PC_WARPS) * 32 + lane] : dv;
                 s_dv[lane] = dv;
                 s_u[lane] = u;
             }
