@@ -616,7 +616,8 @@ def run_bem(a):
 CONFIGS = {
     "c1": {"metric": "s per C1 run: icosphere r2 (2N=960), ka=1, m=1.3116, single orientation, 181 angles, FP64",
            "workload": "icosphere ref 2 (2N=960), ka=1, m=1.3116, quad 7, --single (k=z, E=x/y), 181 angles"},
-    "c2": {"metric": "s/solve at C2: hex prism AR 1.4286 r3 (2N=4608), ka=5, 128 RHS, FP64 LU + solves",
+    "c2": {"metric": "s per C2 run: hex prism AR 1.4286 r3 (2N=4608), ka=5, 128 RHS: assembly + FP64 LU + solves + "
+                     "far field / Mueller",
            "workload": "hex prism AR=1.4286 ref 3 (2N=4608), ka=5, m=1.3116, quad 7, 8x8x1 orientations x 2 pol"},
     "c4": {"metric": "s per batch of 64 seeded hex prisms (2N 1152 / 4608): assembly + LU + solves + Mueller",
            "workload": "64 hex prisms from seed 0: AR U[0.5,2], ref 2 or 3, ka U[1,5], Re m U[1.3,1.6], "
@@ -795,9 +796,11 @@ def run_config(a):
             r = cpu_dense_path(v, t, 1.0, 1.3116, 1, 181, reps=reps)
             return r, r["total"]
         if a.config == "c2":
+            # the whole path at full size (every assembly row, in blocks; the
+            # full LU, solves and far field): a few minutes of CPU
             v, t = bb.hex_prism(1.4286, 3)
-            r = cpu_dense_path(v, t, 5.0, 1.3116, 64, 181, reps=reps, rows=32, n_ff=8)
-            return r, r["solve_only"]
+            r = cpu_dense_path(v, t, 5.0, 1.3116, 64, 181, reps=reps, rows="blocks")
+            return r, r["total"]
         if a.config == "c4":
             parts = bb.c4_particles(0, 64)
             tot, descs, cores = 0.0, [], 1
@@ -957,7 +960,7 @@ def run_config(a):
                      "clocks": clocks})
     line["gpu_launches"] = int(ctx.launches - launches0)
     if not a.no_cpu:
-        r, v = cpu_leg(1 if a.config in ("c4", "c5") else 3)
+        r, v = cpu_leg(3 if a.config == "c1" else 1)
         line["cpu_baseline"] = {"value": v, "unit": "s", "cores": r["cores"], "kind": "port",
                                 "sample": r["description"]}
     print(json.dumps(line), flush=True)

@@ -59,8 +59,10 @@ def time_dense_path(verts, tris, ka, m, n_orient, ntheta=181, rows=None, n_lu=No
                     ff_dirs=None, sing_mesh=None, phases=("assembly", "lu", "solve", "farfield"), seed=0):
     """Times the reference's CPU dense path on the mesh (verts, tris) with
     n_orient orientations x 2 polarisations, on samples (rows / n_lu / n_ff
-    None: the full size).  Returns a dict of seconds per phase (scaled to the
-    full size), their sum, and a description of the samples."""
+    None: the full size; rows "blocks": every test row, in blocks of 256, for
+    sizes whose one-call assembly would not fit the host's memory).  Returns a
+    dict of seconds per phase (scaled to the full size), their sum, and a
+    description of the samples."""
     tris = np.asarray(tris, dtype=np.int64)
     rwg = bo.build_rwg(verts, tris, "cpp")
     N = rwg["N"]
@@ -70,10 +72,27 @@ def time_dense_path(verts, tris, ka, m, n_orient, ntheta=181, rows=None, n_lu=No
     out, desc = {}, []
     if "assembly" in phases:
         H = bo.halves(rwg, verts, tris, 7)
-        r = N if rows is None else max(1, min(N, rows))
+        r = N if rows in (None, "blocks") else max(1, min(N, rows))
         sel = np.arange(r)
         t0 = time.perf_counter()
-        if r == N:
+        if rows == "blocks":
+            # every test row, in blocks of 256 (bounded memory), the same
+            # passes as the sampled rows below
+            for r0 in range(0, N, 256):
+                Hs = [_sub_half(h, np.arange(r0, min(N, r0 + 256))) for h in H]
+                for k in (kx, ki):
+                    for a in range(2):
+                        for b in range(2):
+                            bo._regular_LK(Hs[a], H[b], k, distance="expanded")
+            t_rows = time.perf_counter() - t0
+            t1 = time.perf_counter()
+            for k in (kx, ki):
+                bo.singular_corrections(rwg, verts, tris, k, 7)
+            t_sing = time.perf_counter() - t1
+            t_asm = t_rows * 3.0 / 4.0 + t_sing
+            desc.append(f"assembly: all {N} test rows in blocks of 256 x all columns, 2 media, 4 half pairs in "
+                        f"{t_rows:.2f} s x 3/4 + Graglia terms {t_sing:.2f} s")
+        elif r == N:
             bo.assemble_pmchwt(rwg, verts, tris, kx, ki, ee, ei, 7, distance="expanded")
             t_asm = time.perf_counter() - t0
             desc.append(f"assembly full ({t_asm:.2f} s)")
