@@ -29,6 +29,8 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "bem_internal.h"
@@ -550,6 +552,49 @@ static int panel_cluster_size(int nrows, int w, size_t esz) {
     return 0;
 }
 
+// panel_cluster_size, kept only where a cluster of that size and shared
+// memory can be resident on this device (cudaOccupancyMaxActiveClusters,
+// asked once per shape and remembered); 0: the cooperative panel.
+template <typename R>
+static int panel_cluster_choice(bem_ctx* ctx, int nrows, int iw) {
+    using C2 = typename C2T<R>::type;
+    if (!ctx->panel_clusters) return 0;
+    const int C = panel_cluster_size(nrows, iw, sizeof(C2));
+    if (C < 1) return 0;
+    const int Rp = (nrows + C - 1) / C;
+    const size_t smem = panel_cluster_smem(Rp, iw, sizeof(C2));
+    auto kern = iw <= 8 ? panel_cluster_kernel<R, 8> : iw <= 16 ? panel_cluster_kernel<R, 16> : panel_cluster_kernel<R, 32>;
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, int, size_t>, bool> ok;
+    const auto key = std::make_tuple(ctx->device, (const void*)kern, C, (smem + 4095) / 4096);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = ok.find(key);
+        if (it != ok.end()) return it->second ? C : 0;
+    }
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_CLUSTER_SMEM) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)C);
+    cfg.blockDim = dim3(PC_THREADS);
+    cfg.dynamicSmemBytes = ((smem + 4095) / 4096) * 4096 < PANEL_CLUSTER_SMEM ? ((smem + 4095) / 4096) * 4096 : smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    const bool fits = cudaOccupancyMaxActiveClusters(&ncl, (const void*)kern, &cfg) == cudaSuccess && ncl >= 1;
+    if (!fits) cudaGetLastError();
+    std::lock_guard<std::mutex> lk(mu);
+    ok[key] = fits;
+    return fits ? C : 0;
+}
+
 // One launch of panel_cluster_kernel: `batch` matrices (A + i sA, pivots
 // ipiv + i sPiv, info + i), C CTAs per matrix.
 template <typename R>
@@ -932,7 +977,7 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
         for (int i0 = j0; i0 < j0 + jb; i0 += W) {
             const int iw = std::min(W, j0 + jb - i0);
             const int nrows = n - i0;
-            const int Cl = ctx->panel_clusters ? panel_cluster_size(nrows, iw, sizeof(C2)) : 0;
+            const int Cl = panel_cluster_choice<R>(ctx, nrows, iw);
             if (Cl > 0) {
                 BEM_TRY(launch_panel_cluster<R>(ctx, A, lda, i0, nrows, iw, d_ipiv, d_info, 1, 0, 0, Cl));
             } else {
@@ -1054,7 +1099,7 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
     const size_t smem_max = 220 * 1024;
     // every sub-panel fits one cluster (the first is the tallest): no
     // cooperative grid, no chunking of the batch
-    const bool all_clusters = ctx->panel_clusters && panel_cluster_size(n, W, sizeof(C2)) > 0;
+    const bool all_clusters = panel_cluster_choice<R>(ctx, n, W) > 0;
     const int Rp_max = (int)std::min<int64_t>(n, ((int64_t)smem_max / (int64_t)sizeof(C2) - W) / W);
     if (Rp_max < 2 * W) return fail(ctx, BEM_ERR_INVALID, "batched LU: panel does not fit");
     const int Gm_min = (n + Rp_max - 1) / Rp_max;
@@ -1106,7 +1151,7 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
         for (int i0 = j0; i0 < j0 + jb; i0 += W) {
             const int iw = std::min(W, j0 + jb - i0);
             const int nrows = n - i0;
-            const int Cl = ctx->panel_clusters ? panel_cluster_size(nrows, iw, sizeof(C2)) : 0;
+            const int Cl = panel_cluster_choice<R>(ctx, nrows, iw);
             if (Cl > 0) {
                 BEM_TRY(launch_panel_cluster<R>(ctx, A, lda, i0, nrows, iw, d_ipiv, d_info, batch, sA, n, Cl));
             } else {
