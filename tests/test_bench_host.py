@@ -85,3 +85,24 @@ def test_cpu_dense_path_sample_is_scaled_and_described():
     assert "30 of 120 test rows" in samp["description"] and "median of 3" in samp["description"]
     assert "scaled by (n/96)^3" in samp["description"] and "1 of 2 orientations at 7 of 19" in samp["description"]
     assert 0.2 < samp["assembly"] / full["assembly"] < 5.0
+
+
+def test_options_and_config_switches(monkeypatch):
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--option", "residual_pace_epoch=16", "--option",
+                                      "residual_pace_lead = 1", "--config", "gemm", "--gemm-shape", "solve"])
+    a = bench.parse()
+    assert bench.extra_options(a) == {"residual_pace_epoch": 16, "residual_pace_lead": 1}
+    assert (a.config, a.gemm_shape, a.gemm_n, a.gemm_ncol, a.gemm_pairs) == ("gemm", "solve", 12288, 2790, 1)
+
+
+def test_cpu_dense_path_blocked_assembly_covers_every_row():
+    # the full-size C2 leg times every assembly row in blocks: the same work
+    # as one call, so about the same time, and described as such
+    import bench
+    from oracle import bem_oracle as bo
+    v, t = bo.icosphere(1.0, 1)
+    full = bench.cpu_dense_path(v, t, 1.0, 1.3116, 2, 19)
+    blk = bench.cpu_dense_path(v, t, 1.0, 1.3116, 2, 19, rows="blocks")
+    assert "all 120 test rows in blocks of 256" in blk["description"]
+    assert 0.2 < blk["assembly"] / full["assembly"] < 5.0 and blk["total"] > blk["solve_only"] > 0
