@@ -613,19 +613,18 @@ gemm_persistent_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_c
 // and expects both CTAs' bytes (one arrival, its producer's, plus the
 // transactions of both CTAs' .cta_group::2 loads); empty[s] and tfull[b]
 // receive the MMA commits multicast to the pair; tempty[b] on the even CTA
-// counts the eight epilogue warps of both.  No load is multicast.  A row-major
-// C is written through a per-warp staging buffer: a warp's 32 TMEM rows x 16
-// complex columns go to shared memory and come back as 2 rows x 16 columns
-// per instruction, so every global access of C covers whole 128-byte lines.
+// counts the epilogue warps of both.  No load is multicast.  Eight epilogue
+// warps per CTA: two per TMEM lane quarter, each draining half of the
+// accumulator's columns, so a tile's epilogue takes half as long as with four.
 constexpr int P_ROWS = 128;                               // A rows per CTA
 constexpr int P_BROWS = 128;                              // B' rows per CTA
 constexpr int P_STAGES = 3;
 constexpr int P_A_BYTES = P_ROWS * 128;                   // 16 KB per part
 constexpr int P_B_BYTES = P_BROWS * 128;                  // 16 KB per part
 constexpr int P_STAGE_BYTES = 2 * P_A_BYTES + 2 * P_B_BYTES;  // 64 KB
-constexpr int P_EPI_PITCH = 18;                           // complex per staged row (16 + 2: no bank conflicts)
-constexpr int P_EPI_BYTES = 4 * 32 * P_EPI_PITCH * 8;     // 4 epilogue warps x 32 rows
-constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256 + P_EPI_BYTES;
+constexpr int P_EPI_WARPS = 8;                            // epilogue warps per CTA (2 per lane quarter)
+constexpr int P_THREADS = 64 + 32 * P_EPI_WARPS;           // producer, MMA issuer, epilogue
+constexpr int P_SMEM_BYTES = P_STAGES * P_STAGE_BYTES + 1024 + 256;
 constexpr uint32_t P_IDESC_F16 = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(256 >> 3) << 17) |
                                  ((uint32_t)(256 >> 4) << 24);
 
@@ -710,7 +709,7 @@ struct PairTiles {
     }
 };
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(P_THREADS, 1)
 gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                  const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
                  float2* __restrict__ C, int64_t ldc, int c_colmajor, int M, int Nc, int K2, int lower, int store,
@@ -724,7 +723,6 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
     uint64_t* tfull = bars + 2 * P_STAGES;    // [2]
     uint64_t* tempty = bars + 2 * P_STAGES + 2;  // [2], used in the even CTA
     uint32_t* tmem_slot = (uint32_t*)(bars + 2 * P_STAGES + 4);
-    float2* epi = (float2*)(smem + P_STAGES * P_STAGE_BYTES + 256);  // [4 warps][32 rows][P_EPI_PITCH]
     __shared__ volatile int abort_flag;
     __shared__ int issued_total, consumed_total;
 
@@ -749,7 +747,7 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(smem_u32(&tfull[b]), 1);
-            mbar_init(smem_u32(&tempty[b]), 8);
+            mbar_init(smem_u32(&tempty[b]), 2 * P_EPI_WARPS);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -824,8 +822,9 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
             }
         }
     } else {
-        // epilogue warps 2..5 of both CTAs: TMEM lane quarter = warp % 4
-        const int q = warp & 3;
+        // epilogue warps 2..9 of both CTAs: TMEM lane quarter = warp % 4, and
+        // half of the 256 accumulator columns each
+        const int q = warp & 3, chalf = (warp - 2) >> 2;
         const uint32_t te0 = cl_map(smem_u32(&tempty[0]), 0), te1 = cl_map(smem_u32(&tempty[1]), 0);
         int lt = 0;
         for (int t = cid; t < ntiles; t += ncl) {
@@ -843,7 +842,7 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
             const int row = mt * 2 * P_ROWS + (int)rank * P_ROWS + q * 32 + lane;
             const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
 #pragma unroll 1
-            for (int ch = 0; ch < 256 / 32 && write; ch++) {
+            for (int ch = chalf * 4; ch < chalf * 4 + 4 && write; ch++) {
                 float v[32];
                 tmem_ld32(base + ch * 32, v);
                 const int c0 = nt * P_BROWS + ch * 16;
@@ -856,11 +855,31 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
                         v[2 * j + 1] *= f;
                     }
                     if (!c_colmajor) {
-                        // staged: this thread's row into shared memory ...
-                        float4* st4 = reinterpret_cast<float4*>(epi + ((size_t)q * 32 + lane) * P_EPI_PITCH);
+                        float2* p = &C[(int64_t)row * ldc + c0];
+                        const bool vec = ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && (c0 + 16 <= Nc);
+                        if (vec) {
+                            float4* p4 = reinterpret_cast<float4*>(p);
+                            float4 c[8];
 #pragma unroll
-                        for (int j = 0; j < 8; j++)
-                            st4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                            for (int j = 0; j < 8; j++) c[j] = store ? make_float4(0.f, 0.f, 0.f, 0.f) : p4[j];
+#pragma unroll
+                            for (int j = 0; j < 8; j++) {
+                                c[j].x -= v[4 * j];
+                                c[j].y -= v[4 * j + 1];
+                                c[j].z -= v[4 * j + 2];
+                                c[j].w -= v[4 * j + 3];
+                                p4[j] = c[j];
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 16; j++)
+                                if (c0 + j < Nc) {
+                                    float2 c = store ? make_float2(0.f, 0.f) : p[j];
+                                    c.x -= v[2 * j];
+                                    c.y -= v[2 * j + 1];
+                                    p[j] = c;
+                                }
+                        }
                     } else {
                         const int nj = min(16, Nc - c0);
                         float2 c[16];
@@ -875,31 +894,6 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
                                 C[(int64_t)(c0 + j) * ldc + row] = c[j];
                             }
                     }
-                }
-                if (!c_colmajor) {
-                    // ... and back as 2 rows x 16 complex columns per instruction: whole
-                    // 128-byte lines of C per access
-                    __syncwarp();
-                    const int row0 = mt * 2 * P_ROWS + (int)rank * P_ROWS + q * 32;
-                    const int cj = lane & 15, col = c0 + cj;
-                    float2 c[16];
-#pragma unroll
-                    for (int it = 0; it < 16; it++) {  // the reads in flight together
-                        const int grow = row0 + 2 * it + (lane >> 4);
-                        c[it] = (store || grow >= M || col >= Nc) ? make_float2(0.f, 0.f)
-                                                                   : C[(int64_t)grow * ldc + col];
-                    }
-#pragma unroll
-                    for (int it = 0; it < 16; it++) {
-                        const int r = 2 * it + (lane >> 4), grow = row0 + r;
-                        if (grow < M && col < Nc) {
-                            const float2 a = epi[((size_t)q * 32 + r) * P_EPI_PITCH + cj];
-                            c[it].x -= a.x;
-                            c[it].y -= a.y;
-                            C[(int64_t)grow * ldc + col] = c[it];
-                        }
-                    }
-                    __syncwarp();
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1315,7 +1309,7 @@ int tc_gemm_ex(bem_ctx* ctx, int M, int N, int K, const float2* A, int64_t lda, 
         const int nm = (M + 2 * tc::P_ROWS - 1) / (2 * tc::P_ROWS), nn = (2 * N + 255) / 256;
         const int ntiles = o.lower ? nm * std::min(nn, 2 * nm) : nm * nn;  // an upper bound for the lower raster
         const int grid = 2 * std::max(1, std::min(ntiles, ctx->sm_count / 2));
-        tc::gemm_pair_kernel<<<grid, 192, tc::P_SMEM_BYTES, ctx->stream>>>(
+        tc::gemm_pair_kernel<<<grid, tc::P_THREADS, tc::P_SMEM_BYTES, ctx->stream>>>(
             mah, mal, pbh, pbl, C, ldc, c_colmajor ? 1 : 0, M, N, ld, o.lower ? 1 : 0, o.store ? 1 : 0,
             std::max(1, ctx->tc_group_m / 2), ctx->d_status, sc_a, sc_b);
     } else if (ctx->tc_persistent) {
