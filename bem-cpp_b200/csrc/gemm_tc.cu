@@ -824,7 +824,9 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
     } else {
         // epilogue warps 2..9 of both CTAs: TMEM lane quarter = warp % 4, and
         // half of the 256 accumulator columns each
-        const int q = warp & 3, chalf = (warp - 2) >> 2;
+        // chunks [ch0, ch1) of the 8 32-column chunks for this warp
+        const int q = warp & 3, part = (warp - 2) >> 2, nparts = P_EPI_WARPS / 4;
+        const int ch0 = part * 8 / nparts, ch1 = (part + 1) * 8 / nparts;
         const uint32_t te0 = cl_map(smem_u32(&tempty[0]), 0), te1 = cl_map(smem_u32(&tempty[1]), 0);
         int lt = 0;
         for (int t = cid; t < ntiles; t += ncl) {
@@ -842,7 +844,7 @@ gemm_pair_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constan
             const int row = mt * 2 * P_ROWS + (int)rank * P_ROWS + q * 32 + lane;
             const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
 #pragma unroll 1
-            for (int ch = chalf * 4; ch < chalf * 4 + 4 && write; ch++) {
+            for (int ch = ch0; ch < ch1 && write; ch++) {
                 float v[32];
                 tmem_ld32(base + ch * 32, v);
                 const int c0 = nt * P_BROWS + ch * 16;
