@@ -15,8 +15,9 @@
 //       laswp + small TRSM + thin GEMM for the rest of the block column
 //     laswp of the block's pivots on the other columns
 //     U12 = L11^-1 A12  (blocked TRSM)
-//     A22 -= L21 U12    (the trailing update: CUDA-core GEMM for FP64,
-//                        3xTF32 tcgen05 GEMM for FP32)
+//     A22 -= L21 U12    (the trailing update: FP64 on the FP64 tensor path,
+//                        mma.sync f64, three real products per complex
+//                        one; FP32 on tcgen05 with FP16 (or TF32) parts)
 //
 // The pivot rule is the one of LAPACK izamax: largest |re| + |im|, first
 // index on ties.
@@ -59,27 +60,36 @@ int cgemm(bem_ctx* ctx, int M, int N, int K, const typename C2T<R>::type* A, int
     if (sizeof(R) == 8) {
         // FP64: the m8n8k4 f64 tensor path (zgemm_dmma.cuh)
         // the attribute is per device: one bit per (kernel variant, device id)
-        static std::atomic<unsigned long long> attr[4];
+        // (three real products per complex one unless the context asks for four)
+        static std::atomic<unsigned long long> attr[8];
         const double2* Ad = reinterpret_cast<const double2*>(A);
         const double2* Bd = reinterpret_cast<const double2*>(B);
         double2* Cd = reinterpret_cast<double2*>(C);
         double2 al = make_double2(alpha.x, alpha.y), be = make_double2(beta.x, beta.y);
-        auto go = [&](auto kern, int slot) -> int {
+        auto go = [&](auto kern, int slot, int threads, int smem) -> int {
             const unsigned long long bit = 1ull << (ctx->device & 63);
             if (!(attr[slot].load() & bit)) {
-                BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       dmma::SMEM_BYTES));
+                BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
                 attr[slot].fetch_or(bit);
             }
-            kern<<<grid, 128, dmma::SMEM_BYTES, ctx->stream>>>(M, N, K, Ad, lda, Bd, ldb, Cd, ldc, al, be, sA, sB,
-                                                               sC);
+            kern<<<grid, threads, smem, ctx->stream>>>(M, N, K, Ad, lda, Bd, ldb, Cd, ldc, al, be, sA, sB, sC);
             return BEM_OK;
         };
+        const int t4 = 128, s4 = dmma::SMEM_BYTES, t3 = dmma::M3_THREADS, s3 = dmma::M3_SMEM_BYTES;
         int s;
-        if (b_kmajor)
-            s = c_colmajor ? go(dmma::zgemm_kernel<true, true>, 0) : go(dmma::zgemm_kernel<true, false>, 1);
-        else
-            s = c_colmajor ? go(dmma::zgemm_kernel<false, true>, 2) : go(dmma::zgemm_kernel<false, false>, 3);
+        if (ctx->dmma_3m) {
+            if (b_kmajor)
+                s = c_colmajor ? go(dmma::zgemm3m_kernel<true, true>, 4, t3, s3)
+                               : go(dmma::zgemm3m_kernel<true, false>, 5, t3, s3);
+            else
+                s = c_colmajor ? go(dmma::zgemm3m_kernel<false, true>, 6, t3, s3)
+                               : go(dmma::zgemm3m_kernel<false, false>, 7, t3, s3);
+        } else if (b_kmajor) {
+            s = c_colmajor ? go(dmma::zgemm_kernel<true, true>, 0, t4, s4) : go(dmma::zgemm_kernel<true, false>, 1, t4, s4);
+        } else {
+            s = c_colmajor ? go(dmma::zgemm_kernel<false, true>, 2, t4, s4)
+                           : go(dmma::zgemm_kernel<false, false>, 3, t4, s4);
+        }
         BEM_TRY(s);
     } else if (b_kmajor) {
         if (c_colmajor)

@@ -17,6 +17,20 @@
 // shape (M = N = 16384, K = 256, beta = 1) 32.7 TF/s against 30.7 TF/s for
 // 3 stages at 2 CTAs per SM; the third resident CTA hides the barrier and
 // the epilogue of the others.
+//
+// zgemm3m_kernel takes the complex product with three real products instead
+// of four (Gauss; Higham, "Stability of a method for multiplying complex
+// matrices with three real matrix multiplications", SIMAX 13, 1992):
+//   T1 = Ar Br,  T2 = Ai Bi,  T3 = (Ar + Ai)(Br + Bi),
+//   Re C = T1 - T2,  Im C = T3 - T1 - T2,
+// 6MNK real multiply-adds instead of 8MNK.  The error stays normwise at the
+// FP64 unit roundoff: |Im error| <= ~K u (|Ar| + |Ai|)(|Br| + |Bi|) instead of
+// K u (|Ar||Bi| + |Ai||Br|).  CTA: 8 warps (2 x 4), the same 64 x 64 complex
+// tile; each warp 32 x 16 complex with three accumulators (48 FP64 per
+// thread); one 128-bit shared load gives a thread both parts of its A (or B)
+// fragment element, and the sums Ar + Ai, Br + Bi are formed in registers.
+// At M = N = 16384, K = 256, beta = 1: 40.4 (N-major B) / 41.2 (K-major B)
+// TF/s counted as 8MNK against 32.2 / 32.5 for zgemm_kernel.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -171,6 +185,147 @@ zgemm_kernel(int M, int N, int K, const double2* __restrict__ A, int64_t lda, co
                 int64_t idx = C_COLMAJOR ? (int64_t)gj * ldc + gi : (int64_t)gi * ldc + gj;
                 if (has_beta) {
                     double2 c = C[idx];
+                    v.x += beta.x * c.x - beta.y * c.y;
+                    v.y += beta.x * c.y + beta.y * c.x;
+                }
+                C[idx] = v;
+            }
+    }
+}
+
+
+// ----------------------------------------------------------------- 3M form
+constexpr int M3_WM = 2, M3_WN = 4, M3_NJ = 2;  // warps along M / N, 8-column tiles per warp
+constexpr int M3_THREADS = 32 * M3_WM * M3_WN;
+constexpr int M3_AROW = 2 * BKC + 8;   // doubles: 20 16-byte units, 4 mod 8 (conflict-free 128-bit reads)
+constexpr int M3_BROW_K = 2 * BKC + 8;
+constexpr int M3_BROW_N = 2 * BN + 4;  // 66 16-byte units, 2 mod 8
+constexpr int M3_A_STAGE = BM * M3_AROW;
+constexpr int M3_B_STAGE = BN * M3_BROW_K > BKC * M3_BROW_N ? BN * M3_BROW_K : BKC * M3_BROW_N;
+constexpr int M3_SMEM_BYTES = STAGES * (M3_A_STAGE + M3_B_STAGE) * 8;
+static_assert(32 * M3_WM == BM && 8 * M3_NJ * M3_WN == BN, "3M tile");
+
+template <bool B_KMAJOR, bool C_COLMAJOR>
+__global__ void __launch_bounds__(M3_THREADS, 2)
+zgemm3m_kernel(int M, int N, int K, const double2* __restrict__ A, int64_t lda, const double2* __restrict__ B,
+               int64_t ldb, double2* __restrict__ C, int64_t ldc, double2 alpha, double2 beta, int64_t sA = 0,
+               int64_t sB = 0, int64_t sC = 0) {
+    constexpr int NJ = M3_NJ;
+    A += blockIdx.z * sA;
+    B += blockIdx.z * sB;
+    C += blockIdx.z * sC;
+    extern __shared__ __align__(16) double sm[];
+    double* As = sm;                          // STAGES x M3_A_STAGE
+    double* Bs = sm + STAGES * M3_A_STAGE;    // STAGES x M3_B_STAGE
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp / M3_WN) * 32, wn = (warp % M3_WN) * 8 * NJ;  // warp tile origin (complex)
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nst = (K + BKC - 1) / BKC;
+
+    auto load_stage = [&](int st, int buf) {
+        const int k0 = st * BKC;
+        double* as = As + buf * M3_A_STAGE;
+        double* bs = Bs + buf * M3_B_STAGE;
+        // A and B: 64 rows x 16 complex each = 1024 copies of 16 B, 4 per thread
+#pragma unroll
+        for (int l = 0; l < BM * BKC / M3_THREADS; l++) {
+            const int e = tid + M3_THREADS * l;
+            const int r = e >> 4, kc = e & 15;
+            const int gi = m0 + r, gk = k0 + kc;
+            const bool ok = gi < M && gk < K;
+            cp16(as + r * M3_AROW + 2 * kc, A + (ok ? (int64_t)gi * lda + gk : 0), ok);
+        }
+#pragma unroll
+        for (int l = 0; l < BN * BKC / M3_THREADS; l++) {
+            const int e = tid + M3_THREADS * l;
+            if (B_KMAJOR) {
+                const int j = e >> 4, kc = e & 15;
+                const int gj = n0 + j, gk = k0 + kc;
+                const bool ok = gj < N && gk < K;
+                cp16(bs + j * M3_BROW_K + 2 * kc, B + (ok ? (int64_t)gj * ldb + gk : 0), ok);
+            } else {
+                const int kr = e >> 6, j = e & 63;
+                const int gj = n0 + j, gk = k0 + kr;
+                const bool ok = gj < N && gk < K;
+                cp16(bs + kr * M3_BROW_N + 2 * j, B + (ok ? (int64_t)gk * ldb + gj : 0), ok);
+            }
+        }
+    };
+
+    double t1[4][NJ][2], t2[4][NJ][2], t3[4][NJ][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < NJ; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) t1[i][j][h] = t2[i][j][h] = t3[i][j][h] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < nst) load_stage(s, s);
+        cp_commit();
+    }
+    const int fr = lane >> 2, fk = lane & 3;  // fragment row (A) / column (B), k within the m8n8k4 step
+    for (int st = 0; st < nst; st++) {
+        cp_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            const int nx = st + STAGES - 1;
+            if (nx < nst) load_stage(nx, nx % STAGES);
+            cp_commit();
+        }
+        const int buf = st % STAGES;
+        const double* as = As + buf * M3_A_STAGE;
+        const double* bs = Bs + buf * M3_B_STAGE;
+#pragma unroll
+        for (int kk = 0; kk < BKC / 4; kk++) {  // complex K steps of 4
+            const int kc = 4 * kk + fk;
+            double ar[4], ai[4], asum[4], br[NJ], bi[NJ], bsum[NJ];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const double2 v = *reinterpret_cast<const double2*>(as + (wm + 8 * i + fr) * M3_AROW + 2 * kc);
+                ar[i] = v.x;
+                ai[i] = v.y;
+                asum[i] = v.x + v.y;
+            }
+#pragma unroll
+            for (int j = 0; j < NJ; j++) {
+                const int n = wn + 8 * j + fr;
+                const double2 v = B_KMAJOR ? *reinterpret_cast<const double2*>(bs + n * M3_BROW_K + 2 * kc)
+                                           : *reinterpret_cast<const double2*>(bs + kc * M3_BROW_N + 2 * n);
+                br[j] = v.x;
+                bi[j] = v.y;
+                bsum[j] = v.x + v.y;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < NJ; j++) {
+                    dmma(t1[i][j][0], t1[i][j][1], ar[i], br[j]);
+                    dmma(t2[i][j][0], t2[i][j][1], ai[i], bi[j]);
+                    dmma(t3[i][j][0], t3[i][j][1], asum[i], bsum[j]);
+                }
+        }
+    }
+    cp_wait<0>();
+    // epilogue: thread holds C(row 8i + lane/4, cols 8j + 2(lane%4) + {0,1})
+    const bool has_beta = beta.x != 0.0 || beta.y != 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int gi = m0 + wm + 8 * i + fr;
+        if (gi >= M) continue;
+#pragma unroll
+        for (int j = 0; j < NJ; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int gj = n0 + wn + 8 * j + 2 * fk + h;
+                if (gj >= N) continue;
+                const double ar = t1[i][j][h] - t2[i][j][h];
+                const double ai = t3[i][j][h] - t1[i][j][h] - t2[i][j][h];
+                double2 v = make_double2(alpha.x * ar - alpha.y * ai, alpha.x * ai + alpha.y * ar);
+                const int64_t idx = C_COLMAJOR ? (int64_t)gj * ldc + gi : (int64_t)gi * ldc + gj;
+                if (has_beta) {
+                    const double2 c = C[idx];
                     v.x += beta.x * c.x - beta.y * c.y;
                     v.y += beta.x * c.y + beta.y * c.x;
                 }

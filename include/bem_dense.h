@@ -119,6 +119,11 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * ~6000 -- are factored by one thread-block cluster per matrix, one cluster
  * barrier per column; 0: every sub-panel on the cooperative grid, one grid
  * barrier per column; both give the same pivots and factors),
+ * "fp64_gemm_3m" (1, default: the complex FP64 GEMMs of the pivoted LU, its
+ * solves and the FP64 residual take three real products per complex product,
+ * Re = Ar Br - Ai Bi, Im = (Ar + Ai)(Br + Bi) - Ar Br - Ai Bi, on the FP64
+ * tensor path: 6MNK instead of 8MNK multiply-adds, error normwise at the FP64
+ * unit roundoff; 0: four real products),
  * "gemm_pairs" (1, default: the FP16-part tensor-core GEMM on 256-row tiles
  * of CTA pairs, tcgen05.mma.cta_group::2, each CTA loading half of a tile's
  * B operand; 0: 128-row tiles, one CTA each),

@@ -49,6 +49,50 @@ def test_pivot_sequence_matches_lapack(ctx):
     assert rel(F, lu2) < 1e-12
 
 
+@pytest.mark.parametrize("n", [700, 1500])
+def test_fp64_gemm_3m_against_4m(ctx, n):
+    # the FP64 trailing updates and solves with three real products per
+    # complex one (default) against four: the same pivots (LAPACK's), and
+    # backward errors of the factors and of the solutions within a small
+    # factor of the four-product ones (3M's normwise bound is ~1.3x larger
+    # in a NumPy emulation of this blocked LU; forward errors of random
+    # matrices scatter by several times either way, so they are not compared)
+    import bem_b200 as bb
+    from scipy.linalg import lu_factor
+    A = _rand(n, 40 + n)
+    B = _rand(n, 41 + n)[:, :24]
+    out = {}
+    try:
+        for m3 in (1, 0):
+            bb.set_option(ctx, "fp64_gemm_3m", m3)
+            F, ipiv, info = bb.lu_factorize_cuda(ctx, A)
+            assert info == 0
+            out[m3] = (F, ipiv, bb.lu_solve_cuda(ctx, F, ipiv, B))
+    finally:
+        bb.set_option(ctx, "fp64_gemm_3m", 1)
+    _, piv2 = lu_factor(A)
+    assert np.array_equal(out[1][1], out[0][1])
+    assert np.array_equal(out[1][1] - 1, piv2)
+    nA = np.linalg.norm(A)
+
+    def factor_backward(F, ipiv):
+        PA = A.copy()
+        for i, p in enumerate(ipiv - 1):  # LAPACK row interchanges, in order
+            PA[[i, p]] = PA[[p, i]]
+        L = np.tril(F, -1) + np.eye(n)
+        return np.linalg.norm(PA - L @ np.triu(F)) / nA
+
+    def solve_backward(X):
+        return np.linalg.norm(A @ X - B) / (nA * np.linalg.norm(X))
+
+    f3, f4 = factor_backward(*out[1][:2]), factor_backward(*out[0][:2])
+    s3, s4 = solve_backward(out[1][2]), solve_backward(out[0][2])
+    # (measured: f4 1.2e-14 / 2.5e-14, f3 1.8e-14 / 4.1e-14 at n = 700 / 1500)
+    assert f3 < 1e-16 * n and f3 <= 2 * f4, (f3, f4)
+    assert s3 < 1e-16 * n and s3 <= 2 * s4, (s3, s4)
+    assert rel(out[1][2], np.linalg.solve(A, B)) < 1e-10
+
+
 def test_singular_reports_info(ctx):
     import bem_b200 as bb
     A = _rand(64, 4)
