@@ -19,7 +19,7 @@ struct PanelWS {
     int* status;       // sticky status word (BEM_ERR_TIMEOUT on a failed wait)
 };
 
-// Optional replacement of the CUDA-core GEMM for the big updates
+// Optional replacement of the FP64-path GEMM (cgemm) for the big updates
 // C -= A * B (A: M x K, K contiguous; B: K x N).  fn: B row-major (the U12
 // block of the factor), C row-major.  fn_solve: B and C column-major.
 // Options of the three-product tensor-core GEMM C -= op(A) op(B) (complex64).
