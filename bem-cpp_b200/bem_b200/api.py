@@ -62,7 +62,8 @@ class Context:
     def launches(self) -> int:
         return int(lib().bem_ctx_launch_count(self.h))
 
-    PROF_CLASSES = ("lu_update", "solve_update", "residual", "panel", "assembly", "farfield", "verify")
+    PROF_CLASSES = ("lu_update", "solve_update", "residual", "panel", "assembly", "farfield", "verify", "trsm",
+                    "interchanges", "panel_update")
 
     def profile(self, enable=True):
         self.check(lib().bem_ctx_profile(self.h, int(bool(enable))))

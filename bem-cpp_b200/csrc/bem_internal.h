@@ -169,7 +169,10 @@ enum ProfClass {
     PROF_ASSEMBLY = 4,     // PMCHWT assembly kernel
     PROF_FARFIELD = 5,     // far-field / Mueller kernel
     PROF_VERIFY = 6,       // FP64 residual of the columns checked after the refinement
-    PROF_NCLASS = 7
+    PROF_TRSM = 7,         // triangular solves with a 256-row diagonal block (factorisations and solves)
+    PROF_PIVOT = 8,        // row interchanges and permutations
+    PROF_PANEL_UPDATE = 9, // updates inside a block column (sub-panel GEMMs; L21 of the L D L^T blocks)
+    PROF_NCLASS = 10
 };
 
 struct ProfPending {
@@ -191,6 +194,7 @@ struct bem_ctx {
     bool tc_pair = true;        // FP16-part GEMM on CTA pairs (cta_group::2, 256-row tiles)
     bool tc_pair_attr = false;
     bool dmma_3m = true;        // complex FP64 GEMMs as three real products (Gauss) instead of four
+    bool solve_inv = true;      // L D L^T solves: diagonal blocks by products with their stored inverses
     int tc_split = 1;           // FP32 operand split: 1 = 3xFP16 with power-of-two row / column scales, 0 = 3xTF32
     int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)
     int oz_digits = 7;           // int8 digits of the Ozaki residual (0: FP64 DMMA residual)

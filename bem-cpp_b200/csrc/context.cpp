@@ -305,6 +305,8 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
         ctx->tc_group_m = value;
     } else if (!std::strcmp(name, "persistent_gemm")) {
         ctx->tc_persistent = value != 0;
+    } else if (!std::strcmp(name, "solve_block_inverse")) {
+        ctx->solve_inv = value != 0;
     } else if (!std::strcmp(name, "fp64_gemm_3m")) {
         ctx->dmma_3m = value != 0;
     } else if (!std::strcmp(name, "gemm_pairs")) {

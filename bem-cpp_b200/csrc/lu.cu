@@ -769,6 +769,7 @@ template <typename R> struct TBsel { static constexpr int v = 16; };
 // TRSM_DIVDIAG divides the solution of a unit-lower T by T's diagonal (the D
 // of L D L^T) when it is stored.
 constexpr int TRSM_KB = 256, TRSM_TS = 16, TRSM_PITCH = TRSM_KB + 1;
+static_assert(TRSM_KB == TRSM_BLOCK, "diagonal block rows");
 constexpr int TRSM_TRANS = 1, TRSM_UNIT = 2, TRSM_DIVDIAG = 4;
 
 template <typename C2> __device__ __forceinline__ C2 cdiv(C2 a, C2 d) {
@@ -926,9 +927,13 @@ int trsm_block(bem_ctx* ctx, const typename C2T<R>::type* T, int64_t ldt, int r0
         attr_set.fetch_or(bit);
     }
     const dim3 grid((c1 - c0 + RB - 1) / RB, batch);
+    cudaEvent_t ev = ctx->prof_begin(PROF_TRSM);
     trsm_block_kernel<R, UPPER, B_ROWMAJOR, RB, MODE><<<grid, TRSM_KB, smem, ctx->stream>>>(T, ldt, r0, kb, B, ldb,
                                                                                            br0, c0, c1, sT, sB);
     BEM_LAUNCHED(ctx);
+    if (ev)
+        ctx->prof_end(PROF_TRSM, ev, 4.0 * kb * (double)kb * (c1 - c0) * batch,
+                      (double)sizeof(C2) * ((double)kb * kb / 2 + 2.0 * kb * (c1 - c0)) * batch);
     return BEM_OK;
 }
 
@@ -1014,24 +1019,28 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
             int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
             int ncol = (ca1 - ca0) + (cb1 - cb0);
             if (ncol > 0) {
+                cudaEvent_t ev = ctx->prof_begin(PROF_PIVOT);
                 laswp_kernel<R><<<(ncol + 255) / 256, 256, 0, ctx->stream>>>(A, lda, d_ipiv, i0, i0 + iw,
                                                                           ca0, ca1, cb0, cb1);
                 BEM_LAUNCHED(ctx);
+                if (ev) ctx->prof_end(PROF_PIVOT, ev, 0.0, 4.0 * sizeof(C2) * iw * (double)ncol);
             }
             if (cb1 > cb0) {
                 BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, i0, iw, cb0, cb1));
                 BEM_TRY(cgemm<R>(ctx, n - i0 - iw, cb1 - cb0, iw, A + (int64_t)(i0 + iw) * lda + i0, lda,
                                  A + (int64_t)i0 * lda + cb0, lda, false,
                                  A + (int64_t)(i0 + iw) * lda + cb0, lda, false, mk<C2>(-1, 0),
-                                 mk<C2>(1, 0)));
+                                 mk<C2>(1, 0), PROF_PANEL_UPDATE));
             }
         }
         // interchanges on the columns outside the block column
         int ncol = j0 + (n - j0 - jb);
         if (ncol > 0) {
+            cudaEvent_t ev = ctx->prof_begin(PROF_PIVOT);
             laswp_kernel<R><<<(ncol + 255) / 256, 256, 0, ctx->stream>>>(A, lda, d_ipiv, j0, j0 + jb, 0,
                                                                       j0, j0 + jb, n);
             BEM_LAUNCHED(ctx);
+            if (ev) ctx->prof_end(PROF_PIVOT, ev, 0.0, 4.0 * sizeof(C2) * jb * (double)ncol);
         }
         const int c0 = j0 + jb;
         if (c0 < n) {
@@ -1185,22 +1194,26 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
             const int ca0 = j0, ca1 = i0, cb0 = i0 + iw, cb1 = j0 + jb;
             const int ncol = (ca1 - ca0) + (cb1 - cb0);
             if (ncol > 0) {
+                cudaEvent_t ev = ctx->prof_begin(PROF_PIVOT);
                 laswp_kernel<R><<<dim3((ncol + 255) / 256, batch), 256, 0, ctx->stream>>>(
                     A, lda, d_ipiv, i0, i0 + iw, ca0, ca1, cb0, cb1, sA, n);
                 BEM_LAUNCHED(ctx);
+                if (ev) ctx->prof_end(PROF_PIVOT, ev, 0.0, 4.0 * sizeof(C2) * iw * (double)ncol * batch);
             }
             if (cb1 > cb0) {
                 BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, i0, iw, cb0, cb1, batch, sA));
                 BEM_TRY(cgemm<R>(ctx, n - i0 - iw, cb1 - cb0, iw, A + (int64_t)(i0 + iw) * lda + i0, lda,
                                  A + (int64_t)i0 * lda + cb0, lda, false, A + (int64_t)(i0 + iw) * lda + cb0, lda,
-                                 false, m1, p1, -1, batch, sA, sA, sA));
+                                 false, m1, p1, PROF_PANEL_UPDATE, batch, sA, sA, sA));
             }
         }
         const int ncol = j0 + (n - j0 - jb);
         if (ncol > 0) {
+            cudaEvent_t ev = ctx->prof_begin(PROF_PIVOT);
             laswp_kernel<R><<<dim3((ncol + 255) / 256, batch), 256, 0, ctx->stream>>>(A, lda, d_ipiv, j0, j0 + jb, 0,
                                                                                       j0, j0 + jb, n, sA, n);
             BEM_LAUNCHED(ctx);
+            if (ev) ctx->prof_end(PROF_PIVOT, ev, 0.0, 4.0 * sizeof(C2) * jb * (double)ncol * batch);
         }
         const int c0 = j0 + jb;
         if (c0 < n) {
@@ -1536,7 +1549,22 @@ __global__ void neg_eye_kernel(float2* __restrict__ W, int jb) {
 // inverse factor W = L11^-T D^-1 comes from a block TRSM on -I; the panel
 // below becomes L21 = S21 W in one tensor-core GEMM (in place: the operands
 // are packed before the product is written); then the lower-triangle update.
-int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
+// L[c * 256 + r] = W[c * 256 + r] d_r for r, c < jb (W = -L11^-1 D^-1 of the
+// diagonal block at j0, d_r its pivots), 0 elsewhere: -L11^-1 itself.
+__global__ void linv_from_w_kernel(const float2* __restrict__ W, const float2* __restrict__ A, int64_t lda, int j0,
+                                   int jb, float2* __restrict__ L) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= TRSM_KB * TRSM_KB) return;
+    const int c = t / TRSM_KB, r = t % TRSM_KB;
+    float2 v = make_float2(0.f, 0.f);
+    if (r < jb && c < jb) {
+        const float2 w = W[t], d = A[(int64_t)(j0 + r) * lda + j0 + r];
+        v = make_float2(w.x * d.x - w.y * d.y, w.x * d.y + w.y * d.x);
+    }
+    L[t] = v;
+}
+
+int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info, float2* Linv) {
     using C2 = float2;
     const int NB = TRSM_KB;
     const size_t smem = ldlt_smem_bytes(sizeof(C2));
@@ -1555,26 +1583,33 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info) {
     // the diagonal block at j0 and its panel below: L D L^T of the block,
     // then L21 = S21 L11^-T D^-1 for the rows [j0 + jb, n)
     auto factor_block = [&](int j0, int jb) -> int {
+        const int below = n - j0 - jb;
         cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
         ldlt_diag_kernel<float><<<1, 1024, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
         BEM_LAUNCHED(ctx);
-        const int below = n - j0 - jb;
-        if (below > 0) {
+        if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3, 16.0 * (double)jb * jb);
+        if (below > 0 || Linv) {
             // column c of W.p solves L11 x = -e_c, then x_r /= d_r:
             // W.p[c * 256 + r] = -L11^-1[r][c] / d_r
             neg_eye_kernel<<<(jb * NB + 255) / 256, 256, 0, ctx->stream>>>(W.p, jb);
             BEM_LAUNCHED(ctx);
             BEM_TRY((trsm_block<float, false, false, TRSM_DIVDIAG>(ctx, A, lda, j0, jb, W.p, NB, 0, jb, 0)));
+        }
+        if (Linv) {
+            linv_from_w_kernel<<<NB * NB / 256, 256, 0, ctx->stream>>>(W.p, A, lda, j0, jb,
+                                                                     Linv + (size_t)(j0 / NB) * NB * NB);
+            BEM_LAUNCHED(ctx);
+        }
+        if (below > 0) {
             // L21 = S21 L11^-T D^-1: B given row-major (K x N) is
             // B[k][j] = W.p[k * 256 + j] = -(L11^-T D^-1)[k][j]; the store mode writes C = -A B
             TcOpts o;
             o.b_rowmajor = true;
             o.store = true;
+            o.prof_cls = PROF_PANEL_UPDATE;
             float2* S21 = A + (int64_t)(j0 + jb) * lda + j0;
             BEM_TRY(tc_gemm_ex(ctx, below, jb, jb, S21, lda, W.p, NB, S21, lda, o));
         }
-        if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3 + 8.0 * below * (double)jb * jb / 2,
-                              8.0 * (double)(jb + below) * jb * 2);
         return (int)BEM_OK;
     };
     // Super-blocks of two 256-column blocks: block 1 is factored and updates
@@ -1623,7 +1658,7 @@ __global__ void diag_div_kernel(const float2* __restrict__ A, int64_t lda, float
 
 // X = S^-1 B with S = L D L^T (B, X column-major complex64; X may alias B).
 int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2* B, int64_t ldb, float2* X,
-                int64_t ldx, int nrhs) {
+                int64_t ldx, int nrhs, const float2* Linv, float2* tmp) {
     const int NB = TRSM_KB;
     if (nrhs <= 0) return BEM_OK;
     int64_t tot = (int64_t)n * nrhs;
@@ -1644,13 +1679,31 @@ int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2*
         o.prof_cls = PROF_SOLVE_UPDATE;
         return tc_gemm_ex(ctx, M, nrhs, K, Ablk, lda, Bx, ldx, Cx, ldx, o);
     };
+    // the diagonal block at J0 (jb rows): X_blk = L11^-1 X_blk (back: L11^-T),
+    // as -(-L11^-1) tmp with tmp a copy of X_blk, or a block triangular solve
+    auto diag = [&](int J0, int jb, bool back) -> int {
+        if (!Linv || !tmp) {
+            if (back)
+                return trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, J0, jb, X, ldx, 0, nrhs);
+            return trsm_block<float, false, false>(ctx, A, lda, J0, jb, X, ldx, 0, nrhs);
+        }
+        BEM_TRY_CUDA(ctx, cudaMemcpy2DAsync(tmp, NB * sizeof(float2), X + J0, ldx * sizeof(float2),
+                                            jb * sizeof(float2), nrhs, cudaMemcpyDeviceToDevice, ctx->stream));
+        TcOpts o;
+        o.c_colmajor = true;
+        o.store = true;
+        o.a_trans = !back;  // forward: A[r][c] = Li[c * 256 + r]; back: A[r][c] = Li[r * 256 + c]
+        o.prof_cls = PROF_TRSM;
+        const float2* Li = Linv + (size_t)(J0 / NB) * NB * NB;
+        return tc_gemm_ex(ctx, jb, nrhs, jb, Li, NB, tmp, NB, X + J0, ldx, o);
+    };
     // L z = b
     for (int J0 = 0; J0 < n; J0 += SB) {
         const int JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
-        BEM_TRY((trsm_block<float, false, false>(ctx, A, lda, J0, jb1, X, ldx, 0, nrhs)));
+        BEM_TRY(diag(J0, jb1, false));
         if (jb2 > 0) {
             BEM_TRY(update(jb2, jb1, A + (int64_t)(J0 + jb1) * lda + J0, false, X + J0, X + J0 + jb1));
-            BEM_TRY((trsm_block<float, false, false>(ctx, A, lda, J0 + jb1, jb2, X, ldx, 0, nrhs)));
+            BEM_TRY(diag(J0 + jb1, jb2, false));
         }
         const int below = n - J0 - JB;
         if (below > 0) BEM_TRY(update(below, JB, A + (int64_t)(J0 + JB) * lda + J0, false, X + J0, X + J0 + JB));
@@ -1663,12 +1716,11 @@ int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2*
     for (int bi = nsb - 1; bi >= 0; bi--) {
         const int J0 = bi * SB, JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
         if (jb2 > 0) {
-            BEM_TRY((trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, J0 + jb1, jb2, X, ldx, 0,
-                                                                           nrhs)));
+            BEM_TRY(diag(J0 + jb1, jb2, true));
             // X[J0:J0+jb1] -= (L[J0+jb1:J0+JB, J0:J0+jb1])^T X[J0+jb1:J0+JB]
             BEM_TRY(update(jb1, jb2, A + (int64_t)(J0 + jb1) * lda + J0, true, X + J0 + jb1, X + J0));
         }
-        BEM_TRY((trsm_block<float, true, false, TRSM_TRANS | TRSM_UNIT>(ctx, A, lda, J0, jb1, X, ldx, 0, nrhs)));
+        BEM_TRY(diag(J0, jb1, true));
         // X[0:J0] -= (L[J0:J0+JB, 0:J0])^T X[J0:J0+JB]
         if (J0 > 0) BEM_TRY(update(J0, JB, A + (int64_t)J0 * lda, true, X + J0, X));
     }

@@ -67,9 +67,15 @@ void pivots_to_perm(const std::vector<int>& ipiv, std::vector<int>& perm);
 // Complex-symmetric S = L D L^T without pivoting (complex64, lower triangle,
 // tensor-core updates) and its multi-RHS solve.
 int sym_structure(bem_ctx* ctx, const double2* Z, int64_t ldz, int n, bool* sym, bool* sym_half);
-int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info);
+constexpr int TRSM_BLOCK = 256;  // rows of the diagonal blocks of the blocked factorisations and solves
+// Linv (optional, ceil(n / 256) blocks of 256 x 256): the factorisation
+// also stores -L11^-1 of every 256-row diagonal block b at Linv + b 256^2,
+// element (r, c) at [c * 256 + r]; the solve then applies the diagonal
+// blocks as tensor-core products with these inverses (tmp: 256 x nrhs
+// complex64 scratch) instead of block triangular solves.
+int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info, float2* Linv = nullptr);
 int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2* B, int64_t ldb, float2* X,
-                int64_t ldx, int nrhs);
+                int64_t ldx, int nrhs, const float2* Linv = nullptr, float2* tmp = nullptr);
 
 // Factorisation without the int8 digit planes of Z (residual_digits false:
 // a factorisation used only as a preconditioner), its order, and one

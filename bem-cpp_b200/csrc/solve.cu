@@ -28,6 +28,10 @@ struct bem_lu {
     double t_factor_ms = 0.0;
     bool ldlt = false;      // FP32 factors are L D L^T of Z diag(s) (no pivoting)
     bool dhalf = false;     // s = (I, -I) (else s = 1)
+    float2* Linv = nullptr; // L D L^T: -L11^-1 of every 256-row diagonal block (owned; null: block TRSMs)
+    size_t linv_bytes = 0;
+    float2* stmp = nullptr; // 256 x nrhs scratch of the solves with Linv (owned)
+    size_t stmp_bytes = 0;
     bem::OzakiZ oz;         // int8 digit planes of Z for the refinement residual (oz.A null: FP64 GEMM)
 };
 
@@ -155,7 +159,20 @@ __global__ void negate_rows_kernel(float2* __restrict__ X, int64_t ldx, int r0, 
 static int solve32(bem_ctx* ctx, bem_lu* lu, const float2* S, float2* D, int nrhs, const TrailingUpdate<float>* tc) {
     const int n = lu->n;
     if (!lu->ldlt) return getrs<float>(ctx, lu->A32, n, n, lu->d_perm, S, n, D, n, nrhs, tc);
-    BEM_TRY(sytrs_nopiv(ctx, lu->A32, n, n, S, n, D, n, nrhs));
+    if (lu->Linv) {
+        const size_t need = (size_t)TRSM_BLOCK * nrhs * sizeof(float2);
+        if (need > lu->stmp_bytes) {
+            if (lu->stmp) {
+                BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+                cudaFree(lu->stmp);
+            }
+            lu->stmp = nullptr;
+            lu->stmp_bytes = 0;
+            BEM_TRY_CUDA(ctx, cudaMalloc(&lu->stmp, need));
+            lu->stmp_bytes = need;
+        }
+    }
+    BEM_TRY(sytrs_nopiv(ctx, lu->A32, n, n, S, n, D, n, nrhs, lu->Linv, lu->stmp));
     if (lu->dhalf) {
         const int64_t tot = (int64_t)(n - n / 2) * nrhs;
         negate_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(D, n, n / 2, n, nrhs);
@@ -247,6 +264,8 @@ static void lu_release(bem_lu* lu) {
     if (!lu) return;
     cudaSetDevice(lu->device);
     if (lu->A32) bem::devmem_free(lu->device, lu->A32, (size_t)lu->n * lu->n * sizeof(float2), lu->ctx);
+    if (lu->Linv) bem::devmem_free(lu->device, lu->Linv, lu->linv_bytes, lu->ctx);
+    if (lu->stmp) cudaFree(lu->stmp);
     if (lu->d_ipiv) cudaFree(lu->d_ipiv);
     if (lu->d_perm) cudaFree(lu->d_perm);
     bem::ozaki_free(&lu->oz);
@@ -325,7 +344,13 @@ int lu_factor_ex(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bool 
                 ozaki_prepare_z(ctx, &lu->oz, lu->Z, ldz, n, ctx->oz_digits) != BEM_OK)
                 ozaki_free(&lu->oz);
             if (lu->ldlt) {
-                s = sytrf_nopiv(ctx, lu->A32, n, n, d_info);
+                if (ctx->solve_inv) {
+                    // inverses of the diagonal blocks for the solves (without
+                    // room for them the solves keep block triangular solves)
+                    lu->linv_bytes = (size_t)((n + TRSM_BLOCK - 1) / TRSM_BLOCK) * TRSM_BLOCK * TRSM_BLOCK * sizeof(float2);
+                    lu->Linv = (float2*)devmem_alloc(ctx->device, lu->linv_bytes, ctx);
+                }
+                s = sytrf_nopiv(ctx, lu->A32, n, n, d_info, lu->Linv);
                 if (s != BEM_OK) break;
                 int h[2] = {0, 0};
                 if (cudaMemcpyAsync(&h[0], d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
@@ -347,6 +372,8 @@ int lu_factor_ex(bem_ctx* ctx, void* Z, int n, int64_t ldz, int precision, bool 
                 }
                 // a zero pivot without pivoting: partial pivoting instead
                 lu->ldlt = lu->dhalf = false;
+                if (lu->Linv) devmem_free(ctx->device, lu->Linv, lu->linv_bytes, ctx);
+                lu->Linv = nullptr;
             }
             s = factor_lu32(ctx, lu, d_info, fro, info);
             break;
@@ -601,6 +628,8 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
             return fail(ctx, BEM_ERR_OOM, "lu workspace");
         }
         lu->ldlt = lu->dhalf = false;
+        if (lu->Linv) devmem_free(ctx->device, lu->Linv, lu->linv_bytes, ctx);
+        lu->Linv = nullptr;
         auto tf = std::chrono::steady_clock::now();
         int info = 0;
         int fs = factor_lu32(ctx, lu, d_info, fro, &info);

@@ -67,7 +67,11 @@ int64_t bem_ctx_launch_count(const bem_ctx* ctx);
  * starts recording, 0 stops.  Classes: 0 LU trailing update, 1 triangular
  * solve block updates, 2 FP64 refinement residual, 3 panel factorisation,
  * 4 assembly, 5 far field / Mueller, 6 the FP64 residual of the columns
- * checked after the refinement.  flops / bytes are the algorithmic
+ * checked after the refinement, 7 triangular solves with a diagonal block,
+ * 8 row interchanges and permutations, 9 updates inside a block column (the
+ * pivoted LU's sub-panel GEMMs, L21 of the L D L^T diagonal blocks); class 3
+ * is then the panel kernels and the L D L^T diagonal blocks alone.  flops /
+ * bytes are the algorithmic
  * counts of the recorded launches (complex GEMM: 8 M N K flop). */
 int bem_ctx_profile(bem_ctx* ctx, int enable);
 /* FP32 factorisation / solve updates on the tensor cores (three tcgen05
@@ -124,6 +128,11 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * Re = Ar Br - Ai Bi, Im = (Ar + Ai)(Br + Bi) - Ar Br - Ai Bi, on the FP64
  * tensor path: 6MNK instead of 8MNK multiply-adds, error normwise at the FP64
  * unit roundoff; 0: four real products),
+ * "solve_block_inverse" (1, default: the FP32 L D L^T factorisation also
+ * keeps -L11^-1 of each 256-row diagonal block (n^2 / 256 complex64, 8 n^2 /
+ * 256 bytes), and its solves apply the diagonal blocks as tensor-core
+ * products with them; 0, or without memory for them: block triangular
+ * solves; set before the factorisation),
  * "gemm_pairs" (1, default: the FP16-part tensor-core GEMM on 256-row tiles
  * of CTA pairs, tcgen05.mma.cta_group::2, each CTA loading half of a tile's
  * B operand; 0: 128-row tiles, one CTA each),

@@ -79,6 +79,39 @@ def test_pmchwt_ldlt_matches_fp64(ctx, pmchwt):
     assert st1["update_hist"][0] < 20 * st0["update_hist"][0]
 
 
+@pytest.mark.parametrize("case", ["pmchwt", 300, 700])
+def test_block_inverse_solves_match_triangular_solves(ctx, pmchwt, case):
+    # solve_block_inverse (default): the diagonal blocks of the L D L^T solves
+    # as tensor-core products with the stored -L11^-1; 0: block triangular
+    # solves.  Both converge to the FP64 solution and precondition alike
+    # (ragged last blocks for n = 300, 700)
+    import scipy.linalg as sl
+    import bem_b200 as bb
+    if case == "pmchwt":
+        Z, B = pmchwt
+        sym = 1
+    else:
+        rng = np.random.default_rng(case)
+        A = _cplx(rng, case, case)
+        Z = A + A.T + 4 * np.sqrt(case) * np.eye(case)
+        B = _cplx(rng, case, 9)
+        sym = 1
+    Xr = sl.lu_solve(sl.lu_factor(Z), B)
+    out = {}
+    try:
+        for inv in (1, 0):
+            bb.set_option(ctx, "solve_block_inverse", inv)
+            out[inv] = _solve(ctx, Z, B, sym=sym)
+    finally:
+        bb.set_option(ctx, "solve_block_inverse", 1)
+    for X, st in out.values():
+        assert st["factorization"] in (1, 2) and st["converged"]
+        err = np.linalg.norm(X - Xr, axis=0) / np.linalg.norm(Xr, axis=0)
+        assert err.max() < 1e-10
+    u1, u0 = out[1][1]["update_hist"][0], out[0][1]["update_hist"][0]
+    assert u1 < 3 * u0, (u1, u0)
+
+
 @pytest.mark.parametrize("n", [1, 7, 256, 300, 700])
 def test_symmetric_random_uses_ldlt(ctx, n):
     rng = np.random.default_rng(n)
