@@ -453,8 +453,11 @@ __global__ void slice_rows_kernel(const double2* __restrict__ Z, int64_t ldz, in
 }
 
 // B digit planes: B[t][2j + p][k'] for X' rows (Re, -Im) / (Im, Re).
+// fix (optional): the value the S digits represent, x~ = 2^ex sum_s q_s
+// 128^-(s+1) (exact in FP64 for S <= 7: 49 bits), replaces x there (src.X)
+// or corrects it (src.D: fix += x~ - x).
 __global__ void slice_cols_kernel(ColSrc src, int n, int nrhs, const int* __restrict__ f, int8_t* __restrict__ B,
-                                  int64_t ldk, int64_t plane, int S) {
+                                  int64_t ldk, int64_t plane, int S, double2* __restrict__ fix, int64_t ldfix) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t kc = ldk / 2;
     if (t >= (int64_t)nrhs * kc) return;
@@ -465,6 +468,23 @@ __global__ void slice_cols_kernel(ColSrc src, int n, int nrhs, const int* __rest
     const double sc = pow2i(-ex);
     digits(x.x * sc, qr);
     digits(x.y * sc, qi);
+    if (fix && k < n) {
+        double rr = 0.0, ri = 0.0;
+        for (int s = S - 1; s >= 0; s--) {  // Horner in base 128: exact
+            rr = (rr + (double)qr[s]) * (1.0 / 128.0);
+            ri = (ri + (double)qi[s]) * (1.0 / 128.0);
+        }
+        const double up = pow2i(ex);
+        rr *= up;
+        ri *= up;
+        double2* p = fix + (int64_t)j * ldfix + k;
+        if (src.X) {
+            *p = make_double2(rr, ri);
+        } else {
+            const double2 v = *p;
+            *p = make_double2(v.x + (rr - x.x), v.y + (ri - x.y));
+        }
+    }
     for (int s = 0; s < S; s++) {
         char2 r0, r1;
         r0.x = qr[s];
@@ -536,13 +556,18 @@ void ozaki_free(OzakiZ* oz_) {
     oz_->e = nullptr;
 }
 
-// R -= Z X with the first S digits of Z and of X (S <= the digits of Z).
-static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2* R, int64_t ldr, int nrhs, int S) {
+// R -= Z X with the first S digits of Z and the first Sx <= S of X (S <= the
+// digits of Z): the digit pairs s + t <= S - 1 (0-based) with t < Sx.  fix:
+// see slice_cols_kernel.
+static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2* R, int64_t ldr, int nrhs, int S,
+                       int Sx, double2* fix, int64_t ldfix) {
     const int n = oz_->n;
     if (S < 2 || S > oz_->S) return fail(ctx, BEM_ERR_INVALID, "ozaki residual: %d digits of %d", S, oz_->S);
+    if (Sx < 1 || Sx > S || (fix && Sx > 7))
+        return fail(ctx, BEM_ERR_INVALID, "ozaki residual: %d digits of X for %d of Z", Sx, S);
     const int64_t ldk = oz_->ldk;
     const int64_t bplane = (int64_t)2 * nrhs * ldk;
-    size_t need = (size_t)S * bplane + (size_t)nrhs * sizeof(int) + 512;
+    size_t need = (size_t)Sx * bplane + (size_t)nrhs * sizeof(int) + 512;
     if (need > ctx->oz_bytes) {
         if (ctx->oz_buf) {
             BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -558,17 +583,17 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
         ctx->oz_bytes = need;
     }
     int8_t* Bd = (int8_t*)ctx->oz_buf;
-    int* f = (int*)((char*)ctx->oz_buf + (((size_t)S * bplane + 255) & ~(size_t)255));
+    int* f = (int*)((char*)ctx->oz_buf + (((size_t)Sx * bplane + 255) & ~(size_t)255));
     cudaEvent_t ev = ctx->prof_begin(PROF_RESIDUAL);
     oz::col_exp_kernel<<<nrhs, 256, 0, ctx->stream>>>(src, n, f);
     BEM_LAUNCHED(ctx);
     int64_t tot = (int64_t)nrhs * (ldk / 2);
     oz::slice_cols_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(src, n, nrhs, f, Bd, ldk, bplane,
-                                                                                  S);
+                                                                                  Sx, fix, ldfix);
     BEM_LAUNCHED(ctx);
     CUtensorMap tA, tB;
     BEM_TRY(encode_i8(ctx, &tA, oz_->A, (int64_t)oz_->S * n, ldk, oz::BM));
-    BEM_TRY(encode_i8(ctx, &tB, Bd, (int64_t)S * 2 * nrhs, ldk, oz::BN));
+    BEM_TRY(encode_i8(ctx, &tB, Bd, (int64_t)Sx * 2 * nrhs, ldk, oz::BN));
     // digit pairs s + t <= S + 1 (1-based), grouped by d = s + t, <= MAXP per group
     // int32 safety: maxp pairs of |q q| <= 2^12 over ldk terms stay below 2^31
     const int maxp = (int)std::min<int64_t>(oz::MAXP, ((int64_t)1 << 31) / ((int64_t)4096 * ldk + 1));
@@ -579,7 +604,7 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
         cur.d = d;
         for (int s = 1; s < d; s++) {
             int t = d - s;
-            if (s > S || t > S) continue;
+            if (s > S || t > Sx) continue;
             cur.s[cur.np] = s - 1;
             cur.t[cur.np] = t - 1;
             if (++cur.np == maxp) {
@@ -608,7 +633,7 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
         int pairs = 0;
         for (int i = 0; i < G.ng; i++) pairs += G.g[i].np;
         double ops = (double)pairs * 2.0 * n * (2.0 * nrhs) * (2.0 * n);
-        double bytes = (double)S * n * 2.0 * n + (double)S * 2.0 * nrhs * 2.0 * n + 32.0 * n * (double)nrhs;
+        double bytes = (double)S * n * 2.0 * n + (double)Sx * 2.0 * nrhs * 2.0 * n + 32.0 * n * (double)nrhs;
         ctx->prof_end(PROF_RESIDUAL, ev, ops, bytes);
     }
     return BEM_OK;
@@ -616,9 +641,10 @@ static int ozaki_apply(bem_ctx* ctx, const OzakiZ* oz_, oz::ColSrc src, double2*
 
 // R -= Z X (R already holds B).  X, R: column-major n x nrhs complex128.
 int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ldx, double2* R, int64_t ldr,
-                   int nrhs) {
+                   int nrhs, int x_digits, double2* round_x) {
     oz::ColSrc src{X, nullptr, nullptr, ldx};
-    return ozaki_apply(ctx, oz_, src, R, ldr, nrhs, oz_->S);
+    const bool rnd = x_digits > 0 && x_digits < oz_->S && round_x == X;
+    return ozaki_apply(ctx, oz_, src, R, ldr, nrhs, oz_->S, rnd ? x_digits : oz_->S, rnd ? round_x : nullptr, ldx);
 }
 
 // R -= Z (scale D): the residual of the next refinement iterate from the
@@ -626,9 +652,10 @@ int ozaki_residual(bem_ctx* ctx, const OzakiZ* oz_, const double2* X, int64_t ld
 // (it is small against the iterate, so fewer digits reach the same absolute
 // accuracy).
 int ozaki_residual_update(bem_ctx* ctx, const OzakiZ* oz_, const float2* D, int64_t ldd, const double* scale,
-                          double2* R, int64_t ldr, int nrhs, int digits) {
+                          double2* R, int64_t ldr, int nrhs, int digits, int d_digits, double2* fix_x, int64_t ldfix) {
     oz::ColSrc src{nullptr, D, scale, ldd};
-    return ozaki_apply(ctx, oz_, src, R, ldr, nrhs, digits);
+    const bool rnd = d_digits > 0 && d_digits < digits && fix_x;
+    return ozaki_apply(ctx, oz_, src, R, ldr, nrhs, digits, rnd ? d_digits : digits, rnd ? fix_x : nullptr, ldfix);
 }
 
 }  // namespace bem

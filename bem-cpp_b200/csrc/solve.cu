@@ -530,11 +530,17 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
         if (!exact && it > 1 && prev_upd < 0.5 && !fresh) {
             const double lg = prev_upd > 0 ? -std::log2(prev_upd) + 1.0 : 1e9;
             const int digits = std::min(lu->oz.S, std::max(2, lu->oz.S - (int)std::min(64.0, std::floor(lg / 7.0))));
-            rs = ozaki_residual_update(ctx, &lu->oz, D, n, scale, R, n, nrhs, digits);
+            // the correction keeps oz_xdigits digits: X, which already holds
+            // x + d, becomes x + (d rounded), for which the update is exact
+            rs = ozaki_residual_update(ctx, &lu->oz, D, n, scale, R, n, nrhs, digits, ctx->oz_xdigits, X, ldx);
         } else if (!exact) {
             copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, R, n, n, nrhs);
             BEM_LAUNCHED(ctx);
-            rs = ozaki_residual(ctx, &lu->oz, X, ldx, R, n, nrhs);
+            // the first iterate (the FP32 solve's, ~1e-4 relative accuracy) is
+            // rounded to oz_xdigits digits (2^-21 of its column's largest entry
+            // for 3) and kept so: its residual needs only the digit pairs of
+            // those digits, and is exact for it up to Z's digit truncation
+            rs = ozaki_residual(ctx, &lu->oz, X, ldx, R, n, nrhs, it == 1 ? ctx->oz_xdigits : 0, it == 1 ? X : nullptr);
         }
         fresh = false;
         if (rs == BEM_ERR_OOM) {

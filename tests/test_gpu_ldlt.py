@@ -112,6 +112,31 @@ def test_block_inverse_solves_match_triangular_solves(ctx, pmchwt, case):
     assert u1 < 3 * u0, (u1, u0)
 
 
+@pytest.mark.parametrize("xd", [3, 2])
+def test_rounded_iterates_keep_the_fp64_solution(ctx, pmchwt, xd):
+    # residual_x_digits (default 3): the first iterate and the corrections are
+    # rounded to their first digits and kept so; the int8 residual then needs
+    # fewer digit pairs and is exact for the rounded iterate, so the refined
+    # solution is the FP64 one as with every digit (0)
+    import scipy.linalg as sl
+    import bem_b200 as bb
+    Z, B = pmchwt
+    Xr = sl.lu_solve(sl.lu_factor(Z), B)
+    out = {}
+    try:
+        for d in (xd, 0):
+            bb.set_option(ctx, "residual_x_digits", d)
+            out[d] = _solve(ctx, Z, B, tol=2e-10)
+    finally:
+        bb.set_option(ctx, "residual_x_digits", 3)
+    for X, st in out.values():
+        assert st["converged"]
+        err = np.linalg.norm(X - Xr, axis=0) / np.linalg.norm(Xr, axis=0)
+        assert err.max() < 1e-10
+        assert st["verified_rel_error"] < 1e-9
+    assert out[xd][1]["iterations"] <= out[0][1]["iterations"] + 1
+
+
 @pytest.mark.parametrize("n", [1, 7, 256, 300, 700])
 def test_symmetric_random_uses_ldlt(ctx, n):
     rng = np.random.default_rng(n)
