@@ -198,7 +198,7 @@ struct bem_ctx {
     int tc_split = 1;           // FP32 operand split: 1 = 3xFP16 with power-of-two row / column scales, 0 = 3xTF32
     int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)
     int oz_digits = 7;           // int8 digits of the Ozaki residual (0: FP64 DMMA residual)
-    int oz_xdigits = 3;          // digits the refinement keeps of its first iterate and of its corrections (0: all)
+    int oz_xdigits = 2;          // digits the refinement keeps of its first iterate and of its corrections (0: all)
     void* oz_buf = nullptr;      // digit planes of X for the residual
     size_t oz_bytes = 0;
     bool oz_attr = false;

@@ -164,11 +164,12 @@ static int solve32(bem_ctx* ctx, bem_lu* lu, const float2* S, float2* D, int nrh
         if (need > lu->stmp_bytes) {
             if (lu->stmp) {
                 BEM_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-                cudaFree(lu->stmp);
+                devmem_free(ctx->device, lu->stmp, lu->stmp_bytes, ctx);
             }
             lu->stmp = nullptr;
             lu->stmp_bytes = 0;
-            BEM_TRY_CUDA(ctx, cudaMalloc(&lu->stmp, need));
+            lu->stmp = (float2*)devmem_alloc(ctx->device, need, ctx);
+            if (!lu->stmp) return fail(ctx, BEM_ERR_OOM, "solve scratch (%zu bytes)", need);
             lu->stmp_bytes = need;
         }
     }
@@ -265,7 +266,7 @@ static void lu_release(bem_lu* lu) {
     cudaSetDevice(lu->device);
     if (lu->A32) bem::devmem_free(lu->device, lu->A32, (size_t)lu->n * lu->n * sizeof(float2), lu->ctx);
     if (lu->Linv) bem::devmem_free(lu->device, lu->Linv, lu->linv_bytes, lu->ctx);
-    if (lu->stmp) cudaFree(lu->stmp);
+    if (lu->stmp) bem::devmem_free(lu->device, lu->stmp, lu->stmp_bytes, lu->ctx);
     if (lu->d_ipiv) cudaFree(lu->d_ipiv);
     if (lu->d_perm) cudaFree(lu->d_perm);
     bem::ozaki_free(&lu->oz);
@@ -537,8 +538,8 @@ int lu_solve(bem_ctx* ctx, bem_lu* lu, const void* Bv, int64_t ldb, void* Xv, in
             copy_cols_kernel<<<nblk(nn), 256, 0, ctx->stream>>>(B, ldb, R, n, n, nrhs);
             BEM_LAUNCHED(ctx);
             // the first iterate (the FP32 solve's, ~1e-4 relative accuracy) is
-            // rounded to oz_xdigits digits (2^-21 of its column's largest entry
-            // for 3) and kept so: its residual needs only the digit pairs of
+            // rounded to oz_xdigits digits (2^-14 of its column's largest entry
+            // for 2) and kept so: its residual needs only the digit pairs of
             // those digits, and is exact for it up to Z's digit truncation
             rs = ozaki_residual(ctx, &lu->oz, X, ldx, R, n, nrhs, it == 1 ? ctx->oz_xdigits : 0, it == 1 ? X : nullptr);
         }

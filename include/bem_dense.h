@@ -128,13 +128,15 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * Re = Ar Br - Ai Bi, Im = (Ar + Ai)(Br + Bi) - Ar Br - Ai Bi, on the FP64
  * tensor path: 6MNK instead of 8MNK multiply-adds, error normwise at the FP64
  * unit roundoff; 0: four real products),
- * "residual_x_digits" (3, default: the refinement rounds its first iterate
+ * "residual_x_digits" (2, default: the refinement rounds its first iterate
  * (the FP32 solve's) and each correction it sums with the int8 residual's
- * update form to their first 3 digits of 7 bits below their column's
+ * update form to their first 2 digits of 7 bits below their column's
  * largest entry, and keeps the rounded values, so the int8 residual needs
- * only the digit pairs of those digits -- 18 instead of 28 for the first
- * residual, 12 instead of 15 for a 5-digit update -- and stays exact for the
- * iterate it belongs to; 0: every digit, 1..7: that many),
+ * only the digit pairs of those digits -- 13 instead of 28 for the first
+ * residual, 11 instead of 21 for a 6-digit update -- and stays exact for the
+ * iterate it belongs to; the rounding, 2^-14 of the column's largest entry,
+ * is below the FP32 solve's own error and the next sweep removes it; 0:
+ * every digit, 1..7: that many),
  * "solve_block_inverse" (1, default: the FP32 L D L^T factorisation also
  * keeps -L11^-1 of each 256-row diagonal block (n^2 / 256 complex64, 8 n^2 /
  * 256 bytes), and its solves apply the diagonal blocks as tensor-core

@@ -114,7 +114,7 @@ def test_block_inverse_solves_match_triangular_solves(ctx, pmchwt, case):
 
 @pytest.mark.parametrize("xd", [3, 2])
 def test_rounded_iterates_keep_the_fp64_solution(ctx, pmchwt, xd):
-    # residual_x_digits (default 3): the first iterate and the corrections are
+    # residual_x_digits (default 2): the first iterate and the corrections are
     # rounded to their first digits and kept so; the int8 residual then needs
     # fewer digit pairs and is exact for the rounded iterate, so the refined
     # solution is the FP64 one as with every digit (0)
@@ -128,7 +128,7 @@ def test_rounded_iterates_keep_the_fp64_solution(ctx, pmchwt, xd):
             bb.set_option(ctx, "residual_x_digits", d)
             out[d] = _solve(ctx, Z, B, tol=2e-10)
     finally:
-        bb.set_option(ctx, "residual_x_digits", 3)
+        bb.set_option(ctx, "residual_x_digits", 2)
     for X, st in out.values():
         assert st["converged"]
         err = np.linalg.norm(X - Xr, axis=0) / np.linalg.norm(Xr, axis=0)
