@@ -1388,74 +1388,86 @@ __global__ void sym_check_kernel(const double2* __restrict__ Z, int64_t ldz, int
 
 // Factors the jb x jb diagonal block at (j0, j0) in place: the strict lower
 // triangle receives L, the diagonal D (the upper triangle is not touched).
-// One CTA of 1024 threads; 32-column sub-panels of the block's rows are
-// eliminated column by column in shared memory, then the rest of the block's
-// lower triangle is updated with them: T = D L^T of the sub-panel is formed
-// once in shared memory, and each thread accumulates a 4 x 4 set of outputs
-// of a 128 x 128 block (rows ty + 32 r, columns tx + 32 c), so that the 32
-// threads of a warp read one L entry by broadcast and 32 consecutive T
-// entries per k.  *info: first zero pivot (1-based).
-constexpr int LDLT_SP = 32, LDLT_PITCH = LDLT_SP + 1, LDLT_TP = 256;
+// One CTA of 256 threads, thread i owning row i of the block.  The block is
+// taken in 32-column sub-panels: each thread keeps its row's 32 sub-panel
+// entries in registers and the columns are eliminated one at a time, with
+// one block barrier per column (the pivot and the unscaled pivot column are
+// published in shared memory, double-buffered by column parity); every row
+// then scales by the pivot's reciprocal and applies the rank-1 update to
+// its own registers.  The rest of the block's lower triangle is updated
+// with the sub-panel: T = D L^T of the sub-panel is formed once in shared
+// memory, and each thread accumulates an 8 x 4 set of outputs of a
+// 128 x 64 block (rows ty + 16 r, columns tx + 16 c).  *info: first zero
+// pivot (1-based).
+constexpr int LDLT_SP = 32, LDLT_PITCH = LDLT_SP + 1, LDLT_TP = 256, LDLT_THREADS = 256;
 constexpr size_t ldlt_smem_bytes(size_t esz) {
     return ((size_t)256 * LDLT_PITCH + (size_t)LDLT_SP * LDLT_TP) * esz;
 }
 
 template <typename R>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(LDLT_THREADS, 1)
 ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int jb, int* __restrict__ info) {
     using C2 = typename C2T<R>::type;
     extern __shared__ __align__(16) unsigned char ldlt_smem[];
-    C2* P = reinterpret_cast<C2*>(ldlt_smem);  // [jb][LDLT_PITCH]: rows c0.. of the block, sub-panel columns
-    const int tid = threadIdx.x, nth = blockDim.x;
+    C2* P = reinterpret_cast<C2*>(ldlt_smem);  // [jb][LDLT_PITCH]: the eliminated sub-panel, rows c0..
+    __shared__ C2 s_piv[2];                    // the pivot d of the column, by column parity
+    __shared__ C2 s_col[2][LDLT_SP];           // unscaled column entries a[c][jj] of the sub-panel rows
+    const int tid = threadIdx.x;
     C2 zero;
     zero.x = 0;
     zero.y = 0;
     for (int c0 = 0; c0 < jb; c0 += LDLT_SP) {
         const int w = min(LDLT_SP, jb - c0), rows = jb - c0;
-        for (int e = tid; e < rows * w; e += nth) {
-            const int i = e / w, c = e % w;
-            P[i * LDLT_PITCH + c] = A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + c];
+        const int i = tid;  // this thread's row of the sub-panel
+        const bool act = i < rows;
+        // x[c] holds a[i][jj + c]: column jj is always x[0], the row shifting
+        // left as columns retire (static register indices)
+        C2 x[LDLT_SP];
+#pragma unroll
+        for (int c = 0; c < LDLT_SP; c++)
+            x[c] = (act && c < w) ? A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + c] : zero;
+        for (int jj = 0; jj < w; jj++) {
+            const int par = jj & 1;
+            if (i == jj) s_piv[par] = x[0];
+            if (i > jj && i < w) s_col[par][i] = x[0];
+            __syncthreads();
+            const C2 d = s_piv[par];
+            const bool zp = (d.x == 0 && d.y == 0);
+            if (zp && i == jj) atomicCAS(info, 0, j0 + c0 + jj + 1);
+            if (act && i > jj) {
+                C2 one;
+                one.x = 1;
+                one.y = 0;
+                const C2 inv = zp ? zero : cdiv(one, d);
+                C2 l;
+                l.x = x[0].x * inv.x - x[0].y * inv.y;
+                l.y = x[0].x * inv.y + x[0].y * inv.x;
+                // a[i][c] -= l_i (d l_c), d l_c being the unscaled a[c][jj]
+#pragma unroll
+                for (int c = 1; c < LDLT_SP; c++) {
+                    if (jj + c < w) {
+                        const C2 u = s_col[par][jj + c];
+                        x[c].x -= l.x * u.x - l.y * u.y;
+                        x[c].y -= l.x * u.y + l.y * u.x;
+                    }
+                }
+                x[0] = l;
+            }
+            // column jj is final for this row: to shared memory, and its lower part to global
+            if (act) {
+                P[i * LDLT_PITCH + jj] = x[0];
+                if (jj <= i) A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + jj] = x[0];
+            }
+#pragma unroll
+            for (int c = 0; c + 1 < LDLT_SP; c++) x[c] = x[c + 1];
+            x[LDLT_SP - 1] = zero;
         }
         __syncthreads();
-        __shared__ C2 wcol[LDLT_SP];  // the unscaled column jj of the sub-block's rows
-        for (int jj = 0; jj < w; jj++) {
-            const C2 d = P[jj * LDLT_PITCH + jj];
-            const bool zp = (d.x == 0 && d.y == 0);
-            if (zp && tid == 0) atomicCAS(info, 0, j0 + c0 + jj + 1);
-            // column jj: keep the sub-block rows' unscaled values, then scale to L
-            // (one division per row)
-            for (int i = jj + 1 + tid; i < rows; i += nth) {
-                const C2 v = P[i * LDLT_PITCH + jj];
-                if (i < w) wcol[i] = v;
-                P[i * LDLT_PITCH + jj] = zp ? zero : cdiv(v, d);
-            }
-            __syncthreads();
-            // rank-1 update of the sub-panel's remaining columns (lower part):
-            // a[i][c] -= l_i (d l_c), d l_c being the unscaled a[c][jj]; a
-            // warp per row, lane = column (LDLT_SP = 32), no index division
-            if (!zp && jj + 1 < w) {
-                const int c = tid & 31;
-                const C2 wc = wcol[c < w ? c : 0];
-                for (int i = jj + 1 + (tid >> 5); i < rows; i += nth >> 5) {
-                    if (c <= jj || c >= w || c > i) continue;
-                    const C2 l = P[i * LDLT_PITCH + jj];
-                    C2 x = P[i * LDLT_PITCH + c];
-                    x.x -= l.x * wc.x - l.y * wc.y;
-                    x.y -= l.x * wc.y + l.y * wc.x;
-                    P[i * LDLT_PITCH + c] = x;
-                }
-            }
-            __syncthreads();
-        }
-        for (int e = tid; e < rows * w; e += nth) {
-            const int i = e / w, c = e % w;
-            if (c <= i) A[(int64_t)(j0 + c0 + i) * lda + j0 + c0 + c] = P[i * LDLT_PITCH + c];
-        }
         // the block's remaining lower triangle: A[i][c] -= sum_k L[i][k] d_k L[c][k]
         const int rest = rows - w;
         if (rest > 0) {
             C2* T = P + (size_t)256 * LDLT_PITCH;  // [k][c] = d_k L[w + c][k]
-            for (int e = tid; e < w * rest; e += nth) {
+            for (int e = tid; e < w * rest; e += LDLT_THREADS) {
                 const int k = e / rest, c = e % rest;
                 const C2 dk = P[k * LDLT_PITCH + k], lc = P[(w + c) * LDLT_PITCH + k];
                 C2 t;
@@ -1464,31 +1476,32 @@ ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int
                 T[k * LDLT_TP + c] = t;
             }
             __syncthreads();
-            const int ty = tid >> 5, tx = tid & 31, nbk = (rest + 127) / 128;
-            for (int bi = 0; bi < nbk; bi++)
-                for (int bc = 0; bc <= bi; bc++) {
-                    C2 acc[4][4];
-                    int ii[4], cc[4];
+            // 128 x 64 output blocks of the lower triangle, 8 x 4 per thread
+            const int ty = tid >> 4, tx = tid & 15, nbr = (rest + 127) / 128;
+            for (int bi = 0; bi < nbr; bi++)
+                for (int bc = 0; bc * 64 < min(rest, bi * 128 + 128); bc++) {
+                    C2 acc[8][4];
+                    int ii[8], cc[4];
 #pragma unroll
-                    for (int r = 0; r < 4; r++) ii[r] = bi * 128 + ty + 32 * r;
+                    for (int r = 0; r < 8; r++) ii[r] = bi * 128 + ty + 16 * r;
 #pragma unroll
-                    for (int c = 0; c < 4; c++) cc[c] = bc * 128 + tx + 32 * c;
+                    for (int c = 0; c < 4; c++) cc[c] = bc * 64 + tx + 16 * c;
 #pragma unroll
-                    for (int r = 0; r < 4; r++)
+                    for (int r = 0; r < 8; r++)
 #pragma unroll
                         for (int c = 0; c < 4; c++)
                             acc[r][c] = (ii[r] < rest && cc[c] <= ii[r])
                                             ? A[(int64_t)(j0 + c0 + w + ii[r]) * lda + j0 + c0 + w + cc[c]]
                                             : zero;
-#pragma unroll 4
+#pragma unroll 2
                     for (int k = 0; k < w; k++) {
-                        C2 a[4], b[4];
+                        C2 a[8], b[4];
 #pragma unroll
-                        for (int r = 0; r < 4; r++) a[r] = ii[r] < rest ? P[(w + ii[r]) * LDLT_PITCH + k] : zero;
+                        for (int r = 0; r < 8; r++) a[r] = ii[r] < rest ? P[(w + ii[r]) * LDLT_PITCH + k] : zero;
 #pragma unroll
                         for (int c = 0; c < 4; c++) b[c] = T[k * LDLT_TP + cc[c]];
 #pragma unroll
-                        for (int r = 0; r < 4; r++)
+                        for (int r = 0; r < 8; r++)
 #pragma unroll
                             for (int c = 0; c < 4; c++) {
                                 acc[r][c].x -= a[r].x * b[c].x - a[r].y * b[c].y;
@@ -1496,7 +1509,7 @@ ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int
                             }
                     }
 #pragma unroll
-                    for (int r = 0; r < 4; r++)
+                    for (int r = 0; r < 8; r++)
 #pragma unroll
                         for (int c = 0; c < 4; c++)
                             if (ii[r] < rest && cc[c] <= ii[r])
@@ -1585,7 +1598,7 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info, float2
     auto factor_block = [&](int j0, int jb) -> int {
         const int below = n - j0 - jb;
         cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
-        ldlt_diag_kernel<float><<<1, 1024, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
+        ldlt_diag_kernel<float><<<1, LDLT_THREADS, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
         BEM_LAUNCHED(ctx);
         if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3, 16.0 * (double)jb * jb);
         if (below > 0 || Linv) {
