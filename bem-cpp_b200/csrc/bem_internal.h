@@ -211,8 +211,8 @@ struct bem_ctx {
                                  // differences of reassembled operators
     int verify_cols = 64;        // refinement: columns whose error is measured with an FP64 residual
                                  // at convergence (0: none, -1: all)
-    int factor_sb = 2;           // L D L^T: 256-column blocks per trailing update (1 or 2)
-    int solve_sb = 2;            // L D L^T solves: 256-row blocks per update (1 or 2)
+    int factor_sb = 4;           // L D L^T: 256-column blocks per trailing update (1..4)
+    int solve_sb = 4;            // L D L^T solves: 256-row blocks per update (1..4)
     int oz_pace_epoch = 32;      // int8 residual: K slabs per pacing epoch (0: no pacing)
     int oz_pace_lead = 2;        // epochs of lead over the grid average before a CTA waits
     bool prof = false;

@@ -290,7 +290,7 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
             return bem::fail(ctx, BEM_ERR_INVALID, "gmres_digits must be 0 or 2..%d", bem::oz::S_MAX);
         ctx->gmres_digits = value;
     } else if (!std::strcmp(name, "factor_superblock") || !std::strcmp(name, "solve_superblock")) {
-        if (value != 1 && value != 2) return bem::fail(ctx, BEM_ERR_INVALID, "%s must be 1 or 2", name);
+        if (value < 1 || value > 4) return bem::fail(ctx, BEM_ERR_INVALID, "%s must be 1..4", name);
         (name[0] == 'f' ? ctx->factor_sb : ctx->solve_sb) = value;
     } else if (!std::strcmp(name, "cache_factor_memory")) {
         bem::devmem_cache_enable(ctx->device, value != 0);

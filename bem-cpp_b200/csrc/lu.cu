@@ -1625,28 +1625,32 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info, float2
         }
         return (int)BEM_OK;
     };
-    // Super-blocks of two 256-column blocks: block 1 is factored and updates
-    // block column 2 alone (a thin GEMM), block 2 is factored, and the
-    // lower-triangle update of the rest takes both (K = 512: half the launches
-    // and half the read-modify-write of the trailing matrix).
-    const int SB = (ctx->factor_sb == 2 ? 2 : 1) * NB;
+    // Super-blocks of factor_sb 256-column blocks: each block is factored and
+    // updates the super-block's later block columns alone (thin GEMMs), and
+    // the lower-triangle update of the rest takes the whole super-block
+    // (K = 256 factor_sb: fewer launches and fewer read-modify-writes of the
+    // trailing matrix).
+    const int SB = std::max(1, std::min(4, ctx->factor_sb)) * NB;
     for (int J0 = 0; J0 < n; J0 += SB) {
-        const int JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
-        BEM_TRY(factor_block(J0, jb1));
-        if (jb2 > 0) {
-            // S[J0+jb1:, J0+jb1:J0+JB] -= L21 D1 (rows J0+jb1.. of L21)^T
-            TcOpts o;
-            o.bscale = A + (int64_t)J0 * lda + J0;
-            o.bscale_stride = lda + 1;
-            o.prof_cls = PROF_LU_UPDATE;
-            const float2* L21 = A + (int64_t)(J0 + jb1) * lda + J0;
-            BEM_TRY(tc_gemm_ex(ctx, n - J0 - jb1, jb2, jb1, L21, lda, L21, lda,
-                               A + (int64_t)(J0 + jb1) * lda + J0 + jb1, lda, o));
-            BEM_TRY(factor_block(J0 + jb1, jb2));
+        const int JB = std::min(SB, n - J0);
+        for (int j = J0; j < J0 + JB; j += NB) {
+            const int jb = std::min(NB, J0 + JB - j);
+            BEM_TRY(factor_block(j, jb));
+            const int nc = J0 + JB - j - jb;  // the super-block's columns after this block
+            if (nc > 0) {
+                // S[j+jb:, j+jb:J0+JB] -= L21 D L21^T (rows j+jb.. of this block's L21)
+                TcOpts o;
+                o.bscale = A + (int64_t)j * lda + j;
+                o.bscale_stride = lda + 1;
+                o.prof_cls = PROF_LU_UPDATE;
+                const float2* L21 = A + (int64_t)(j + jb) * lda + j;
+                BEM_TRY(tc_gemm_ex(ctx, n - j - jb, nc, jb, L21, lda, L21, lda, A + (int64_t)(j + jb) * lda + j + jb,
+                                   lda, o));
+            }
         }
         const int below = n - J0 - JB;
         if (below > 0) {
-            // S22 -= L21 D L21^T over both blocks, lower triangle
+            // S22 -= L21 D L21^T over the super-block, lower triangle
             TcOpts o;
             o.lower = true;
             o.bscale = A + (int64_t)J0 * lda + J0;
@@ -1680,11 +1684,11 @@ int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2*
                                                                                          nrhs);
         BEM_LAUNCHED(ctx);
     }
-    // Super-blocks of two 256-row diagonal blocks (ctx->solve_sb = 2): the
-    // second block is updated by the first with a thin GEMM, so the update of
-    // all rows below runs with K = 512 (half the launches and half the
-    // read-modify-write of X).
-    const int SB = (ctx->solve_sb == 2 ? 2 : 1) * NB;
+    // Super-blocks of solve_sb 256-row diagonal blocks: the blocks of a
+    // super-block update one another with thin GEMMs, so the update of all
+    // rows beyond runs with K = 256 solve_sb (fewer launches and fewer
+    // read-modify-writes of X).
+    const int SB = std::max(1, std::min(4, ctx->solve_sb)) * NB;
     auto update = [&](int M, int K, const float2* Ablk, bool trans, float2* Bx, float2* Cx) {
         TcOpts o;
         o.c_colmajor = true;
@@ -1712,11 +1716,12 @@ int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2*
     };
     // L z = b
     for (int J0 = 0; J0 < n; J0 += SB) {
-        const int JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
-        BEM_TRY(diag(J0, jb1, false));
-        if (jb2 > 0) {
-            BEM_TRY(update(jb2, jb1, A + (int64_t)(J0 + jb1) * lda + J0, false, X + J0, X + J0 + jb1));
-            BEM_TRY(diag(J0 + jb1, jb2, false));
+        const int JB = std::min(SB, n - J0);
+        for (int j = J0; j < J0 + JB; j += NB) {
+            const int jb = std::min(NB, J0 + JB - j), nc = J0 + JB - j - jb;
+            BEM_TRY(diag(j, jb, false));
+            // the super-block's later rows: X[j+jb:J0+JB] -= L[j+jb:J0+JB, j:j+jb] X[j:j+jb]
+            if (nc > 0) BEM_TRY(update(nc, jb, A + (int64_t)(j + jb) * lda + j, false, X + j, X + j + jb));
         }
         const int below = n - J0 - JB;
         if (below > 0) BEM_TRY(update(below, JB, A + (int64_t)(J0 + JB) * lda + J0, false, X + J0, X + J0 + JB));
@@ -1727,13 +1732,13 @@ int sytrs_nopiv(bem_ctx* ctx, const float2* A, int64_t lda, int n, const float2*
     // L^T x = y, super-blocks from the last
     const int nsb = (n + SB - 1) / SB;
     for (int bi = nsb - 1; bi >= 0; bi--) {
-        const int J0 = bi * SB, JB = std::min(SB, n - J0), jb1 = std::min(NB, JB), jb2 = JB - jb1;
-        if (jb2 > 0) {
-            BEM_TRY(diag(J0 + jb1, jb2, true));
-            // X[J0:J0+jb1] -= (L[J0+jb1:J0+JB, J0:J0+jb1])^T X[J0+jb1:J0+JB]
-            BEM_TRY(update(jb1, jb2, A + (int64_t)(J0 + jb1) * lda + J0, true, X + J0 + jb1, X + J0));
+        const int J0 = bi * SB, JB = std::min(SB, n - J0);
+        for (int j = J0 + ((JB - 1) / NB) * NB; j >= J0; j -= NB) {
+            const int jb = std::min(NB, J0 + JB - j);
+            BEM_TRY(diag(j, jb, true));
+            // the super-block's earlier rows: X[J0:j] -= (L[j:j+jb, J0:j])^T X[j:j+jb]
+            if (j > J0) BEM_TRY(update(j - J0, jb, A + (int64_t)j * lda + J0, true, X + j, X + J0));
         }
-        BEM_TRY(diag(J0, jb1, true));
         // X[0:J0] -= (L[J0:J0+JB, 0:J0])^T X[J0:J0+JB]
         if (J0 > 0) BEM_TRY(update(J0, JB, A + (int64_t)J0 * lda, true, X + J0, X));
     }

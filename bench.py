@@ -78,9 +78,9 @@ def parse():
                     help="refinement target: estimated max-column relative error")
     ap.add_argument("--residual-digits", type=int, default=7,
                     help="int8 digits of the refinement residual (0: FP64 DMMA GEMM)")
-    ap.add_argument("--factor-superblock", type=int, default=2, choices=[1, 2],
+    ap.add_argument("--factor-superblock", type=int, default=4, choices=[1, 2, 3, 4],
                     help="256-column blocks per L D L^T trailing update")
-    ap.add_argument("--solve-superblock", type=int, default=2, choices=[1, 2],
+    ap.add_argument("--solve-superblock", type=int, default=4, choices=[1, 2, 3, 4],
                     help="256-row blocks per L D L^T solve update")
     ap.add_argument("--gemm-group-m", type=int, default=16,
                     help="row tiles per raster group of the tensor-core GEMM")
@@ -717,7 +717,8 @@ def _roofline_from_profile(prof, bf16):
 def run_gemm(a):
     """The FP32 tensor-core GEMM of the factorisation alone: C -= A B with
     complex64 A (n x 512), B (512 x n) and a square row-major C (n x n), the
-    shape of an L D L^T super-block trailing update, timed with CUDA events
+    shape of a two-block L D L^T super-block trailing update (the default
+    super-block has four, K = 1024), timed with CUDA events
     over the steps (C larger than L2 for n >= 4096)."""
     import torch
 

@@ -95,8 +95,10 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * residual's CTAs report every 32 K slabs and wait, softly, when more than 2
  * epochs ahead of the grid average, so a wave shares its digit rows in L2;
  * epoch 0 turns the pacing off), "factor_superblock" / "solve_superblock"
- * (2, default: the L D L^T factorisation and solves update with two 256-wide
- * blocks at once, K = 512; 1: one block), "gmres_digits" (0, default: GMRES
+ * (4, default: the L D L^T factorisation and solves update with four
+ * 256-wide blocks at once, K = 1024; 1..3: that many blocks, K = 256 per
+ * block),
+ * "gmres_digits" (0, default: GMRES
  * products with Z on the FP64 GEMM; 2..8: int8 Ozaki digits),
  * "cache_factor_memory" (0, default; 1: the FP32 factors and int8 digit planes
  * of a freed factorisation stay allocated on this context's device and are

@@ -112,6 +112,30 @@ def test_block_inverse_solves_match_triangular_solves(ctx, pmchwt, case):
     assert u1 < 3 * u0, (u1, u0)
 
 
+@pytest.mark.parametrize("fsb,ssb", [(1, 1), (2, 2), (3, 4), (4, 3)])
+def test_superblocks_of_any_width_solve(ctx, fsb, ssb):
+    # factor_superblock / solve_superblock 1..4: the diagonal blocks of a
+    # super-block update one another, the rest is updated once with K = 256 sb;
+    # n = 1100 leaves a ragged last block and a short last super-block
+    import bem_b200 as bb
+    rng = np.random.default_rng(fsb * 10 + ssb)
+    n = 1100
+    A = _cplx(rng, n, n)
+    Z = A + A.T + 4 * np.sqrt(n) * np.eye(n)
+    B = _cplx(rng, n, 7)
+    try:
+        bb.set_option(ctx, "factor_superblock", fsb)
+        bb.set_option(ctx, "solve_superblock", ssb)
+        X, st = _solve(ctx, Z, B)
+    finally:
+        bb.set_option(ctx, "factor_superblock", 4)
+        bb.set_option(ctx, "solve_superblock", 4)
+    assert st["factorization"] == 1 and st["converged"]
+    assert rel(X, np.linalg.solve(Z, B)) < 1e-11
+    with pytest.raises(bb.BemError):
+        bb.set_option(ctx, "factor_superblock", 5)
+
+
 @pytest.mark.parametrize("xd", [3, 2])
 def test_rounded_iterates_keep_the_fp64_solution(ctx, pmchwt, xd):
     # residual_x_digits (default 2): the first iterate and the corrections are
