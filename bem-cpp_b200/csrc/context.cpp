@@ -64,7 +64,7 @@ void bem_ctx::prof_end(int cls, cudaEvent_t a, double flops, double bytes) {
     }
     cudaEventRecord(b, stream);
     prof_pending.push_back({cls, a, b, flops, bytes});
-    if (prof_pending.size() > 4096) prof_collect();
+    if (prof_pending.size() > 65536) prof_collect();  // (collecting synchronizes the stream)
 }
 
 int bem_ctx::prof_collect() {
