@@ -308,6 +308,8 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
     } else if (!std::strcmp(name, "residual_x_digits")) {
         if (value < 0 || value > 7) return bem::fail(ctx, BEM_ERR_INVALID, "residual_x_digits must be 0..7");
         ctx->oz_xdigits = value;
+    } else if (!std::strcmp(name, "lu_u12_slabs")) {
+        ctx->lu_u12_slabs = value != 0;
     } else if (!std::strcmp(name, "solve_block_inverse")) {
         ctx->solve_inv = value != 0;
     } else if (!std::strcmp(name, "fp64_gemm_3m")) {

@@ -945,6 +945,28 @@ int trsm_rows_lower_unit(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, in
     return trsm_block<R, false, true>(ctx, A, lda, r0, kb, A, lda, c0, c1, -1, batch, sA, sA);
 }
 
+// U12 = L11^-1 A12 for the jb x jb unit lower block at (j0, j0), columns
+// [c0, n), as a blocked forward substitution: 64-row slabs solved by the
+// block triangular solve, each followed by the GEMM update of the slabs
+// below (on the FP64 tensor path).  The same arithmetic as the block solve
+// of all jb rows, regrouped: three quarters of its flops move to the GEMM.
+constexpr int U12_SLAB = 64;
+template <typename R>
+static int u12_blocked(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int j0, int jb, int c0, int n, int batch,
+                       int64_t sA) {
+    using C2 = typename C2T<R>::type;
+    const int nc = n - c0;
+    for (int s0 = 0; s0 < jb; s0 += U12_SLAB) {
+        const int sb = std::min(U12_SLAB, jb - s0), below = jb - s0 - sb;
+        BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0 + s0, sb, c0, n, batch, sA));
+        if (below > 0)
+            BEM_TRY(cgemm<R>(ctx, below, nc, sb, A + (int64_t)(j0 + s0 + sb) * lda + j0 + s0, lda,
+                             A + (int64_t)(j0 + s0) * lda + c0, lda, false, A + (int64_t)(j0 + s0 + sb) * lda + c0, lda,
+                             false, mk<C2>(-1, 0), mk<C2>(1, 0), PROF_TRSM, batch, sA, sA, sA));
+    }
+    return BEM_OK;
+}
+
 // ------------------------------------------------------------------ getrf
 template <typename R>
 int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipiv, int* d_info,
@@ -986,7 +1008,9 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
     pw.status = ctx->d_status;
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
-
+    // FP64: U12 = L11^-1 A12 by 64-row slabs with GEMM updates between them
+    // (u12_blocked) instead of one block triangular solve of 256 rows
+    const bool u12b = sizeof(R) == 8 && ctx->lu_u12_slabs;
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = std::min(NB, n - j0);
         for (int i0 = j0; i0 < j0 + jb; i0 += W) {
@@ -1044,7 +1068,11 @@ int getrf(bem_ctx* ctx, typename C2T<R>::type* A, int64_t lda, int n, int* d_ipi
         }
         const int c0 = j0 + jb;
         if (c0 < n) {
-            BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0, jb, c0, n));
+            if (u12b) {
+                BEM_TRY(u12_blocked<R>(ctx, A, lda, j0, jb, c0, n, 1, 0));
+            } else {
+                BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0, jb, c0, n));
+            }
             const int Mt = n - c0;
             if (tc && tc->fn)
                 BEM_TRY(tc->fn(ctx, tc->state, Mt, Mt, jb, A + (int64_t)c0 * lda + j0, lda,
@@ -1165,6 +1193,8 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, batch * sizeof(int), ctx->stream));
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
     const C2 m1 = mk<C2>(-1, 0), p1 = mk<C2>(1, 0);
+    // U12 by 64-row slabs, as in getrf (the same arithmetic per matrix)
+    const bool u12b = ctx->lu_u12_slabs;
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int jb = std::min(NB, n - j0);
         for (int i0 = j0; i0 < j0 + jb; i0 += W) {
@@ -1217,7 +1247,10 @@ int getrf_batched(bem_ctx* ctx, double2* A, int64_t lda, int64_t sA, int n, int 
         }
         const int c0 = j0 + jb;
         if (c0 < n) {
-            BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0, jb, c0, n, batch, sA));
+            if (u12b)
+                BEM_TRY(u12_blocked<R>(ctx, A, lda, j0, jb, c0, n, batch, sA));
+            else
+                BEM_TRY(trsm_rows_lower_unit<R>(ctx, A, lda, j0, jb, c0, n, batch, sA));
             const int Mt = n - c0;
             BEM_TRY(cgemm<R>(ctx, Mt, Mt, jb, A + (int64_t)c0 * lda + j0, lda, A + (int64_t)j0 * lda + c0, lda, false,
                              A + (int64_t)c0 * lda + c0, lda, false, m1, p1, PROF_LU_UPDATE, batch, sA, sA, sA));

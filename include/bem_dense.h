@@ -139,6 +139,11 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * iterate it belongs to; the rounding, 2^-14 of the column's largest entry,
  * is below the FP32 solve's own error and the next sweep removes it; 0:
  * every digit, 1..7: that many),
+ * "lu_u12_slabs" (1, default: the FP64 LU forms U12 = L11^-1 A12 of
+ * every 256-column block by 64-row slabs, each solved by the block
+ * triangular solve and followed by the GEMM update of the slabs below on
+ * the FP64 tensor path -- the same substitution regrouped, three quarters
+ * of its flops in the GEMM; 0: one block triangular solve of 256 rows),
  * "solve_block_inverse" (1, default: the FP32 L D L^T factorisation also
  * keeps -L11^-1 of each 256-row diagonal block (n^2 / 256 complex64, 8 n^2 /
  * 256 bytes), and its solves apply the diagonal blocks as tensor-core

@@ -93,6 +93,39 @@ def test_fp64_gemm_3m_against_4m(ctx, n):
     assert rel(out[1][2], np.linalg.solve(A, B)) < 1e-10
 
 
+@pytest.mark.parametrize("n", [600, 1300])
+def test_fp64_u12_slabs_against_triangular_solve(ctx, n):
+    # lu_u12_slabs (default): U12 = L11^-1 A12 by 64-row slabs with GEMM
+    # updates between them; 0: one block triangular solve.  Same pivots
+    # (LAPACK's), backward errors of the factors and solutions within a small
+    # factor of each other
+    import bem_b200 as bb
+    from scipy.linalg import lu_factor
+    A = _rand(n, 70 + n)
+    B = _rand(n, 71 + n)[:, :12]
+    out = {}
+    try:
+        for inv in (1, 0):
+            bb.set_option(ctx, "lu_u12_slabs", inv)
+            F, ipiv, info = bb.lu_factorize_cuda(ctx, A)
+            assert info == 0
+            out[inv] = (F, ipiv, bb.lu_solve_cuda(ctx, F, ipiv, B))
+    finally:
+        bb.set_option(ctx, "lu_u12_slabs", 1)
+    _, piv2 = lu_factor(A)
+    assert np.array_equal(out[1][1], out[0][1])
+    assert np.array_equal(out[1][1] - 1, piv2)
+    nA = np.linalg.norm(A)
+    fb = []
+    for F, ipiv, X in out.values():
+        PA = A.copy()
+        for i, p in enumerate(ipiv - 1):
+            PA[[i, p]] = PA[[p, i]]
+        fb.append(np.linalg.norm(PA - (np.tril(F, -1) + np.eye(n)) @ np.triu(F)) / nA)
+        assert np.linalg.norm(A @ X - B) / (nA * np.linalg.norm(X)) < 1e-16 * n
+    assert fb[0] < 1e-16 * n and fb[0] <= 3 * fb[1], fb
+
+
 def test_singular_reports_info(ctx):
     import bem_b200 as bb
     A = _rand(64, 4)
