@@ -3,7 +3,7 @@
 // (output.cpp:5-64).  Assembly, factorisation, the solve of every
 // orientation x polarisation and the far field / Mueller reduction run on the
 // device through bem_dense_run.  Iterative-solver flags are accepted and
-// ignored with a warning (this build provides the dense path only).
+// ignored with a warning (bem_cuda provides the dense path only).
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -68,7 +68,7 @@ int main(int argc, char** argv) {
         else if (is("--solver", 1)) {
             const char* s = argv[++i];
             if (std::strcmp(s, "dense") != 0 && std::strcmp(s, "auto") != 0) {
-                std::fprintf(stderr, "Solver '%s' is not provided by this build (dense only)\n", s);
+                std::fprintf(stderr, "Solver '%s' is not provided by bem_cuda (dense only)\n", s);
                 return 1;
             }
         } else if (is("--shape", 1)) shape = argv[++i];
