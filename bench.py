@@ -102,6 +102,8 @@ def parse():
                          "tensor-core GEMM alone at the L D L^T trailing-update shape")
     ap.add_argument("--gemm-n", type=int, default=12288, help="--config gemm: rows of C (complex)")
     ap.add_argument("--gemm-ncol", type=int, default=2790, help="--config gemm --gemm-shape solve: columns of C")
+    ap.add_argument("--gemm-k", type=int, default=512,
+                    help="--config gemm: K (complex), 256 per diagonal block of a super-block")
     ap.add_argument("--gemm-shape", default="factor", choices=["factor", "solve"],
                     help="--config gemm: factor: square row-major C -= A B (B row-major); solve: C (n x 2790, "
                          "column-major, --gemm-ncol) -= A B with B column-major, the multi-RHS solve's update")
@@ -716,10 +718,11 @@ def _roofline_from_profile(prof, bf16):
 
 def run_gemm(a):
     """The FP32 tensor-core GEMM of the factorisation alone: C -= A B with
-    complex64 A (n x 512), B (512 x n) and a square row-major C (n x n), the
-    shape of a two-block L D L^T super-block trailing update (the default
-    super-block has four, K = 1024), timed with CUDA events
-    over the steps (C larger than L2 for n >= 4096)."""
+    complex64 A (n x K), B (K x n) and a square row-major C (n x n), the
+    shape of an L D L^T super-block trailing update (K = 256 per diagonal
+    block: --gemm-k 1024 for the default four-block super-block, 512 by
+    default here), timed with CUDA events over the steps (C larger than L2
+    for n >= 4096)."""
     import torch
 
     import bem_b200 as bb
@@ -734,7 +737,7 @@ def run_gemm(a):
     bb.set_option(ctx, "gemm_group_m", a.gemm_group_m)
     for name, value in extra_options(a).items():
         bb.set_option(ctx, name, value)
-    n, K = a.gemm_n, 512
+    n, K = a.gemm_n, a.gemm_k
     solve = a.gemm_shape == "solve"
     ncol = a.gemm_ncol if solve else n
     g = torch.Generator(device="cuda:0").manual_seed(0)
