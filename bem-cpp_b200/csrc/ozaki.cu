@@ -12,6 +12,10 @@
 // with the same s + t share one TMEM accumulator in groups of at most four
 // (4 * 2^12 * 2^17 < 2^31).  The epilogue scales by 2^(e_i + f_j - 7(s+t))
 // (exact) and subtracts from R in FP64.  With S = 7 the digits carry 48 bits.
+// X' may keep fewer digits, Sx <= S (1-based t <= Sx): the refinement rounds
+// its iterates to their first Sx digits and keeps the rounded values, so the
+// pairs with t > Sx, zero for them, are not computed (slice_cols_kernel
+// writes the rounded value back).
 //
 // The int8 GEMM is the persistent warp-specialised tcgen05 kernel of
 // gemm_tc.cu with kind::i8 (M = 128, N = 256, K = 32 per MMA), 4 stages of
