@@ -161,6 +161,24 @@ def test_rounded_iterates_keep_the_fp64_solution(ctx, pmchwt, xd):
     assert out[xd][1]["iterations"] <= out[0][1]["iterations"] + 1
 
 
+def test_rounded_iterates_with_zero_and_extreme_columns(ctx, pmchwt):
+    # the rounding is relative to each column's largest entry: a zero column
+    # stays exactly zero, columns scaled by 1e-150 / 1e+150 converge like the
+    # others (the digit exponents follow the column)
+    import scipy.linalg as sl
+    Z, B0 = pmchwt
+    B = B0[:, :6].copy()
+    B[:, 0] = 0.0
+    B[:, 1] *= 1e-150
+    B[:, 2] *= 1e150
+    X, st = _solve(ctx, Z, B, tol=2e-10)
+    assert st["converged"]
+    assert np.all(X[:, 0] == 0)
+    Xr = sl.lu_solve(sl.lu_factor(Z), B)
+    err = np.linalg.norm(X[:, 1:] - Xr[:, 1:], axis=0) / np.linalg.norm(Xr[:, 1:], axis=0)
+    assert err.max() < 1e-10, err
+
+
 @pytest.mark.parametrize("n", [1, 7, 256, 300, 700])
 def test_symmetric_random_uses_ldlt(ctx, n):
     rng = np.random.default_rng(n)
