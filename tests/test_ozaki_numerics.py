@@ -109,3 +109,46 @@ def test_update_form_digits_keep_the_absolute_accuracy(prev_upd):
     if d > 2:
         assert not (2.0 ** (4 - 7 * (d - 1)) * prev_upd <= 2.0 * 2.0 ** (4 - 7 * S))
     assert {1.1e-4: 5, 5.6e-5: 5}.get(prev_upd, d) == d
+
+
+def _ozaki_product_sx(A, B, S, Sx):
+    """The product with B's columns kept to Sx digits: pairs s <= S, t <= Sx,
+    s + t <= S + 1 (1-based), and the value B~ those Sx digits represent."""
+    ea = _exp(np.abs(A).max(axis=1))
+    eb = _exp(np.abs(B).max(axis=0))
+    qa, _ = _digits(A * np.ldexp(1.0, -ea)[:, None], S)
+    qb, _ = _digits(B * np.ldexp(1.0, -eb)[None, :], Sx)
+    # the rounded B, rebuilt from its digits by Horner in base 128 (exact)
+    Bt = np.zeros_like(B)
+    for t in range(Sx - 1, -1, -1):
+        Bt = (Bt + qb[t]) / 128.0
+    Bt = Bt * np.ldexp(1.0, eb)[None, :]
+    out = np.zeros((A.shape[0], B.shape[1]))
+    for s in range(1, S + 1):
+        for t in range(1, min(Sx, S + 1 - s) + 1):
+            out += np.ldexp((qa[s - 1] @ qb[t - 1]).astype(np.float64), -7 * (s + t))
+    return out * np.ldexp(1.0, ea)[:, None] * np.ldexp(1.0, eb)[None, :], Bt
+
+
+@pytest.mark.parametrize("Sx", [2, 3])
+def test_rounded_iterate_is_exact_and_needs_fewer_pairs(Sx):
+    # the refinement's iterate kept to Sx digits: the rebuilt value equals the
+    # sum of its digits exactly, lies within 2^(-7 Sx - 1) of its column's
+    # scale from the original, and the product over the pairs t <= Sx is the
+    # product with the rounded iterate to the same bound as with every digit
+    rng = np.random.default_rng(3 + Sx)
+    K, S = 256, 7
+    A = rng.standard_normal((40, K)) * 10.0 ** rng.uniform(-2, 2, (40, 1))
+    X = rng.standard_normal((K, 6)) * 10.0 ** rng.uniform(-5, 5, (1, 6))
+    P, Xt = _ozaki_product_sx(A, X, S, Sx)
+    eb = _exp(np.abs(X).max(axis=0))
+    assert np.all(np.abs(Xt - X) <= np.ldexp(2.0 ** (-7 * Sx - 1), eb)[None, :])
+    qb, _ = _digits(Xt * np.ldexp(1.0, -eb)[None, :], S)
+    assert not qb[Sx:].any()  # the rounded iterate has no digits beyond Sx
+    exact = A.astype(np.longdouble) @ Xt.astype(np.longdouble)
+    scale = np.abs(A).max(axis=1)[:, None] * np.abs(Xt).max(axis=0)[None, :]
+    err = np.abs(P - exact.astype(np.float64)) / (K * scale)
+    assert err.max() <= 2.0 ** (4 - 7 * S) + 4 * 2.0 ** -53
+    # 13 pairs instead of 28 for Sx = 2 (18 for 3)
+    pairs = sum(1 for s in range(1, S + 1) for t in range(1, min(Sx, S + 1 - s) + 1))
+    assert pairs == {2: 13, 3: 18}[Sx]
