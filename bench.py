@@ -9,9 +9,10 @@ A step is one solve: FP32 factorisation of the FP64-assembled Z (tensor-core
 updates with FP32 operands split into three FP16 products after power-of-two
 row / column scaling; --tensor-split 0: three TF32 products), the
 2790-column triangular solves, and FP64
-iterative refinement until every column's estimated relative error is below
-2e-10 (the metric asks for 1e-9; the measured error against the FP64 LU
-solution is reported as max_rel_err_vs_fp64).
+iterative refinement (int8 digit-pair residuals of iterates kept to two
+digits) until every column's estimated relative error is below 2e-10 (the
+metric asks for 1e-9; the measured error against the FP64 LU solution is
+reported as max_rel_err_vs_fp64).
 value = seconds per solve: the device time of the K timed steps (one region
 bracketed by barrier + synchronize, CUDA events) divided by K, max over
 ranks; step_times_s lists the steps.  The
