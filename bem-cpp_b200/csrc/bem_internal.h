@@ -195,6 +195,7 @@ struct bem_ctx {
     bool tc_pair_attr = false;
     bool dmma_3m = true;        // complex FP64 GEMMs as three real products (Gauss) instead of four
     bool solve_inv = true;      // L D L^T solves: diagonal blocks by products with their stored inverses
+    bool ldlt_cluster = true;   // L D L^T factor: diagonal blocks on an 8-CTA cluster (else one CTA)
     bool lu_u12_slabs = true;  // FP64 LU: U12 by 64-row slabs with GEMM updates between them
     int tc_split = 1;           // FP32 operand split: 1 = 3xFP16 with power-of-two row / column scales, 0 = 3xTF32
     int sym_mode = 1;            // FP32 factorisation of symmetric-structured Z as L D L^T (0: always LU)

@@ -312,6 +312,8 @@ int bem_ctx_set_option(bem_ctx* ctx, const char* name, int value) {
         ctx->lu_u12_slabs = value != 0;
     } else if (!std::strcmp(name, "solve_block_inverse")) {
         ctx->solve_inv = value != 0;
+    } else if (!std::strcmp(name, "ldlt_cluster_diag")) {
+        ctx->ldlt_cluster = value != 0;
     } else if (!std::strcmp(name, "fp64_gemm_3m")) {
         ctx->dmma_3m = value != 0;
     } else if (!std::strcmp(name, "gemm_pairs")) {

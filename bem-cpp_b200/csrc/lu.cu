@@ -1553,6 +1553,237 @@ ldlt_diag_kernel(typename C2T<R>::type* __restrict__ A, int64_t lda, int j0, int
     }
 }
 
+// ------------------------------------- cluster L D L^T diagonal-block kernel
+// The block of ldlt_diag_kernel (complex64) on one cluster of 8 CTAs, the
+// block kept in distributed shared memory: CTA q holds block rows
+// 32q..32q+31, columns 0..32q+31, so no entry makes a round trip through
+// L2 between sub-panels.  Per 32-column sub-panel p:
+//   A. CTA p factors the 32 x 32 diagonal sub-block with one warp (lane i:
+//      row i, column by column), keeping the unscaled column entries in U;
+//   cluster barrier;
+//   B. every CTA q > p copies U and the pivots from CTA p and eliminates
+//      the sub-panel columns of its own rows (one thread per row);
+//   cluster barrier;
+//   C. every CTA q > p updates its rows' lower triangle right of the
+//      sub-panel: T = D L^T of block rows 32(p+1)..32q+31 is gathered from
+//      CTAs p+1..q, then each thread accumulates 4 rows x 7 column groups.
+// Every entry goes through the same operations, in the same order, as in
+// ldlt_diag_kernel (the same pivot reciprocal, rank-1 updates in column
+// order, T = d_k l_c, the trailing sums in k order).  2 np + 1 cluster
+// barriers for np sub-panels, each at the top level of the kernel so that
+// every thread of the cluster reaches it; no spin loop.  *info: first zero
+// pivot (1-based).
+constexpr int LDC_CTAS = 8, LDC_ROWS = 32, LDC_PITCH = 8 * LDC_ROWS + 1, LDC_UP = LDC_ROWS + 1,
+              LDC_TP = 7 * LDC_ROWS + 1;
+constexpr size_t ldlt_cluster_smem_bytes() {
+    return ((size_t)LDC_ROWS * LDC_PITCH + 2 * (size_t)LDC_ROWS * LDC_UP + (size_t)LDC_ROWS * LDC_TP + 4 * LDC_ROWS) *
+           sizeof(float2);
+}
+
+__global__ void __launch_bounds__(LDLT_THREADS, 1)
+ldlt_diag_cluster_kernel(float2* __restrict__ A, int64_t lda, int j0, int jb, int* __restrict__ info) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char ldc_smem[];
+    float2* S = reinterpret_cast<float2*>(ldc_smem);  // [32][LDC_PITCH]: this CTA's block rows
+    float2* U = S + LDC_ROWS * LDC_PITCH;              // [32][LDC_UP]: unscaled sub-block entries (phase A)
+    float2* UL = U + LDC_ROWS * LDC_UP;                // [32][LDC_UP]: CTA p's U (phase B)
+    float2* T = UL + LDC_ROWS * LDC_UP;                // [32][LDC_TP]: d_k L[c][k] (phase C)
+    float2* dk = T + LDC_ROWS * LDC_TP;                // [32]: the sub-panel's pivots
+    float2* dinv = dk + LDC_ROWS;                      // [32]: their reciprocals (0 for a zero pivot)
+    float2* s_col = dinv + LDC_ROWS;                   // [2][32]: column entries of phase A, by parity
+    const int q = (int)cluster.block_rank(), tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int r0 = q * LDC_ROWS;                       // this CTA's first block row
+    const int nr = max(0, min(LDC_ROWS, jb - r0));     // its rows inside the block
+    const int ncol = min(r0 + LDC_ROWS, jb);           // columns kept: 0..ncol-1
+    const float2 zero = make_float2(0.f, 0.f), one = make_float2(1.f, 0.f);
+    for (int r = wid; r < nr; r += LDLT_THREADS / 32)
+        for (int c = lane; c < ncol; c += 32) S[r * LDC_PITCH + c] = A[(int64_t)(j0 + r0 + r) * lda + j0 + c];
+    __syncthreads();
+    const int np = (jb + LDC_ROWS - 1) / LDC_ROWS;
+    for (int p = 0; p < np; p++) {
+        const int c0 = p * LDC_ROWS, w = min(LDC_ROWS, jb - c0);
+        // A. the diagonal sub-block (rows c0.. of the block are this CTA's rows 0..w-1)
+        if (q == p && wid == 0) {
+            const int i = lane;
+            const bool act = i < w;
+            float2 x[LDC_ROWS];  // x[c] = a[i][jj + c], shifted left as columns retire
+#pragma unroll
+            for (int c = 0; c < LDC_ROWS; c++) x[c] = (act && c < w) ? S[i * LDC_PITCH + c0 + c] : zero;
+            for (int jj = 0; jj < w; jj++) {
+                const int par = jj & 1;
+                if (act) s_col[par * LDC_ROWS + i] = x[0];
+                __syncwarp();
+                const float2 d = s_col[par * LDC_ROWS + jj];
+                const bool zp = (d.x == 0 && d.y == 0);
+                if (zp && i == jj) atomicCAS(info, 0, j0 + c0 + jj + 1);
+                if (act && i > jj) {
+                    const float2 inv = zp ? zero : cdiv(one, d);
+                    float2 l;
+                    l.x = x[0].x * inv.x - x[0].y * inv.y;
+                    l.y = x[0].x * inv.y + x[0].y * inv.x;
+#pragma unroll
+                    for (int c = 1; c < LDC_ROWS; c++) {
+                        if (jj + c < w) {
+                            const float2 u = s_col[par * LDC_ROWS + jj + c];
+                            x[c].x -= l.x * u.x - l.y * u.y;
+                            x[c].y -= l.x * u.y + l.y * u.x;
+                        }
+                    }
+                    U[i * LDC_UP + jj] = x[0];
+                    x[0] = l;
+                }
+                if (act && jj <= i) S[i * LDC_PITCH + c0 + jj] = x[0];
+#pragma unroll
+                for (int c = 0; c + 1 < LDC_ROWS; c++) x[c] = x[c + 1];
+                x[LDC_ROWS - 1] = zero;
+            }
+        }
+        cluster.sync();
+        // B. this CTA's rows below the sub-block
+        if (q > p && nr > 0) {
+            const float2* Up = cluster.map_shared_rank(U, p);
+            const float2* Sp = cluster.map_shared_rank(S, p);
+            for (int e = tid; e < w * w; e += LDLT_THREADS) {
+                const int r = e / w, c = e % w;
+                if (c < r) UL[r * LDC_UP + c] = Up[r * LDC_UP + c];
+            }
+            if (tid < w) {
+                const float2 d = Sp[tid * LDC_PITCH + c0 + tid];
+                dk[tid] = d;
+                dinv[tid] = (d.x == 0 && d.y == 0) ? zero : cdiv(one, d);
+            }
+            __syncthreads();
+            if (wid == 0 && lane < nr) {
+                const int i = lane;
+                float2 x[LDC_ROWS];
+#pragma unroll
+                for (int c = 0; c < LDC_ROWS; c++) x[c] = c < w ? S[i * LDC_PITCH + c0 + c] : zero;
+                for (int jj = 0; jj < w; jj++) {
+                    const float2 inv = dinv[jj];
+                    float2 l;
+                    l.x = x[0].x * inv.x - x[0].y * inv.y;
+                    l.y = x[0].x * inv.y + x[0].y * inv.x;
+#pragma unroll
+                    for (int c = 1; c < LDC_ROWS; c++) {
+                        if (jj + c < w) {
+                            const float2 u = UL[(jj + c) * LDC_UP + jj];
+                            x[c].x -= l.x * u.x - l.y * u.y;
+                            x[c].y -= l.x * u.y + l.y * u.x;
+                        }
+                    }
+                    S[i * LDC_PITCH + c0 + jj] = l;
+#pragma unroll
+                    for (int c = 0; c + 1 < LDC_ROWS; c++) x[c] = x[c + 1];
+                    x[LDC_ROWS - 1] = zero;
+                }
+            }
+        }
+        cluster.sync();
+        // C. this CTA's rows, columns cs..r0+31 of the lower triangle
+        if (q > p && nr > 0) {
+            const int cs = c0 + w, nc = r0 + LDC_ROWS - cs, ng = nc / 32;  // ng = q - p <= 7
+            for (int e = tid; e < w * nc; e += LDLT_THREADS) {
+                const int c = e / w, k = e % w, row = cs + c;
+                float2 lc = zero;
+                if (row < jb) lc = cluster.map_shared_rank(S, row / LDC_ROWS)[(row % LDC_ROWS) * LDC_PITCH + c0 + k];
+                const float2 d = dk[k];
+                float2 t;
+                t.x = d.x * lc.x - d.y * lc.y;
+                t.y = d.x * lc.y + d.y * lc.x;
+                T[k * LDC_TP + c] = t;
+            }
+            __syncthreads();
+            float2 acc[4][7];
+            bool ok[4][7];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int g = 0; g < 7; g++) {
+                    const int i = wid * 4 + r, col = cs + lane + 32 * g;
+                    ok[r][g] = g < ng && i < nr && col <= r0 + i;
+                    acc[r][g] = ok[r][g] ? S[i * LDC_PITCH + col] : zero;
+                }
+#pragma unroll 2
+            for (int k = 0; k < w; k++) {
+                float2 a[4], b[7];
+#pragma unroll
+                for (int r = 0; r < 4; r++) a[r] = S[(wid * 4 + r) * LDC_PITCH + c0 + k];
+#pragma unroll
+                for (int g = 0; g < 7; g++) b[g] = g < ng ? T[k * LDC_TP + lane + 32 * g] : zero;
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int g = 0; g < 7; g++) {
+                        acc[r][g].x -= a[r].x * b[g].x - a[r].y * b[g].y;
+                        acc[r][g].y -= a[r].x * b[g].y + a[r].y * b[g].x;
+                    }
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int g = 0; g < 7; g++)
+                    if (ok[r][g]) S[(wid * 4 + r) * LDC_PITCH + cs + lane + 32 * g] = acc[r][g];
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    for (int r = wid; r < nr; r += LDLT_THREADS / 32)
+        for (int c = lane; c <= r0 + r; c += 32) A[(int64_t)(j0 + r0 + r) * lda + j0 + c] = S[r * LDC_PITCH + c];
+    // no CTA leaves while another may still read its shared memory
+    cluster.sync();
+}
+
+// Whether the cluster diagonal-block kernel can be resident on this device
+// (8 CTAs with its shared memory; asked once per device and remembered).
+static bool ldlt_cluster_fits(bem_ctx* ctx) {
+    static std::mutex mu;
+    static std::map<int, bool> ok;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = ok.find(ctx->device);
+    if (it != ok.end()) return it->second;
+    bool fits = cudaFuncSetAttribute(ldlt_diag_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)ldlt_cluster_smem_bytes()) == cudaSuccess;
+    if (fits) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(LDC_CTAS);
+        cfg.blockDim = dim3(LDLT_THREADS);
+        cfg.dynamicSmemBytes = ldlt_cluster_smem_bytes();
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = LDC_CTAS;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        fits = cudaOccupancyMaxActiveClusters(&ncl, (const void*)ldlt_diag_cluster_kernel, &cfg) == cudaSuccess &&
+               ncl >= 1;
+    }
+    if (!fits) cudaGetLastError();
+    ok[ctx->device] = fits;
+    return fits;
+}
+
+static int launch_ldlt_diag_cluster(bem_ctx* ctx, float2* A, int64_t lda, int j0, int jb, int* d_info) {
+    if (jb < 1 || jb > LDC_CTAS * LDC_ROWS) return fail(ctx, BEM_ERR_INVALID, "cluster diagonal block: jb out of range");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(LDC_CTAS);
+    cfg.blockDim = dim3(LDLT_THREADS);
+    cfg.dynamicSmemBytes = ldlt_cluster_smem_bytes();
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = LDC_CTAS;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    BEM_TRY_CUDA(ctx, cudaLaunchKernelEx(&cfg, ldlt_diag_cluster_kernel, A, lda, j0, jb, d_info));
+    BEM_LAUNCHED(ctx);
+    return BEM_OK;
+}
+
 int sym_structure(bem_ctx* ctx, const double2* Z, int64_t ldz, int n, bool* sym, bool* sym_half) {
     unsigned* d_flags = nullptr;
     BEM_TRY_CUDA(ctx, cudaMalloc(&d_flags, sizeof(unsigned)));
@@ -1617,6 +1848,8 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info, float2
     static_assert(ldlt_smem_bytes(sizeof(float2)) <= 227 * 1024, "L D L^T diagonal block shared memory");
     BEM_TRY_CUDA(ctx, cudaFuncSetAttribute(ldlt_diag_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
+    // the diagonal blocks on one 8-CTA cluster where it fits, else on one CTA
+    const bool diag_cluster = ctx->ldlt_cluster && ldlt_cluster_fits(ctx);
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(d_info, 0, sizeof(int), ctx->stream));
     BEM_TRY_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
     struct Buf {
@@ -1631,8 +1864,12 @@ int sytrf_nopiv(bem_ctx* ctx, float2* A, int64_t lda, int n, int* d_info, float2
     auto factor_block = [&](int j0, int jb) -> int {
         const int below = n - j0 - jb;
         cudaEvent_t ev = ctx->prof_begin(PROF_PANEL);
-        ldlt_diag_kernel<float><<<1, LDLT_THREADS, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
-        BEM_LAUNCHED(ctx);
+        if (diag_cluster) {
+            BEM_TRY(launch_ldlt_diag_cluster(ctx, A, lda, j0, jb, d_info));
+        } else {
+            ldlt_diag_kernel<float><<<1, LDLT_THREADS, smem, ctx->stream>>>(A, lda, j0, jb, d_info);
+            BEM_LAUNCHED(ctx);
+        }
         if (ev) ctx->prof_end(PROF_PANEL, ev, 8.0 * jb * (double)jb * jb / 3, 16.0 * (double)jb * jb);
         if (below > 0 || Linv) {
             // column c of W.p solves L11 x = -e_c, then x_r /= d_r:

@@ -149,6 +149,11 @@ int bem_ctx_set_symmetric(bem_ctx* ctx, int mode);
  * 256 bytes), and its solves apply the diagonal blocks as tensor-core
  * products with them; 0, or without memory for them: block triangular
  * solves; set before the factorisation),
+ * "ldlt_cluster_diag" (1, default: the FP32 L D L^T factors each 256 x 256
+ * diagonal block on one cluster of 8 CTAs that holds the block in
+ * distributed shared memory, 32 rows per CTA; 0, or where such a cluster
+ * cannot be resident: on one CTA; both take every entry through the same
+ * operations in the same order),
  * "gemm_pairs" (1, default: the FP16-part tensor-core GEMM on 256-row tiles
  * of CTA pairs, tcgen05.mma.cta_group::2, each CTA loading half of a tile's
  * B operand; 0: 128-row tiles, one CTA each),

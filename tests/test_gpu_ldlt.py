@@ -112,6 +112,40 @@ def test_block_inverse_solves_match_triangular_solves(ctx, pmchwt, case):
     assert u1 < 3 * u0, (u1, u0)
 
 
+@pytest.mark.parametrize("case", ["pmchwt", 100, 300, 1100])
+def test_cluster_diagonal_blocks_match_one_cta(ctx, pmchwt, case):
+    # ldlt_cluster_diag (default): the 256 x 256 diagonal blocks of the
+    # L D L^T factored by an 8-CTA cluster holding the block in distributed
+    # shared memory; 0: by one CTA.  Both take every entry through the same
+    # operations in the same order, so the solutions agree to the last bits
+    # of the refinement; n = 100, 300, 1100 leave ragged last blocks and
+    # partial 32-column sub-panels
+    import scipy.linalg as sl
+    import bem_b200 as bb
+    if case == "pmchwt":
+        Z, B = pmchwt
+    else:
+        rng = np.random.default_rng(case)
+        A = _cplx(rng, case, case)
+        Z = A + A.T + 4 * np.sqrt(case) * np.eye(case)
+        B = _cplx(rng, case, 5)
+    Xr = sl.lu_solve(sl.lu_factor(Z), B)
+    out = {}
+    try:
+        for cl in (1, 0):
+            bb.set_option(ctx, "ldlt_cluster_diag", cl)
+            out[cl] = _solve(ctx, Z, B)
+    finally:
+        bb.set_option(ctx, "ldlt_cluster_diag", 1)
+    for X, st in out.values():
+        assert st["factorization"] in (1, 2) and st["converged"]
+        err = np.linalg.norm(X - Xr, axis=0) / np.linalg.norm(Xr, axis=0)
+        assert err.max() < 1e-10
+    (X1, s1), (X0, s0) = out[1], out[0]
+    assert rel(X1, X0) < 1e-12
+    assert s1["update_hist"][0] == pytest.approx(s0["update_hist"][0], rel=1e-3)
+
+
 @pytest.mark.parametrize("fsb,ssb", [(1, 1), (2, 2), (3, 4), (4, 3)])
 def test_superblocks_of_any_width_solve(ctx, fsb, ssb):
     # factor_superblock / solve_superblock 1..4: the diagonal blocks of a
