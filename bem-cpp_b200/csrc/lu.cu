@@ -1597,8 +1597,21 @@ ldlt_diag_cluster_kernel(float2* __restrict__ A, int64_t lda, int j0, int jb, in
     const int nr = max(0, min(LDC_ROWS, jb - r0));     // its rows inside the block
     const int ncol = min(r0 + LDC_ROWS, jb);           // columns kept: 0..ncol-1
     const float2 zero = make_float2(0.f, 0.f), one = make_float2(1.f, 0.f);
-    for (int r = wid; r < nr; r += LDLT_THREADS / 32)
-        for (int c = lane; c < ncol; c += 32) S[r * LDC_PITCH + c] = A[(int64_t)(j0 + r0 + r) * lda + j0 + c];
+    // this CTA's rows, columns 0..ncol-1, eight independent loads in flight per thread
+    const int nload = nr * ncol;
+    for (int e0 = 0; e0 < nload; e0 += 8 * LDLT_THREADS) {
+        float2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int e = e0 + u * LDLT_THREADS + tid;
+            if (e < nload) v[u] = A[(int64_t)(j0 + r0 + e / ncol) * lda + j0 + e % ncol];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int e = e0 + u * LDLT_THREADS + tid;
+            if (e < nload) S[(e / ncol) * LDC_PITCH + e % ncol] = v[u];
+        }
+    }
     __syncthreads();
     const int np = (jb + LDC_ROWS - 1) / LDC_ROWS;
     for (int p = 0; p < np; p++) {
@@ -1683,15 +1696,27 @@ ldlt_diag_cluster_kernel(float2* __restrict__ A, int64_t lda, int j0, int jb, in
         // C. this CTA's rows, columns cs..r0+31 of the lower triangle
         if (q > p && nr > 0) {
             const int cs = c0 + w, nc = r0 + LDC_ROWS - cs, ng = nc / 32;  // ng = q - p <= 7
-            for (int e = tid; e < w * nc; e += LDLT_THREADS) {
-                const int c = e / w, k = e % w, row = cs + c;
-                float2 lc = zero;
-                if (row < jb) lc = cluster.map_shared_rank(S, row / LDC_ROWS)[(row % LDC_ROWS) * LDC_PITCH + c0 + k];
-                const float2 d = dk[k];
-                float2 t;
-                t.x = d.x * lc.x - d.y * lc.y;
-                t.y = d.x * lc.y + d.y * lc.x;
-                T[k * LDC_TP + c] = t;
+            // four independent remote loads in flight per thread
+            for (int e0 = 0; e0 < w * nc; e0 += 4 * LDLT_THREADS) {
+                float2 lc[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int e = e0 + u * LDLT_THREADS + tid, c = e / w, k = e % w, row = cs + c;
+                    lc[u] = zero;
+                    if (e < w * nc && row < jb)
+                        lc[u] = cluster.map_shared_rank(S, row / LDC_ROWS)[(row % LDC_ROWS) * LDC_PITCH + c0 + k];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int e = e0 + u * LDLT_THREADS + tid, c = e / w, k = e % w;
+                    if (e < w * nc) {
+                        const float2 d = dk[k];
+                        float2 t;
+                        t.x = d.x * lc[u].x - d.y * lc[u].y;
+                        t.y = d.x * lc[u].y + d.y * lc[u].x;
+                        T[k * LDC_TP + c] = t;
+                    }
+                }
             }
             __syncthreads();
             float2 acc[4][7];
@@ -1706,17 +1731,18 @@ ldlt_diag_cluster_kernel(float2* __restrict__ A, int64_t lda, int j0, int jb, in
                 }
 #pragma unroll 2
             for (int k = 0; k < w; k++) {
-                float2 a[4], b[7];
+                float2 a[4];
 #pragma unroll
                 for (int r = 0; r < 4; r++) a[r] = S[(wid * 4 + r) * LDC_PITCH + c0 + k];
 #pragma unroll
-                for (int g = 0; g < 7; g++) b[g] = g < ng ? T[k * LDC_TP + lane + 32 * g] : zero;
+                for (int g = 0; g < 7; g++)
+                    if (g < ng) {  // the column groups this CTA has at this sub-panel
+                        const float2 b = T[k * LDC_TP + lane + 32 * g];
 #pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int g = 0; g < 7; g++) {
-                        acc[r][g].x -= a[r].x * b[g].x - a[r].y * b[g].y;
-                        acc[r][g].y -= a[r].x * b[g].y + a[r].y * b[g].x;
+                        for (int r = 0; r < 4; r++) {
+                            acc[r][g].x -= a[r].x * b.x - a[r].y * b.y;
+                            acc[r][g].y -= a[r].x * b.y + a[r].y * b.x;
+                        }
                     }
             }
 #pragma unroll
