@@ -571,7 +571,8 @@ int mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X, int64_t ldx, con
 // Scratch of bem_farfield_mueller_noalloc: a file-scope device array, so the
 // entry point needs no cudaMalloc.  Host code must not use the symbol as an
 // address: its device address is looked up per device with
-// cudaGetSymbolAddress on the first call there.
+// cudaGetSymbolAddress on the first call there, which should therefore come
+// before any stream capture begins.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[BEM_NOALLOC_SCRATCH_BYTES];
 static void* g_noalloc_dev_ptr[64];
 static std::mutex g_noalloc_mu;

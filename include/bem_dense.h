@@ -441,7 +441,8 @@ int bem_farfield_mueller_dev(bem_ctx* ctx, const bem_geom* g, const void* X_dev,
  * may still be read afterwards, so keep pinned RT and w unchanged until that
  * stream has passed the call.  M_avg_dev: caller's device buffer of
  * 16*ntheta doubles, written on the context's stream.  The first call on a device looks
- * up the scratch address (cudaGetSymbolAddress).  All calls share the one array: calls that overlap on
+ * up the scratch address (cudaGetSymbolAddress), so make that first call before
+ * any stream capture begins.  All calls share the one array: calls that overlap on
  * the GPU (different streams or contexts on one device) race on it. */
 #define BEM_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 int bem_farfield_mueller_noalloc(bem_ctx* ctx, const bem_geom* g, const void* X_dev, int64_t ldx,
